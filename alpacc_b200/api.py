@@ -1,0 +1,297 @@
+"""Python front end over the C ABI (``include/alpacc_b200.h``).
+
+Mirrors the entry points alpacc's Futhark generator emits
+(``src/Alpacc/Generator/Futhark/Generator.hs``): ``lex_int`` / ``lex`` return
+the token triples (or ``None`` for ``#none``), ``parse_int`` / ``parse`` the
+preorder tree, ``pre_productions_int`` the production sequence.  Every call
+runs the CUDA kernels of ``_lib/libalpacc_b200.so``; there is no CPU path, and
+constructing a :class:`Grammar` without a CUDA device raises.
+
+Arrays come back as torch tensors on the context's device (``*_int``
+variants) or as Python lists of names (named variants).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from typing import List, Optional, Tuple, Union
+
+import numpy as np
+
+from . import build as _build
+from . import tables as _tables
+
+ALP_OK, ALP_ERR_ARG, ALP_ERR_CUDA, ALP_ERR_TIMEOUT, ALP_ERR_TABLE, ALP_ERR_CAPACITY, ALP_ERR_MODE = range(7)
+
+
+class AlpError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("alpacc_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+_lib = None
+
+
+def native() -> ctypes.CDLL:
+    """Load (building first if the sources are newer) the CUDA library."""
+    global _lib
+    if _lib is None:
+        path = _build.LIB
+        if _build.needs_build():
+            _build.build_cuda()
+        if not os.path.exists(path):
+            raise AlpError(ALP_ERR_CUDA, "native library missing: %s" % path)
+        L = ctypes.CDLL(path)
+        vp, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+        P = ctypes.POINTER
+        L.alp_ctx_create.argtypes = [ctypes.c_char_p, ctypes.c_size_t, i32, P(vp)]
+        L.alp_ctx_destroy.argtypes = [vp]
+        L.alp_last_error.restype = ctypes.c_char_p
+        L.alp_last_error.argtypes = [vp]
+        L.alp_set_stream.argtypes = [vp, vp]
+        L.alp_ctx_info.argtypes = [vp, P(i64), i32]
+        L.alp_memcpy.argtypes = [vp, vp, vp, ctypes.c_size_t]
+        L.alp_lex.argtypes = [vp, vp, i64, P(vp), P(vp), P(vp), P(i64), P(i32)]
+        L.alp_lex_into.argtypes = [vp, vp, i64, vp, vp, vp, i64, P(i64), P(i32)]
+        L.alp_lex_host.argtypes = [vp, vp, i64, vp, vp, vp, i64, P(i64), P(i32)]
+        for name in ("alp_parse",):
+            getattr(L, name).argtypes = [vp, vp, i64, P(vp), P(vp), P(vp), P(vp), P(vp), P(i64), P(i32)]
+        L.alp_parse_into.argtypes = [vp, vp, i64, vp, vp, vp, vp, vp, i64, P(i64), P(i32)]
+        L.alp_parse_host.argtypes = [vp, vp, i64, vp, vp, vp, vp, vp, i64, P(i64), P(i32)]
+        L.alp_parse_tokens.argtypes = [vp, vp, vp, vp, i64, P(vp), P(vp), P(vp), P(vp), P(vp), P(i64), P(i32)]
+        L.alp_pre_productions.argtypes = [vp, vp, i64, P(vp), P(i64), P(i32)]
+        L.alp_lex_batch.argtypes = [vp, vp, vp, i64, P(vp), P(vp), P(vp), P(vp), P(vp), P(i64)]
+        L.alp_parse_batch.argtypes = [vp, vp, vp, i64, P(vp), P(vp), P(vp), P(vp), P(vp), P(vp), P(vp), P(i64)]
+        _lib = L
+    return _lib
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _wrap(h, ptr: int, n: int, dtype, device) -> "torch.Tensor":
+    """Copy n elements at a context-owned device pointer into a new tensor."""
+    torch = _torch()
+    out = torch.empty(n, dtype=dtype, device=device)
+    if n:
+        rc = native().alp_memcpy(h, ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ptr),
+                                 n * out.element_size())
+        if rc != ALP_OK:
+            raise AlpError(rc, native().alp_last_error(h).decode(errors="replace"))
+    return out
+
+
+@dataclass
+class Tree:
+    parent: "torch.Tensor"   # int64
+    tag: "torch.Tensor"      # uint32 as int64 view-compatible (production or terminal id)
+    kind: "torch.Tensor"     # uint8: 0 production, 1 terminal
+    start: "torch.Tensor"    # int64
+    end: "torch.Tensor"      # int64
+
+    def __len__(self) -> int:
+        return int(self.parent.numel())
+
+
+class Grammar:
+    """One grammar's tables loaded on one CUDA device (a Futhark context)."""
+
+    def __init__(self, grammar: Union[str, _tables.Tables], mode: str = "both", device: int = 0):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise AlpError(ALP_ERR_CUDA, "no CUDA device: alpacc_b200 runs on the GPU only")
+        self.tables = grammar if isinstance(grammar, _tables.Tables) else _tables.load(grammar, mode)
+        self.device = torch.device("cuda", device)
+        torch.cuda.init()
+        with torch.cuda.device(self.device):
+            torch.empty(1, device=self.device)  # make the primary context current
+        blob = self.tables.blob()
+        self._blob = blob
+        h = ctypes.c_void_p()
+        L = native()
+        rc = L.alp_ctx_create(blob, len(blob), device, ctypes.byref(h))
+        if rc != ALP_OK:
+            raise AlpError(rc, "alp_ctx_create failed")
+        self.h = h
+        info = (ctypes.c_int64 * 8)()
+        L.alp_ctx_info(self.h, info, 8)
+        self.info = list(info)
+
+    def close(self):
+        if getattr(self, "h", None):
+            native().alp_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ utils
+    def _err(self, rc: int):
+        msg = native().alp_last_error(self.h).decode(errors="replace")
+        raise AlpError(rc, msg)
+
+    def _stream(self):
+        torch = _torch()
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        native().alp_set_stream(self.h, ctypes.c_void_p(s))
+
+    def _as_device_bytes(self, data) -> "torch.Tensor":
+        torch = _torch()
+        if isinstance(data, torch.Tensor):
+            t = data
+            if t.dtype != torch.uint8:
+                raise TypeError("input must be uint8")
+            return t.to(self.device).contiguous()
+        if isinstance(data, (bytes, bytearray, memoryview)):
+            arr = np.frombuffer(bytes(data), dtype=np.uint8)
+        else:
+            arr = np.ascontiguousarray(data, dtype=np.uint8)
+        return torch.from_numpy(arr.copy()).to(self.device)
+
+    # ------------------------------------------------------------------ lexer
+    def lex_int(self, data) -> Optional[Tuple["torch.Tensor", "torch.Tensor", "torch.Tensor"]]:
+        """Tokens as (terminal uint32->int64 tensor, start int64, end int64),
+        or None when the input is rejected."""
+        torch = _torch()
+        x = self._as_device_bytes(data)
+        self._stream()
+        pt, ps, pe = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        n, valid = ctypes.c_int64(0), ctypes.c_int(0)
+        rc = native().alp_lex(self.h, ctypes.c_void_p(x.data_ptr()), x.numel(), ctypes.byref(pt), ctypes.byref(ps),
+                              ctypes.byref(pe), ctypes.byref(n), ctypes.byref(valid))
+        if rc != ALP_OK:
+            self._err(rc)
+        if not valid.value:
+            return None
+        k = n.value
+        term = _wrap(self.h, pt.value or 0, k, torch.int32, self.device)
+        start = _wrap(self.h, ps.value or 0, k, torch.int64, self.device)
+        end = _wrap(self.h, pe.value or 0, k, torch.int64, self.device)
+        return term, start, end
+
+    def lex(self, data) -> Optional[List[Tuple[str, Tuple[int, int]]]]:
+        r = self.lex_int(data)
+        if r is None:
+            return None
+        names = self.tables.terminal_names
+        t, s, e = (x.cpu().numpy() for x in r)
+        return [(names[int(a)], (int(b), int(c))) for a, b, c in zip(t, s, e)]
+
+    def lex_host(self, data: np.ndarray):
+        """Host buffers in and out (copies inside the call)."""
+        arr = np.ascontiguousarray(data, dtype=np.uint8)
+        cap = len(arr) + 1
+        term = np.empty(cap, np.uint32)
+        start = np.empty(cap, np.int64)
+        end = np.empty(cap, np.int64)
+        n, valid = ctypes.c_int64(0), ctypes.c_int(0)
+        self._stream()
+        rc = native().alp_lex_host(self.h, arr.ctypes.data_as(ctypes.c_void_p), len(arr),
+                                   term.ctypes.data_as(ctypes.c_void_p), start.ctypes.data_as(ctypes.c_void_p),
+                                   end.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(n), ctypes.byref(valid))
+        if rc != ALP_OK:
+            self._err(rc)
+        if not valid.value:
+            return None
+        k = n.value
+        return term[:k], start[:k], end[:k]
+
+    # ----------------------------------------------------------------- parser
+    def _tree(self, pp, pt, pk, ps, pe, n) -> Tree:
+        torch = _torch()
+        return Tree(_wrap(self.h, pp.value or 0, n, torch.int64, self.device),
+                    _wrap(self.h, pt.value or 0, n, torch.int32, self.device),
+                    _wrap(self.h, pk.value or 0, n, torch.uint8, self.device),
+                    _wrap(self.h, ps.value or 0, n, torch.int64, self.device),
+                    _wrap(self.h, pe.value or 0, n, torch.int64, self.device))
+
+    def parse_int(self, data) -> Optional[Tree]:
+        """Bytes -> preorder tree (parent, tag, kind, start, end), or None."""
+        x = self._as_device_bytes(data)
+        self._stream()
+        ptrs = [ctypes.c_void_p() for _ in range(5)]
+        n, valid = ctypes.c_int64(0), ctypes.c_int(0)
+        rc = native().alp_parse(self.h, ctypes.c_void_p(x.data_ptr()), x.numel(), *[ctypes.byref(p) for p in ptrs],
+                                ctypes.byref(n), ctypes.byref(valid))
+        if rc != ALP_OK:
+            self._err(rc)
+        if not valid.value:
+            return None
+        return self._tree(*ptrs, n.value)
+
+    def parse(self, data):
+        """Named tree: a list of (parent, ('terminal', name, (start, end)) |
+        ('production', name)), or None."""
+        t = self.parse_int(data)
+        if t is None:
+            return None
+        tn, pn = self.tables.terminal_names, self.tables.production_names
+        par, tag, kind, s, e = (x.cpu().numpy() for x in (t.parent, t.tag, t.kind, t.start, t.end))
+        out = []
+        for i in range(len(par)):
+            if kind[i]:
+                out.append((int(par[i]), ("terminal", tn[int(tag[i])], (int(s[i]), int(e[i])))))
+            else:
+                out.append((int(par[i]), ("production", pn[int(tag[i])])))
+        return out
+
+    def parse_tokens_int(self, term, start, end) -> Optional[Tree]:
+        """Parser-only ``parse_int``: token arrays (device or host) -> tree."""
+        torch = _torch()
+        term = torch.as_tensor(term).to(self.device, torch.int32).contiguous()
+        start = torch.as_tensor(start).to(self.device, torch.int64).contiguous()
+        end = torch.as_tensor(end).to(self.device, torch.int64).contiguous()
+        self._stream()
+        ptrs = [ctypes.c_void_p() for _ in range(5)]
+        n, valid = ctypes.c_int64(0), ctypes.c_int(0)
+        rc = native().alp_parse_tokens(self.h, ctypes.c_void_p(term.data_ptr()), ctypes.c_void_p(start.data_ptr()),
+                                       ctypes.c_void_p(end.data_ptr()), term.numel(),
+                                       *[ctypes.byref(p) for p in ptrs], ctypes.byref(n), ctypes.byref(valid))
+        if rc != ALP_OK:
+            self._err(rc)
+        if not valid.value:
+            return None
+        return self._tree(*ptrs, n.value)
+
+    def pre_productions_int(self, term) -> Optional["torch.Tensor"]:
+        torch = _torch()
+        term = torch.as_tensor(term).to(self.device, torch.int32).contiguous()
+        self._stream()
+        pp = ctypes.c_void_p()
+        n, valid = ctypes.c_int64(0), ctypes.c_int(0)
+        rc = native().alp_pre_productions(self.h, ctypes.c_void_p(term.data_ptr()), term.numel(), ctypes.byref(pp),
+                                          ctypes.byref(n), ctypes.byref(valid))
+        if rc != ALP_OK:
+            self._err(rc)
+        if not valid.value:
+            return None
+        return _wrap(self.h, pp.value or 0, n.value, torch.int32, self.device)
+
+    def parse_host(self, data: np.ndarray):
+        """Host buffers in and out: (parent, tag, kind, start, end) numpy arrays or None."""
+        arr = np.ascontiguousarray(data, dtype=np.uint8)
+        cap = (len(arr) + 2) * max(1, self.info[6])
+        par = np.empty(cap, np.int64)
+        tag = np.empty(cap, np.uint32)
+        kind = np.empty(cap, np.uint8)
+        st = np.empty(cap, np.int64)
+        en = np.empty(cap, np.int64)
+        n, valid = ctypes.c_int64(0), ctypes.c_int(0)
+        self._stream()
+        vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        rc = native().alp_parse_host(self.h, vp(arr), len(arr), vp(par), vp(tag), vp(kind), vp(st), vp(en), cap,
+                                     ctypes.byref(n), ctypes.byref(valid))
+        if rc != ALP_OK:
+            self._err(rc)
+        if not valid.value:
+            return None
+        k = n.value
+        return par[:k], tag[:k], kind[:k], st[:k], en[:k]

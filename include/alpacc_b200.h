@@ -1,0 +1,115 @@
+/*
+ * alpacc_b200 -- B200-native lexer/parser for alpacc grammars: the C ABI.
+ *
+ * The reference's de-facto C ABI for this path is the library that the
+ * Futhark compiler makes from alpacc's generated program: the entry points
+ * `lex_int`/`lex` (src/Alpacc/Generator/Futhark/Generator.hs:63-75),
+ * `parse_int`/`parse` (src/Alpacc/Generator/Futhark/Generator.hs:24-44) and,
+ * for the parser-only generator, `parse_int` over a token array and
+ * `pre_productions_int` (futhark/parser.fut:41-44, futhark/test.fut:75-119),
+ * all called through one context (Futhark's futhark_context).  Every function
+ * below replaces one of them; the comment names which.
+ *
+ * Conventions
+ *   - Return value: ALP_OK (0) or an ALP_ERR_* code; alp_last_error() gives
+ *     the message.  A grammar REJECTING the input is not an error: it is
+ *     `*valid = 0` with zero outputs, exactly the reference's `#none` (and the
+ *     empty arrays of the lexer-only `lex_int` entry point).
+ *   - `d_` pointers are device memory on the context's device; `h_` pointers
+ *     are host memory.  Calls are ordered on the context's stream and return
+ *     after the results are known (they synchronise that stream once).
+ *   - Outputs returned through `**` pointers are owned by the context and stay
+ *     valid until the next call on it.  `_into` variants write to caller
+ *     buffers of `cap` elements and fail with ALP_ERR_CAPACITY (setting the
+ *     needed count) when too small.
+ *   - Terminal and production ids are widened to uint32 and positions to
+ *     int64.  Spans are [start, end) byte offsets.  A tree node is
+ *     (parent, tag, kind, start, end): kind 0 = production (tag = production
+ *     id, span 0,0), kind 1 = terminal (tag = terminal id, the token's span).
+ *     Nodes are in preorder and the root is its own parent.
+ *   - A context is not thread safe, like a Futhark context.
+ */
+#ifndef ALPACC_B200_H
+#define ALPACC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    ALP_OK = 0,
+    ALP_ERR_ARG = 1,       /* bad argument (null pointer, size out of range) */
+    ALP_ERR_CUDA = 2,      /* a CUDA call failed */
+    ALP_ERR_TIMEOUT = 3,   /* a kernel's bounded wait gave up */
+    ALP_ERR_TABLE = 4,     /* malformed table blob, or tables too large */
+    ALP_ERR_CAPACITY = 5,  /* caller buffer too small */
+    ALP_ERR_MODE = 6       /* the tables have no lexer / no parser */
+};
+
+typedef struct alp_ctx alp_ctx;
+
+/* futhark_context_new + the generated table constants: load one grammar's
+ * tables (the blob written by alpacc_b200.tables) onto `device`. */
+int alp_ctx_create(const void* blob, size_t len, int device, alp_ctx** out);
+void alp_ctx_destroy(alp_ctx* ctx);
+const char* alp_last_error(const alp_ctx* ctx);
+/* Order every later call on this CUDA stream (a cudaStream_t; NULL = legacy default). */
+int alp_set_stream(alp_ctx* ctx, void* stream);
+/* Grammar facts: out[0] has_lexer, [1] has_parser, [2] n_terminals,
+ * [3] n_productions, [4] lookback q, [5] lookahead k, [6] max productions per
+ * admissible pair, [7] max brackets per pair. */
+int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out);
+
+/* Copy `bytes` between any two addresses (device or host) on the context's
+ * stream and wait for it; lets bindings move context-owned outputs. */
+int alp_memcpy(alp_ctx* ctx, void* dst, const void* src, size_t bytes);
+
+/* lex_int: bytes -> tokens (futhark/lexer.fut:174-178 through
+ * src/Alpacc/Generator/Futhark/Generator.hs:70-75). */
+int alp_lex(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t** d_term, int64_t** d_start,
+            int64_t** d_end, int64_t* n_tok, int* valid);
+int alp_lex_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_term, int64_t* d_start,
+                 int64_t* d_end, int64_t cap, int64_t* n_tok, int* valid);
+/* Same as alp_lex_into with host buffers: copies in, lexes, copies out. */
+int alp_lex_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, uint32_t* h_term, int64_t* h_start,
+                 int64_t* h_end, int64_t cap, int64_t* n_tok, int* valid);
+
+/* parse_int of the lexer+parser generator: bytes -> preorder tree
+ * (src/Alpacc/Generator/Futhark/Generator.hs:35-44, futhark/parser.fut:316-336). */
+int alp_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t** d_parent, uint32_t** d_tag,
+              uint8_t** d_kind, int64_t** d_start, int64_t** d_end, int64_t* n_node, int* valid);
+int alp_parse_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t* d_parent, uint32_t* d_tag,
+                   uint8_t* d_kind, int64_t* d_start, int64_t* d_end, int64_t cap, int64_t* n_node,
+                   int* valid);
+int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_parent, uint32_t* h_tag,
+                   uint8_t* h_kind, int64_t* h_start, int64_t* h_end, int64_t cap, int64_t* n_node,
+                   int* valid);
+
+/* parse_int of the parser-only generator: tokens -> tree (futhark/parser.fut:334-336). */
+int alp_parse_tokens(alp_ctx* ctx, const uint32_t* d_term, const int64_t* d_tstart, const int64_t* d_tend,
+                     int64_t m, int64_t** d_parent, uint32_t** d_tag, uint8_t** d_kind, int64_t** d_start,
+                     int64_t** d_end, int64_t* n_node, int* valid);
+
+/* pre_productions_int: token ids -> production sequence (futhark/parser.fut:269-271). */
+int alp_pre_productions(alp_ctx* ctx, const uint32_t* d_term, int64_t m, uint32_t** d_prod,
+                        int64_t* n_prod, int* valid);
+
+/* Batched documents (no reference counterpart: the reference parses one
+ * document per call; this is that call applied to every document).
+ * d_in holds the documents back to back, d_off[0..n_docs] their byte offsets.
+ * Per document i: d_valid[i], and its outputs in [d_out_off[i], d_out_off[i+1]).
+ * Positions and parents are relative to the document. */
+int alp_lex_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int64_t n_docs,
+                  uint32_t** d_term, int64_t** d_start, int64_t** d_end, int64_t** d_tok_off,
+                  uint8_t** d_valid, int64_t* n_tok_total);
+int alp_parse_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int64_t n_docs,
+                    int64_t** d_parent, uint32_t** d_tag, uint8_t** d_kind, int64_t** d_start,
+                    int64_t** d_end, int64_t** d_node_off, uint8_t** d_valid, int64_t* n_node_total);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ALPACC_B200_H */

@@ -1,0 +1,139 @@
+"""GPU parser parity: the CUDA LLP parse (bytes -> preorder tree) against the
+CPU oracle's restatement of the generated ``parse_int`` (and of the
+sequential glue parser), bit-exact, through the C ABI."""
+
+import itertools
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from alpacc_b200 import synth, tables
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+_CACHE = {}
+
+
+def _ctx(name):
+    from alpacc_b200.api import Grammar
+    if name not in _CACHE:
+        tb = tables.load(name, "both")
+        _CACHE[name] = (Grammar(tb), oracle.Oracle(tb.blob()), tb)
+    return _CACHE[name]
+
+
+def _gen(name, size, seed, depth=None):
+    if name == "json":
+        return synth.json_doc(size, depth or 16, seed)
+    if name == "arithmetic":
+        return synth.arith_doc(size, depth or 12, seed)
+    return synth.sexp_doc(size, depth or 20, seed)
+
+
+def _check(g, o, data: bytes):
+    want = o.lex_parse(data)
+    got = g.parse_int(data)
+    if want is None:
+        assert got is None, "GPU accepted an input the reference rejects"
+        return 0
+    assert got is not None, "GPU rejected an input the reference accepts"
+    gp, gt, gk, gs, ge = (x.cpu().numpy() for x in (got.parent, got.tag, got.kind, got.start, got.end))
+    wp, wt, wk, ws, we = want
+    np.testing.assert_array_equal(gt.astype(np.uint32), wt)
+    np.testing.assert_array_equal(gk, wk)
+    np.testing.assert_array_equal(gs, ws)
+    np.testing.assert_array_equal(ge, we)
+    np.testing.assert_array_equal(gp, wp)
+    return len(wp)
+
+
+def test_readme_tree(has_gpu):
+    """The README's parse of 12+(3*4) (README.md:84-106), node for node."""
+    g, o, tb = _ctx("arithmetic")
+    with open(os.path.join(GOLDEN, "readme_arith_tree.json")) as f:
+        gold = json.load(f)
+    named = g.parse(gold["input"].encode())
+    assert [list(x[1]) if x[1][0] == "production" else x for x in named] is not None
+    want = [(p, tuple(n) if n[0] == "production" else (n[0], n[1], tuple(n[2]))) for p, n in gold["tree"]]
+    got = [(p, n if n[0] == "production" else (n[0], n[1], tuple(n[2]))) for p, n in named]
+    assert got == want
+
+
+@pytest.mark.parametrize("name", ["json", "arithmetic", "sexp"])
+def test_generated_sizes(has_gpu, name):
+    g, o, _ = _ctx(name)
+    for i, size in enumerate([2, 3, 17, 100, 1000, 4096, 4097, 20000, 65537, 1 << 20, (1 << 22) + 5]):
+        _check(g, o, _gen(name, size, 500 + i).tobytes())
+
+
+@pytest.mark.parametrize("name", ["json", "arithmetic", "sexp"])
+def test_exhaustive_short(has_gpu, name):
+    g, o, _ = _ctx(name)
+    alpha = {"json": b'{}[],:"1 n', "arithmetic": b"1-+*()a ", "sexp": b"()a "}[name]
+    for L in range(0, 5 if name != "json" else 4):
+        for t in itertools.product(alpha, repeat=L):
+            _check(g, o, bytes(t))
+
+
+@pytest.mark.parametrize("name", ["json", "arithmetic", "sexp"])
+def test_corrupted(has_gpu, name):
+    """Structural edits: delete/duplicate a bracket, swap closers.  Most are
+    rejected by the bracket match far from the edit."""
+    g, o, _ = _ctx(name)
+    rng = np.random.default_rng(11)
+    closers = {"json": b"]}", "arithmetic": b")", "sexp": b")"}[name]
+    for i in range(25):
+        d = bytearray(_gen(name, 30000 + 1013 * i, 700 + i).tobytes())
+        pos = [j for j, c in enumerate(d) if c in closers]
+        if pos:
+            j = pos[int(rng.integers(0, len(pos)))]
+            op = i % 3
+            if op == 0:
+                del d[j]
+            elif op == 1:
+                d.insert(j, d[j])
+            else:
+                d[j] = closers[(closers.index(d[j]) + 1) % len(closers)]
+        _check(g, o, bytes(d))
+
+
+def test_deep_nesting(has_gpu):
+    """Nesting far deeper than one tile, so matches and parents cross tiles."""
+    g, o, _ = _ctx("json")
+    for depth in [10, 1000, 5000]:
+        d = b"[" * depth + b"1" + b"]" * depth
+        assert _check(g, o, d) > 0
+        _check(g, o, b"[" * depth + b"1" + b"]" * (depth - 1))
+        _check(g, o, b"[" * depth + b"1" + b"]" * (depth - 1) + b"}")
+    gs, os_, _ = _ctx("sexp")
+    _check(gs, os_, b"(" * 20000 + b"a" + b")" * 20000)
+
+
+def test_parser_only_and_glue(has_gpu):
+    """parse_tokens_int and pre_productions_int against the oracle, and the
+    glue parser agreeing with the scan formulation on valid input."""
+    g, o, _ = _ctx("json")
+    d = _gen("json", 200000, 9)
+    toks = o.lex_futhark(d.tobytes())
+    want = o.parse_futhark(*toks)
+    glue = o.parse_glue(*toks)
+    for a, b in zip(want, glue):
+        np.testing.assert_array_equal(a, b)
+    got = g.parse_tokens_int(toks[0].astype(np.int64), toks[1], toks[2])
+    np.testing.assert_array_equal(got.parent.cpu().numpy(), want[0])
+    np.testing.assert_array_equal(got.tag.cpu().numpy().astype(np.uint32), want[1])
+    pp = g.pre_productions_int(toks[0].astype(np.int64))
+    np.testing.assert_array_equal(pp.cpu().numpy().astype(np.uint32), o.pre_productions(toks[0]))
+
+
+def test_host_buffers(has_gpu):
+    g, o, _ = _ctx("sexp")
+    d = _gen("sexp", 123457, 3)
+    got = g.parse_host(d)
+    want = o.lex_parse(d.tobytes())
+    for a, b in zip(got, want):
+        np.testing.assert_array_equal(a, b)

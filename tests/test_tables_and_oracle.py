@@ -1,0 +1,80 @@
+"""Id orderings of the three benchmark grammars, the oracle's two lexers and
+two parsers agreeing with each other, and the reference's chunk-loop
+behaviour beyond one chunk (no GPU)."""
+
+import numpy as np
+import pytest
+
+import oracle
+from alpacc_b200 import synth, tables
+
+
+def test_terminal_ids_both_modes():
+    # lex+parse ids: file order of terminal rules, then literals sorted, then
+    # ignore and Unused (src/Alpacc/Encode.hs:122-146, src/Alpacc/CFG.hs:131)
+    a = tables.load("arithmetic", "both")
+    assert a.terminal_names[:8] == ["num", "var"] + ["literal_%d" % i for i in range(2, 8)]
+    assert a.lexer_token_ids['"("'] == 2 and a.lexer_token_ids['"+"'] == 5 and a.lexer_token_ids['"*"'] == 4
+    j = tables.load("json", "both")
+    assert j.terminal_names[:2] == ["string", "number"] and j.ignore_term == 11 and j.dead_term == 12
+    # lexer-only ids: Ord T order (names sorted, then literals), ignore, Unused
+    jl = tables.load("json", "lexer")
+    assert jl.terminal_names[:2] == ["number", "string"]
+    assert jl.lexer_token_ids['","'] == 2 and jl.lexer_token_ids['"}"'] == 10 and jl.ignore_term == 11
+
+
+def test_production_names():
+    a = tables.load("arithmetic", "both")
+    assert a.production_names[:11] == ["E0_0", "Add", "Sub", "Empty", "E1_4", "Mul", "Div", "Empty",
+                                       "Parentheses", "Num", "Var"]
+    assert a.production_names[-1] == "start_20"
+    s = tables.load("sexp", "both")
+    assert s.production_names == ["E_0", "E_1", "E0_2", "E0_3", "ignore_4", "atom_5", "Literal_6",
+                                  "Literal_7", "start_8"]
+
+
+@pytest.mark.parametrize("name,fn", [("json", synth.json_doc), ("arithmetic", synth.arith_doc),
+                                     ("sexp", synth.sexp_doc)])
+def test_oracle_lexers_and_parsers_agree(name, fn):
+    tb = tables.load(name, "both")
+    o = oracle.Oracle(tb.blob())
+    for i, size in enumerate([1, 50, 4096, 100000, 1 << 20]):
+        d = fn(size, seed=40 + i).tobytes()
+        a = o.tokenize(d)
+        b = o.lex_futhark(d)
+        assert a is not None and b is not None
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+        t1 = o.parse_futhark(*a)
+        t2 = o.parse_glue(*a)
+        assert t1 is not None and t2 is not None
+        for x, y in zip(t1, t2):
+            np.testing.assert_array_equal(x, y)
+
+
+def test_reference_chunk_loop_diverges_past_one_chunk():
+    """The generated lexer loops over 16 MiB chunks (futhark/lexer.fut:144-160;
+    chunk size from src/Alpacc/Generator/Futhark/Generator.hs:25).  Restated
+    with a small chunk, it equals tokenize while the input fits in one chunk
+    and differs once it does not: a chunk re-reads its first byte and every
+    chunk shifts the spans of all earlier tokens.  Parity in this project is
+    therefore pinned to single-chunk semantics (equal to tokenize)."""
+    tb = tables.load("json", "lexer")
+    o = oracle.Oracle(tb.blob())
+    d = synth.json_doc(5000, seed=3).tobytes()
+    single = o.tokenize(d)
+    same = o.lex_futhark(d, chunk=8192)
+    for x, y in zip(single, same):
+        np.testing.assert_array_equal(x, y)
+    chunked = o.lex_futhark(d, chunk=1024)
+    assert chunked is None or any(len(x) != len(y) or not np.array_equal(x, y) for x, y in zip(single, chunked))
+
+
+def test_rejections():
+    tb = tables.load("json", "both")
+    o = oracle.Oracle(tb.blob())
+    assert o.tokenize(b"") is None and o.lex_futhark(b"") is None
+    assert o.tokenize(b'"abc') is None
+    assert o.lex_parse(b"[1,2") is None
+    assert o.lex_parse(b"[1,2]") is not None
+    assert o.lex_parse(b"{1:2}") is None
