@@ -54,6 +54,8 @@ def native() -> ctypes.CDLL:
         L.alp_set_stream.argtypes = [vp, vp]
         L.alp_ctx_info.argtypes = [vp, P(i64), i32]
         L.alp_memcpy.argtypes = [vp, vp, vp, ctypes.c_size_t]
+        L.alp_ctx_profile.argtypes = [vp, i32]
+        L.alp_ctx_timings.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
         L.alp_lex.argtypes = [vp, vp, i64, P(vp), P(vp), P(vp), P(i64), P(i32)]
         L.alp_lex_into.argtypes = [vp, vp, i64, vp, vp, vp, i64, P(i64), P(i32)]
         L.alp_lex_host.argtypes = [vp, vp, i64, vp, vp, vp, i64, P(i64), P(i32)]
@@ -132,6 +134,19 @@ class Grammar:
             self.close()
         except Exception:
             pass
+
+    # ------------------------------------------------------------- profiling
+    def profile(self, on: bool = True) -> None:
+        native().alp_ctx_profile(self.h, 1 if on else 0)
+
+    def timings(self) -> List[Tuple[str, float]]:
+        buf = ctypes.create_string_buffer(1 << 16)
+        native().alp_ctx_timings(self.h, buf, len(buf))
+        out = []
+        for line in buf.value.decode().splitlines():
+            name, ms = line.rsplit(" ", 1)
+            out.append((name, float(ms)))
+        return out
 
     # ------------------------------------------------------------------ utils
     def _err(self, rc: int):

@@ -49,9 +49,22 @@ struct alp_ctx {
     DevBuf out[8];                        // context-owned outputs
     DevBuf tmp[24];                       // intermediates
     AlpResult* h_res = nullptr;           // pinned
+    // optional per-kernel timing (alp_ctx_profile)
+    int prof = 0;
+    std::vector<std::pair<const char*, cudaEvent_t>> marks;
 };
 
 namespace {
+
+// Record a named event on the context stream when profiling is on; the time
+// between consecutive marks is attributed to the later mark's name.
+void mark(alp_ctx* ctx, const char* name) {
+    if (!ctx->prof) return;
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, ctx->stream);
+    ctx->marks.emplace_back(name, e);
+}
 
 int fail(alp_ctx* c, int code, const char* fmt, ...) {
     char buf[512];
@@ -188,8 +201,10 @@ int launch_lex(alp_ctx* ctx, const uint8_t* d_in, long long n, void* term, void*
     a.cap = cap;
     auto k = lex_kernel<ITEMS, TermT, PosT>;
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->lex_smem));
+    mark(ctx, "start");
     k<<<(unsigned)tiles, LEX_THREADS, ctx->lex_smem, ctx->stream>>>(a);
     CK(cudaGetLastError());
+    mark(ctx, "lex_kernel");
     CK(cudaMemcpyAsync(ctx->h_res, a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
@@ -288,8 +303,10 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     a.esc_cap = n;
     a.res = d_res;
     CK(cudaFuncSetAttribute(ple_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PLE_SMEM));
+    mark(ctx, "start");
     ple_tile_kernel<<<(unsigned)tiles, PLE_THREADS, PLE_SMEM, ctx->stream>>>(a);
     CK(cudaGetLastError());
+    mark(ctx, sym ? "ple_tile_kernel(brackets)" : "ple_tile_kernel(nodes)");
     tile_min_levels_kernel<<<(unsigned)((n32 + 255) / 256), 256, 0, ctx->stream>>>(
         a.tile_min, tiles, (int32_t*)ctx->tmp[first + 1].p, (int32_t*)ctx->tmp[first + 2].p);
     CK(cudaGetLastError());
@@ -308,6 +325,7 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     e.res = d_res;
     ple_escape_kernel<<<148 * 4, 256, 0, ctx->stream>>>(e);
     CK(cudaGetLastError());
+    mark(ctx, sym ? "tile_min+ple_escape(brackets)" : "tile_min+ple_escape(nodes)");
     return ALP_OK;
 }
 
@@ -338,10 +356,13 @@ int parse_tokens_core(alp_ctx* ctx, long long m, ParseOut* o, int64_t cap, int c
     a.res = d_res;
     const size_t sm1 = sizeof(PairInfo) * ctx->pt.n_pairs + (size_t)(PP_TILE + ctx->pt.q + ctx->pt.k) * 4;
     CK(cudaFuncSetAttribute(parse_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+    mark(ctx, "start");
     parse_pairs_kernel<<<(unsigned)tiles, PP_THREADS, sm1, ctx->stream>>>(a);
     CK(cudaGetLastError());
+    mark(ctx, "parse_pairs_kernel");
     scan_tiles_kernel<<<1, 1024, 0, ctx->stream>>>(a.tile_sums, tiles, d_res);
     CK(cudaGetLastError());
+    mark(ctx, "scan_tiles_kernel");
     if ((rc = read_result(ctx, d_res))) return rc;
     const long long N = ctx->h_res->aux[0], B = ctx->h_res->aux[1], D = ctx->h_res->aux[2], NT = ctx->h_res->aux[4];
     if (!ctx->h_res->valid || D != 0) return ALP_OK;  // rejected
@@ -375,8 +396,10 @@ int parse_tokens_core(alp_ctx* ctx, long long m, ParseOut* o, int64_t cap, int c
     a.cap_brs = B;
     const size_t sm2 = sizeof(PairInfo) * ctx->pt.n_pairs + (size_t)ctx->pt.n_prods * 8;
     CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    mark(ctx, "start");
     parse_expand_kernel<<<(unsigned)tiles, PP_THREADS, sm2, ctx->stream>>>(a);
     CK(cudaGetLastError());
+    mark(ctx, "parse_expand_kernel");
     if (want_tree) {
         if ((rc = run_ple(ctx, a.vbuf, N, nullptr, o->parent, T_N_TMIN, d_res))) return rc;
     }
@@ -496,6 +519,32 @@ int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out) {
                     ctx->ph.n_prods, ctx->ph.q, ctx->ph.k, ctx->ph.max_prods, ctx->ph.max_brackets};
     for (int i = 0; i < n_out && i < 8; ++i) out[i] = v[i];
     return ALP_OK;
+}
+
+int alp_ctx_profile(alp_ctx* ctx, int on) {
+    if (!ctx) return ALP_ERR_ARG;
+    for (auto& m : ctx->marks) cudaEventDestroy(m.second);
+    ctx->marks.clear();
+    ctx->prof = on ? 1 : 0;
+    return ALP_OK;
+}
+
+int alp_ctx_timings(alp_ctx* ctx, char* buf, size_t len) {
+    if (!ctx || !buf || !len) return ALP_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::string out;
+    for (size_t i = 1; i < ctx->marks.size(); ++i) {
+        if (strcmp(ctx->marks[i].first, "start") == 0) continue;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->marks[i - 1].second, ctx->marks[i].second);
+        char line[160];
+        snprintf(line, sizeof line, "%s %.6f\n", ctx->marks[i].first, ms);
+        out += line;
+    }
+    for (auto& m : ctx->marks) cudaEventDestroy(m.second);
+    ctx->marks.clear();
+    snprintf(buf, len, "%s", out.c_str());
+    return out.size() < len ? ALP_OK : ALP_ERR_CAPACITY;
 }
 
 int alp_memcpy(alp_ctx* ctx, void* dst, const void* src, size_t bytes) {

@@ -63,6 +63,12 @@ int alp_set_stream(alp_ctx* ctx, void* stream);
  * admissible pair, [7] max brackets per pair. */
 int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out);
 
+/* Per-kernel timing (no reference counterpart; measurement support): when on,
+ * every later call records a CUDA event after each kernel; alp_ctx_timings
+ * writes "kernel_name milliseconds" lines for the recorded calls and clears them. */
+int alp_ctx_profile(alp_ctx* ctx, int on);
+int alp_ctx_timings(alp_ctx* ctx, char* buf, size_t len);
+
 /* Copy `bytes` between any two addresses (device or host) on the context's
  * stream and wait for it; lets bindings move context-owned outputs. */
 int alp_memcpy(alp_ctx* ctx, void* dst, const void* src, size_t bytes);
