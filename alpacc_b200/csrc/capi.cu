@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -565,6 +566,104 @@ int alp_lex_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_term,
         return fail(ctx, ALP_ERR_ARG, "null output");
     CK(cudaSetDevice(ctx->device));
     return lex_core<uint32_t, int64_t>(ctx, d_in, n, d_term, d_start, d_end, cap, n_tok, valid);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Scratch-free lexing: alp_lex_noalloc
+//
+// Some callers cannot allocate device memory at the moment they lex: code that
+// owns every byte of the device through its own pool, code on a latency-bound
+// path where cudaMalloc/cudaFree would synchronise the device, or a host
+// callback that must not enter the allocator.  alp_lex_noalloc serves them:
+// the look-back status words and the result block live in the fixed array
+// below, compiled into the library, instead of in context scratch that grows
+// with cudaMalloc.  The caller still passes the input and the output buffers.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr long long NOALLOC_MAX_BYTES = 128ll << 20;                    // largest input
+constexpr long long NOALLOC_MAX_TILES = NOALLOC_MAX_BYTES / LEX_TILE;  // 32768 tiles
+constexpr size_t NOALLOC_SCRATCH_BYTES = 256 + 12 * (size_t)NOALLOC_MAX_TILES;  // 393,472 bytes
+
+// Every GPU that loads this library holds one copy until the process exits.
+// Host code must not pass `g_noalloc_scratch` itself to a kernel: on the host
+// the name is only a stand-in, so its device address comes from
+// cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::once_flag g_noalloc_once[NOALLOC_MAX_DEVICES];
+void* g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+cudaError_t g_noalloc_err[NOALLOC_MAX_DEVICES];
+
+// Device address of the fixed scratch on `device` (which must be current),
+// looked up once per device.
+void* noalloc_scratch(int device, cudaError_t* err) {
+    std::call_once(g_noalloc_once[device], [device] {
+        void* p = nullptr;
+        g_noalloc_err[device] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        g_noalloc_ptr[device] = g_noalloc_err[device] == cudaSuccess ? p : nullptr;
+    });
+    *err = g_noalloc_err[device];
+    return g_noalloc_ptr[device];
+}
+
+}  // namespace
+
+extern "C" {
+
+int alp_lex_noalloc(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_term, int64_t* d_start,
+                    int64_t* d_end, int64_t cap, int64_t* n_tok, int* valid) {
+    if (!ctx) return ALP_ERR_ARG;
+    if (n < 0 || (n > 0 && !d_in)) return fail(ctx, ALP_ERR_ARG, "alp_lex_noalloc: bad input");
+    if (n > NOALLOC_MAX_BYTES)
+        return fail(ctx, ALP_ERR_ARG, "alp_lex_noalloc: input of %lld bytes exceeds the %lld-byte limit",
+                    (long long)n, NOALLOC_MAX_BYTES);
+    if (!n_tok || !valid || (cap > 0 && (!d_term || !d_start || !d_end)))
+        return fail(ctx, ALP_ERR_ARG, "alp_lex_noalloc: null output");
+    if (!ctx->has_lexer) return fail(ctx, ALP_ERR_MODE, "these tables have no lexer");
+    if (ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES) return fail(ctx, ALP_ERR_ARG, "device id too large");
+    *n_tok = 0;
+    *valid = 0;
+    CK(cudaSetDevice(ctx->device));
+    if (n == 0) {
+        *valid = (ctx->h_tokinfo[1] & TOK_ACCEPT) ? 1 : 0;
+        return ALP_OK;
+    }
+    cudaError_t se;
+    uint8_t* base = reinterpret_cast<uint8_t*>(noalloc_scratch(ctx->device, &se));
+    if (!base) return fail(ctx, ALP_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(se));
+    const long long tiles = (n + LEX_TILE - 1) / LEX_TILE;
+    const size_t used = 256 + 12 * (size_t)tiles;
+    // the array keeps the previous call's words: clear the part this call uses
+    CK(cudaMemsetAsync(base, 0, used, ctx->stream));
+    LexArgs a;
+    a.in = d_in;
+    a.n = n;
+    a.aligned16 = ((reinterpret_cast<uintptr_t>(d_in) & 15u) == 0) ? 1 : 0;
+    a.t = ctx->lt;
+    a.res = reinterpret_cast<AlpResult*>(base);
+    a.ticket = reinterpret_cast<unsigned int*>(base + 128);
+    a.stB = reinterpret_cast<unsigned long long*>(base + 256);
+    a.stA = reinterpret_cast<uint32_t*>(base + 256 + 8 * (size_t)tiles);
+    a.out_term = d_term;
+    a.out_start = d_start;
+    a.out_end = d_end;
+    a.cap = cap;
+    auto k = lex_kernel<LEX_ITEMS, uint32_t, int64_t>;
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->lex_smem));
+    k<<<(unsigned)tiles, LEX_THREADS, ctx->lex_smem, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->h_res, a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
+    *valid = ctx->h_res->valid;
+    *n_tok = ctx->h_res->count;
+    if (ctx->h_res->error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
+    if (!*valid) *n_tok = 0;
+    return ALP_OK;
 }
 
 int alp_lex(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t** d_term, int64_t** d_start,

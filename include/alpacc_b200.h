@@ -83,6 +83,25 @@ int alp_lex_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_term,
 int alp_lex_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, uint32_t* h_term, int64_t* h_start,
                  int64_t* h_end, int64_t cap, int64_t* n_tok, int* valid);
 
+/* lex_int without any device allocation (no counterpart in the reference).
+ * For callers that cannot allocate device memory when they lex -- a caller
+ * whose own pool owns all device memory, a latency-bound path where
+ * cudaMalloc/cudaFree would synchronise the device, or a host callback that
+ * must not enter the allocator.  Same results as alp_lex_into.
+ *   - Input is limited to 128 MiB (134217728 bytes); larger inputs fail with
+ *     ALP_ERR_ARG and a message naming the limit.
+ *   - Scratch is one fixed 393,472-byte array compiled into the library; every
+ *     GPU that loads the library holds it until the process exits.  The
+ *     outputs are the caller's buffers of `cap` tokens.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls share the one array: calls that overlap on the GPU (other
+ *     streams, other contexts on the same device) race and must not overlap.
+ *   - The call makes no cudaMalloc/cudaFree and no allocating library call;
+ *     only its error paths write the context's host-side message. */
+int alp_lex_noalloc(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_term, int64_t* d_start,
+                    int64_t* d_end, int64_t cap, int64_t* n_tok, int* valid);
+
 /* parse_int of the lexer+parser generator: bytes -> preorder tree
  * (src/Alpacc/Generator/Futhark/Generator.hs:35-44, futhark/parser.fut:316-336). */
 int alp_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t** d_parent, uint32_t** d_tag,
