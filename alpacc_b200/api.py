@@ -310,3 +310,51 @@ class Grammar:
             return None
         k = n.value
         return par[:k], tag[:k], kind[:k], st[:k], en[:k]
+
+    # ---------------------------------------------------------------- batches
+    def _batch_inputs(self, data, offsets):
+        torch = _torch()
+        x = self._as_device_bytes(data)
+        off = torch.as_tensor(np.ascontiguousarray(offsets, dtype=np.int64)).to(self.device)
+        if off.numel() < 2 or int(off[-1]) != x.numel():
+            raise ValueError("offsets must run from 0 to len(data)")
+        return x, off
+
+    def lex_batch_int(self, data, offsets):
+        """Documents back to back (offsets[0..n]) -> (term, start, end,
+        tok_off[n+1], valid[n]); spans are relative to each document and a
+        document's tokens are meaningful only when valid[d] is 1."""
+        torch = _torch()
+        x, off = self._batch_inputs(data, offsets)
+        nd = off.numel() - 1
+        self._stream()
+        ptrs = [ctypes.c_void_p() for _ in range(5)]
+        total = ctypes.c_int64(0)
+        rc = native().alp_lex_batch(self.h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(off.data_ptr()), nd,
+                                    *[ctypes.byref(p) for p in ptrs], ctypes.byref(total))
+        if rc != ALP_OK:
+            self._err(rc)
+        k = total.value
+        return (_wrap(self.h, ptrs[0].value or 0, k, torch.int32, self.device),
+                _wrap(self.h, ptrs[1].value or 0, k, torch.int64, self.device),
+                _wrap(self.h, ptrs[2].value or 0, k, torch.int64, self.device),
+                _wrap(self.h, ptrs[3].value or 0, nd + 1, torch.int64, self.device),
+                _wrap(self.h, ptrs[4].value or 0, nd, torch.uint8, self.device))
+
+    def parse_batch_int(self, data, offsets):
+        """Documents back to back -> (Tree, node_off[n+1], valid[n]); parents
+        and spans are relative to each document."""
+        torch = _torch()
+        x, off = self._batch_inputs(data, offsets)
+        nd = off.numel() - 1
+        self._stream()
+        ptrs = [ctypes.c_void_p() for _ in range(7)]
+        total = ctypes.c_int64(0)
+        rc = native().alp_parse_batch(self.h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(off.data_ptr()), nd,
+                                      *[ctypes.byref(p) for p in ptrs], ctypes.byref(total))
+        if rc != ALP_OK:
+            self._err(rc)
+        k = total.value
+        tree = self._tree(*ptrs[:5], k)
+        return (tree, _wrap(self.h, ptrs[5].value or 0, nd + 1, torch.int64, self.device),
+                _wrap(self.h, ptrs[6].value or 0, nd, torch.uint8, self.device))

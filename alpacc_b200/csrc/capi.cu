@@ -13,6 +13,8 @@
 #include "common.cuh"
 #include "lexer.cuh"
 #include "parser.cuh"
+#include "mlp.cuh"
+#include "spec.cuh"
 
 using namespace alp;
 
@@ -48,11 +50,15 @@ struct alp_ctx {
     std::vector<void*> owned;             // table allocations
     DevBuf scratch;                       // look-back status words, results
     DevBuf out[8];                        // context-owned outputs
-    DevBuf tmp[24];                       // intermediates
+    DevBuf tmp[32];                       // intermediates
+    long long* h_stage = nullptr;         // pinned staging for small host->device values
     AlpResult* h_res = nullptr;           // pinned
     // optional per-kernel timing (alp_ctx_profile)
     int prof = 0;
     std::vector<std::pair<const char*, cudaEvent_t>> marks;
+    uint8_t* state_out = nullptr;         // set only inside alp_lex_states
+    DevBuf mlp[16];                       // MLP training activations
+    DevBuf spec[16];                      // speculative lexer chunk arrays
 };
 
 namespace {
@@ -200,10 +206,18 @@ int launch_lex(alp_ctx* ctx, const uint8_t* d_in, long long n, void* term, void*
     a.out_start = start;
     a.out_end = end;
     a.cap = cap;
+    a.num_tiles = (unsigned)tiles;
+    a.state_out = ctx->state_out;
     auto k = lex_kernel<ITEMS, TermT, PosT>;
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->lex_smem));
+    // persistent: as many CTAs as fit at once, each loops over tile tickets
+    int per_sm = 0, sms = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, LEX_THREADS, ctx->lex_smem));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    long long grid = (long long)(per_sm > 0 ? per_sm : 1) * sms;
+    if (grid > tiles) grid = tiles;
     mark(ctx, "start");
-    k<<<(unsigned)tiles, LEX_THREADS, ctx->lex_smem, ctx->stream>>>(a);
+    k<<<(unsigned)grid, LEX_THREADS, ctx->lex_smem, ctx->stream>>>(a);
     CK(cudaGetLastError());
     mark(ctx, "lex_kernel");
     CK(cudaMemcpyAsync(ctx->h_res, a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
@@ -245,7 +259,8 @@ int lex_core(alp_ctx* ctx, const uint8_t* d_in, int64_t n, TermT* term, PosT* st
 enum {
     T_HIN = 0, T_TTERM, T_TSTART, T_TEND, T_PID, T_TSUMS, T_VBUF, T_BRBUF, T_DSBUF,
     T_N_TMIN, T_N_M32, T_N_M1024, T_N_SVAL, T_N_SIDX, T_N_SLEN, T_N_ESC,
-    T_B_TMIN, T_B_M32, T_B_M1024, T_B_SVAL, T_B_SIDX, T_B_SLEN, T_B_ESC, T_CNT
+    T_B_TMIN, T_B_M32, T_B_M1024, T_B_SVAL, T_B_SIDX, T_B_SLEN, T_B_ESC,
+    T_DOCOFF, T_TOKOFF, T_NODEOFF, T_BROFF, T_DVALID, T_CNT
 };
 
 struct ParseOut {
@@ -275,7 +290,7 @@ int read_result(alp_ctx* ctx, AlpResult* d_res) {
 // Previous-smaller-or-equal over `n` values (nodes: writes parent; brackets:
 // checks each right bracket against its match and clears res->valid).
 int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, int64_t* parent, int first,
-            AlpResult* d_res) {
+            const long long* seg_off, long long n_seg, uint8_t* seg_valid, AlpResult* d_res) {
     if (n == 0) return ALP_OK;
     const long long tiles = (n + PLE_TILE - 1) / PLE_TILE;
     const long long n32 = (tiles + 31) / 32, n1024 = (tiles + 1023) / 1024;
@@ -295,6 +310,9 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     a.n = n;
     a.sym = sym;
     a.out_parent = reinterpret_cast<long long*>(parent);
+    a.seg_off = seg_off;
+    a.n_seg = n_seg;
+    a.seg_valid = seg_valid;
     a.tile_min = (int32_t*)ctx->tmp[first + 0].p;
     a.stair_val = (int32_t*)ctx->tmp[first + 3].p;
     a.stair_idx = (uint32_t*)ctx->tmp[first + 4].p;
@@ -323,6 +341,9 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     e.stair_len = a.stair_len;
     e.sym = sym;
     e.out_parent = a.out_parent;
+    e.seg_off = seg_off;
+    e.n_seg = n_seg;
+    e.seg_valid = seg_valid;
     e.res = d_res;
     ple_escape_kernel<<<148 * 4, 256, 0, ctx->stream>>>(e);
     CK(cudaGetLastError());
@@ -330,43 +351,125 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     return ALP_OK;
 }
 
-// Tokens already in tmp[T_TTERM..T_TEND] (m of them) -> tree.  `want_tree`
-// 0 gives the production sequence only (tags, subst off, no parents).
-int parse_tokens_core(alp_ctx* ctx, long long m, ParseOut* o, int64_t cap, int ctx_out, int64_t* n_node,
-                      int* valid, int want_tree) {
+// Segmented lexer over documents at d_off[0..nd] (device).  sentinels: the
+// parser layout (⊢ tokens ⊣ per document) into tmp[T_TTERM..T_TEND] with
+// u16/u32 types; otherwise the lexer API layout into the given buffers.
+// Per-document token offsets land in tmp[T_TOKOFF], validity in `valid`.
+template <typename TermT, typename PosT>
+int lex_seg(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_off, long long nd, int sentinels,
+            TermT* term, PosT* start, PosT* end, long long cap, uint8_t* valid, long long* total) {
+    *total = 0;
+    int rc;
+    if ((rc = grow(ctx, ctx->tmp[T_TOKOFF], (size_t)(nd + 1) * 8))) return rc;
+    if (n == 0) {
+        // every document is empty: rejected, no tokens
+        CK(cudaMemsetAsync(ctx->tmp[T_TOKOFF].p, 0, (size_t)(nd + 1) * 8, ctx->stream));
+        CK(cudaMemsetAsync(valid, 0, (size_t)nd, ctx->stream));
+        if (sentinels) {
+            // ⊢ ⊣ for each document
+            std::vector<uint16_t> h(2 * nd);
+            for (long long i = 0; i < nd; ++i) { h[2 * i] = (uint16_t)ctx->pt.start; h[2 * i + 1] = (uint16_t)ctx->pt.end; }
+            if (2 * nd > cap) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
+            CK(cudaMemcpy(term, h.data(), 2 * nd * sizeof(uint16_t), cudaMemcpyHostToDevice));
+        }
+        return ALP_OK;
+    }
+    const long long tiles = (n + LEX_TILE - 1) / LEX_TILE;
+    size_t sbytes = 256 + 8 * (size_t)tiles + 4 * (size_t)tiles;
+    if ((rc = grow(ctx, ctx->scratch, sbytes))) return rc;
+    uint8_t* base = reinterpret_cast<uint8_t*>(ctx->scratch.p);
+    CK(cudaMemsetAsync(base, 0, sbytes, ctx->stream));
+    LexArgs a;
+    a.in = d_in;
+    a.n = n;
+    a.aligned16 = ((reinterpret_cast<uintptr_t>(d_in) & 15u) == 0) ? 1 : 0;
+    a.t = ctx->lt;
+    a.res = reinterpret_cast<AlpResult*>(base);
+    a.ticket = reinterpret_cast<unsigned int*>(base + 128);
+    a.stB = reinterpret_cast<unsigned long long*>(base + 256);
+    a.stA = reinterpret_cast<uint32_t*>(base + 256 + 8 * (size_t)tiles);
+    a.out_term = term;
+    a.out_start = start;
+    a.out_end = end;
+    a.cap = cap;
+    a.num_tiles = (unsigned)tiles;
+    a.state_out = nullptr;
+    LexSeg sg;
+    sg.doc_off = d_off;
+    sg.n_docs = nd;
+    sg.tok_off = (long long*)ctx->tmp[T_TOKOFF].p;
+    sg.valid = valid;
+    sg.sentinels = sentinels;
+    sg.sent_l = ctx->has_parser ? ctx->pt.start : 0;
+    sg.sent_r = ctx->has_parser ? ctx->pt.end : 0;
+    auto k = lex_seg_kernel<LEX_ITEMS, TermT, PosT>;
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->lex_smem));
+    int per_sm = 0, sms = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, LEX_THREADS, ctx->lex_smem));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    long long grid = (long long)(per_sm > 0 ? per_sm : 1) * sms;
+    if (grid > tiles) grid = tiles;
+    mark(ctx, "start");
+    k<<<(unsigned)grid, LEX_THREADS, ctx->lex_smem, ctx->stream>>>(a, sg);
+    CK(cudaGetLastError());
+    mark(ctx, "lex_seg_kernel");
+    CK(cudaMemcpyAsync(ctx->h_res, a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
+    *total = ctx->h_res->count;
+    if (ctx->h_res->error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
+    return ALP_OK;
+}
+
+int put_doc_off(alp_ctx* ctx, long long n) {
+    int rc = grow(ctx, ctx->tmp[T_DOCOFF], 16);
+    if (rc) return rc;
+    ctx->h_stage[0] = 0;
+    ctx->h_stage[1] = n;
+    CK(cudaMemcpyAsync(ctx->tmp[T_DOCOFF].p, ctx->h_stage, 16, cudaMemcpyHostToDevice, ctx->stream));
+    return ALP_OK;
+}
+
+// Positions (⊢ tokens ⊣ per document, L of them) already in
+// tmp[T_TTERM..T_TEND] and per-document validity in `dvalid` -> tree.
+// `want_tree` 0 gives the production sequence only.  Node offsets of the
+// documents land in tmp[T_NODEOFF].
+int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, ParseOut* o, int64_t cap, int ctx_out,
+                    int64_t* n_node, int want_tree) {
     *n_node = 0;
-    *valid = 0;
-    const long long L = m + 2;
     const long long tiles = (L + PP_TILE - 1) / PP_TILE;
     int rc;
-    if ((rc = grow(ctx, ctx->tmp[T_PID], (size_t)L * 2 + 64)) || (rc = grow(ctx, ctx->tmp[T_TSUMS], tiles * sizeof(PosSums))))
+    if ((rc = grow(ctx, ctx->tmp[T_PID], (size_t)L * 2 + 64)) || (rc = grow(ctx, ctx->tmp[T_TSUMS], tiles * sizeof(PosSums))) ||
+        (rc = grow(ctx, ctx->tmp[T_NODEOFF], (size_t)(nd + 1) * 8)) || (rc = grow(ctx, ctx->tmp[T_BROFF], (size_t)(nd + 1) * 8)) ||
+        (rc = grow(ctx, ctx->scratch, 256)))
         return rc;
-    if ((rc = grow(ctx, ctx->scratch, 256))) return rc;
     AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
     if ((rc = set_result(ctx, d_res, 1))) return rc;
     ParseArgs a;
     memset(&a, 0, sizeof a);
     a.t = ctx->pt;
-    a.tterm = (const uint16_t*)ctx->tmp[T_TTERM].p;
-    a.tstart = (const uint32_t*)ctx->tmp[T_TSTART].p;
-    a.tend = (const uint32_t*)ctx->tmp[T_TEND].p;
-    a.m = m;
+    a.P = (const uint16_t*)ctx->tmp[T_TTERM].p;
+    a.pstart = (const uint32_t*)ctx->tmp[T_TSTART].p;
+    a.pend = (const uint32_t*)ctx->tmp[T_TEND].p;
     a.L = L;
+    a.n_docs = nd;
     a.pid = (uint16_t*)ctx->tmp[T_PID].p;
     a.tile_sums = (PosSums*)ctx->tmp[T_TSUMS].p;
     a.res = d_res;
+    a.node_off = (long long*)ctx->tmp[T_NODEOFF].p;
+    a.br_off = (long long*)ctx->tmp[T_BROFF].p;
+    a.doc_valid = dvalid;
     const size_t sm1 = sizeof(PairInfo) * ctx->pt.n_pairs + (size_t)(PP_TILE + ctx->pt.q + ctx->pt.k) * 4;
     CK(cudaFuncSetAttribute(parse_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
     mark(ctx, "start");
     parse_pairs_kernel<<<(unsigned)tiles, PP_THREADS, sm1, ctx->stream>>>(a);
     CK(cudaGetLastError());
     mark(ctx, "parse_pairs_kernel");
-    scan_tiles_kernel<<<1, 1024, 0, ctx->stream>>>(a.tile_sums, tiles, d_res);
+    scan_tiles_kernel<<<1, 1024, 0, ctx->stream>>>(a.tile_sums, tiles, d_res, a.node_off, a.br_off, nd);
     CK(cudaGetLastError());
     mark(ctx, "scan_tiles_kernel");
     if ((rc = read_result(ctx, d_res))) return rc;
-    const long long N = ctx->h_res->aux[0], B = ctx->h_res->aux[1], D = ctx->h_res->aux[2], NT = ctx->h_res->aux[4];
-    if (!ctx->h_res->valid || D != 0) return ALP_OK;  // rejected
+    const long long N = ctx->h_res->aux[0], B = ctx->h_res->aux[1];
     if (N > 0xffffffffLL || B > 0xffffffffLL) return fail(ctx, ALP_ERR_ARG, "tree too large");
     if (ctx_out) {
         if ((rc = grow(ctx, ctx->out[3], N * 8 + 8)) || (rc = grow(ctx, ctx->out[4], N * 4 + 8)) ||
@@ -385,9 +488,9 @@ int parse_tokens_core(alp_ctx* ctx, long long m, ParseOut* o, int64_t cap, int c
     if ((rc = grow(ctx, ctx->tmp[T_VBUF], N * 4 + 8)) || (rc = grow(ctx, ctx->tmp[T_BRBUF], B * 4 + 8)) ||
         (rc = grow(ctx, ctx->tmp[T_DSBUF], B * 4 + 8)))
         return rc;
-    a.subst_terminals = (want_tree && NT == m) ? 1 : 0;
     a.tag = o->tag;
-    a.kind = want_tree ? o->kind : (uint8_t*)ctx->tmp[T_VBUF].p;  // kind unused for productions only
+    a.kind = o->kind;
+    a.subst_terminals = want_tree;
     a.nstart = o->start;
     a.nend = o->end;
     a.vbuf = (int32_t*)ctx->tmp[T_VBUF].p;
@@ -395,20 +498,27 @@ int parse_tokens_core(alp_ctx* ctx, long long m, ParseOut* o, int64_t cap, int c
     a.dsbuf = (int32_t*)ctx->tmp[T_DSBUF].p;
     a.cap_nodes = N;
     a.cap_brs = B;
-    const size_t sm2 = sizeof(PairInfo) * ctx->pt.n_pairs + (size_t)ctx->pt.n_prods * 8;
+    const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_prods);
     CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
     mark(ctx, "start");
     parse_expand_kernel<<<(unsigned)tiles, PP_THREADS, sm2, ctx->stream>>>(a);
     CK(cudaGetLastError());
     mark(ctx, "parse_expand_kernel");
     if (want_tree) {
-        if ((rc = run_ple(ctx, a.vbuf, N, nullptr, o->parent, T_N_TMIN, d_res))) return rc;
+        if ((rc = run_ple(ctx, a.vbuf, N, nullptr, o->parent, T_N_TMIN, a.node_off, nd, dvalid, d_res))) return rc;
     }
-    if ((rc = run_ple(ctx, a.dsbuf, B, a.brbuf, nullptr, T_B_TMIN, d_res))) return rc;
+    if ((rc = run_ple(ctx, a.dsbuf, B, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res))) return rc;
     if ((rc = read_result(ctx, d_res))) return rc;
-    if (!ctx->h_res->valid) return ALP_OK;
-    *valid = 1;
     *n_node = N;
+    return ALP_OK;
+}
+
+int read_valid0(alp_ctx* ctx, const uint8_t* dvalid, int* valid) {
+    uint8_t v = 0;
+    CK(cudaMemcpyAsync(ctx->h_stage, dvalid, 1, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    memcpy(&v, ctx->h_stage, 1);
+    *valid = v ? 1 : 0;
     return ALP_OK;
 }
 
@@ -418,44 +528,86 @@ int parse_core(alp_ctx* ctx, const uint8_t* d_in, int64_t n, ParseOut* o, int64_
     *valid = 0;
     if (!ctx->has_lexer || !ctx->has_parser) return fail(ctx, ALP_ERR_MODE, "these tables are not lexer+parser tables");
     int rc;
-    if ((rc = grow(ctx, ctx->tmp[T_TTERM], (size_t)n * 2 + 16)) || (rc = grow(ctx, ctx->tmp[T_TSTART], (size_t)n * 4 + 16)) ||
-        (rc = grow(ctx, ctx->tmp[T_TEND], (size_t)n * 4 + 16)))
+    const size_t tcap = (size_t)n + 2 + 16;
+    if ((rc = grow(ctx, ctx->tmp[T_TTERM], tcap * 2)) || (rc = grow(ctx, ctx->tmp[T_TSTART], tcap * 4)) ||
+        (rc = grow(ctx, ctx->tmp[T_TEND], tcap * 4)) || (rc = grow(ctx, ctx->tmp[T_DVALID], 16)) ||
+        (rc = put_doc_off(ctx, n)))
         return rc;
-    int64_t m = 0;
-    int lv = 0;
-    rc = lex_core<uint16_t, uint32_t>(ctx, d_in, n, (uint16_t*)ctx->tmp[T_TTERM].p, (uint32_t*)ctx->tmp[T_TSTART].p,
-                                      (uint32_t*)ctx->tmp[T_TEND].p, n + 1, &m, &lv);
+    uint8_t* dvalid = (uint8_t*)ctx->tmp[T_DVALID].p;
+    long long m = 0;
+    rc = lex_seg<uint16_t, uint32_t>(ctx, d_in, n, (const long long*)ctx->tmp[T_DOCOFF].p, 1, 1,
+                                     (uint16_t*)ctx->tmp[T_TTERM].p, (uint32_t*)ctx->tmp[T_TSTART].p,
+                                     (uint32_t*)ctx->tmp[T_TEND].p, (long long)tcap, dvalid, &m);
     if (rc) return rc;
+    int lv = 0;
+    if ((rc = read_valid0(ctx, dvalid, &lv))) return rc;
     if (!lv) return ALP_OK;
-    return parse_tokens_core(ctx, m, o, cap, ctx_out, n_node, valid, 1);
+    int64_t N = 0;
+    rc = parse_positions(ctx, m + 2, 1, dvalid, o, cap, ctx_out, &N, 1);
+    if (rc) { *n_node = N; return rc; }
+    if ((rc = read_valid0(ctx, dvalid, valid))) return rc;
+    *n_node = *valid ? N : 0;
+    return ALP_OK;
 }
 
-// Token arrays from the caller (uint32 ids, int64 spans) -> internal form.
-__global__ void tokens_in_kernel(const uint32_t* term, const int64_t* ts, const int64_t* te, long long m, uint16_t* t16,
-                                 uint32_t* s32, uint32_t* e32, AlpResult* res) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
-        const uint32_t t = term[i];
-        if (t > 0xffffu) res->valid = 0;
-        t16[i] = (uint16_t)t;
-        s32[i] = ts ? (uint32_t)ts[i] : 0u;
-        e32[i] = te ? (uint32_t)te[i] : 0u;
+// Token arrays from the caller (uint32 ids, int64 spans) -> positions ⊢ tokens ⊣.
+__global__ void tokens_in_kernel(const uint32_t* term, const int64_t* ts, const int64_t* te, long long m, uint16_t* P,
+                                 uint32_t* s32, uint32_t* e32, uint32_t sl, uint32_t sr, AlpResult* res) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m + 2; i += (long long)gridDim.x * blockDim.x) {
+        if (i == 0 || i == m + 1) {
+            P[i] = (uint16_t)(i == 0 ? sl : sr);
+            s32[i] = 0;
+            e32[i] = 0;
+            continue;
+        }
+        const uint32_t t = term[i - 1];
+        if (t > 0xffffu || t == sl || t == sr) res->valid = 0;
+        P[i] = (uint16_t)t;
+        s32[i] = ts ? (uint32_t)ts[i - 1] : 0u;
+        e32[i] = te ? (uint32_t)te[i - 1] : 0u;
     }
 }
 
 int tokens_in(alp_ctx* ctx, const uint32_t* term, const int64_t* ts, const int64_t* te, int64_t m) {
     int rc;
-    if ((rc = grow(ctx, ctx->tmp[T_TTERM], (size_t)m * 2 + 16)) || (rc = grow(ctx, ctx->tmp[T_TSTART], (size_t)m * 4 + 16)) ||
-        (rc = grow(ctx, ctx->tmp[T_TEND], (size_t)m * 4 + 16)) || (rc = grow(ctx, ctx->scratch, 256)))
+    if ((rc = grow(ctx, ctx->tmp[T_TTERM], (size_t)(m + 2) * 2 + 16)) || (rc = grow(ctx, ctx->tmp[T_TSTART], (size_t)(m + 2) * 4 + 16)) ||
+        (rc = grow(ctx, ctx->tmp[T_TEND], (size_t)(m + 2) * 4 + 16)) || (rc = grow(ctx, ctx->scratch, 256)) ||
+        (rc = grow(ctx, ctx->tmp[T_DVALID], 16)))
         return rc;
-    if (m == 0) return ALP_OK;
     AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
     if ((rc = set_result(ctx, d_res, 1))) return rc;
     tokens_in_kernel<<<148 * 4, 256, 0, ctx->stream>>>(term, ts, te, m, (uint16_t*)ctx->tmp[T_TTERM].p,
-                                                      (uint32_t*)ctx->tmp[T_TSTART].p, (uint32_t*)ctx->tmp[T_TEND].p, d_res);
+                                                      (uint32_t*)ctx->tmp[T_TSTART].p, (uint32_t*)ctx->tmp[T_TEND].p,
+                                                      ctx->pt.start, ctx->pt.end, d_res);
     CK(cudaGetLastError());
     if ((rc = read_result(ctx, d_res))) return rc;
     if (!ctx->h_res->valid) return fail(ctx, ALP_ERR_ARG, "terminal id out of range");
+    CK(cudaMemsetAsync(ctx->tmp[T_DVALID].p, 1, 1, ctx->stream));
     return ALP_OK;
+}
+
+
+// ---- learned speculation: MLP training and inference, speculative lexer ----
+enum { M_X = 0, M_Z1, M_H1, M_H1B, M_Z2, M_H2, M_H2B, M_Z3, M_DZ3, M_DZ3B, M_DH, M_DZ, M_DZB, M_DX, M_SCAL, M_CNT };
+
+__global__ void positions_kernel(long long* pos, long long count, long long C) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x)
+        pos[i] = (i + 1) * C;
+}
+
+int gemm(alp_ctx* ctx, const __nv_bfloat16* A, long long sa_m, long long sa_k, const __nv_bfloat16* B, long long sb_k,
+         long long sb_n, float* C, long long ldc, int M, int N, int K) {
+    GemmArgs g{A, sa_m, sa_k, B, sb_k, sb_n, C, ldc, M, N, K, 0};
+    dim3 grid((N + 63) / 64, (M + 63) / 64);
+    gemm_bf16_kernel<<<grid, 128, 0, ctx->stream>>>(g);
+    CK(cudaGetLastError());
+    return ALP_OK;
+}
+
+inline unsigned grid_for(long long n) {
+    long long g = (n + 255) / 256;
+    if (g > 148 * 16) g = 148 * 16;
+    return (unsigned)(g < 1 ? 1 : g);
 }
 
 }  // namespace
@@ -485,6 +637,7 @@ int alp_ctx_create(const void* blob, size_t len, int device, alp_ctx** out) {
     if (!rc && hp) ctx->has_parser = true;
     if (!rc && cudaMallocHost(&ctx->h_res, sizeof(AlpResult)) != cudaSuccess)
         rc = fail(ctx, ALP_ERR_CUDA, "cudaMallocHost failed");
+    if (!rc && cudaMallocHost(&ctx->h_stage, 256) != cudaSuccess) rc = fail(ctx, ALP_ERR_CUDA, "cudaMallocHost failed");
     if (rc) {
         alp_ctx_destroy(ctx);
         return rc;
@@ -502,7 +655,13 @@ void alp_ctx_destroy(alp_ctx* ctx) {
         if (b.p) cudaFree(b.p);
     for (auto& b : ctx->tmp)
         if (b.p) cudaFree(b.p);
+    for (auto& b : ctx->mlp)
+        if (b.p) cudaFree(b.p);
+    for (auto& b : ctx->spec)
+        if (b.p) cudaFree(b.p);
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+    for (auto& m : ctx->marks) cudaEventDestroy(m.second);
     delete ctx;
 }
 
@@ -652,6 +811,8 @@ int alp_lex_noalloc(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_te
     a.out_start = d_start;
     a.out_end = d_end;
     a.cap = cap;
+    a.num_tiles = (unsigned)tiles;
+    a.state_out = nullptr;
     auto k = lex_kernel<LEX_ITEMS, uint32_t, int64_t>;
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->lex_smem));
     k<<<(unsigned)tiles, LEX_THREADS, ctx->lex_smem, ctx->stream>>>(a);
@@ -780,8 +941,12 @@ int alp_parse_tokens(alp_ctx* ctx, const uint32_t* d_term, const int64_t* d_tsta
     int rc = tokens_in(ctx, d_term, d_tstart, d_tend, m);
     if (rc) return rc;
     ParseOut o{};
-    rc = parse_tokens_core(ctx, m, &o, 0, 1, n_node, valid, 1);
+    uint8_t* dvalid = (uint8_t*)ctx->tmp[T_DVALID].p;
+    int64_t N = 0;
+    rc = parse_positions(ctx, m + 2, 1, dvalid, &o, 0, 1, &N, 1);
     if (rc) return rc;
+    if ((rc = read_valid0(ctx, dvalid, valid))) return rc;
+    *n_node = *valid ? N : 0;
     *d_parent = o.parent;
     *d_tag = o.tag;
     *d_kind = o.kind;
@@ -800,20 +965,317 @@ int alp_pre_productions(alp_ctx* ctx, const uint32_t* d_term, int64_t m, uint32_
     int rc = tokens_in(ctx, d_term, nullptr, nullptr, m);
     if (rc) return rc;
     ParseOut o{};
-    rc = parse_tokens_core(ctx, m, &o, 0, 1, n_prod, valid, 0);
+    uint8_t* dvalid = (uint8_t*)ctx->tmp[T_DVALID].p;
+    int64_t N = 0;
+    rc = parse_positions(ctx, m + 2, 1, dvalid, &o, 0, 1, &N, 0);
     if (rc) return rc;
+    if ((rc = read_valid0(ctx, dvalid, valid))) return rc;
+    *n_prod = *valid ? N : 0;
     *d_prod = o.tag;
     return ALP_OK;
 }
 
-// Entry points whose kernels are not in this build yet report ALP_ERR_MODE.
-int alp_lex_batch(alp_ctx* ctx, const uint8_t*, const int64_t*, int64_t, uint32_t**, int64_t**, int64_t**,
-                  int64_t**, uint8_t**, int64_t*) {
-    return fail(ctx, ALP_ERR_MODE, "alp_lex_batch: not available in this build");
+
+int alp_lex_states(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint8_t* d_states) {
+    int rc = check_in(ctx, d_in, n);
+    if (rc) return rc;
+    if (!d_states && n > 0) return fail(ctx, ALP_ERR_ARG, "null state buffer");
+    uint32_t* t;
+    int64_t *st, *en;
+    int64_t m;
+    int valid;
+    ctx->state_out = d_states;
+    rc = alp_lex(ctx, d_in, n, &t, &st, &en, &m, &valid);
+    ctx->state_out = nullptr;
+    return rc;
 }
-int alp_parse_batch(alp_ctx* ctx, const uint8_t*, const int64_t*, int64_t, int64_t**, uint32_t**, uint8_t**,
-                    int64_t**, int64_t**, int64_t**, uint8_t**, int64_t*) {
-    return fail(ctx, ALP_ERR_MODE, "alp_parse_batch: not available in this build");
+
+int alp_mlp_train_step(alp_ctx* ctx, float* params, uint16_t* wbf, float* grads, float* adam_m, float* adam_v,
+                       int n_states, const uint8_t* d_win, const uint8_t* d_lab, int batch, float lr, float wd,
+                       int step, int update, float* h_loss, float* h_acc) {
+    if (!ctx) return ALP_ERR_ARG;
+    if (!params || !wbf || !grads || !d_win || !d_lab || batch < 16 || (batch & 15) || n_states < 1 ||
+        n_states > MLP_OUT || (update && (!adam_m || !adam_v || step < 1)))
+        return fail(ctx, ALP_ERR_ARG, "bad MLP training arguments");
+    CK(cudaSetDevice(ctx->device));
+    const long long M = batch;
+    int rc;
+    static_assert(M_CNT <= 16, "scratch slots");
+    DevBuf* sb = ctx->mlp;
+    if ((rc = grow(ctx, sb[M_X], M * MLP_IN * 2)) || (rc = grow(ctx, sb[M_Z1], M * MLP_H * 4)) ||
+        (rc = grow(ctx, sb[M_H1], M * MLP_H * 4)) || (rc = grow(ctx, sb[M_H1B], M * MLP_H * 2)) ||
+        (rc = grow(ctx, sb[M_Z2], M * MLP_H * 4)) || (rc = grow(ctx, sb[M_H2], M * MLP_H * 4)) ||
+        (rc = grow(ctx, sb[M_H2B], M * MLP_H * 2)) || (rc = grow(ctx, sb[M_Z3], M * MLP_OUT * 4)) ||
+        (rc = grow(ctx, sb[M_DZ3], M * MLP_OUT * 4)) || (rc = grow(ctx, sb[M_DZ3B], M * MLP_OUT * 2)) ||
+        (rc = grow(ctx, sb[M_DH], M * MLP_H * 4)) || (rc = grow(ctx, sb[M_DZ], M * MLP_H * 4)) ||
+        (rc = grow(ctx, sb[M_DZB], M * MLP_H * 2)) || (rc = grow(ctx, sb[M_DX], M * MLP_IN * 4)) ||
+        (rc = grow(ctx, sb[M_SCAL], 64)))
+        return rc;
+    __nv_bfloat16* emb_b = reinterpret_cast<__nv_bfloat16*>(wbf);
+    __nv_bfloat16* w1_b = emb_b + 256 * MLP_EMB;
+    __nv_bfloat16* w2_b = w1_b + MLP_IN * MLP_H;
+    __nv_bfloat16* w3_b = w2_b + MLP_H * MLP_H;
+    auto bf = [&](int i) { return reinterpret_cast<__nv_bfloat16*>(sb[i].p); };
+    auto f32 = [&](int i) { return reinterpret_cast<float*>(sb[i].p); };
+    float* scal = f32(M_SCAL);
+    CK(cudaMemsetAsync(scal, 0, 64, ctx->stream));
+    const unsigned g1 = grid_for(M * MLP_IN);
+    // forward
+    gather_embed_kernel<<<g1, 256, 0, ctx->stream>>>(d_win, batch, emb_b, bf(M_X));
+    if ((rc = gemm(ctx, bf(M_X), MLP_IN, 1, w1_b, MLP_H, 1, f32(M_Z1), MLP_H, batch, MLP_H, MLP_IN))) return rc;
+    bias_relu_kernel<<<grid_for(M * MLP_H), 256, 0, ctx->stream>>>(f32(M_Z1), params + P_B1, batch, MLP_H, f32(M_H1), bf(M_H1B));
+    if ((rc = gemm(ctx, bf(M_H1B), MLP_H, 1, w2_b, MLP_H, 1, f32(M_Z2), MLP_H, batch, MLP_H, MLP_H))) return rc;
+    bias_relu_kernel<<<grid_for(M * MLP_H), 256, 0, ctx->stream>>>(f32(M_Z2), params + P_B2, batch, MLP_H, f32(M_H2), bf(M_H2B));
+    if ((rc = gemm(ctx, bf(M_H2B), MLP_H, 1, w3_b, MLP_OUT, 1, f32(M_Z3), MLP_OUT, batch, MLP_OUT, MLP_H))) return rc;
+    softmax_ce_kernel<<<grid_for(M * 32), 256, 0, ctx->stream>>>(f32(M_Z3), params + P_B3, d_lab, batch, n_states,
+                                                                 f32(M_DZ3), bf(M_DZ3B), scal,
+                                                                 reinterpret_cast<unsigned int*>(scal + 1));
+    // backward
+    if ((rc = gemm(ctx, bf(M_H2B), 1, MLP_H, bf(M_DZ3B), MLP_OUT, 1, grads + P_W3, MLP_OUT, MLP_H, MLP_OUT, batch))) return rc;
+    colsum_kernel<<<MLP_OUT, 256, 0, ctx->stream>>>(f32(M_DZ3), batch, MLP_OUT, grads + P_B3);
+    if ((rc = gemm(ctx, bf(M_DZ3B), MLP_OUT, 1, w3_b, 1, MLP_OUT, f32(M_DH), MLP_H, batch, MLP_H, MLP_OUT))) return rc;
+    relu_back_kernel<<<grid_for(M * MLP_H), 256, 0, ctx->stream>>>(f32(M_DH), f32(M_H2), M * MLP_H, bf(M_DZB), f32(M_DZ));
+    if ((rc = gemm(ctx, bf(M_H1B), 1, MLP_H, bf(M_DZB), MLP_H, 1, grads + P_W2, MLP_H, MLP_H, MLP_H, batch))) return rc;
+    colsum_kernel<<<MLP_H, 256, 0, ctx->stream>>>(f32(M_DZ), batch, MLP_H, grads + P_B2);
+    if ((rc = gemm(ctx, bf(M_DZB), MLP_H, 1, w2_b, 1, MLP_H, f32(M_DH), MLP_H, batch, MLP_H, MLP_H))) return rc;
+    relu_back_kernel<<<grid_for(M * MLP_H), 256, 0, ctx->stream>>>(f32(M_DH), f32(M_H1), M * MLP_H, bf(M_DZB), f32(M_DZ));
+    if ((rc = gemm(ctx, bf(M_X), 1, MLP_IN, bf(M_DZB), MLP_H, 1, grads + P_W1, MLP_H, MLP_IN, MLP_H, batch))) return rc;
+    colsum_kernel<<<MLP_H, 256, 0, ctx->stream>>>(f32(M_DZ), batch, MLP_H, grads + P_B1);
+    if ((rc = gemm(ctx, bf(M_DZB), MLP_H, 1, w1_b, 1, MLP_H, f32(M_DX), MLP_IN, batch, MLP_IN, MLP_H))) return rc;
+    CK(cudaMemsetAsync(grads + P_EMB, 0, 256 * MLP_EMB * 4, ctx->stream));
+    scatter_embed_kernel<<<g1, 256, 0, ctx->stream>>>(d_win, batch, f32(M_DX), grads + P_EMB);
+    CK(cudaGetLastError());
+    if (update) {
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float bc1 = 1.f - powf(b1, (float)step), bc2 = 1.f - powf(b2, (float)step);
+        adamw_kernel<<<grid_for(P_TOTAL), 256, 0, ctx->stream>>>(params, grads, adam_m, adam_v, P_TOTAL, lr, b1, b2,
+                                                                 1e-8f, wd, bc1, bc2, emb_b, w1_b, w2_b, w3_b);
+        CK(cudaGetLastError());
+    }
+    if (h_loss || h_acc) {
+        float hs[2];
+        CK(cudaMemcpyAsync(hs, scal, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        unsigned int corr;
+        memcpy(&corr, &hs[1], 4);
+        if (h_loss) *h_loss = hs[0] / (float)batch;
+        if (h_acc) *h_acc = (float)corr / (float)batch;
+    }
+    return ALP_OK;
+}
+
+int alp_mlp_predict(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_states, const uint8_t* d_in, int64_t n,
+                    const int64_t* d_pos, int64_t count, uint8_t* d_pred) {
+    if (!ctx) return ALP_ERR_ARG;
+    if (!wbf || !wf32 || n_states < 1 || n_states > MLP_OUT || count < 0 || (count > 0 && (!d_pos || !d_pred)))
+        return fail(ctx, ALP_ERR_ARG, "bad MLP arguments");
+    CK(cudaSetDevice(ctx->device));
+    if (count == 0) return ALP_OK;
+    MlpWeights w;
+    w.emb = reinterpret_cast<const __nv_bfloat16*>(wbf);
+    w.w1 = w.emb + 256 * MLP_EMB;
+    w.w2 = w.w1 + MLP_IN * MLP_H;
+    w.w3 = w.w2 + MLP_H * MLP_H;
+    w.b1 = wf32 + P_B1;
+    w.b2 = wf32 + P_B2;
+    w.b3 = wf32 + P_B3;
+    w.n_states = n_states;
+    CK(cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM));
+    mark(ctx, "start");
+    mlp_infer_kernel<<<(unsigned)((count + INF_ROWS - 1) / INF_ROWS), 256, INF_SMEM, ctx->stream>>>(
+        w, d_in, n, reinterpret_cast<const long long*>(d_pos), count, d_pred);
+    CK(cudaGetLastError());
+    mark(ctx, "mlp_infer_kernel");
+    return ALP_OK;
+}
+
+int alp_lex_speculative(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_states, const uint8_t* d_in,
+                        int64_t n, int64_t chunk, uint32_t** d_term, int64_t** d_start, int64_t** d_end,
+                        int64_t* n_tok, int* valid, int64_t* stats) {
+    int rc = check_in(ctx, d_in, n);
+    if (rc) return rc;
+    if (!d_term || !d_start || !d_end || !n_tok || !valid) return fail(ctx, ALP_ERR_ARG, "null output");
+    if (chunk < 64 || (chunk & 15)) return fail(ctx, ALP_ERR_ARG, "chunk must be a multiple of 16, at least 64");
+    if (!ctx->has_lexer) return fail(ctx, ALP_ERR_MODE, "these tables have no lexer");
+    if (ctx->S > 255) return fail(ctx, ALP_ERR_TABLE, "too many states for byte-sized predictions");
+    CK(cudaSetDevice(ctx->device));
+    *n_tok = 0;
+    *valid = 0;
+    if (stats) for (int i = 0; i < 4; ++i) stats[i] = 0;
+    if (n == 0) {
+        *valid = (ctx->h_tokinfo[1] & TOK_ACCEPT) ? 1 : 0;
+        return ALP_OK;
+    }
+    const long long K = (n + chunk - 1) / chunk;
+    const long long nb = (K + SPEC_SCAN_BLOCK - 1) / SPEC_SCAN_BLOCK;
+    DevBuf* sb = ctx->spec;
+    if ((rc = grow(ctx, sb[0], K + 16)) || (rc = grow(ctx, sb[1], K + 16)) || (rc = grow(ctx, sb[2], K * 4 + 16)) ||
+        (rc = grow(ctx, sb[3], K * 4 + 16)) || (rc = grow(ctx, sb[4], K * 4 + 16)) || (rc = grow(ctx, sb[5], K * 4 + 16)) ||
+        (rc = grow(ctx, sb[6], K * 4 + 16)) || (rc = grow(ctx, sb[7], K * 4 + 16)) || (rc = grow(ctx, sb[8], nb * 4 + 16)) ||
+        (rc = grow(ctx, sb[9], nb * 4 + 16)) || (rc = grow(ctx, sb[10], K * 8 + 16)) || (rc = grow(ctx, sb[11], 64)))
+        return rc;
+    int64_t cap = n / 2 + 1024;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        if ((rc = grow(ctx, ctx->out[0], cap * 4)) || (rc = grow(ctx, ctx->out[1], cap * 8)) ||
+            (rc = grow(ctx, ctx->out[2], cap * 8)))
+            return rc;
+        cap = (int64_t)(ctx->out[1].bytes / 8);
+        SpecArgs a;
+        memset(&a, 0, sizeof a);
+        a.in = d_in;
+        a.n = n;
+        a.C = chunk;
+        a.K = K;
+        a.t = ctx->lt;
+        a.st = (uint8_t*)sb[0].p;
+        a.en = (uint8_t*)sb[1].p;
+        a.cnt = (uint32_t*)sb[2].p;
+        a.lastp = (uint32_t*)sb[3].p;
+        uint32_t* lists[2] = {(uint32_t*)sb[4].p, (uint32_t*)sb[5].p};
+        uint32_t* ex_c = (uint32_t*)sb[6].p;
+        uint32_t* ex_p = (uint32_t*)sb[7].p;
+        unsigned int* next_n = (unsigned int*)sb[11].p;
+        const size_t ssm = spec_smem_bytes(ctx->S, ctx->C + 1);
+        // 1) predictions at every chunk boundary; chunk 0 starts in the initial state
+        CK(cudaMemsetAsync(a.st, 1, 1, ctx->stream));
+        if (K > 1) {
+            long long* pos = (long long*)sb[10].p;
+            positions_kernel<<<grid_for(K - 1), 256, 0, ctx->stream>>>(pos, K - 1, chunk);
+            if ((rc = alp_mlp_predict(ctx, wbf, wf32, n_states, d_in, n, reinterpret_cast<const int64_t*>(pos), K - 1, a.st + 1))) return rc;
+        }
+        // 2) run every chunk, 3) fix and re-run until every start is exact
+        mark(ctx, "start");
+        spec_run_kernel<<<grid_for(K), 256, ssm, ctx->stream>>>(a);
+        CK(cudaGetLastError());
+        mark(ctx, "spec_run_kernel");
+        long long reruns = 0, first = -1, rounds = 0;
+        int cur = 0;
+        while (true) {
+            CK(cudaMemsetAsync(next_n, 0, 4, ctx->stream));
+            a.next_list = lists[cur];
+            a.next_n = next_n;
+            spec_fix_kernel<<<grid_for(K), 256, 0, ctx->stream>>>(a);
+            CK(cudaGetLastError());
+            unsigned int h_next = 0;
+            CK(cudaMemcpyAsync(ctx->h_stage, next_n, 4, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            memcpy(&h_next, ctx->h_stage, 4);
+            if (first < 0) first = h_next;
+            if (h_next == 0) break;
+            ++rounds;
+            reruns += h_next;
+            a.list = lists[cur];
+            a.list_n = h_next;
+            spec_run_kernel<<<grid_for(h_next), 256, ssm, ctx->stream>>>(a);
+            CK(cudaGetLastError());
+            a.list = nullptr;
+            cur ^= 1;
+            if (rounds > 4096) return fail(ctx, ALP_ERR_TIMEOUT, "speculation did not settle");
+        }
+        mark(ctx, "spec_verify");
+        // 4) token offsets per chunk, 5) emit
+        spec_scan_local<<<(unsigned)nb, SPEC_SCAN_BLOCK, 0, ctx->stream>>>(a.cnt, a.lastp, K, ex_c, ex_p, (uint32_t*)sb[8].p,
+                                                                          (uint32_t*)sb[9].p);
+        spec_scan_blocks<<<1, 1024, 0, ctx->stream>>>((uint32_t*)sb[8].p, (uint32_t*)sb[9].p, nb);
+        spec_scan_add<<<(unsigned)((K + 255) / 256), 256, 0, ctx->stream>>>(ex_c, ex_p, K, (uint32_t*)sb[8].p,
+                                                                            (uint32_t*)sb[9].p);
+        CK(cudaGetLastError());
+        if ((rc = grow(ctx, ctx->scratch, 256))) return rc;
+        AlpResult* res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
+        CK(cudaMemsetAsync(res, 0, sizeof(AlpResult), ctx->stream));
+        a.cnt_excl = ex_c;
+        a.pos_excl = ex_p;
+        a.out_term = (uint32_t*)ctx->out[0].p;
+        a.out_start = (int64_t*)ctx->out[1].p;
+        a.out_end = (int64_t*)ctx->out[2].p;
+        a.cap = cap;
+        a.res = res;
+        spec_emit_kernel<<<grid_for(K), 256, ssm, ctx->stream>>>(a);
+        CK(cudaGetLastError());
+        mark(ctx, "spec_emit_kernel");
+        if ((rc = read_result(ctx, res)) && rc != ALP_ERR_CAPACITY) return rc;
+        if (rc == ALP_ERR_CAPACITY || ctx->h_res->count > cap) {
+            cap = ctx->h_res->count + 1;
+            continue;
+        }
+        *valid = ctx->h_res->valid;
+        *n_tok = *valid ? ctx->h_res->count : 0;
+        if (stats) { stats[0] = K; stats[1] = first; stats[2] = reruns; stats[3] = rounds; }
+        break;
+    }
+    *d_term = (uint32_t*)ctx->out[0].p;
+    *d_start = (int64_t*)ctx->out[1].p;
+    *d_end = (int64_t*)ctx->out[2].p;
+    return ALP_OK;
+}
+
+int alp_lex_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int64_t n_docs, uint32_t** d_term,
+                  int64_t** d_start, int64_t** d_end, int64_t** d_tok_off, uint8_t** d_valid, int64_t* n_tok_total) {
+    if (!ctx) return ALP_ERR_ARG;
+    if (n_docs < 1 || !d_off || !d_term || !d_start || !d_end || !d_tok_off || !d_valid || !n_tok_total)
+        return fail(ctx, ALP_ERR_ARG, "bad batch arguments");
+    if (!ctx->has_lexer) return fail(ctx, ALP_ERR_MODE, "these tables have no lexer");
+    CK(cudaSetDevice(ctx->device));
+    int64_t n = 0;
+    CK(cudaMemcpyAsync(ctx->h_stage, d_off + n_docs, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    n = ctx->h_stage[0];
+    int rc = check_in(ctx, d_in, n);
+    if (rc) return rc;
+    if ((rc = grow(ctx, ctx->out[0], (size_t)n * 4 + 16)) || (rc = grow(ctx, ctx->out[1], (size_t)n * 8 + 16)) ||
+        (rc = grow(ctx, ctx->out[2], (size_t)n * 8 + 16)) || (rc = grow(ctx, ctx->tmp[T_DVALID], (size_t)n_docs + 16)))
+        return rc;
+    long long total = 0;
+    rc = lex_seg<uint32_t, int64_t>(ctx, d_in, n, (const long long*)d_off, n_docs, 0, (uint32_t*)ctx->out[0].p,
+                                    (int64_t*)ctx->out[1].p, (int64_t*)ctx->out[2].p, n + 1,
+                                    (uint8_t*)ctx->tmp[T_DVALID].p, &total);
+    if (rc) return rc;
+    *d_term = (uint32_t*)ctx->out[0].p;
+    *d_start = (int64_t*)ctx->out[1].p;
+    *d_end = (int64_t*)ctx->out[2].p;
+    *d_tok_off = (int64_t*)ctx->tmp[T_TOKOFF].p;
+    *d_valid = (uint8_t*)ctx->tmp[T_DVALID].p;
+    *n_tok_total = total;
+    return ALP_OK;
+}
+
+int alp_parse_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int64_t n_docs, int64_t** d_parent,
+                    uint32_t** d_tag, uint8_t** d_kind, int64_t** d_start, int64_t** d_end, int64_t** d_node_off,
+                    uint8_t** d_valid, int64_t* n_node_total) {
+    if (!ctx) return ALP_ERR_ARG;
+    if (n_docs < 1 || !d_off || !d_parent || !d_tag || !d_kind || !d_start || !d_end || !d_node_off || !d_valid ||
+        !n_node_total)
+        return fail(ctx, ALP_ERR_ARG, "bad batch arguments");
+    if (!ctx->has_lexer || !ctx->has_parser) return fail(ctx, ALP_ERR_MODE, "these tables are not lexer+parser tables");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(ctx->h_stage, d_off + n_docs, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const int64_t n = ctx->h_stage[0];
+    int rc = check_in(ctx, d_in, n);
+    if (rc) return rc;
+    const size_t tcap = (size_t)n + 2 * (size_t)n_docs + 16;
+    if ((rc = grow(ctx, ctx->tmp[T_TTERM], tcap * 2)) || (rc = grow(ctx, ctx->tmp[T_TSTART], tcap * 4)) ||
+        (rc = grow(ctx, ctx->tmp[T_TEND], tcap * 4)) || (rc = grow(ctx, ctx->tmp[T_DVALID], (size_t)n_docs + 16)))
+        return rc;
+    uint8_t* dvalid = (uint8_t*)ctx->tmp[T_DVALID].p;
+    long long m = 0;
+    rc = lex_seg<uint16_t, uint32_t>(ctx, d_in, n, (const long long*)d_off, n_docs, 1, (uint16_t*)ctx->tmp[T_TTERM].p,
+                                     (uint32_t*)ctx->tmp[T_TSTART].p, (uint32_t*)ctx->tmp[T_TEND].p, (long long)tcap,
+                                     dvalid, &m);
+    if (rc) return rc;
+    ParseOut o{};
+    int64_t N = 0;
+    rc = parse_positions(ctx, m + 2 * n_docs, n_docs, dvalid, &o, 0, 1, &N, 1);
+    if (rc) return rc;
+    *d_parent = o.parent;
+    *d_tag = o.tag;
+    *d_kind = o.kind;
+    *d_start = o.start;
+    *d_end = o.end;
+    *d_node_off = (int64_t*)ctx->tmp[T_NODEOFF].p;
+    *d_valid = dvalid;
+    *n_node_total = N;
+    return ALP_OK;
 }
 
 }  // extern "C"

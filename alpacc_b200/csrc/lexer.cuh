@@ -47,6 +47,8 @@ struct LexArgs {
     void* out_end;
     long long cap;
     AlpResult* res;
+    unsigned int num_tiles;        // tiles of the input; CTAs loop over tickets until done
+    uint8_t* state_out;            // optional: DFA state entering each ITEMS-byte chunk (exact)
 };
 
 __host__ __device__ inline size_t lex_smem_bytes(int S, int C1, int E) {
@@ -79,10 +81,12 @@ __global__ void __launch_bounds__(LEX_THREADS) lex_kernel(LexArgs a) {
     for (int i = tid; i < S; i += LEX_THREADS) s_tok[i] = a.t.tokinfo[i];
     for (int i = tid; i < S * C1; i += LEX_THREADS) s_cd[i] = a.t.cdelta[i];
     for (int i = tid; i < E * C1; i += LEX_THREADS) s_step[i] = a.t.step[i];
+    const long long n = a.n;
+    for (;;) {
     if (tid == 0) s_tile = atomicAdd(a.ticket, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
-    const long long n = a.n;
+    if (tile >= a.num_tiles) break;
     const long long my = (long long)tile * TILE + (long long)tid * ITEMS;
     const uint8_t PAD = (uint8_t)(C1 - 1);
 
@@ -169,21 +173,29 @@ __global__ void __launch_bounds__(LEX_THREADS) lex_kernel(LexArgs a) {
     __syncthreads();
     const uint32_t fexc = __ldg(&a.t.comp[s_wexc[warp] * E + excl]);
     const uint32_t s0 = __ldg(&a.t.apply[fexc * S + s_sin]);
+    if (a.state_out && my < n) a.state_out[my / ITEMS] = (uint8_t)s0;
 
-    // ---- phase B, pass 1: token count and last token start ----------------
-    uint32_t cnt = 0, lastp = ALP_NONE32;
+    // ---- phase B: run the DFA once, recording token ends and starts -------
+    // bit j of emit: a token ends just before byte j (its terminal in tk[j]);
+    // bit j of stt: a token starts at byte j.
+    uint32_t cnt = 0, lastp = ALP_NONE32, emit = 0, stt = 0;
+    uint32_t tk[ITEMS];
+    uint32_t s_last;
     {
         uint32_t s = s0;
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
             uint32_t e = s_cd[s * C1 + c[j]];
             uint32_t s2 = e & 0x7fffu;
+            tk[j] = 0;
             if (e & 0x8000u) {
-                if (!(s_tok[s] & TOK_IGNORE)) ++cnt;
-                if (!(s_tok[s2] & TOK_IGNORE)) lastp = (uint32_t)(my + j);
+                const uint32_t ti = s_tok[s];
+                if (!(ti & TOK_IGNORE)) { ++cnt; emit |= 1u << j; tk[j] = ti & TOK_TERM_MASK; }
+                if (!(s_tok[s2] & TOK_IGNORE)) { lastp = (uint32_t)(my + j); stt |= 1u << j; }
             }
             s = s2;
         }
+        s_last = s;
     }
     uint32_t ic = cnt, ip = lastp;
     warp_scan_cs(ic, ip, lane);
@@ -250,27 +262,21 @@ __global__ void __launch_bounds__(LEX_THREADS) lex_kernel(LexArgs a) {
     TermT* o_term = reinterpret_cast<TermT*>(a.out_term);
     PosT* o_start = reinterpret_cast<PosT*>(a.out_start);
     PosT* o_end = reinterpret_cast<PosT*>(a.out_end);
-    uint32_t s = s0;
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
-        uint32_t e = s_cd[s * C1 + c[j]];
-        uint32_t s2 = e & 0x7fffu;
-        if (e & 0x8000u) {
-            uint32_t ti = s_tok[s];
-            if (!(ti & TOK_IGNORE)) {
-                if ((long long)tcount < a.cap) {
-                    o_term[tcount] = (TermT)(ti & TOK_TERM_MASK);
-                    o_start[tcount] = (PosT)cur;
-                    o_end[tcount] = (PosT)(my + j);
-                } else {
-                    atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
-                }
-                ++tcount;
+        if (emit & (1u << j)) {
+            if ((long long)tcount < a.cap) {
+                o_term[tcount] = (TermT)tk[j];
+                o_start[tcount] = (PosT)cur;
+                o_end[tcount] = (PosT)(my + j);
+            } else {
+                atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
             }
-            if (!(s_tok[s2] & TOK_IGNORE)) cur = (uint32_t)(my + j);
+            ++tcount;
         }
-        s = s2;
+        if (stt & (1u << j)) cur = (uint32_t)(my + j);
     }
+    const uint32_t s = s_last;
     // ---- the final token and the accept test ------------------------------
     if (my <= n - 1 && n - 1 < my + ITEMS) {
         uint32_t ti = s_tok[s];
@@ -287,6 +293,353 @@ __global__ void __launch_bounds__(LEX_THREADS) lex_kernel(LexArgs a) {
         }
         a.res->count = total;
         a.res->valid = (ti & TOK_ACCEPT) ? 1 : 0;
+    }
+    __syncthreads();  // shared words are rewritten by the next tile
+    }
+}
+
+}  // namespace alp
+
+namespace alp {
+
+// ---------------------------------------------------------------------------
+// Segmented lexer: many documents back to back in one launch.
+//
+// Each document is lexed exactly as the single-document kernel lexes one
+// input (the reference API lexes one document per call): at a document's
+// first byte the DFA restarts from the initial state and a token start is
+// forced; at its last byte its final token is appended and its accept bit is
+// its validity.  In the endomorphism scan a restart is a constant function,
+// encoded as id E + state (ext_* below), so the same scan and look-backs
+// carry it across threads and tiles.
+//
+// Outputs: tokens compacted in document order with spans relative to their
+// document, tok_off[d] = index of document d's first token, valid[d].  With
+// `sentinels` the tokens are laid out for the parser instead: document d
+// occupies [tok_off[d] + 2d, tok_off[d+1] + 2d + 2) as ⊢, its tokens, ⊣.
+// ---------------------------------------------------------------------------
+struct LexSeg {
+    const long long* doc_off;  // [n_docs + 1], doc_off[n_docs] = n
+    long long n_docs;
+    long long* tok_off;        // [n_docs + 1] out
+    uint8_t* valid;            // [n_docs] out
+    int sentinels;
+    uint32_t sent_l, sent_r;   // ⊢ and ⊣ terminal ids
+};
+
+__device__ __forceinline__ uint32_t ext_apply(const LexTables& t, uint32_t f, uint32_t s) {
+    return f >= (uint32_t)t.E ? f - t.E : __ldg(&t.apply[f * t.S + s]);
+}
+__device__ __forceinline__ uint32_t ext_comp(const LexTables& t, uint32_t a, uint32_t b) {
+    if (b >= (uint32_t)t.E) return b;
+    if (a >= (uint32_t)t.E) return t.E + __ldg(&t.apply[b * t.S + (a - t.E)]);
+    return __ldg(&t.comp[a * t.E + b]);
+}
+
+// largest d in [lo, hi] with off[d] <= p
+__device__ __forceinline__ long long doc_upper(const long long* off, long long lo, long long hi, long long p) {
+    while (lo < hi) {
+        const long long mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= p) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+// smallest d in [lo, hi] with off[d] >= p
+__device__ __forceinline__ long long doc_lower(const long long* off, long long lo, long long hi, long long p) {
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (off[mid] >= p) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+template <int ITEMS, typename TermT, typename PosT>
+__global__ void __launch_bounds__(LEX_THREADS) lex_seg_kernel(LexArgs a, LexSeg sg) {
+    constexpr int TILE = LEX_THREADS * ITEMS;
+    static_assert(ITEMS <= 32, "bit masks hold one bit per byte");
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int S = a.t.S, C1 = a.t.C1, E = a.t.E;
+    uint8_t* s_cls = smem;
+    uint32_t* s_tok = reinterpret_cast<uint32_t*>(smem + 256);
+    uint16_t* s_cd = reinterpret_cast<uint16_t*>(smem + 256 + 4 * S);
+    size_t off_step = (256 + 4 * (size_t)S + 2 * (size_t)S * C1 + 15) & ~(size_t)15;
+    uint16_t* s_step = reinterpret_cast<uint16_t*>(smem + off_step);
+
+    __shared__ uint32_t s_tile;
+    __shared__ long long s_d0, s_d1;
+    __shared__ uint32_t s_wagg[LEX_THREADS / 32];
+    __shared__ uint32_t s_wexc[LEX_THREADS / 32];
+    __shared__ uint32_t s_sin;
+    __shared__ uint32_t s_wc[LEX_THREADS / 32], s_wp[LEX_THREADS / 32];
+    __shared__ uint32_t s_xc, s_xp;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < 256; i += LEX_THREADS) s_cls[i] = a.t.cls[i];
+    for (int i = tid; i < S; i += LEX_THREADS) s_tok[i] = a.t.tokinfo[i];
+    for (int i = tid; i < S * C1; i += LEX_THREADS) s_cd[i] = a.t.cdelta[i];
+    for (int i = tid; i < E * C1; i += LEX_THREADS) s_step[i] = a.t.step[i];
+    const long long n = a.n;
+    const long long ND = sg.n_docs;
+    const uint8_t PAD = (uint8_t)(C1 - 1);
+    const uint32_t INIT = 1u;
+    for (;;) {
+        if (tid == 0) {
+            s_tile = atomicAdd(a.ticket, 1u);
+            if (s_tile < a.num_tiles) {
+                const long long t0 = (long long)s_tile * TILE;
+                const long long t1 = min(t0 + TILE, n) - 1;
+                s_d0 = doc_upper(sg.doc_off, 0, ND - 1, t0);
+                s_d1 = doc_upper(sg.doc_off, 0, ND - 1, t1);
+            }
+        }
+        __syncthreads();
+        const uint32_t tile = s_tile;
+        if (tile >= a.num_tiles) break;
+        const long long my = (long long)tile * TILE + (long long)tid * ITEMS;
+        const long long d0 = s_d0, d1 = s_d1;
+
+        // ---- bytes, document heads and last bytes of this thread ----------
+        uint8_t c[ITEMS];
+        if (a.aligned16 && my + ITEMS <= n) {
+#pragma unroll
+            for (int v = 0; v < ITEMS / 16; ++v) {
+                uint4 w = __ldg(reinterpret_cast<const uint4*>(a.in + my) + v);
+                uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                for (int j = 0; j < 16; ++j) c[v * 16 + j] = s_cls[(ws[j >> 2] >> (8 * (j & 3))) & 0xff];
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) c[j] = (my + j < n) ? s_cls[a.in[my + j]] : PAD;
+        }
+        uint32_t head = 0, last = 0;
+        long long mydoc = 0;
+        if (my < n) {
+            mydoc = doc_upper(sg.doc_off, d0, d1, my);
+            if (sg.doc_off[mydoc] == my) head |= 1u;
+            for (long long d = mydoc + 1; d <= ND; ++d) {
+                const long long h = sg.doc_off[d];
+                if (h > my + ITEMS || h > n) break;
+                if (h - 1 >= my) last |= 1u << (int)(h - 1 - my);
+                if (h < n && h < my + ITEMS) head |= 1u << (int)(h - my);
+            }
+        }
+
+        // ---- phase A ------------------------------------------------------
+        uint32_t f = 0;
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (head & (1u << j)) f = E + (s_cd[INIT * C1 + c[j]] & 0x7fffu);
+            else if (f >= (uint32_t)E) f = E + (s_cd[(f - E) * C1 + c[j]] & 0x7fffu);
+            else f = s_step[f * C1 + c[j]];
+        }
+        uint32_t incl = f;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t o = __shfl_up_sync(ALP_FULL_MASK, incl, d);
+            if (lane >= d) incl = ext_comp(a.t, o, incl);
+        }
+        uint32_t excl = __shfl_up_sync(ALP_FULL_MASK, incl, 1);
+        if (lane == 0) excl = 0;
+        if (lane == 31) s_wagg[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = lane < LEX_THREADS / 32 ? s_wagg[lane] : 0u;
+            uint32_t wi = w;
+#pragma unroll
+            for (int d = 1; d < LEX_THREADS / 32; d <<= 1) {
+                uint32_t o = __shfl_up_sync(ALP_FULL_MASK, wi, d);
+                if (lane >= d) wi = ext_comp(a.t, o, wi);
+            }
+            uint32_t we = __shfl_up_sync(ALP_FULL_MASK, wi, 1);
+            if (lane == 0) we = 0;
+            if (lane < LEX_THREADS / 32) s_wexc[lane] = we;
+            const uint32_t F = __shfl_sync(ALP_FULL_MASK, wi, LEX_THREADS / 32 - 1);
+            uint32_t sin;
+            if (tile == 0) {
+                sin = INIT;
+                if (lane == 0) st_volatile32(&a.stA[0], (ST_P << 30) | ext_apply(a.t, F, sin));
+            } else {
+                if (lane == 0) st_volatile32(&a.stA[tile], (ST_A << 30) | F);
+                uint32_t acc = 0;
+                long long end = tile;
+                while (true) {
+                    long long idx = end - 32 + lane;
+                    uint32_t w2 = idx >= 0 ? wait32(&a.stA[idx], &a.res->error) : ((ST_P << 30) | INIT);
+                    uint32_t flag = w2 >> 30, val = w2 & 0x3fffffffu;
+                    uint32_t pm = __ballot_sync(ALP_FULL_MASK, flag == ST_P);
+                    if (pm) {
+                        int p = 31 - __clz(pm);
+                        uint32_t s = __shfl_sync(ALP_FULL_MASK, val, p);
+                        for (int j = p + 1; j < 32; ++j) {
+                            uint32_t aj = __shfl_sync(ALP_FULL_MASK, val, j);
+                            s = ext_apply(a.t, aj, s);
+                        }
+                        sin = acc ? ext_apply(a.t, acc, s) : s;
+                        break;
+                    }
+                    uint32_t g = 0;
+                    for (int j = 0; j < 32; ++j) {
+                        uint32_t aj = __shfl_sync(ALP_FULL_MASK, val, j);
+                        g = ext_comp(a.t, g, aj);
+                    }
+                    acc = ext_comp(a.t, g, acc);
+                    end -= 32;
+                }
+                if (lane == 0) st_volatile32(&a.stA[tile], (ST_P << 30) | ext_apply(a.t, F, sin));
+            }
+            if (lane == 0) s_sin = sin;
+        }
+        __syncthreads();
+        const uint32_t fexc = ext_comp(a.t, s_wexc[warp], excl);
+        const uint32_t s0 = ext_apply(a.t, fexc, s_sin);
+
+        // ---- phase B: one DFA pass, recording ends / starts / finals -------
+        uint32_t cnt = 0, lastp = ALP_NONE32, emit = 0, stt = 0, fin = 0, acc_bits = 0;
+        uint32_t tk[ITEMS], ftk[ITEMS];
+        {
+            uint32_t s = s0;
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+                tk[j] = 0;
+                ftk[j] = 0;
+                if (head & (1u << j)) { s = INIT; stt |= 1u << j; lastp = (uint32_t)(my + j); }
+                uint32_t e = s_cd[s * C1 + c[j]];
+                uint32_t s2 = e & 0x7fffu;
+                if (e & 0x8000u) {
+                    const uint32_t ti = s_tok[s];
+                    if (!(ti & TOK_IGNORE)) { ++cnt; emit |= 1u << j; tk[j] = ti & TOK_TERM_MASK; }
+                    if (!(s_tok[s2] & TOK_IGNORE)) { lastp = (uint32_t)(my + j); stt |= 1u << j; }
+                }
+                s = s2;
+                if (last & (1u << j)) {
+                    const uint32_t ti = s_tok[s];
+                    if (!(ti & TOK_IGNORE)) { ++cnt; fin |= 1u << j; ftk[j] = ti & TOK_TERM_MASK; }
+                    if (ti & TOK_ACCEPT) acc_bits |= 1u << j;
+                }
+            }
+        }
+        uint32_t ic = cnt, ip = lastp;
+        warp_scan_cs(ic, ip, lane);
+        uint32_t ec = __shfl_up_sync(ALP_FULL_MASK, ic, 1), ep = __shfl_up_sync(ALP_FULL_MASK, ip, 1);
+        if (lane == 0) { ec = 0; ep = ALP_NONE32; }
+        if (lane == 31) { s_wc[warp] = ic; s_wp[warp] = ip; }
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t wc = lane < LEX_THREADS / 32 ? s_wc[lane] : 0u;
+            uint32_t wp = lane < LEX_THREADS / 32 ? s_wp[lane] : ALP_NONE32;
+            uint32_t bc = wc, bp = wp;
+            warp_scan_cs(bc, bp, lane);
+            uint32_t xc = __shfl_up_sync(ALP_FULL_MASK, bc, 1), xp = __shfl_up_sync(ALP_FULL_MASK, bp, 1);
+            if (lane == 0) { xc = 0; xp = ALP_NONE32; }
+            if (lane < LEX_THREADS / 32) { s_wc[lane] = xc; s_wp[lane] = xp; }
+            const uint32_t Bc = __shfl_sync(ALP_FULL_MASK, bc, LEX_THREADS / 32 - 1);
+            const uint32_t Bp = __shfl_sync(ALP_FULL_MASK, bp, LEX_THREADS / 32 - 1);
+            uint32_t Xc, Xp;
+            if (tile == 0) {
+                Xc = 0; Xp = 0;
+                if (lane == 0) st_volatile64(&a.stB[0], cs_pack(ST_P, Bc, Bp != ALP_NONE32 ? Bp : 0u));
+            } else {
+                if (lane == 0) st_volatile64(&a.stB[tile], cs_pack(ST_A, Bc, Bp));
+                uint32_t acc_c = 0, acc_p = ALP_NONE32;
+                long long end = tile;
+                while (true) {
+                    long long idx = end - 32 + lane;
+                    unsigned long long w2 = idx >= 0 ? wait64(&a.stB[idx], &a.res->error) : cs_pack(ST_P, 0, 0);
+                    uint32_t flag = (uint32_t)(w2 >> 62);
+                    uint32_t pm = __ballot_sync(ALP_FULL_MASK, flag == ST_P);
+                    int p = pm ? 31 - __clz(pm) : -1;
+                    uint32_t vc = lane >= p ? cs_count(w2) : 0u;
+                    uint32_t vp = lane >= p ? cs_pos(w2) : ALP_NONE32;
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        uint32_t oc = __shfl_down_sync(ALP_FULL_MASK, vc, d);
+                        uint32_t op = __shfl_down_sync(ALP_FULL_MASK, vp, d);
+                        if (lane + d < 32) {
+                            vc += oc;
+                            if (op != ALP_NONE32) vp = op;
+                        }
+                    }
+                    vc = __shfl_sync(ALP_FULL_MASK, vc, 0);
+                    vp = __shfl_sync(ALP_FULL_MASK, vp, 0);
+                    acc_c += vc;
+                    if (acc_p == ALP_NONE32) acc_p = vp;
+                    if (pm) break;
+                    end -= 32;
+                }
+                Xc = acc_c; Xp = acc_p;
+                if (lane == 0) st_volatile64(&a.stB[tile], cs_pack(ST_P, Xc + Bc, Bp != ALP_NONE32 ? Bp : Xp));
+            }
+            if (lane == 0) { s_xc = Xc; s_xp = Xp; }
+        }
+        __syncthreads();
+
+        // ---- emit -----------------------------------------------------------
+        const uint32_t wxc = s_wc[warp], wxp = s_wp[warp];
+        uint32_t tcount = s_xc + wxc + ec;
+        uint32_t cur = ep != ALP_NONE32 ? ep : (wxp != ALP_NONE32 ? wxp : s_xp);
+        TermT* o_term = reinterpret_cast<TermT*>(a.out_term);
+        PosT* o_start = reinterpret_cast<PosT*>(a.out_start);
+        PosT* o_end = reinterpret_cast<PosT*>(a.out_end);
+        long long doc = mydoc;
+        long long base = my < n ? sg.doc_off[doc] : 0;
+        const long long sent = sg.sentinels ? 1 : 0;
+        auto put = [&](long long idx, uint32_t term, long long st, long long en) {
+            if (idx < a.cap) {
+                o_term[idx] = (TermT)term;
+                o_start[idx] = (PosT)st;
+                o_end[idx] = (PosT)en;
+            } else {
+                atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
+            }
+        };
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const long long pos = my + j;
+            if (head & (1u << j)) {
+                // every document starting here (empty ones first, then the real one)
+                doc = doc_upper(sg.doc_off, d0, d1, pos);
+                const long long dl = doc_lower(sg.doc_off, 0, doc, pos);  // empty documents here too
+                base = pos;
+                for (long long e = dl; e <= doc; ++e) {
+                    sg.tok_off[e] = tcount;
+                    if (sent) put((long long)tcount + 2 * e, sg.sent_l, 0, 0);
+                    if (e < doc) {
+                        sg.valid[e] = 0;
+                        if (sent) put((long long)tcount + 2 * e + 1, sg.sent_r, 0, 0);
+                    }
+                }
+                cur = (uint32_t)pos;
+            }
+            if (emit & (1u << j)) {
+                put((long long)tcount + sent * (2 * doc + 1), tk[j], (long long)cur - base, pos - base);
+                ++tcount;
+            }
+            if (stt & (1u << j)) cur = (uint32_t)pos;
+            if (fin & (1u << j)) {
+                put((long long)tcount + sent * (2 * doc + 1), ftk[j], (long long)cur - base, pos + 1 - base);
+                ++tcount;
+            }
+            if (last & (1u << j)) {
+                sg.valid[doc] = (acc_bits & (1u << j)) ? 1 : 0;
+                if (sent) put((long long)tcount + 2 * doc + 1, sg.sent_r, 0, 0);
+            }
+        }
+        if (my <= n - 1 && n - 1 < my + ITEMS) {
+            // documents that start at n (empty, at the end) and the closing offset
+            for (long long e = doc + 1; e < ND; ++e) {
+                sg.tok_off[e] = tcount;
+                sg.valid[e] = 0;
+                if (sent) {
+                    put((long long)tcount + 2 * e, sg.sent_l, 0, 0);
+                    put((long long)tcount + 2 * e + 1, sg.sent_r, 0, 0);
+                }
+            }
+            sg.tok_off[ND] = tcount;
+            a.res->count = tcount;
+            a.res->valid = 1;
+        }
+        __syncthreads();
     }
 }
 

@@ -41,6 +41,9 @@ struct ParseTables {
     const uint32_t* pseq;       // production ids
     const int32_t* arity;       // [n_prods]
     const int32_t* prod_term;   // [n_prods] terminal id or -1
+    const int16_t* pseq_v;      // [n_pseq] sum of (arity-1) over the pair's earlier productions
+    const int16_t* pseq_t;      // [n_pseq] terminal productions among the pair's earlier productions
+    const int16_t* stack_d;     // [n_stack] depth change before this bracket within its pair
     int q, k, T, n_pairs, n_prods;
     uint32_t empty, start, end;
 };
@@ -133,6 +136,20 @@ inline int load_parser(ParseTables& pt, ParseHost& ph, const uint8_t* p, const u
         if ((int)pi.n_prod > maxp) maxp = pi.n_prod;
         if ((int)pi.n_br > maxb) maxb = pi.n_br;
     }
+    std::vector<int16_t> pv(n_pseq, 0), ptm(n_pseq, 0), sd(n_stack, 0);
+    for (uint32_t i = 0; i < n_pairs; ++i) {
+        int acc_v = 0, acc_t = 0, acc_d = 0;
+        for (uint32_t j = raw[4 * i + 2]; j < raw[4 * i + 3]; ++j) {
+            pv[j] = (int16_t)acc_v;
+            ptm[j] = (int16_t)acc_t;
+            acc_v += arity[pseq[j]] - 1;
+            acc_t += pterm[pseq[j]] >= 0 ? 1 : 0;
+        }
+        for (uint32_t j = raw[4 * i]; j < raw[4 * i + 1]; ++j) {
+            sd[j] = (int16_t)acc_d;
+            acc_d += (stack[j] >> 31) ? 1 : -1;
+        }
+    }
     auto up = [&](const void* h, size_t bytes, const void** d) -> bool {
         void* x = nullptr;
         if (cudaMalloc(&x, bytes < 16 ? 16 : bytes) != cudaSuccess) return false;
@@ -146,7 +163,10 @@ inline int load_parser(ParseTables& pt, ParseHost& ph, const uint8_t* p, const u
               up(stack.data(), stack.size() * 4, (const void**)&pt.stack) &&
               up(pseq.data(), pseq.size() * 4, (const void**)&pt.pseq) &&
               up(arity.data(), arity.size() * 4, (const void**)&pt.arity) &&
-              up(pterm.data(), pterm.size() * 4, (const void**)&pt.prod_term);
+              up(pterm.data(), pterm.size() * 4, (const void**)&pt.prod_term) &&
+              up(pv.data(), pv.size() * 2, (const void**)&pt.pseq_v) &&
+              up(ptm.data(), ptm.size() * 2, (const void**)&pt.pseq_t) &&
+              up(sd.data(), sd.size() * 2, (const void**)&pt.stack_d);
     if (!ok) { err = "cudaMalloc/cudaMemcpy failed for parser tables"; return 2; }
     pt.q = (int)q; pt.k = (int)k; pt.T = (int)T; pt.n_pairs = (int)n_pairs; pt.n_prods = (int)n_prods;
     pt.empty = empty; pt.start = start; pt.end = end;
@@ -167,92 +187,147 @@ constexpr int PLE_ITEMS = 16;
 constexpr int PLE_TILE = PLE_THREADS * PLE_ITEMS;  // elements per tile
 constexpr uint16_t NO_PAIR = 0xffff;
 
-// Per-tile sums of the per-position counts (and, after the scan, the
-// exclusive prefixes).  Field order is the scan order.
+// Running sums over positions.  Positions are the documents' ⊢ tokens ⊣
+// sequences back to back; nodes, brackets and heads (⊢ count) run over all
+// documents, depth / v / terminals restart at every ⊢ (a segmented scan).
 struct __align__(16) PosSums {
     unsigned long long nodes;   // productions
     unsigned long long brs;     // brackets
-    long long depth;            // lefts - rights
-    long long v;                // sum of (arity - 1)
-    unsigned long long terms;   // terminal productions
-    unsigned long long pad[3];
+    long long depth;            // lefts - rights since the last ⊢
+    long long v;                // sum of (arity - 1) since the last ⊢
+    unsigned long long terms;   // terminal productions since the last ⊢
+    unsigned long long heads;   // ⊢ positions
+    long long hpos;             // position of the last ⊢ (-1: none)
+    unsigned long long pad;
 };
 
 __device__ __forceinline__ void possums_zero(PosSums& s) {
-    s.nodes = 0; s.brs = 0; s.depth = 0; s.v = 0; s.terms = 0;
+    s.nodes = 0; s.brs = 0; s.depth = 0; s.v = 0; s.terms = 0; s.heads = 0; s.hpos = -1; s.pad = 0;
+}
+__device__ __forceinline__ PosSums ps_combine(const PosSums& a, const PosSums& b) {
+    PosSums r;
+    r.nodes = a.nodes + b.nodes;
+    r.brs = a.brs + b.brs;
+    r.heads = a.heads + b.heads;
+    if (b.heads) { r.depth = b.depth; r.v = b.v; r.terms = b.terms; r.hpos = b.hpos; }
+    else { r.depth = a.depth + b.depth; r.v = a.v + b.v; r.terms = a.terms + b.terms; r.hpos = a.hpos; }
+    r.pad = 0;
+    return r;
+}
+__device__ __forceinline__ PosSums ps_shfl_up(const PosSums& x, int d) {
+    PosSums r;
+    r.nodes = __shfl_up_sync(ALP_FULL_MASK, x.nodes, d);
+    r.brs = __shfl_up_sync(ALP_FULL_MASK, x.brs, d);
+    r.depth = __shfl_up_sync(ALP_FULL_MASK, x.depth, d);
+    r.v = __shfl_up_sync(ALP_FULL_MASK, x.v, d);
+    r.terms = __shfl_up_sync(ALP_FULL_MASK, x.terms, d);
+    r.heads = __shfl_up_sync(ALP_FULL_MASK, x.heads, d);
+    r.hpos = __shfl_up_sync(ALP_FULL_MASK, x.hpos, d);
+    r.pad = 0;
+    return r;
+}
+// inclusive warp scan (lanes in order)
+__device__ __forceinline__ PosSums ps_warp_scan(PosSums x, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        PosSums o = ps_shfl_up(x, d);
+        if (lane >= d) x = ps_combine(o, x);
+    }
+    return x;
+}
+__device__ __forceinline__ PosSums ps_elem(const PairInfo* s_pi, uint16_t p, bool head, long long i) {
+    PosSums e;
+    possums_zero(e);
+    if (p != NO_PAIR) {
+        const PairInfo& pi = s_pi[p];
+        e.nodes = pi.n_prod; e.brs = pi.n_br; e.depth = pi.d_depth; e.v = pi.d_v; e.terms = pi.n_term;
+    }
+    if (head) { e.heads = 1; e.hpos = i; }
+    return e;
 }
 
 struct ParseArgs {
     ParseTables t;
-    const uint16_t* tterm;      // [m] token terminal ids
-    const uint32_t* tstart;     // [m]
-    const uint32_t* tend;       // [m]
-    long long m;                // tokens
-    long long L;                // positions = m + 2
+    const uint16_t* P;          // [L] ⊢ tokens ⊣ per document: terminal ids
+    const uint32_t* pstart;     // [L] token spans (document-relative), same layout
+    const uint32_t* pend;
+    long long L;                // positions
+    long long n_docs;
     uint16_t* pid;              // [L] pair id per position
     PosSums* tile_sums;         // [tiles] K1 output, scanned in place to exclusive prefixes
-    AlpResult* res;             // valid flag, error bits; aux[0..4] totals
+    AlpResult* res;             // aux[0..5] totals
     // K2 outputs
-    int subst_terminals;
     uint32_t* tag;
     uint8_t* kind;
     int64_t* nstart;
     int64_t* nend;
-    int32_t* vbuf;              // node values exscan(arity-1)
+    int32_t* vbuf;              // node values exscan(arity-1), per document
     uint32_t* brbuf;            // bracket symbol | left<<31
-    int32_t* dsbuf;             // bracket depth value (before a left, after a right)
+    int32_t* dsbuf;             // bracket depth value (before a left, after a right), per document
+    long long* node_off;        // [n_docs + 1] first node of each document
+    long long* br_off;          // [n_docs + 1] first bracket of each document
+    uint8_t* doc_valid;         // [n_docs] cleared on rejection
+    int subst_terminals;        // 1: wrapper productions become terminal nodes (parse_int); 0: production ids
     long long cap_nodes;
     long long cap_brs;
 };
 
-// Terminal symbol at padded position i of ⊢ tokens ⊣ (empty outside).
 __device__ __forceinline__ uint32_t pos_term(const ParseArgs& a, long long i) {
-    if (i < 0 || i >= a.L) return a.t.empty;
-    if (i == 0) return a.t.start;
-    if (i == a.L - 1) return a.t.end;
-    return a.tterm[i - 1];
+    return (i < 0 || i >= a.L) ? a.t.empty : (uint32_t)a.P[i];
 }
 
 // ---------------------------------------------------------------------------
-// K1: pair ids and per-tile sums
+// K1: pair ids and per-tile (segmented) sums
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     PairInfo* s_pi = reinterpret_cast<PairInfo*>(smem);
     uint32_t* s_term = reinterpret_cast<uint32_t*>(smem + sizeof(PairInfo) * a.t.n_pairs);
     __shared__ PosSums s_w[PP_THREADS / 32];
+    __shared__ uint32_t s_pow[17];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int q = a.t.q, k = a.t.k, W = q + k, T = a.t.T;
+    const int q = a.t.q, k = a.t.k, W = q + k;
     for (int i = tid; i < a.t.n_pairs * (int)(sizeof(PairInfo) / 4); i += PP_THREADS)
         reinterpret_cast<uint32_t*>(s_pi)[i] = reinterpret_cast<const uint32_t*>(a.t.pairs)[i];
+    if (tid == 0) {
+        uint32_t pw = 1;
+        for (int j = 0; j < W; ++j) { s_pow[W - 1 - j] = pw; pw *= (uint32_t)a.t.T; }
+    }
     const long long base = (long long)blockIdx.x * PP_TILE;
     const int span = PP_TILE + W;  // window [base - q, base + PP_TILE + k)
     for (int i = tid; i < span; i += PP_THREADS) s_term[i] = pos_term(a, base - q + i);
     __syncthreads();
+    const uint32_t SL = a.t.start, SR = a.t.end, EMPTY = a.t.empty;
     PosSums acc;
     possums_zero(acc);
-    bool bad = false;
     uint16_t ids[PP_ITEMS];
 #pragma unroll
     for (int j = 0; j < PP_ITEMS; ++j) {
         const long long i = base + tid * PP_ITEMS + j;
         uint16_t p = NO_PAIR;
+        bool head = false;
         if (i < a.L) {
-            long long x = 0;
             const int o = tid * PP_ITEMS + j;  // s_term[o + jj] is position i - q + jj
-            for (int jj = 0; jj < W; ++jj) x = x * T + s_term[o + jj];
-            p = __ldg(&a.t.key_index[x]);
-            if (p == NO_PAIR) bad = true;
-            else {
-                const PairInfo& pi = s_pi[p];
-                acc.nodes += pi.n_prod;
-                acc.brs += pi.n_br;
-                acc.depth += pi.d_depth;
-                acc.v += pi.d_v;
-                acc.terms += pi.n_term;
+            const uint32_t c = s_term[o + q];
+            head = c == SL;
+            // a window never reaches past its document's ⊢ (left) or ⊣ (right)
+            uint32_t x = c * s_pow[q];
+            bool ok = c != SL;
+            for (int jj = q - 1; jj >= 0; --jj) {
+                const uint32_t t = s_term[o + jj];
+                x += (ok ? t : EMPTY) * s_pow[jj];
+                ok = ok && t != SL;
             }
+            ok = c != SR;
+            for (int jj = q + 1; jj < W; ++jj) {
+                const uint32_t t = s_term[o + jj];
+                x += (ok ? t : EMPTY) * s_pow[jj];
+                ok = ok && t != SR;
+            }
+            p = __ldg(&a.t.key_index[x]);
         }
         ids[j] = p;
+        if (i < a.L) acc = ps_combine(acc, ps_elem(s_pi, p, head, i));
     }
     const long long i0 = base + tid * PP_ITEMS;
     if (i0 + PP_ITEMS <= a.L && ((i0 & 7) == 0)) {
@@ -266,31 +341,23 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
         for (int j = 0; j < PP_ITEMS; ++j)
             if (i0 + j < a.L) a.pid[i0 + j] = ids[j];
     }
-    if (__any_sync(ALP_FULL_MASK, bad) && lane == 0) a.res->valid = 0;
-    // block reduce
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) {
-        acc.nodes += __shfl_down_sync(ALP_FULL_MASK, acc.nodes, d);
-        acc.brs += __shfl_down_sync(ALP_FULL_MASK, acc.brs, d);
-        acc.depth += __shfl_down_sync(ALP_FULL_MASK, acc.depth, d);
-        acc.v += __shfl_down_sync(ALP_FULL_MASK, acc.v, d);
-        acc.terms += __shfl_down_sync(ALP_FULL_MASK, acc.terms, d);
-    }
-    if (lane == 0) s_w[warp] = acc;
+    // ordered block reduce
+    PosSums inc = ps_warp_scan(acc, lane);
+    if (lane == 31) s_w[warp] = inc;
     __syncthreads();
     if (tid == 0) {
-        PosSums t;
-        possums_zero(t);
-        for (int w = 0; w < PP_THREADS / 32; ++w) {
-            t.nodes += s_w[w].nodes; t.brs += s_w[w].brs; t.depth += s_w[w].depth;
-            t.v += s_w[w].v; t.terms += s_w[w].terms;
-        }
+        PosSums t = s_w[0];
+        for (int w = 1; w < PP_THREADS / 32; ++w) t = ps_combine(t, s_w[w]);
         a.tile_sums[blockIdx.x] = t;
     }
 }
 
-// Exclusive scan of the tile sums in place (one block); totals to res->aux.
-__global__ void __launch_bounds__(1024) scan_tiles_kernel(PosSums* s, long long tiles, AlpResult* res) {
+// Exclusive segmented scan of the tile sums in place (one block); totals to
+// res->aux (nodes, brackets, final depth, -, -, heads) and the closing entries
+// of node_off / br_off.
+__global__ void __launch_bounds__(1024) scan_tiles_kernel(PosSums* s, long long tiles, AlpResult* res,
+                                                          long long* node_off, long long* br_off,
+                                                          long long n_docs) {
     __shared__ PosSums s_w[32];
     __shared__ PosSums s_carry;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -299,58 +366,23 @@ __global__ void __launch_bounds__(1024) scan_tiles_kernel(PosSums* s, long long 
     for (long long b = 0; b < tiles; b += 1024) {
         PosSums v;
         if (b + tid < tiles) v = s[b + tid]; else possums_zero(v);
-        PosSums inc = v;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            unsigned long long n1 = __shfl_up_sync(ALP_FULL_MASK, inc.nodes, d);
-            unsigned long long n2 = __shfl_up_sync(ALP_FULL_MASK, inc.brs, d);
-            long long n3 = __shfl_up_sync(ALP_FULL_MASK, inc.depth, d);
-            long long n4 = __shfl_up_sync(ALP_FULL_MASK, inc.v, d);
-            unsigned long long n5 = __shfl_up_sync(ALP_FULL_MASK, inc.terms, d);
-            if (lane >= d) { inc.nodes += n1; inc.brs += n2; inc.depth += n3; inc.v += n4; inc.terms += n5; }
-        }
+        PosSums inc = ps_warp_scan(v, lane);
+        PosSums ex = ps_shfl_up(inc, 1);
+        if (lane == 0) possums_zero(ex);
         if (lane == 31) s_w[warp] = inc;
         __syncthreads();
         if (warp == 0) {
             PosSums w = s_w[lane];
-            PosSums wi = w;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                unsigned long long n1 = __shfl_up_sync(ALP_FULL_MASK, wi.nodes, d);
-                unsigned long long n2 = __shfl_up_sync(ALP_FULL_MASK, wi.brs, d);
-                long long n3 = __shfl_up_sync(ALP_FULL_MASK, wi.depth, d);
-                long long n4 = __shfl_up_sync(ALP_FULL_MASK, wi.v, d);
-                unsigned long long n5 = __shfl_up_sync(ALP_FULL_MASK, wi.terms, d);
-                if (lane >= d) { wi.nodes += n1; wi.brs += n2; wi.depth += n3; wi.v += n4; wi.terms += n5; }
-            }
-            // exclusive warp prefix
-            PosSums we;
-            we.nodes = wi.nodes - w.nodes; we.brs = wi.brs - w.brs; we.depth = wi.depth - w.depth;
-            we.v = wi.v - w.v; we.terms = wi.terms - w.terms;
+            PosSums wi = ps_warp_scan(w, lane);
+            PosSums we = ps_shfl_up(wi, 1);
+            if (lane == 0) possums_zero(we);
             s_w[lane] = we;
         }
         __syncthreads();
-        PosSums c = s_carry, wp = s_w[warp];
-        if (b + tid < tiles) {
-            PosSums o;
-            o.nodes = c.nodes + wp.nodes + inc.nodes - v.nodes;
-            o.brs = c.brs + wp.brs + inc.brs - v.brs;
-            o.depth = c.depth + wp.depth + inc.depth - v.depth;
-            o.v = c.v + wp.v + inc.v - v.v;
-            o.terms = c.terms + wp.terms + inc.terms - v.terms;
-            o.pad[0] = o.pad[1] = o.pad[2] = 0;
-            s[b + tid] = o;
-        }
+        const PosSums pre = ps_combine(s_carry, s_w[warp]);
+        if (b + tid < tiles) s[b + tid] = ps_combine(pre, ex);
         __syncthreads();
-        if (tid == 1023) {
-            PosSums nc;
-            nc.nodes = c.nodes + wp.nodes + inc.nodes;
-            nc.brs = c.brs + wp.brs + inc.brs;
-            nc.depth = c.depth + wp.depth + inc.depth;
-            nc.v = c.v + wp.v + inc.v;
-            nc.terms = c.terms + wp.terms + inc.terms;
-            s_carry = nc;
-        }
+        if (tid == 1023) s_carry = ps_combine(pre, inc);
         __syncthreads();
     }
     if (tid == 0) {
@@ -359,109 +391,178 @@ __global__ void __launch_bounds__(1024) scan_tiles_kernel(PosSums* s, long long 
         res->aux[2] = s_carry.depth;
         res->aux[3] = s_carry.v;
         res->aux[4] = (long long)s_carry.terms;
+        res->aux[5] = (long long)s_carry.heads;
+        node_off[n_docs] = (long long)s_carry.nodes;
+        br_off[n_docs] = (long long)s_carry.brs;
     }
 }
 
 // ---------------------------------------------------------------------------
 // K2: expand every position's productions and brackets
+//
+// One tile = PP_TILE positions.  The block scans the per-position sums into
+// shared memory, then hands out output elements (nodes, then brackets)
+// round-robin over threads: element e of the tile finds its position by binary
+// search over the scanned offsets, so consecutive threads write consecutive
+// nodes and every output store is coalesced.
 // ---------------------------------------------------------------------------
+constexpr size_t EXPAND_SMEM_POS = (size_t)PP_TILE * (4 * 7 + 2) + 16;
+
+__host__ __device__ inline size_t expand_smem_bytes(int n_pairs, int n_prods) {
+    return ((sizeof(PairInfo) * n_pairs + (size_t)n_prods * 8 + 15) & ~(size_t)15) + EXPAND_SMEM_POS;
+}
+
+// largest p in [0, n) with off[p] <= e  (off ascending, off[0] = 0)
+__device__ __forceinline__ int find_pos(const uint32_t* off, int n, uint32_t e) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= e) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 __global__ void __launch_bounds__(PP_THREADS) parse_expand_kernel(ParseArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     PairInfo* s_pi = reinterpret_cast<PairInfo*>(smem);
     int32_t* s_ar = reinterpret_cast<int32_t*>(smem + sizeof(PairInfo) * a.t.n_pairs);
     int32_t* s_pt = s_ar + a.t.n_prods;
+    uint8_t* pbase = smem + ((sizeof(PairInfo) * a.t.n_pairs + (size_t)a.t.n_prods * 8 + 15) & ~(size_t)15);
+    uint32_t* s_noff = reinterpret_cast<uint32_t*>(pbase);            // node offset in tile
+    uint32_t* s_boff = s_noff + PP_TILE;                              // bracket offset in tile
+    int32_t* s_dep = reinterpret_cast<int32_t*>(s_boff + PP_TILE);    // depth before position
+    int32_t* s_v = s_dep + PP_TILE;                                   // v before position
+    uint32_t* s_tr = reinterpret_cast<uint32_t*>(s_v + PP_TILE);      // terminal rank before position
+    uint32_t* s_hp = s_tr + PP_TILE;                                  // ⊢ position of its document
+    uint32_t* s_doc = s_hp + PP_TILE;                                 // document index
+    uint16_t* s_pid = reinterpret_cast<uint16_t*>(s_doc + PP_TILE);
     __shared__ PosSums s_w[PP_THREADS / 32];
+    __shared__ uint32_t s_tn, s_tb;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < a.t.n_pairs * (int)(sizeof(PairInfo) / 4); i += PP_THREADS)
         reinterpret_cast<uint32_t*>(s_pi)[i] = reinterpret_cast<const uint32_t*>(a.t.pairs)[i];
     for (int i = tid; i < a.t.n_prods; i += PP_THREADS) { s_ar[i] = a.t.arity[i]; s_pt[i] = a.t.prod_term[i]; }
     __syncthreads();
-    const long long i0 = (long long)blockIdx.x * PP_TILE + tid * PP_ITEMS;
+    const uint32_t SL = a.t.start, SR = a.t.end;
+    const long long tbase = (long long)blockIdx.x * PP_TILE;
+    const long long i0 = tbase + tid * PP_ITEMS;
     uint16_t ids[PP_ITEMS];
+    uint32_t hm = 0, em = 0;  // head / end bits of this thread's positions
 #pragma unroll
-    for (int j = 0; j < PP_ITEMS; ++j) ids[j] = (i0 + j < a.L) ? a.pid[i0 + j] : NO_PAIR;
+    for (int j = 0; j < PP_ITEMS; ++j) {
+        ids[j] = NO_PAIR;
+        if (i0 + j < a.L) {
+            ids[j] = a.pid[i0 + j];
+            const uint32_t c = a.P[i0 + j];
+            if (c == SL) hm |= 1u << j;
+            if (c == SR) em |= 1u << j;
+        }
+    }
     PosSums mine;
     possums_zero(mine);
 #pragma unroll
-    for (int j = 0; j < PP_ITEMS; ++j) {
-        if (ids[j] == NO_PAIR) continue;
-        const PairInfo& pi = s_pi[ids[j]];
-        mine.nodes += pi.n_prod; mine.brs += pi.n_br; mine.depth += pi.d_depth; mine.v += pi.d_v;
-        mine.terms += pi.n_term;
-    }
-    PosSums inc = mine;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        unsigned long long n1 = __shfl_up_sync(ALP_FULL_MASK, inc.nodes, d);
-        unsigned long long n2 = __shfl_up_sync(ALP_FULL_MASK, inc.brs, d);
-        long long n3 = __shfl_up_sync(ALP_FULL_MASK, inc.depth, d);
-        long long n4 = __shfl_up_sync(ALP_FULL_MASK, inc.v, d);
-        unsigned long long n5 = __shfl_up_sync(ALP_FULL_MASK, inc.terms, d);
-        if (lane >= d) { inc.nodes += n1; inc.brs += n2; inc.depth += n3; inc.v += n4; inc.terms += n5; }
-    }
+    for (int j = 0; j < PP_ITEMS; ++j)
+        if (i0 + j < a.L) mine = ps_combine(mine, ps_elem(s_pi, ids[j], (hm >> j) & 1u, i0 + j));
+    PosSums inc = ps_warp_scan(mine, lane);
+    PosSums ex = ps_shfl_up(inc, 1);
+    if (lane == 0) possums_zero(ex);
     if (lane == 31) s_w[warp] = inc;
     __syncthreads();
     if (warp == 0) {
-        PosSums w = lane < PP_THREADS / 32 ? s_w[lane] : PosSums{};
-        if (lane >= PP_THREADS / 32) possums_zero(w);
-        PosSums wi = w;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            unsigned long long n1 = __shfl_up_sync(ALP_FULL_MASK, wi.nodes, d);
-            unsigned long long n2 = __shfl_up_sync(ALP_FULL_MASK, wi.brs, d);
-            long long n3 = __shfl_up_sync(ALP_FULL_MASK, wi.depth, d);
-            long long n4 = __shfl_up_sync(ALP_FULL_MASK, wi.v, d);
-            unsigned long long n5 = __shfl_up_sync(ALP_FULL_MASK, wi.terms, d);
-            if (lane >= d) { wi.nodes += n1; wi.brs += n2; wi.depth += n3; wi.v += n4; wi.terms += n5; }
-        }
-        if (lane < PP_THREADS / 32) {
-            PosSums we;
-            we.nodes = wi.nodes - w.nodes; we.brs = wi.brs - w.brs; we.depth = wi.depth - w.depth;
-            we.v = wi.v - w.v; we.terms = wi.terms - w.terms;
-            s_w[lane] = we;
-        }
+        PosSums w;
+        if (lane < PP_THREADS / 32) w = s_w[lane]; else possums_zero(w);
+        PosSums wi = ps_warp_scan(w, lane);
+        PosSums we = ps_shfl_up(wi, 1);
+        if (lane == 0) possums_zero(we);
+        if (lane < PP_THREADS / 32) s_w[lane] = we;
+        if (lane == PP_THREADS / 32 - 1) { s_tn = (uint32_t)wi.nodes; s_tb = (uint32_t)wi.brs; }
     }
     __syncthreads();
     const PosSums tp = a.tile_sums[blockIdx.x];
-    const PosSums wp = s_w[warp];
-    unsigned long long nd = tp.nodes + wp.nodes + inc.nodes - mine.nodes;
-    unsigned long long bi = tp.brs + wp.brs + inc.brs - mine.brs;
-    long long depth = tp.depth + wp.depth + inc.depth - mine.depth;
-    long long v = tp.v + wp.v + inc.v - mine.v;
-    unsigned long long tr = tp.terms + wp.terms + inc.terms - mine.terms;
-    bool neg = false;
-    for (int j = 0; j < PP_ITEMS; ++j) {
-        if (ids[j] == NO_PAIR) continue;
-        const PairInfo pi = s_pi[ids[j]];
-        for (int t = 0; t < pi.n_br; ++t, ++bi) {
-            const uint32_t sym = __ldg(&a.t.stack[pi.stack_begin + t]);
-            int32_t ds;
-            if (sym >> 31) { ds = (int32_t)depth; ++depth; }
-            else { --depth; ds = (int32_t)depth; if (depth < 0) neg = true; }
-            if ((long long)bi < a.cap_brs) { a.brbuf[bi] = sym; a.dsbuf[bi] = ds; }
-        }
-        for (int t = 0; t < pi.n_prod; ++t, ++nd) {
-            const uint32_t p = __ldg(&a.t.pseq[pi.prod_begin + t]);
-            const int32_t pt = s_pt[p];
-            if ((long long)nd < a.cap_nodes) {
-                a.vbuf[nd] = (int32_t)v;
-                if (pt >= 0 && a.subst_terminals && (long long)tr < a.m) {
-                    a.tag[nd] = (uint32_t)pt;
-                    a.kind[nd] = 1;
-                    a.nstart[nd] = (int64_t)a.tstart[tr];
-                    a.nend[nd] = (int64_t)a.tend[tr];
-                } else {
-                    a.tag[nd] = p;
-                    a.kind[nd] = 0;
-                    a.nstart[nd] = 0;
-                    a.nend[nd] = 0;
+    {
+        PosSums run = ps_combine(ps_combine(tp, s_w[warp]), ex);  // before this thread's first position
+        const uint32_t nd0 = (uint32_t)(run.nodes - tp.nodes), bi0 = (uint32_t)(run.brs - tp.brs);
+        uint32_t nd = nd0, bi = bi0;
+#pragma unroll
+        for (int j = 0; j < PP_ITEMS; ++j) {
+            const int o = tid * PP_ITEMS + j;
+            const long long i = i0 + j;
+            const bool head = (hm >> j) & 1u;
+            s_noff[o] = nd;
+            s_boff[o] = bi;
+            s_pid[o] = ids[j];
+            if (i < a.L) {
+                const long long dep = head ? 0 : run.depth;
+                const long long v = head ? 0 : run.v;
+                const unsigned long long tr = head ? 0 : run.terms;
+                const long long hp = head ? i : run.hpos;
+                const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
+                s_dep[o] = (int32_t)dep; s_v[o] = (int32_t)v; s_tr[o] = (uint32_t)tr;
+                s_hp[o] = (uint32_t)hp; s_doc[o] = (uint32_t)doc;
+                if (head && doc >= 0 && doc < a.n_docs) {
+                    a.node_off[doc] = (long long)(tp.nodes + nd);
+                    a.br_off[doc] = (long long)(tp.brs + bi);
                 }
+                int32_t dd = 0;
+                if (ids[j] == NO_PAIR) {
+                    if (doc >= 0 && doc < a.n_docs) a.doc_valid[doc] = 0;  // no admissible pair
+                } else {
+                    const PairInfo& pi = s_pi[ids[j]];
+                    nd += pi.n_prod; bi += pi.n_br; dd = pi.d_depth;
+                }
+                if (((em >> j) & 1u) && (dep + dd != 0) && doc >= 0 && doc < a.n_docs)
+                    a.doc_valid[doc] = 0;  // unbalanced at the end
+                run = ps_combine(run, ps_elem(s_pi, ids[j], head, i));
+            } else {
+                s_dep[o] = 0; s_v[o] = 0; s_tr[o] = 0; s_hp[o] = 0; s_doc[o] = 0;
             }
-            v += s_ar[p] - 1;
-            if (pt >= 0) ++tr;
         }
     }
-    if (__any_sync(ALP_FULL_MASK, neg) && lane == 0) a.res->valid = 0;
+    __syncthreads();
+    const uint32_t tn = s_tn, tb = s_tb;
+    const unsigned long long nbase = tp.nodes, bbase = tp.brs;
+    for (uint32_t e = tid; e < tn; e += PP_THREADS) {
+        const int p = find_pos(s_noff, PP_TILE, e);
+        if (s_pid[p] == NO_PAIR) continue;
+        const PairInfo& pi = s_pi[s_pid[p]];
+        const uint32_t j = pi.prod_begin + (e - s_noff[p]);
+        const uint32_t prod = __ldg(&a.t.pseq[j]);
+        const int32_t pt = s_pt[prod];
+        const unsigned long long nd = nbase + e;
+        if ((long long)nd >= a.cap_nodes) break;
+        a.vbuf[nd] = s_v[p] + __ldg(&a.t.pseq_v[j]);
+        if (pt >= 0 && a.subst_terminals) {
+            // the k-th terminal production of a document takes its k-th token's span
+            const long long ti = (long long)s_hp[p] + 1 + s_tr[p] + (uint32_t)__ldg(&a.t.pseq_t[j]);
+            a.tag[nd] = (uint32_t)pt;
+            a.kind[nd] = 1;
+            a.nstart[nd] = ti < a.L ? (int64_t)__ldg(&a.pstart[ti]) : 0;
+            a.nend[nd] = ti < a.L ? (int64_t)__ldg(&a.pend[ti]) : 0;
+        } else {
+            a.tag[nd] = prod;
+            a.kind[nd] = 0;
+            a.nstart[nd] = 0;
+            a.nend[nd] = 0;
+        }
+    }
+    for (uint32_t e = tid; e < tb; e += PP_THREADS) {
+        const int p = find_pos(s_boff, PP_TILE, e);
+        if (s_pid[p] == NO_PAIR) continue;
+        const PairInfo& pi = s_pi[s_pid[p]];
+        const uint32_t j = pi.stack_begin + (e - s_boff[p]);
+        const uint32_t sym = __ldg(&a.t.stack[j]);
+        const int32_t before = s_dep[p] + __ldg(&a.t.stack_d[j]);
+        int32_t ds;
+        if (sym >> 31) ds = before;
+        else {
+            ds = before - 1;
+            if (ds < 0 && (long long)s_doc[p] < a.n_docs) a.doc_valid[s_doc[p]] = 0;  // depth below zero
+        }
+        const unsigned long long bi = bbase + e;
+        if ((long long)bi >= a.cap_brs) break;
+        a.brbuf[bi] = sym;
+        a.dsbuf[bi] = ds;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -471,7 +572,10 @@ struct PleArgs {
     const int32_t* val;          // [n] values
     long long n;
     const uint32_t* sym;         // brackets: symbol|left<<31 (queries only at rights); nodes: null
-    long long* out_parent;       // nodes: answer index per element (root 0)
+    long long* out_parent;       // nodes: parent index relative to its document (root 0)
+    const long long* seg_off;    // [n_seg + 1] first element of each document
+    long long n_seg;
+    uint8_t* seg_valid;          // brackets: cleared for a document with a mismatch
     int32_t* tile_min;           // [tiles]
     int32_t* stair_val;          // [tiles * PLE_TILE]
     uint32_t* stair_idx;         // [tiles * PLE_TILE] global index
@@ -482,15 +586,31 @@ struct PleArgs {
     AlpResult* res;
 };
 
-// Escapee record: element index in the high 32 bits, its value in the low 32.
-constexpr size_t PLE_SMEM = (2 * PLE_TILE + PLE_TILE) * 4;  // min tree + symbols
+// Shared memory: a min tree over the tile (leaves at PLE_TILE..2*PLE_TILE-1)
+// and, for brackets, the symbols.
+constexpr size_t PLE_SMEM = (size_t)(2 * PLE_TILE + PLE_TILE) * 4;
 
+// largest d in [lo, hi] with off[d] <= g
+__device__ __forceinline__ long long seg_upper(const long long* off, long long lo, long long hi, long long g) {
+    while (lo < hi) {
+        const long long mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Each thread owns PLE_ITEMS consecutive elements.  It answers them against
+// its own earlier elements in registers first; the rest walk a shared-memory
+// min tree of the tile (up to the nearest left subtree holding a value <= x,
+// then down to its last such leaf).  Elements smaller than everything before
+// them in the tile escape to ple_escape_kernel.
 __global__ void __launch_bounds__(PLE_THREADS) ple_tile_kernel(PleArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     int32_t* tree = reinterpret_cast<int32_t*>(smem);
     uint32_t* s_sym = reinterpret_cast<uint32_t*>(smem + 2 * PLE_TILE * 4);
     __shared__ int32_t s_suf[PLE_THREADS];
     __shared__ uint32_t s_cnt[PLE_THREADS / 32];
+    __shared__ long long s_sd0, s_sd1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long long base = (long long)blockIdx.x * PLE_TILE;
     const bool brackets = a.sym != nullptr;
@@ -498,6 +618,10 @@ __global__ void __launch_bounds__(PLE_THREADS) ple_tile_kernel(PleArgs a) {
         const long long g = base + j;
         tree[PLE_TILE + j] = g < a.n ? a.val[g] : INT32_MAX;
         if (brackets) s_sym[j] = g < a.n ? a.sym[g] : 0u;
+    }
+    if (tid == 0) {
+        s_sd0 = seg_upper(a.seg_off, 0, a.n_seg - 1, base);
+        s_sd1 = seg_upper(a.seg_off, 0, a.n_seg - 1, min(base + PLE_TILE, a.n) - 1);
     }
     __syncthreads();
     for (int width = PLE_TILE / 2; width >= 1; width >>= 1) {
@@ -507,70 +631,90 @@ __global__ void __launch_bounds__(PLE_THREADS) ple_tile_kernel(PleArgs a) {
         }
         __syncthreads();
     }
-    // local answers
-    bool mismatch = false;
-    for (int jj = 0; jj < PLE_ITEMS; ++jj) {
-        const int j = tid * PLE_ITEMS + jj;
-        const long long g = base + j;
-        if (g >= a.n) break;
-        if (brackets && (s_sym[j] >> 31)) continue;  // lefts ask nothing
-        const int32_t v = tree[PLE_TILE + j];
-        int node = PLE_TILE + j;
-        bool found = false;
-        while (node > 1) {
-            if ((node & 1) && tree[node - 1] <= v) { node = node - 1; found = true; break; }
-            node >>= 1;
+    int32_t v[PLE_ITEMS];
+#pragma unroll
+    for (int i = 0; i < PLE_ITEMS; ++i) v[i] = tree[PLE_TILE + tid * PLE_ITEMS + i];
+
+    const long long gfirst = base + tid * PLE_ITEMS;
+    long long doc = gfirst < a.n ? seg_upper(a.seg_off, s_sd0, s_sd1, gfirst) : 0;
+    long long dbase = gfirst < a.n ? a.seg_off[doc] : 0;
+    long long dnext = gfirst < a.n ? a.seg_off[doc + 1] : 0;
+#pragma unroll
+    for (int j = 0; j < PLE_ITEMS; ++j) {
+        const int lj = tid * PLE_ITEMS + j;
+        const long long g = base + lj;
+        if (g >= a.n) continue;
+        while (g >= dnext && doc + 1 < a.n_seg) {
+            ++doc;
+            dbase = a.seg_off[doc];
+            dnext = a.seg_off[doc + 1];
         }
-        if (found) {
-            while (node < PLE_TILE) node = (tree[2 * node + 1] <= v) ? 2 * node + 1 : 2 * node;
-            const int ans = node - PLE_TILE;
-            if (brackets) {
-                if ((s_sym[ans] & 0x7fffffffu) != (s_sym[j] & 0x7fffffffu) || !(s_sym[ans] >> 31)) mismatch = true;
-            } else {
-                a.out_parent[g] = base + ans;
+        const uint32_t my_sym = brackets ? s_sym[lj] : 0u;
+        if (brackets && (my_sym >> 31)) continue;  // lefts ask nothing
+        if (!brackets && g == dbase) { a.out_parent[g] = 0; continue; }  // a document's root
+        const int32_t x = v[j];
+        int ans = -1;
+#pragma unroll
+        for (int i = j - 1; i >= 0; --i)
+            if (ans < 0 && v[i] <= x) ans = tid * PLE_ITEMS + i;
+        if (ans < 0) {
+            int node = PLE_TILE + tid * PLE_ITEMS;  // search left of this thread's chunk
+            bool found = false;
+            while (node > 1) {
+                if ((node & 1) && tree[node - 1] <= x) { node = node - 1; found = true; break; }
+                node >>= 1;
             }
-        } else if (g == 0 && !brackets) {
-            a.out_parent[0] = 0;
+            if (found) {
+                while (node < PLE_TILE) node = (tree[2 * node + 1] <= x) ? 2 * node + 1 : 2 * node;
+                ans = node - PLE_TILE;
+            }
+        }
+        if (ans >= 0) {
+            const long long ag = base + ans;
+            if (brackets) {
+                const uint32_t l = s_sym[ans];
+                if (ag < dbase || (l & 0x7fffffffu) != (my_sym & 0x7fffffffu) || !(l >> 31)) a.seg_valid[doc] = 0;
+            } else {
+                a.out_parent[g] = ag - dbase;
+            }
         } else {
             const unsigned int slot = atomicAdd(a.esc_count, 1u);
-            if ((long long)slot < a.esc_cap) a.esc[slot] = ((unsigned long long)g << 32) | (uint32_t)v;
+            if ((long long)slot < a.esc_cap) a.esc[slot] = ((unsigned long long)g << 32) | (uint32_t)x;
             else atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
         }
     }
-    if (mismatch) a.res->valid = 0;
+
     // tile minimum and staircase of suffix minima (values strictly below every later one)
-    int32_t tmin = INT32_MAX;
-    for (int jj = PLE_ITEMS - 1; jj >= 0; --jj) tmin = min(tmin, tree[PLE_TILE + tid * PLE_ITEMS + jj]);
-    s_suf[tid] = tmin;
+    int32_t cm = INT32_MAX;
+#pragma unroll
+    for (int i = 0; i < PLE_ITEMS; ++i) cm = min(cm, v[i]);
+    s_suf[tid] = cm;
     __syncthreads();
-    // suffix min over the threads after this one
-    int32_t after = INT32_MAX;
+    int32_t after;
     {
-        // inclusive suffix scan over s_suf (256 entries) by warps of reversed order
-        int32_t x = s_suf[PLE_THREADS - 1 - tid];  // reversed
+        int32_t y = s_suf[PLE_THREADS - 1 - tid];  // reversed order
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            int32_t o = __shfl_up_sync(ALP_FULL_MASK, x, d);
-            if (lane >= d) x = min(x, o);
+            int32_t o = __shfl_up_sync(ALP_FULL_MASK, y, d);
+            if (lane >= d) y = min(y, o);
         }
         __shared__ int32_t s_wm[PLE_THREADS / 32];
-        if (lane == 31) s_wm[warp] = x;
+        if (lane == 31) s_wm[warp] = y;
         __syncthreads();
         int32_t pre = INT32_MAX;
         for (int w = 0; w < warp; ++w) pre = min(pre, s_wm[w]);
-        x = min(x, pre);  // inclusive min of reversed[0..tid] = min of s_suf[255-tid .. 255]
-        __syncthreads();
-        s_suf[PLE_THREADS - 1 - tid] = x;  // now s_suf[t] = min over threads t..255
+        y = min(y, pre);
+        s_suf[PLE_THREADS - 1 - tid] = y;  // s_suf[t] = min over threads t..end
         __syncthreads();
         after = tid + 1 < PLE_THREADS ? s_suf[tid + 1] : INT32_MAX;
     }
     uint32_t flags = 0;
     int32_t run = after;
-    for (int jj = PLE_ITEMS - 1; jj >= 0; --jj) {
-        const long long g = base + tid * PLE_ITEMS + jj;
-        const int32_t v = tree[PLE_TILE + tid * PLE_ITEMS + jj];
-        if (g < a.n && v < run) flags |= 1u << jj;
-        run = min(run, v);
+#pragma unroll
+    for (int i = PLE_ITEMS - 1; i >= 0; --i) {
+        const long long g = base + tid * PLE_ITEMS + i;
+        if (g < a.n && v[i] < run) flags |= 1u << i;
+        run = min(run, v[i]);
     }
     const uint32_t cnt = __popc(flags);
     const uint32_t incl = warp_scan_add(cnt, lane);
@@ -583,10 +727,11 @@ __global__ void __launch_bounds__(PLE_THREADS) ple_tile_kernel(PleArgs a) {
     }
     uint32_t o = wpre + incl - cnt;
     const long long sbase = (long long)blockIdx.x * PLE_TILE;
-    for (int jj = 0; jj < PLE_ITEMS; ++jj) {
-        if (flags & (1u << jj)) {
-            a.stair_val[sbase + o] = tree[PLE_TILE + tid * PLE_ITEMS + jj];
-            a.stair_idx[sbase + o] = (uint32_t)(base + tid * PLE_ITEMS + jj);
+#pragma unroll
+    for (int i = 0; i < PLE_ITEMS; ++i) {
+        if (flags & (1u << i)) {
+            a.stair_val[sbase + o] = v[i];
+            a.stair_idx[sbase + o] = (uint32_t)(base + tid * PLE_ITEMS + i);
             ++o;
         }
     }
@@ -654,6 +799,9 @@ struct EscArgs {
     const int32_t* stair_len;
     const uint32_t* sym;         // brackets mode when non-null
     long long* out_parent;       // nodes mode
+    const long long* seg_off;
+    long long n_seg;
+    uint8_t* seg_valid;
     AlpResult* res;
 };
 
@@ -675,14 +823,16 @@ __global__ void ple_escape_kernel(EscArgs a) {
             }
             ans = a.stair_idx[u * PLE_TILE + lo];
         }
+        const long long doc = seg_upper(a.seg_off, 0, a.n_seg - 1, g);
+        const long long dbase = a.seg_off[doc];
         if (a.sym) {
-            if (ans < 0) a.res->valid = 0;
+            if (ans < dbase) a.seg_valid[doc] = 0;
             else {
                 const uint32_t l = a.sym[ans], rr = a.sym[g];
-                if (!(l >> 31) || (l & 0x7fffffffu) != (rr & 0x7fffffffu)) a.res->valid = 0;
+                if (!(l >> 31) || (l & 0x7fffffffu) != (rr & 0x7fffffffu)) a.seg_valid[doc] = 0;
             }
         } else {
-            a.out_parent[g] = g == 0 ? 0 : ans;
+            a.out_parent[g] = ans < 0 ? -1 : ans - dbase;
         }
     }
 }

@@ -122,6 +122,35 @@ int alp_parse_tokens(alp_ctx* ctx, const uint32_t* d_term, const int64_t* d_tsta
 int alp_pre_productions(alp_ctx* ctx, const uint32_t* d_term, int64_t m, uint32_t** d_prod,
                         int64_t* n_prod, int* valid);
 
+/* Learned boundary-state speculation (no reference counterpart).
+ *
+ * alp_lex_states: the exact DFA state entering byte 16*i, for every i with
+ * 16*i < n (the composition scan's own states; training labels).
+ *
+ * The MLP (64-byte window -> 16-d byte embedding -> 128 -> 128 -> state
+ * logits, BF16 weights, FP32 accumulation) lives in caller memory:
+ *   params / grads / adam_m / adam_v: FP32 blocks of 155936 floats laid out
+ *     emb[256*16] w1[1024*128] b1[128] w2[128*128] b2[128] w3[128*32] b3[32];
+ *   wbf: the BF16 copies of emb, w1, w2, w3, back to back (155648 values).
+ * alp_mlp_train_step runs forward + backward (+ AdamW when `update`) on one
+ * batch of windows [batch][64] with labels [batch]; batch % 16 == 0.
+ * alp_mlp_predict writes the argmax state for the window ending before each
+ * position in d_pos.
+ *
+ * alp_lex_speculative: lex_int with chunk starts predicted by the MLP and
+ * verified by re-running mispredicted chunks until every start state is
+ * exact -- the same tokens as alp_lex for any weights.  stats (4 values):
+ * chunks, first-round mismatches, chunks re-run, verification rounds. */
+int alp_lex_states(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint8_t* d_states);
+int alp_mlp_train_step(alp_ctx* ctx, float* params, uint16_t* wbf, float* grads, float* adam_m, float* adam_v,
+                       int n_states, const uint8_t* d_win, const uint8_t* d_lab, int batch, float lr, float wd,
+                       int step, int update, float* h_loss, float* h_acc);
+int alp_mlp_predict(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_states, const uint8_t* d_in,
+                    int64_t n, const int64_t* d_pos, int64_t count, uint8_t* d_pred);
+int alp_lex_speculative(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_states, const uint8_t* d_in,
+                        int64_t n, int64_t chunk, uint32_t** d_term, int64_t** d_start, int64_t** d_end,
+                        int64_t* n_tok, int* valid, int64_t* stats);
+
 /* Batched documents (no reference counterpart: the reference parses one
  * document per call; this is that call applied to every document).
  * d_in holds the documents back to back, d_off[0..n_docs] their byte offsets.

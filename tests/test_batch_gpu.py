@@ -1,0 +1,120 @@
+"""Batched (segmented) lex and parse: every document of a batch against the
+oracle run on that document alone (the reference API lexes/parses one
+document per call), bit-exact, including empty, one-byte, rejected and
+tile-aligned documents."""
+
+import numpy as np
+import pytest
+
+import oracle
+from alpacc_b200 import synth, tables
+
+pytestmark = pytest.mark.gpu
+
+_CACHE = {}
+
+
+def _ctx(name, mode):
+    from alpacc_b200.api import Grammar
+    key = (name, mode)
+    if key not in _CACHE:
+        tb = tables.load(name, mode)
+        _CACHE[key] = (Grammar(tb), oracle.Oracle(tb.blob()))
+    return _CACHE[key]
+
+
+def _docs(name, n_docs, seed, median=600, cap=20000):
+    sizes = synth.lognormal_sizes(n_docs, median=median, sigma=1.5, cap=cap, seed=seed)
+    data, off = synth.batch(name, sizes, 8 if name == "json" else 20, seed)
+    return [data[off[i]:off[i + 1]].tobytes() for i in range(n_docs)]
+
+
+def _special(name):
+    good = {"json": [b"[1]", b"{}", b"  [ 1 , 2 ] ", b"\"x\"", b"7"],
+            "sexp": [b"a", b"()", b"(a (b c))", b" (x) "]}[name]
+    bad = {"json": [b"[1", b"\"open", b"#", b"]"], "sexp": [b"(a", b")", b"(("]}[name]
+    return good, bad
+
+
+def _layout(name, docs):
+    """Insert empty documents at the front, middle and end, and a padding
+    document so that the next one starts exactly on a 4096-byte tile boundary."""
+    out = [b"", b""] + docs[:3] + [b""] + docs[3:] + [b"", b""]
+    pos = sum(len(d) for d in out[:5])
+    pad = (-pos) % 4096
+    o, c, one = (b"[", b"]", b"1") if name == "json" else (b"(", b")", b"a")
+    if pad == 1:
+        out.insert(5, one)
+    elif pad >= 2:
+        out.insert(5, o + b" " * (pad - 2) + c)
+    return out
+
+
+def _pack(docs):
+    off = np.zeros(len(docs) + 1, np.int64)
+    off[1:] = np.cumsum([len(d) for d in docs])
+    data = np.frombuffer(b"".join(docs), np.uint8) if off[-1] else np.zeros(0, np.uint8)
+    return data, off
+
+
+@pytest.mark.parametrize("name", ["json", "sexp"])
+@pytest.mark.parametrize("mode", ["lexer", "both"])
+def test_lex_batch(has_gpu, name, mode):
+    g, o = _ctx(name, mode)
+    rng = np.random.default_rng(3)
+    good, bad = _special(name)
+    docs = _layout(name, _docs(name, 300, 77) + good + bad)
+    data, off = _pack(docs)
+    term, start, end, tok_off, valid = (x.cpu().numpy() for x in g.lex_batch_int(data, off))
+    assert tok_off[0] == 0 and tok_off[-1] == len(term)
+    for i, d in enumerate(docs):
+        want = o.lex_futhark(d)
+        assert bool(valid[i]) == (want is not None), (i, d[:40])
+        if want is None:
+            continue
+        a, b = tok_off[i], tok_off[i + 1]
+        np.testing.assert_array_equal(term[a:b].astype(np.uint32), want[0])
+        np.testing.assert_array_equal(start[a:b], want[1])
+        np.testing.assert_array_equal(end[a:b], want[2])
+
+
+@pytest.mark.parametrize("name", ["json", "sexp"])
+def test_parse_batch(has_gpu, name):
+    g, o = _ctx(name, "both")
+    rng = np.random.default_rng(5)
+    good, bad = _special(name)
+    docs = _docs(name, 400, 91)
+    # structurally broken documents (a closer removed) among valid ones
+    for i in range(0, 40, 4):
+        d = bytearray(docs[i])
+        j = max((k for k, c in enumerate(d) if c in b")]}"), default=None)
+        if j is not None:
+            del d[j]
+            docs[i] = bytes(d)
+    docs = _layout(name, docs + good + bad)
+    data, off = _pack(docs)
+    tree, node_off, valid = g.parse_batch_int(data, off)
+    par, tag, kind, st, en = (x.cpu().numpy() for x in (tree.parent, tree.tag, tree.kind, tree.start, tree.end))
+    node_off, valid = node_off.cpu().numpy(), valid.cpu().numpy()
+    n_valid = 0
+    for i, d in enumerate(docs):
+        want = o.lex_parse(d)
+        assert bool(valid[i]) == (want is not None), (i, d[:60])
+        if want is None:
+            continue
+        n_valid += 1
+        a, b = node_off[i], node_off[i + 1]
+        for got, w in zip((par[a:b], tag[a:b].astype(np.uint32), kind[a:b], st[a:b], en[a:b]), want):
+            np.testing.assert_array_equal(got, w)
+    assert n_valid > 300
+
+
+def test_single_doc_batch_equals_parse(has_gpu):
+    g, o = _ctx("json", "both")
+    d = synth.json_doc(300000, 16, 12345)
+    data, off = _pack([d.tobytes()])
+    tree, node_off, valid = g.parse_batch_int(data, off)
+    one = g.parse_int(d)
+    assert valid.cpu().numpy()[0] == 1
+    np.testing.assert_array_equal(tree.parent.cpu().numpy(), one.parent.cpu().numpy())
+    np.testing.assert_array_equal(tree.start.cpu().numpy(), one.start.cpu().numpy())
