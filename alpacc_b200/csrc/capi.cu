@@ -374,7 +374,7 @@ int lex_seg(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_o
         }
         return ALP_OK;
     }
-    const long long tiles = (n + LEX_TILE - 1) / LEX_TILE;
+    const long long tiles = (n + SEG_TILE - 1) / SEG_TILE;
     size_t sbytes = 256 + 8 * (size_t)tiles + 4 * (size_t)tiles;
     if ((rc = grow(ctx, ctx->scratch, sbytes))) return rc;
     uint8_t* base = reinterpret_cast<uint8_t*>(ctx->scratch.p);
@@ -402,8 +402,9 @@ int lex_seg(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_o
     sg.sentinels = sentinels;
     sg.sent_l = ctx->has_parser ? ctx->pt.start : 0;
     sg.sent_r = ctx->has_parser ? ctx->pt.end : 0;
-    auto k = lex_seg_kernel<LEX_ITEMS, TermT, PosT>;
+    auto k = lex_seg_kernel<TermT, PosT>;
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->lex_smem));
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     int per_sm = 0, sms = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, LEX_THREADS, ctx->lex_smem));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
@@ -1112,7 +1113,8 @@ int alp_lex_speculative(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, in
     if ((rc = grow(ctx, sb[0], K + 16)) || (rc = grow(ctx, sb[1], K + 16)) || (rc = grow(ctx, sb[2], K * 4 + 16)) ||
         (rc = grow(ctx, sb[3], K * 4 + 16)) || (rc = grow(ctx, sb[4], K * 4 + 16)) || (rc = grow(ctx, sb[5], K * 4 + 16)) ||
         (rc = grow(ctx, sb[6], K * 4 + 16)) || (rc = grow(ctx, sb[7], K * 4 + 16)) || (rc = grow(ctx, sb[8], nb * 4 + 16)) ||
-        (rc = grow(ctx, sb[9], nb * 4 + 16)) || (rc = grow(ctx, sb[10], K * 8 + 16)) || (rc = grow(ctx, sb[11], 64)))
+        (rc = grow(ctx, sb[9], nb * 4 + 16)) || (rc = grow(ctx, sb[10], K * 8 + 16)) || (rc = grow(ctx, sb[11], 64)) ||
+        (rc = grow(ctx, sb[12], K + 16)))
         return rc;
     int64_t cap = n / 2 + 1024;
     for (int attempt = 0; attempt < 2; ++attempt) {
@@ -1154,7 +1156,8 @@ int alp_lex_speculative(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, in
             CK(cudaMemsetAsync(next_n, 0, 4, ctx->stream));
             a.next_list = lists[cur];
             a.next_n = next_n;
-            spec_fix_kernel<<<grid_for(K), 256, 0, ctx->stream>>>(a);
+            spec_flag_kernel<<<grid_for(K), 256, 0, ctx->stream>>>(a, (uint8_t*)sb[12].p);
+            spec_fix_kernel<<<grid_for(K), 256, 0, ctx->stream>>>(a, (const uint8_t*)sb[12].p);
             CK(cudaGetLastError());
             unsigned int h_next = 0;
             CK(cudaMemcpyAsync(ctx->h_stage, next_n, 4, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1170,7 +1173,12 @@ int alp_lex_speculative(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, in
             CK(cudaGetLastError());
             a.list = nullptr;
             cur ^= 1;
-            if (rounds > 4096) return fail(ctx, ALP_ERR_TIMEOUT, "speculation did not settle");
+            if (rounds > 64) break;  // predictions too poor: the plain scan decides
+        }
+        if (rounds > 64) {
+            rc = alp_lex(ctx, d_in, n, d_term, d_start, d_end, n_tok, valid);
+            if (stats) { stats[0] = K; stats[1] = first; stats[2] = reruns; stats[3] = -1; }
+            return rc;
         }
         mark(ctx, "spec_verify");
         // 4) token offsets per chunk, 5) emit

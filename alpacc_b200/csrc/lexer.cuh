@@ -353,10 +353,24 @@ __device__ __forceinline__ long long doc_lower(const long long* off, long long l
     return lo;
 }
 
-template <int ITEMS, typename TermT, typename PosT>
-__global__ void __launch_bounds__(LEX_THREADS) lex_seg_kernel(LexArgs a, LexSeg sg) {
-    constexpr int TILE = LEX_THREADS * ITEMS;
-    static_assert(ITEMS <= 32, "bit masks hold one bit per byte");
+// Bytes of a thread live in four uint4 registers; byte j of the 64.
+__device__ __forceinline__ uint32_t raw_byte(const uint4 (&w)[4], int j) {
+    const uint4 v = w[j >> 4];
+    const int q = (j >> 2) & 3;
+    const uint32_t x = q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+    return (x >> (8 * (j & 3))) & 0xffu;
+}
+
+constexpr int SEG_ITEMS = 64;                      // bytes per thread
+constexpr int SEG_TILE = LEX_THREADS * SEG_ITEMS;  // 16 KiB per tile
+
+// One tile = 256 threads x 64 bytes.  Three short passes over the bytes held
+// in registers: the endomorphism fold, a counting run of the DFA (token
+// count and last start for the second look-back) and the emitting run.
+template <typename TermT, typename PosT>
+__global__ void __launch_bounds__(LEX_THREADS, 4) lex_seg_kernel(LexArgs a, LexSeg sg) {
+    constexpr int ITEMS = SEG_ITEMS;
+    constexpr int TILE = SEG_TILE;
     extern __shared__ __align__(16) uint8_t smem[];
     const int S = a.t.S, C1 = a.t.C1, E = a.t.E;
     uint8_t* s_cls = smem;
@@ -380,7 +394,6 @@ __global__ void __launch_bounds__(LEX_THREADS) lex_seg_kernel(LexArgs a, LexSeg 
     for (int i = tid; i < E * C1; i += LEX_THREADS) s_step[i] = a.t.step[i];
     const long long n = a.n;
     const long long ND = sg.n_docs;
-    const uint8_t PAD = (uint8_t)(C1 - 1);
     const uint32_t INIT = 1u;
     for (;;) {
         if (tid == 0) {
@@ -397,41 +410,49 @@ __global__ void __launch_bounds__(LEX_THREADS) lex_seg_kernel(LexArgs a, LexSeg 
         if (tile >= a.num_tiles) break;
         const long long my = (long long)tile * TILE + (long long)tid * ITEMS;
         const long long d0 = s_d0, d1 = s_d1;
+        const int lim = (int)max(0ll, min((long long)ITEMS, n - my));  // valid bytes of this thread
 
-        // ---- bytes, document heads and last bytes of this thread ----------
-        uint8_t c[ITEMS];
-        if (a.aligned16 && my + ITEMS <= n) {
+        // ---- bytes, document heads and last bytes --------------------------
+        uint4 w[4];
+        if (a.aligned16 && lim == ITEMS) {
 #pragma unroll
-            for (int v = 0; v < ITEMS / 16; ++v) {
-                uint4 w = __ldg(reinterpret_cast<const uint4*>(a.in + my) + v);
-                uint32_t ws[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-                for (int j = 0; j < 16; ++j) c[v * 16 + j] = s_cls[(ws[j >> 2] >> (8 * (j & 3))) & 0xff];
-            }
+            for (int v = 0; v < 4; ++v) w[v] = __ldg(reinterpret_cast<const uint4*>(a.in + my) + v);
         } else {
+            uint32_t x[16];
 #pragma unroll
-            for (int j = 0; j < ITEMS; ++j) c[j] = (my + j < n) ? s_cls[a.in[my + j]] : PAD;
+            for (int q = 0; q < 16; ++q) {
+                uint32_t y = 0;
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                    if (q * 4 + b < lim) y |= (uint32_t)a.in[my + q * 4 + b] << (8 * b);
+                x[q] = y;
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) w[v] = make_uint4(x[4 * v], x[4 * v + 1], x[4 * v + 2], x[4 * v + 3]);
         }
-        uint32_t head = 0, last = 0;
+        unsigned long long head = 0, last = 0;
         long long mydoc = 0;
-        if (my < n) {
+        if (lim > 0) {
             mydoc = doc_upper(sg.doc_off, d0, d1, my);
-            if (sg.doc_off[mydoc] == my) head |= 1u;
+            if (sg.doc_off[mydoc] == my) head |= 1ull;
             for (long long d = mydoc + 1; d <= ND; ++d) {
                 const long long h = sg.doc_off[d];
                 if (h > my + ITEMS || h > n) break;
-                if (h - 1 >= my) last |= 1u << (int)(h - 1 - my);
-                if (h < n && h < my + ITEMS) head |= 1u << (int)(h - my);
+                if (h - 1 >= my) last |= 1ull << (int)(h - 1 - my);
+                if (h < n && h < my + ITEMS) head |= 1ull << (int)(h - my);
             }
         }
 
-        // ---- phase A ------------------------------------------------------
+        // ---- phase A: the endomorphism of this thread's bytes --------------
         uint32_t f = 0;
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
-            if (head & (1u << j)) f = E + (s_cd[INIT * C1 + c[j]] & 0x7fffu);
-            else if (f >= (uint32_t)E) f = E + (s_cd[(f - E) * C1 + c[j]] & 0x7fffu);
-            else f = s_step[f * C1 + c[j]];
+            if (j < lim) {
+                const uint32_t c = s_cls[raw_byte(w, j)];
+                if ((head >> j) & 1ull) f = E + (s_cd[INIT * C1 + c] & 0x7fffu);
+                else if (f >= (uint32_t)E) f = E + (s_cd[(f - E) * C1 + c] & 0x7fffu);
+                else f = s_step[f * C1 + c];
+            }
         }
         uint32_t incl = f;
 #pragma unroll
@@ -444,8 +465,8 @@ __global__ void __launch_bounds__(LEX_THREADS) lex_seg_kernel(LexArgs a, LexSeg 
         if (lane == 31) s_wagg[warp] = incl;
         __syncthreads();
         if (warp == 0) {
-            uint32_t w = lane < LEX_THREADS / 32 ? s_wagg[lane] : 0u;
-            uint32_t wi = w;
+            uint32_t wv = lane < LEX_THREADS / 32 ? s_wagg[lane] : 0u;
+            uint32_t wi = wv;
 #pragma unroll
             for (int d = 1; d < LEX_THREADS / 32; d <<= 1) {
                 uint32_t o = __shfl_up_sync(ALP_FULL_MASK, wi, d);
@@ -470,20 +491,20 @@ __global__ void __launch_bounds__(LEX_THREADS) lex_seg_kernel(LexArgs a, LexSeg 
                     uint32_t pm = __ballot_sync(ALP_FULL_MASK, flag == ST_P);
                     if (pm) {
                         int p = 31 - __clz(pm);
-                        uint32_t s = __shfl_sync(ALP_FULL_MASK, val, p);
+                        uint32_t st = __shfl_sync(ALP_FULL_MASK, val, p);
                         for (int j = p + 1; j < 32; ++j) {
                             uint32_t aj = __shfl_sync(ALP_FULL_MASK, val, j);
-                            s = ext_apply(a.t, aj, s);
+                            st = ext_apply(a.t, aj, st);
                         }
-                        sin = acc ? ext_apply(a.t, acc, s) : s;
+                        sin = acc ? ext_apply(a.t, acc, st) : st;
                         break;
                     }
-                    uint32_t g = 0;
+                    uint32_t gg = 0;
                     for (int j = 0; j < 32; ++j) {
                         uint32_t aj = __shfl_sync(ALP_FULL_MASK, val, j);
-                        g = ext_comp(a.t, g, aj);
+                        gg = ext_comp(a.t, gg, aj);
                     }
-                    acc = ext_comp(a.t, g, acc);
+                    acc = ext_comp(a.t, gg, acc);
                     end -= 32;
                 }
                 if (lane == 0) st_volatile32(&a.stA[tile], (ST_P << 30) | ext_apply(a.t, F, sin));
@@ -491,31 +512,24 @@ __global__ void __launch_bounds__(LEX_THREADS) lex_seg_kernel(LexArgs a, LexSeg 
             if (lane == 0) s_sin = sin;
         }
         __syncthreads();
-        const uint32_t fexc = ext_comp(a.t, s_wexc[warp], excl);
-        const uint32_t s0 = ext_apply(a.t, fexc, s_sin);
+        const uint32_t s0 = ext_apply(a.t, ext_comp(a.t, s_wexc[warp], excl), s_sin);
 
-        // ---- phase B: one DFA pass, recording ends / starts / finals -------
-        uint32_t cnt = 0, lastp = ALP_NONE32, emit = 0, stt = 0, fin = 0, acc_bits = 0;
-        uint32_t tk[ITEMS], ftk[ITEMS];
+        // ---- phase B, pass 1: tokens ending here and the last start --------
+        uint32_t cnt = 0, lastp = ALP_NONE32;
         {
-            uint32_t s = s0;
+            uint32_t st = s0;
 #pragma unroll
             for (int j = 0; j < ITEMS; ++j) {
-                tk[j] = 0;
-                ftk[j] = 0;
-                if (head & (1u << j)) { s = INIT; stt |= 1u << j; lastp = (uint32_t)(my + j); }
-                uint32_t e = s_cd[s * C1 + c[j]];
-                uint32_t s2 = e & 0x7fffu;
-                if (e & 0x8000u) {
-                    const uint32_t ti = s_tok[s];
-                    if (!(ti & TOK_IGNORE)) { ++cnt; emit |= 1u << j; tk[j] = ti & TOK_TERM_MASK; }
-                    if (!(s_tok[s2] & TOK_IGNORE)) { lastp = (uint32_t)(my + j); stt |= 1u << j; }
-                }
-                s = s2;
-                if (last & (1u << j)) {
-                    const uint32_t ti = s_tok[s];
-                    if (!(ti & TOK_IGNORE)) { ++cnt; fin |= 1u << j; ftk[j] = ti & TOK_TERM_MASK; }
-                    if (ti & TOK_ACCEPT) acc_bits |= 1u << j;
+                if (j < lim) {
+                    if ((head >> j) & 1ull) { st = INIT; lastp = (uint32_t)(my + j); }
+                    const uint32_t e = s_cd[st * C1 + s_cls[raw_byte(w, j)]];
+                    const uint32_t s2 = e & 0x7fffu;
+                    if (e & 0x8000u) {
+                        if (!(s_tok[st] & TOK_IGNORE)) ++cnt;
+                        if (!(s_tok[s2] & TOK_IGNORE)) lastp = (uint32_t)(my + j);
+                    }
+                    st = s2;
+                    if (((last >> j) & 1ull) && !(s_tok[st] & TOK_IGNORE)) ++cnt;
                 }
             }
         }
@@ -574,15 +588,14 @@ __global__ void __launch_bounds__(LEX_THREADS) lex_seg_kernel(LexArgs a, LexSeg 
         }
         __syncthreads();
 
-        // ---- emit -----------------------------------------------------------
-        const uint32_t wxc = s_wc[warp], wxp = s_wp[warp];
-        uint32_t tcount = s_xc + wxc + ec;
-        uint32_t cur = ep != ALP_NONE32 ? ep : (wxp != ALP_NONE32 ? wxp : s_xp);
+        // ---- phase B, pass 2: emit -----------------------------------------
+        uint32_t tcount = s_xc + s_wc[warp] + ec;
+        uint32_t cur = ep != ALP_NONE32 ? ep : (s_wp[warp] != ALP_NONE32 ? s_wp[warp] : s_xp);
         TermT* o_term = reinterpret_cast<TermT*>(a.out_term);
         PosT* o_start = reinterpret_cast<PosT*>(a.out_start);
         PosT* o_end = reinterpret_cast<PosT*>(a.out_end);
         long long doc = mydoc;
-        long long base = my < n ? sg.doc_off[doc] : 0;
+        long long base = lim > 0 ? sg.doc_off[doc] : 0;
         const long long sent = sg.sentinels ? 1 : 0;
         auto put = [&](long long idx, uint32_t term, long long st, long long en) {
             if (idx < a.cap) {
@@ -593,36 +606,50 @@ __global__ void __launch_bounds__(LEX_THREADS) lex_seg_kernel(LexArgs a, LexSeg 
                 atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
             }
         };
+        {
+            uint32_t st = s0;
 #pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            const long long pos = my + j;
-            if (head & (1u << j)) {
-                // every document starting here (empty ones first, then the real one)
-                doc = doc_upper(sg.doc_off, d0, d1, pos);
-                const long long dl = doc_lower(sg.doc_off, 0, doc, pos);  // empty documents here too
-                base = pos;
-                for (long long e = dl; e <= doc; ++e) {
-                    sg.tok_off[e] = tcount;
-                    if (sent) put((long long)tcount + 2 * e, sg.sent_l, 0, 0);
-                    if (e < doc) {
-                        sg.valid[e] = 0;
-                        if (sent) put((long long)tcount + 2 * e + 1, sg.sent_r, 0, 0);
+            for (int j = 0; j < ITEMS; ++j) {
+                if (j < lim) {
+                    const long long pos = my + j;
+                    if ((head >> j) & 1ull) {
+                        // every document starting here (empty ones first, then the real one)
+                        doc = doc_upper(sg.doc_off, d0, d1, pos);
+                        const long long dl = doc_lower(sg.doc_off, 0, doc, pos);
+                        base = pos;
+                        for (long long e = dl; e <= doc; ++e) {
+                            sg.tok_off[e] = tcount;
+                            if (sent) put((long long)tcount + 2 * e, sg.sent_l, 0, 0);
+                            if (e < doc) {
+                                sg.valid[e] = 0;
+                                if (sent) put((long long)tcount + 2 * e + 1, sg.sent_r, 0, 0);
+                            }
+                        }
+                        cur = (uint32_t)pos;
+                        st = INIT;
+                    }
+                    const uint32_t e = s_cd[st * C1 + s_cls[raw_byte(w, j)]];
+                    const uint32_t s2 = e & 0x7fffu;
+                    if (e & 0x8000u) {
+                        const uint32_t ti = s_tok[st];
+                        if (!(ti & TOK_IGNORE)) {
+                            put((long long)tcount + sent * (2 * doc + 1), ti & TOK_TERM_MASK, (long long)cur - base, pos - base);
+                            ++tcount;
+                        }
+                        if (!(s_tok[s2] & TOK_IGNORE)) cur = (uint32_t)pos;
+                    }
+                    st = s2;
+                    if ((last >> j) & 1ull) {
+                        const uint32_t ti = s_tok[st];
+                        if (!(ti & TOK_IGNORE)) {
+                            put((long long)tcount + sent * (2 * doc + 1), ti & TOK_TERM_MASK, (long long)cur - base,
+                                pos + 1 - base);
+                            ++tcount;
+                        }
+                        sg.valid[doc] = (ti & TOK_ACCEPT) ? 1 : 0;
+                        if (sent) put((long long)tcount + 2 * doc + 1, sg.sent_r, 0, 0);
                     }
                 }
-                cur = (uint32_t)pos;
-            }
-            if (emit & (1u << j)) {
-                put((long long)tcount + sent * (2 * doc + 1), tk[j], (long long)cur - base, pos - base);
-                ++tcount;
-            }
-            if (stt & (1u << j)) cur = (uint32_t)pos;
-            if (fin & (1u << j)) {
-                put((long long)tcount + sent * (2 * doc + 1), ftk[j], (long long)cur - base, pos + 1 - base);
-                ++tcount;
-            }
-            if (last & (1u << j)) {
-                sg.valid[doc] = (acc_bits & (1u << j)) ? 1 : 0;
-                if (sent) put((long long)tcount + 2 * doc + 1, sg.sent_r, 0, 0);
             }
         }
         if (my <= n - 1 && n - 1 < my + ITEMS) {

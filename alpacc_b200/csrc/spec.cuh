@@ -95,13 +95,22 @@ __global__ void spec_run_kernel(SpecArgs a) {
         spec_chunk(a, a.list ? (long long)a.list[i] : i, s_cls, s_cd, s_tok);
 }
 
-// Chunks whose start differs from the predecessor's end: take that end and
-// queue the chunk for a re-run.
-__global__ void spec_fix_kernel(SpecArgs a) {
+// Verification, step 1: flag every chunk whose start differs from its
+// predecessor's end.
+__global__ void spec_flag_kernel(SpecArgs a, uint8_t* flag) {
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < a.K; j += (long long)gridDim.x * blockDim.x)
+        flag[j] = (j > 0 && a.st[j] != a.en[j - 1]) ? 1 : 0;
+}
+
+// Step 2: a flagged chunk whose predecessor is not flagged takes the
+// predecessor's end as its start and is queued for a re-run.  A chunk behind
+// another flagged chunk waits: that predecessor's end came from a start that is
+// being replaced (often the dead state after a wrong guess), and copying it
+// would carry the error forward one chunk per round.
+__global__ void spec_fix_kernel(SpecArgs a, const uint8_t* flag) {
     for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x + 1; j < a.K; j += (long long)gridDim.x * blockDim.x) {
-        const uint8_t want = a.en[j - 1];
-        if (a.st[j] != want) {
-            a.st[j] = want;
+        if (flag[j] && !flag[j - 1]) {
+            a.st[j] = a.en[j - 1];
             const unsigned int k = atomicAdd(a.next_n, 1u);
             a.next_list[k] = (uint32_t)j;
         }

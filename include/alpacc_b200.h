@@ -140,7 +140,8 @@ int alp_pre_productions(alp_ctx* ctx, const uint32_t* d_term, int64_t m, uint32_
  * alp_lex_speculative: lex_int with chunk starts predicted by the MLP and
  * verified by re-running mispredicted chunks until every start state is
  * exact -- the same tokens as alp_lex for any weights.  stats (4 values):
- * chunks, first-round mismatches, chunks re-run, verification rounds. */
+ * chunks, first-round mismatches, chunks re-run, verification rounds (-1:
+ * more than 64 rounds were needed and the plain scan produced the tokens). */
 int alp_lex_states(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint8_t* d_states);
 int alp_mlp_train_step(alp_ctx* ctx, float* params, uint16_t* wbf, float* grads, float* adam_m, float* adam_v,
                        int n_states, const uint8_t* d_win, const uint8_t* d_lab, int batch, float lr, float wd,
