@@ -12,6 +12,7 @@
 #include "../../include/alpacc_b200.h"
 #include "common.cuh"
 #include "lexer.cuh"
+#include "lex3.cuh"
 #include "parser.cuh"
 #include "mlp.cuh"
 #include "spec.cuh"
@@ -42,6 +43,9 @@ struct alp_ctx {
     std::vector<uint32_t> h_tokinfo;
     LexTables lt{};
     size_t lex_smem = 0;
+    bool lex3 = false;                    // DFA small enough for the three-kernel lexer
+    Lex3Tables l3{};
+    size_t l3_fold_smem = 0, l3_scan_smem = 0, l3_emit_smem = 0;
     // ---- parser tables ----
     bool has_parser = false;
     ParseTables pt{};
@@ -181,6 +185,43 @@ int load_lexer(alp_ctx* ctx, Reader& r) {
     ctx->lex_smem = lex_smem_bytes(S, C1, E);
     if (ctx->lex_smem > 200 * 1024) return fail(ctx, ALP_ERR_TABLE, "lexer tables exceed shared memory");
     ctx->has_lexer = true;
+
+    // Three-kernel lexer tables: apply as [E][32] bytes and a 256-column
+    // transition table whose entries carry the emit / start decisions.
+    bool small = S <= 32 && E + S <= 65535 && lex3_fold_smem(S, C1, E) <= 200 * 1024 &&
+                 lex3_scan_smem(E) <= 160 * 1024 && lex3_emit_smem(S) <= 200 * 1024;
+    for (int s = 0; s < S && small; ++s)
+        if ((ctx->h_tokinfo[s] & TOK_TERM_MASK) > 0xffffu) small = false;
+    if (small) {
+        std::vector<uint8_t> app8((size_t)E * 32);
+        for (int e = 0; e < E; ++e)
+            for (int s = 0; s < 32; ++s) app8[(size_t)e * 32 + s] = (uint8_t)(s < S ? vapp[(size_t)e * S + s] : s);
+        std::vector<uint16_t> ent((size_t)S * LX_ROW + 8, 0);
+        for (int s = 0; s < S; ++s)
+            for (int b = 0; b < 256; ++b) {
+                const uint16_t e = vcd[(size_t)s * C1 + vcls[b]];
+                const uint32_t nx = e & 0x7fffu;
+                uint32_t v = nx;
+                if (e & 0x8000u) {
+                    if (!(ctx->h_tokinfo[s] & TOK_IGNORE)) v |= LX_EMIT;
+                    if (!(ctx->h_tokinfo[nx] & TOK_IGNORE)) v |= LX_START;
+                }
+                ent[(size_t)s * LX_ROW + b] = (uint16_t)v;
+            }
+        ctx->l3.cls = ctx->lt.cls;
+        ctx->l3.cdelta = ctx->lt.cdelta;
+        ctx->l3.step = ctx->lt.step;
+        ctx->l3.tokinfo = ctx->lt.tokinfo;
+        if ((rc = upload(ctx, app8.data(), app8.size(), &ctx->l3.app8))) return rc;
+        if ((rc = upload(ctx, ent.data(), ent.size(), &ctx->l3.ent))) return rc;
+        ctx->l3.S = S;
+        ctx->l3.C1 = C1;
+        ctx->l3.E = E;
+        ctx->l3_fold_smem = lex3_fold_smem(S, C1, E);
+        ctx->l3_scan_smem = lex3_scan_smem(E);
+        ctx->l3_emit_smem = lex3_emit_smem(S);
+        ctx->lex3 = true;
+    }
     return ALP_OK;
 }
 
@@ -232,28 +273,6 @@ int check_in(alp_ctx* ctx, const void* p, int64_t n) {
     if (n > 0 && !p) return fail(ctx, ALP_ERR_ARG, "null input");
     return ALP_OK;
 }
-
-// Lex into typed buffers; sets *count (needed count even when over capacity)
-// and *valid.  Returns ALP_ERR_CAPACITY when cap was too small.
-template <typename TermT, typename PosT>
-int lex_core(alp_ctx* ctx, const uint8_t* d_in, int64_t n, TermT* term, PosT* start, PosT* end, int64_t cap,
-             int64_t* count, int* valid) {
-    *count = 0;
-    *valid = 0;
-    if (!ctx->has_lexer) return fail(ctx, ALP_ERR_MODE, "these tables have no lexer");
-    if (n == 0) {
-        *valid = (ctx->h_tokinfo[1] & TOK_ACCEPT) ? 1 : 0;
-        return ALP_OK;
-    }
-    int rc = launch_lex<LEX_ITEMS, TermT, PosT>(ctx, d_in, n, term, start, end, cap);
-    if (rc) return rc;
-    *valid = ctx->h_res->valid;
-    *count = ctx->h_res->count;
-    if (ctx->h_res->error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
-    if (!*valid) *count = 0;
-    return ALP_OK;
-}
-
 
 // Buffers of one parse (indices into ctx->tmp).
 enum {
@@ -351,6 +370,94 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     return ALP_OK;
 }
 
+// Three-kernel lexer (DFAs of at most 32 states): chunk endomorphisms, the
+// state scan over them, and the token pass.  Same contract as lex_seg.
+template <typename TermT, typename PosT>
+int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_off, long long nd, int sentinels,
+             TermT* term, PosT* start, PosT* end, long long cap, uint8_t* valid, long long* total) {
+    const long long tiles = (n + LX_TILE - 1) / LX_TILE;
+    const long long chunks = (n + LX_ITEMS - 1) / LX_ITEMS;
+    const long long stiles = (chunks + LS_TILE - 1) / LS_TILE;
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t o_cs = 256, o_vec = o_cs + al(8 * (size_t)tiles), o_f = o_vec + al(128 * (size_t)stiles);
+    const size_t o_s = o_f + al(2 * (size_t)chunks + 64), o_td = o_s + al((size_t)chunks + 64);
+    const size_t sbytes = o_td + al(8 * (size_t)tiles);
+    int rc;
+    if ((rc = grow(ctx, ctx->scratch, sbytes))) return rc;
+    uint8_t* base = reinterpret_cast<uint8_t*>(ctx->scratch.p);
+    CK(cudaMemsetAsync(base, 0, o_f, ctx->stream));  // result, tickets, look-back words
+    Lex3Args a;
+    a.in = d_in;
+    a.n = n;
+    a.aligned16 = ((reinterpret_cast<uintptr_t>(d_in) & 15u) == 0) ? 1 : 0;
+    a.t = ctx->l3;
+    a.n_chunks = chunks;
+    a.chunk_f = reinterpret_cast<uint16_t*>(base + o_f);
+    a.chunk_s = base + o_s;
+    a.lb_vec = reinterpret_cast<uint32_t*>(base + o_vec);
+    a.lb_cs = reinterpret_cast<unsigned long long*>(base + o_cs);
+    a.res = reinterpret_cast<AlpResult*>(base);
+    a.tickets = reinterpret_cast<unsigned int*>(base + 128);
+    a.tile_doc = reinterpret_cast<const long long*>(base + o_td);
+    a.out_term = term;
+    a.out_start = start;
+    a.out_end = end;
+    a.cap = cap;
+    a.num_tiles = (unsigned)tiles;
+    a.num_scan_tiles = (unsigned)stiles;
+    LexSeg sg;
+    sg.doc_off = d_off;
+    sg.n_docs = nd;
+    sg.tok_off = (long long*)ctx->tmp[T_TOKOFF].p;
+    sg.valid = valid;
+    sg.sentinels = sentinels;
+    sg.sent_l = ctx->has_parser ? ctx->pt.start : 0;
+    sg.sent_r = ctx->has_parser ? ctx->pt.end : 0;
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    auto grid_of = [&](const void* k, int threads, size_t smem, long long work, unsigned* g) -> int {
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem));
+        long long x = (long long)(per_sm > 0 ? per_sm : 1) * sms;
+        *g = (unsigned)(x < work ? x : work);
+        return ALP_OK;
+    };
+    mark(ctx, "start");
+    if (nd > 1) {
+        const long long gb = (nd + 255) / 256;
+        CK(cudaMemsetAsync(base + o_td, 0, 8 * (size_t)tiles, ctx->stream));
+        lex3_tile_doc_kernel<<<(unsigned)(gb < 4096 ? gb : 4096), 256, 0, ctx->stream>>>(
+            d_off, nd, reinterpret_cast<long long*>(base + o_td), tiles);
+        CK(cudaGetLastError());
+        mark(ctx, "lex3_tile_doc_kernel");
+    }
+    unsigned g1, g2, g3;
+    CK(cudaFuncSetAttribute(lex3_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_fold_smem));
+    CK(cudaFuncSetAttribute(lex3_fold_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    if ((rc = grid_of((const void*)lex3_fold_kernel, LX_THREADS, ctx->l3_fold_smem, tiles, &g1))) return rc;
+    lex3_fold_kernel<<<g1, LX_THREADS, ctx->l3_fold_smem, ctx->stream>>>(a, sg);
+    CK(cudaGetLastError());
+    mark(ctx, "lex3_fold_kernel");
+    CK(cudaFuncSetAttribute(lex3_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_scan_smem));
+    if ((rc = grid_of((const void*)lex3_scan_kernel, LS_WARPS * 32, ctx->l3_scan_smem, stiles, &g2))) return rc;
+    lex3_scan_kernel<<<g2, LS_WARPS * 32, ctx->l3_scan_smem, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    mark(ctx, "lex3_scan_kernel");
+    auto k3 = lex3_emit_kernel<TermT, PosT>;
+    CK(cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_emit_smem));
+    CK(cudaFuncSetAttribute(k3, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    if ((rc = grid_of((const void*)k3, LX_THREADS, ctx->l3_emit_smem, tiles, &g3))) return rc;
+    k3<<<g3, LX_THREADS, ctx->l3_emit_smem, ctx->stream>>>(a, sg);
+    CK(cudaGetLastError());
+    mark(ctx, "lex3_emit_kernel");
+    CK(cudaMemcpyAsync(ctx->h_res, a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
+    *total = ctx->h_res->count;
+    if (ctx->h_res->error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
+    return ALP_OK;
+}
+
 // Segmented lexer over documents at d_off[0..nd] (device).  sentinels: the
 // parser layout (⊢ tokens ⊣ per document) into tmp[T_TTERM..T_TEND] with
 // u16/u32 types; otherwise the lexer API layout into the given buffers.
@@ -374,6 +481,7 @@ int lex_seg(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_o
         }
         return ALP_OK;
     }
+    if (ctx->lex3) return lex3_run<TermT, PosT>(ctx, d_in, n, d_off, nd, sentinels, term, start, end, cap, valid, total);
     const long long tiles = (n + SEG_TILE - 1) / SEG_TILE;
     size_t sbytes = 256 + 8 * (size_t)tiles + 4 * (size_t)tiles;
     if ((rc = grow(ctx, ctx->scratch, sbytes))) return rc;
@@ -522,6 +630,43 @@ int read_valid0(alp_ctx* ctx, const uint8_t* dvalid, int* valid) {
     *valid = v ? 1 : 0;
     return ALP_OK;
 }
+
+// Lex into typed buffers; sets *count (needed count even when over capacity)
+// and *valid.  Returns ALP_ERR_CAPACITY when cap was too small.
+template <typename TermT, typename PosT>
+int lex_core(alp_ctx* ctx, const uint8_t* d_in, int64_t n, TermT* term, PosT* start, PosT* end, int64_t cap,
+             int64_t* count, int* valid) {
+    *count = 0;
+    *valid = 0;
+    if (!ctx->has_lexer) return fail(ctx, ALP_ERR_MODE, "these tables have no lexer");
+    if (n == 0) {
+        *valid = (ctx->h_tokinfo[1] & TOK_ACCEPT) ? 1 : 0;
+        return ALP_OK;
+    }
+    if (ctx->lex3 && !ctx->state_out) {
+        int rc;
+        if ((rc = grow(ctx, ctx->tmp[T_DVALID], 16)) || (rc = put_doc_off(ctx, n))) return rc;
+        uint8_t* dvalid = (uint8_t*)ctx->tmp[T_DVALID].p;
+        long long total = 0;
+        rc = lex_seg<TermT, PosT>(ctx, d_in, n, (const long long*)ctx->tmp[T_DOCOFF].p, 1, 0, term, start, end, cap,
+                                  dvalid, &total);
+        *count = total;
+        if (rc) return rc;
+        int v = 0;
+        if ((rc = read_valid0(ctx, dvalid, &v))) return rc;
+        *valid = v;
+        if (!v) *count = 0;
+        return ALP_OK;
+    }
+    int rc = launch_lex<LEX_ITEMS, TermT, PosT>(ctx, d_in, n, term, start, end, cap);
+    if (rc) return rc;
+    *valid = ctx->h_res->valid;
+    *count = ctx->h_res->count;
+    if (ctx->h_res->error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
+    if (!*valid) *count = 0;
+    return ALP_OK;
+}
+
 
 int parse_core(alp_ctx* ctx, const uint8_t* d_in, int64_t n, ParseOut* o, int64_t cap, int ctx_out,
                int64_t* n_node, int* valid) {

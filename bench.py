@@ -58,57 +58,77 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    """SM clock and clock-event reasons of the timed GPU, read through NVML
+    every 2 ms while the timed region runs (read-only queries)."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.max = None
+        self.err = None
+        self.t = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = None
+            try:
+                import torch
+                p = torch.cuda.get_device_properties(self.index)
+                h = nv.nvmlDeviceGetHandleByPciBusId(
+                    "%08x:%02x:%02x.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id))
+            except Exception:
+                h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.nv, self.h = nv, h
+            self.max = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.reasons_fn = (getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None)
+                               or nv.nvmlDeviceGetCurrentClocksThrottleReasons)
+            self.stop = threading.Event()
+            self._sample()
+            self.t = threading.Thread(target=self._run, daemon=True)
             self.t.start()
-        except Exception:
-            self.proc = None
+        except Exception as e:  # no NVML: the line says so
+            self.err = "%s: %s" % (type(e).__name__, e)
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _sample(self):
+        try:
+            self.samples.append((self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM),
+                                 int(self.reasons_fn(self.h))))
+        except Exception:
+            pass
+
+    def _run(self):
+        while not self.stop.is_set():
+            self._sample()
+            time.sleep(0.002)
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
+        if self.t:
+            self.stop.set()
+            self.t.join(timeout=2)
+            self._sample()
             try:
-                self.proc.wait(timeout=5)
+                self.nv.nvmlShutdown()
             except Exception:
-                self.proc.kill()
+                pass
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[3:7]):
-                if v.lower() == "active":
+        sm = [c for c, _ in self.samples]
+        reasons = set()
+        for _, r in self.samples:
+            for bit, nm in self.REASONS.items():
+                if r & bit:
                     reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max,
+               "reasons": sorted(reasons), "samples": len(sm), "source": "nvml, 2 ms"}
+        if self.err:
+            out["error"] = self.err
+        return out
 
 
 def make_doc(seed: int, size: int) -> np.ndarray:
@@ -281,6 +301,8 @@ def main():
     alg_bytes = size + NODE_BYTES * N
     achieved = alg_bytes / (ms * 1e-3) / 1e9
     total_k = sum(t for _, t in kern) or 1.0
+    # one mark per kernel, except "a+b" marks that cover two launches
+    launches_per_step = sum(1 + k.count("+") for k, _ in kern)
     top = max(kern, key=lambda x: x[1]) if kern else ("", 0.0)
     line = {
         "metric": METRIC,
@@ -308,7 +330,7 @@ def main():
                      "kernel_share": {k: round(t / total_k, 4) for k, t in kern}},
         "e2e": {"value": world * size / (ms_e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": size,
                 "d2h_bytes_per_step": NODE_BYTES * N, "ms_per_step": ms_e2e},
-        "gpu_launches": 9 * args.steps,
+        "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
     }
     if base:

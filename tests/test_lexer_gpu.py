@@ -99,3 +99,24 @@ def test_host_buffers(has_gpu):
     want = o.lex_futhark(d.tobytes())
     for a, b in zip(got, want):
         np.testing.assert_array_equal(a, b)
+
+
+def test_dense_tokens_and_unaligned_input(has_gpu):
+    """Tiles with more tokens than the shared-memory staging holds (every
+    other byte a token) next to sparse tiles, and inputs that start off a
+    16-byte boundary (byte loads instead of vector loads)."""
+    import torch
+    g, o = _ctx("json", "both")
+    dense = b"[" + b"1," * 300000 + b"1]"
+    _check(g, o, dense)
+    mixed = b"[" + b"1," * 20000 + b'"' + b"x" * 50000 + b'",' + b"1," * 20000 + b"1]"
+    _check(g, o, mixed)
+    doc = _gen("json", 200003, 11).tobytes()
+    buf = torch.frombuffer(bytearray(b"   " + doc), dtype=torch.uint8).to("cuda")
+    for off in (1, 3):
+        view = buf[off:]
+        assert view.data_ptr() % 16 != 0
+        got = g.lex_int(view)
+        want = o.lex_futhark(bytes(b"   "[off:]) + doc)
+        for a, b in zip(got, want):
+            np.testing.assert_array_equal(a.cpu().numpy().astype(b.dtype), b)
