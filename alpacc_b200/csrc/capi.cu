@@ -43,9 +43,9 @@ struct alp_ctx {
     std::vector<uint32_t> h_tokinfo;
     LexTables lt{};
     size_t lex_smem = 0;
-    bool lex3 = false;                    // DFA small enough for the three-kernel lexer
+    bool lex3 = false;                    // DFA small enough for the multi-kernel lexer (lex3.cuh)
     Lex3Tables l3{};
-    size_t l3_fold_smem = 0, l3_scan_smem = 0, l3_emit_smem = 0;
+    size_t l3_fold_smem = 0, l3_scan_smem = 0, l3_count_smem = 0, l3_emit_smem = 0;
     // ---- parser tables ----
     bool has_parser = false;
     ParseTables pt{};
@@ -186,16 +186,18 @@ int load_lexer(alp_ctx* ctx, Reader& r) {
     if (ctx->lex_smem > 200 * 1024) return fail(ctx, ALP_ERR_TABLE, "lexer tables exceed shared memory");
     ctx->has_lexer = true;
 
-    // Three-kernel lexer tables: apply as [E][32] bytes and a 256-column
+    // Multi-kernel lexer tables: apply as [E+S][32] bytes and a 256-column
     // transition table whose entries carry the emit / start decisions.
     bool small = S <= 32 && E + S <= 65535 && lex3_fold_smem(S, C1, E) <= 200 * 1024 &&
-                 lex3_scan_smem(E) <= 160 * 1024 && lex3_emit_smem(S) <= 200 * 1024;
+                 lex3_scan_smem(S, E) <= 160 * 1024 && lex3_emit_smem(S) <= 200 * 1024;
     for (int s = 0; s < S && small; ++s)
         if ((ctx->h_tokinfo[s] & TOK_TERM_MASK) > 0xffffu) small = false;
     if (small) {
-        std::vector<uint8_t> app8((size_t)E * 32);
+        std::vector<uint8_t> app8(((size_t)E + S) * 32);
         for (int e = 0; e < E; ++e)
             for (int s = 0; s < 32; ++s) app8[(size_t)e * 32 + s] = (uint8_t)(s < S ? vapp[(size_t)e * S + s] : s);
+        for (int c = 0; c < S; ++c)  // constant functions E + c (the state after a document head)
+            for (int s = 0; s < 32; ++s) app8[((size_t)E + c) * 32 + s] = (uint8_t)c;
         std::vector<uint16_t> ent((size_t)S * LX_ROW + 8, 0);
         for (int s = 0; s < S; ++s)
             for (int b = 0; b < 256; ++b) {
@@ -218,7 +220,8 @@ int load_lexer(alp_ctx* ctx, Reader& r) {
         ctx->l3.C1 = C1;
         ctx->l3.E = E;
         ctx->l3_fold_smem = lex3_fold_smem(S, C1, E);
-        ctx->l3_scan_smem = lex3_scan_smem(E);
+        ctx->l3_scan_smem = lex3_scan_smem(S, E);
+        ctx->l3_count_smem = lex3_count_smem(S);
         ctx->l3_emit_smem = lex3_emit_smem(S);
         ctx->lex3 = true;
     }
@@ -370,22 +373,25 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     return ALP_OK;
 }
 
-// Three-kernel lexer (DFAs of at most 32 states): chunk endomorphisms, the
-// state scan over them, and the token pass.  Same contract as lex_seg.
+// Multi-kernel lexer (DFAs of at most 32 states): chunk endomorphisms, the
+// state scan over them, token counts, the tile scan of the counts, and the
+// token pass.  Same contract as lex_seg.
 template <typename TermT, typename PosT>
 int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_off, long long nd, int sentinels,
              TermT* term, PosT* start, PosT* end, long long cap, uint8_t* valid, long long* total) {
     const long long tiles = (n + LX_TILE - 1) / LX_TILE;
-    const long long chunks = (n + LX_ITEMS - 1) / LX_ITEMS;
+    const long long wide = (n + LX_WIDE - 1) / LX_WIDE;
+    const long long chunks = (n + LX_CHUNK - 1) / LX_CHUNK;
     const long long stiles = (chunks + LS_TILE - 1) / LS_TILE;
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t o_cs = 256, o_vec = o_cs + al(8 * (size_t)tiles), o_f = o_vec + al(128 * (size_t)stiles);
-    const size_t o_s = o_f + al(2 * (size_t)chunks + 64), o_td = o_s + al((size_t)chunks + 64);
+    const size_t o_vec = 256, o_cs = o_vec + al(128 * (size_t)stiles), o_f = o_cs + al(8 * (size_t)tiles);
+    const size_t o_s = o_f + al(2 * (size_t)chunks + 64), o_c = o_s + al((size_t)chunks + 64);
+    const size_t o_td = o_c + al(2 * (size_t)chunks + 64);
     const size_t sbytes = o_td + al(8 * (size_t)tiles);
     int rc;
     if ((rc = grow(ctx, ctx->scratch, sbytes))) return rc;
     uint8_t* base = reinterpret_cast<uint8_t*>(ctx->scratch.p);
-    CK(cudaMemsetAsync(base, 0, o_f, ctx->stream));  // result, tickets, look-back words
+    CK(cudaMemsetAsync(base, 0, o_cs, ctx->stream));  // result, tickets, look-back words
     Lex3Args a;
     a.in = d_in;
     a.n = n;
@@ -394,8 +400,9 @@ int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_
     a.n_chunks = chunks;
     a.chunk_f = reinterpret_cast<uint16_t*>(base + o_f);
     a.chunk_s = base + o_s;
+    a.chunk_c = reinterpret_cast<uint16_t*>(base + o_c);
+    a.tile_cs = reinterpret_cast<unsigned long long*>(base + o_cs);
     a.lb_vec = reinterpret_cast<uint32_t*>(base + o_vec);
-    a.lb_cs = reinterpret_cast<unsigned long long*>(base + o_cs);
     a.res = reinterpret_cast<AlpResult*>(base);
     a.tickets = reinterpret_cast<unsigned int*>(base + 128);
     a.tile_doc = reinterpret_cast<const long long*>(base + o_td);
@@ -404,6 +411,7 @@ int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_
     a.out_end = end;
     a.cap = cap;
     a.num_tiles = (unsigned)tiles;
+    a.num_wide = (unsigned)wide;
     a.num_scan_tiles = (unsigned)stiles;
     LexSeg sg;
     sg.doc_off = d_off;
@@ -422,6 +430,19 @@ int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_
         *g = (unsigned)(x < work ? x : work);
         return ALP_OK;
     };
+    auto k5 = lex3_emit_kernel<TermT, PosT>;
+    unsigned g1, g2, g3, g5;
+    CK(cudaFuncSetAttribute(lex3_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_fold_smem));
+    CK(cudaFuncSetAttribute(lex3_fold_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    CK(cudaFuncSetAttribute(lex3_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_scan_smem));
+    CK(cudaFuncSetAttribute(lex3_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_count_smem));
+    CK(cudaFuncSetAttribute(k5, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_emit_smem));
+    CK(cudaFuncSetAttribute(k5, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    if ((rc = grid_of((const void*)lex3_fold_kernel, LX_THREADS, ctx->l3_fold_smem, wide, &g1)) ||
+        (rc = grid_of((const void*)lex3_scan_kernel, LS_WARPS * 32, ctx->l3_scan_smem, stiles, &g2)) ||
+        (rc = grid_of((const void*)lex3_count_kernel, LX_THREADS, ctx->l3_count_smem, wide, &g3)) ||
+        (rc = grid_of((const void*)k5, LX_THREADS, ctx->l3_emit_smem, tiles, &g5)))
+        return rc;
     mark(ctx, "start");
     if (nd > 1) {
         const long long gb = (nd + 255) / 256;
@@ -431,23 +452,19 @@ int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_
         CK(cudaGetLastError());
         mark(ctx, "lex3_tile_doc_kernel");
     }
-    unsigned g1, g2, g3;
-    CK(cudaFuncSetAttribute(lex3_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_fold_smem));
-    CK(cudaFuncSetAttribute(lex3_fold_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    if ((rc = grid_of((const void*)lex3_fold_kernel, LX_THREADS, ctx->l3_fold_smem, tiles, &g1))) return rc;
     lex3_fold_kernel<<<g1, LX_THREADS, ctx->l3_fold_smem, ctx->stream>>>(a, sg);
     CK(cudaGetLastError());
     mark(ctx, "lex3_fold_kernel");
-    CK(cudaFuncSetAttribute(lex3_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_scan_smem));
-    if ((rc = grid_of((const void*)lex3_scan_kernel, LS_WARPS * 32, ctx->l3_scan_smem, stiles, &g2))) return rc;
     lex3_scan_kernel<<<g2, LS_WARPS * 32, ctx->l3_scan_smem, ctx->stream>>>(a);
     CK(cudaGetLastError());
     mark(ctx, "lex3_scan_kernel");
-    auto k3 = lex3_emit_kernel<TermT, PosT>;
-    CK(cudaFuncSetAttribute(k3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_emit_smem));
-    CK(cudaFuncSetAttribute(k3, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    if ((rc = grid_of((const void*)k3, LX_THREADS, ctx->l3_emit_smem, tiles, &g3))) return rc;
-    k3<<<g3, LX_THREADS, ctx->l3_emit_smem, ctx->stream>>>(a, sg);
+    lex3_count_kernel<<<g3, LX_THREADS, ctx->l3_count_smem, ctx->stream>>>(a, sg);
+    CK(cudaGetLastError());
+    mark(ctx, "lex3_count_kernel");
+    lex3_tile_scan_kernel<<<1, 1024, 0, ctx->stream>>>(a.tile_cs, tiles);
+    CK(cudaGetLastError());
+    mark(ctx, "lex3_tile_scan_kernel");
+    k5<<<g5, LX_THREADS, ctx->l3_emit_smem, ctx->stream>>>(a, sg);
     CK(cudaGetLastError());
     mark(ctx, "lex3_emit_kernel");
     CK(cudaMemcpyAsync(ctx->h_res, a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));

@@ -1,24 +1,30 @@
-// Three-kernel lexer for DFAs of at most 32 states (sm_100a).
+// Multi-kernel lexer for DFAs of at most 32 states (sm_100a).
 //
 // Same results as lex_seg_kernel (futhark/lexer.fut:73-172 per document),
-// split so that no step waits on table lookups through L2:
+// split so that no step waits on another tile or on table lookups in L2:
 //
-//   lex3_fold_kernel  every 32-byte chunk -> its endomorphism id, folded with
-//                     the step table in shared memory (constant E+s after a
-//                     document head).  Streaming; no look-back.
-//   lex3_scan_kernel  the composition scan over chunk endomorphisms.  With
-//                     S <= 32 one warp holds a whole function, lane s the
-//                     image of state s, so composing two functions is one
-//                     shuffle and a tile's aggregate is 32 bytes.  Lanes walk
-//                     the chunks of their warp through the apply table in
-//                     shared memory; tiles chain through a decoupled look-back
-//                     on these vectors.  Output: the state entering each chunk.
-//   lex3_emit_kernel  the token pass (futhark/lexer.fut:103-133): each thread
-//                     runs the DFA over its chunk from the known state with a
-//                     256-column transition table whose entries carry the
-//                     produce/ignore decisions, counts, takes its place
-//                     through a (count, last start) look-back, and stages the
-//                     tile's tokens in shared memory for coalesced stores.
+//   lex3_fold_kernel   every 32-byte chunk -> its endomorphism id, folded with
+//                      the step table in shared memory (constant E+s after a
+//                      document head).  Two independent chunks per thread.
+//   lex3_scan_kernel   the composition scan over chunk endomorphisms.  With
+//                      S <= 32 one warp holds a whole function, lane s the
+//                      image of state s, so composing two functions is one
+//                      shuffle and a tile's aggregate is 32 bytes.  Lanes walk
+//                      the chunks of their warp through the apply table in
+//                      shared memory; tiles chain through a decoupled look-back
+//                      on these vectors.  Output: the state entering each chunk.
+//   lex3_count_kernel  the token-end flags and ignore filter (futhark/lexer.fut:
+//                      103-107) as counts: each thread runs the DFA over two
+//                      chunks from their known states with a 256-column table
+//                      whose entries carry the produce/ignore decisions, and
+//                      stores the chunk's token count and last token start.
+//   lex3_tile_scan_kernel  exclusive (count, last start) over 8 KiB tiles, the
+//                      take_right start scan and the compaction offsets
+//                      (futhark/lexer.fut:83-84,108-120) at tile level.
+//   lex3_emit_kernel   the compaction (futhark/lexer.fut:121-133): places each
+//                      thread from the stored counts, runs the DFA once more,
+//                      stages the tile's tokens in shared memory and writes
+//                      them with coalesced stores.
 #pragma once
 #include "common.cuh"
 #include "lexer.cuh"
@@ -26,9 +32,10 @@
 namespace alp {
 
 constexpr int LX_THREADS = 256;
-constexpr int LX_ITEMS = 32;                    // bytes per thread = one chunk
-constexpr int LX_TILE = LX_THREADS * LX_ITEMS;  // 8 KiB per tile
-constexpr int LX_STAGE = 2560;                  // tokens one tile stages in shared memory
+constexpr int LX_CHUNK = 32;                    // bytes per chunk, the unit of the state scan
+constexpr int LX_TILE = LX_THREADS * LX_CHUNK;  // 8 KiB emit tile: one chunk per thread
+constexpr int LX_WIDE = 2 * LX_TILE;            // 16 KiB fold / count tile: two chunks per thread
+constexpr int LX_STAGE = 2560;                  // tokens one emit tile stages in shared memory
 constexpr int LS_WARPS = 8;
 constexpr int LS_G = 16;                        // chunks per lane in the state scan
 constexpr int LS_TILE = LS_WARPS * 32 * LS_G;   // 4096 chunks per state-scan tile
@@ -37,15 +44,17 @@ constexpr int LS_TILE = LS_WARPS * 32 * LS_G;   // 4096 chunks per state-scan ti
 // lanes reading the same byte in different states hit different banks.
 constexpr int LX_ROW = 258;
 constexpr uint32_t LX_NEXT = 0x1fu;
-constexpr uint32_t LX_EMIT = 1u << 5;   // a kept token of term(st) ends before this byte
-constexpr uint32_t LX_START = 1u << 6;  // a kept token starts at this byte
+constexpr uint32_t LX_START = 1u << 5;  // a kept token starts at this byte
+constexpr uint32_t LX_EMIT = 1u << 6;   // a kept token of term(st) ends before this byte
+constexpr uint32_t LX_NOOFF = 0xffu;    // chunk_c: no token start in the chunk
 
 struct Lex3Tables {
     const uint8_t* cls;       // [256] byte -> class
     const uint16_t* cdelta;   // [S][C1] next | produce<<15
     const uint16_t* step;     // [E][C1] endo after one more byte of the class
-    const uint8_t* app8;      // [E][32] state after endo e from state s (identity for s >= S)
-    const uint16_t* ent;      // [S][LX_ROW] next | LX_EMIT | LX_START (columns 256.. unused)
+    const uint8_t* app8;      // [E+S][32] state after endo f from state s; rows E+s are constant s;
+                              // identity beyond S in rows < E
+    const uint16_t* ent;      // [S][LX_ROW] next | LX_START | LX_EMIT (columns 256.. unused)
     const uint32_t* tokinfo;  // [S] terminal | TOK_ACCEPT | TOK_IGNORE
     int S, C1, E;
 };
@@ -55,20 +64,22 @@ struct Lex3Args {
     long long n;
     int aligned16;
     Lex3Tables t;
-    long long n_chunks;          // ceil(n / 32)
-    uint16_t* chunk_f;           // [n_chunks] endomorphism of each chunk (E + s: constant s)
-    uint8_t* chunk_s;            // [n_chunks] state entering each chunk
-    uint32_t* lb_vec;            // [scan tiles][32] state-scan look-back words
-    unsigned long long* lb_cs;   // [tiles] (count, start) look-back words
-    unsigned int* tickets;       // [0] state scan, [1] emit
-    const long long* tile_doc;   // [tiles] document holding each tile's first byte (n_docs > 1)
+    long long n_chunks;            // ceil(n / 32)
+    uint16_t* chunk_f;             // [n_chunks] endomorphism of each chunk (E + s: constant s)
+    uint8_t* chunk_s;              // [n_chunks] state entering each chunk
+    uint16_t* chunk_c;             // [n_chunks] tokens ending in the chunk | last start offset << 8
+    unsigned long long* tile_cs;   // [tiles] count << 32 | last start; inclusive per tile, then exclusive
+    uint32_t* lb_vec;              // [scan tiles][32] state-scan look-back words
+    unsigned int* tickets;         // [0] state scan
+    const long long* tile_doc;     // [tiles] document holding each 8 KiB tile's first byte (n_docs > 1)
     void* out_term;
     void* out_start;
     void* out_end;
     long long cap;
     AlpResult* res;
-    unsigned int num_tiles;      // 8 KiB tiles
-    unsigned int num_scan_tiles; // LS_TILE-chunk tiles
+    unsigned int num_tiles;        // 8 KiB tiles
+    unsigned int num_wide;         // 16 KiB tiles
+    unsigned int num_scan_tiles;   // LS_TILE-chunk tiles
 };
 
 __host__ __device__ inline size_t lex3_fold_smem(int S, int C1, int E) {
@@ -77,12 +88,13 @@ __host__ __device__ inline size_t lex3_fold_smem(int S, int C1, int E) {
     b += 2 * (size_t)E * C1;
     return (b + 15) & ~(size_t)15;
 }
-__host__ __device__ inline size_t lex3_scan_smem(int E) {
-    return (32 * (size_t)E + 15) & ~(size_t)15;
+__host__ __device__ inline size_t lex3_scan_smem(int S, int E) {
+    return (32 * ((size_t)E + S) + 15) & ~(size_t)15;
 }
 __host__ __device__ inline size_t lex3_tok_off(int S) { return (2 * (size_t)S * LX_ROW + 15) & ~(size_t)15; }
 __host__ __device__ inline size_t lex3_stage_off(int S) { return (lex3_tok_off(S) + 4 * (size_t)S + 15) & ~(size_t)15; }
-__host__ __device__ inline size_t lex3_emit_smem(int S) { return lex3_stage_off(S) + (size_t)LX_STAGE * (2 + 4 + 4); }
+__host__ __device__ inline size_t lex3_count_smem(int S) { return lex3_stage_off(S); }
+__host__ __device__ inline size_t lex3_emit_smem(int S) { return lex3_stage_off(S) + (size_t)LX_STAGE * 8; }
 
 template <int NV>
 __device__ __forceinline__ uint32_t byte_of(const uint4 (&w)[NV], int j) {
@@ -103,103 +115,119 @@ __global__ void lex3_tile_doc_kernel(const long long* off, long long nd, long lo
     }
 }
 
-// Document heads and last bytes of tile [t0, t1] as per-thread bit masks;
-// *s_dmax = the last document with a byte at or before t1.
+// Document heads and last bytes of tile [t0, t1] as per-chunk bit masks
+// (bit j of word c: byte t0 + 32c + j); *s_dmax = the last document with a
+// byte at or before t1.
 __device__ __forceinline__ void lx_mark_docs(const LexSeg& sg, long long n, long long d0, long long t0, long long t1,
                                              uint32_t* s_head, uint32_t* s_last, unsigned long long* s_dmax) {
-    for (long long d = d0 + threadIdx.x; d <= sg.n_docs; d += LX_THREADS) {
+    for (long long d = d0 + threadIdx.x; d <= sg.n_docs; d += blockDim.x) {
         const long long h = sg.doc_off[d];
         if (h > t1 + 1) break;
         if (h >= t0 && h <= t1 && h < n) {
             const long long r = h - t0;
             atomicOr(&s_head[r >> 5], 1u << (r & 31));
         }
-        if (h - 1 >= t0 && h - 1 <= t1 && s_last) {
+        if (s_last && h - 1 >= t0 && h - 1 <= t1) {
             const long long r = h - 1 - t0;
             atomicOr(&s_last[r >> 5], 1u << (r & 31));
         }
-        if (h <= t1 && d < sg.n_docs && s_dmax) atomicMax(s_dmax, (unsigned long long)d);
+        if (s_dmax && h <= t1 && d < sg.n_docs) atomicMax(s_dmax, (unsigned long long)d);
     }
 }
 
-// Load the (up to) 32 bytes of a thread starting at `my`.
-__device__ __forceinline__ void lx_load(const Lex3Args& a, long long my, int lim, uint4 (&w)[2]) {
-    if (a.aligned16 && lim == LX_ITEMS) {
-        w[0] = __ldg(reinterpret_cast<const uint4*>(a.in + my));
-        w[1] = __ldg(reinterpret_cast<const uint4*>(a.in + my) + 1);
-    } else {
-        uint32_t x[8];
+// The (up to) 16*NV bytes starting at `my`.
+template <int NV>
+__device__ __forceinline__ void lx_load(const Lex3Args& a, long long my, int lim, uint4 (&w)[NV]) {
+    if (a.aligned16 && lim == 16 * NV) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int v = 0; v < NV; ++v) w[v] = __ldg(reinterpret_cast<const uint4*>(a.in + my) + v);
+    } else {
+        uint32_t x[4 * NV];
+#pragma unroll
+        for (int q = 0; q < 4 * NV; ++q) {
             uint32_t y = 0;
 #pragma unroll
             for (int b = 0; b < 4; ++b)
                 if (q * 4 + b < lim) y |= (uint32_t)a.in[my + q * 4 + b] << (8 * b);
             x[q] = y;
         }
-        w[0] = make_uint4(x[0], x[1], x[2], x[3]);
-        w[1] = make_uint4(x[4], x[5], x[6], x[7]);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) w[v] = make_uint4(x[4 * v], x[4 * v + 1], x[4 * v + 2], x[4 * v + 3]);
     }
 }
 
 // ---- kernel 1: chunk endomorphisms ------------------------------------------
+
+// One chunk's endomorphism from bytes [b0, b0 + lim) of w, with document heads.
+__device__ __forceinline__ uint32_t lx_fold_slow(const uint4 (&w)[4], int b0, int lim, uint32_t head,
+                                                 const uint8_t* s_cls, const uint16_t* s_cd, const uint16_t* s_step,
+                                                 int C1, uint32_t E) {
+    uint32_t f = 0;
+#pragma unroll
+    for (int j = 0; j < LX_CHUNK; ++j) {
+        if (j < lim) {
+            const uint32_t c = s_cls[byte_of(w, b0 + j)];
+            if ((head >> j) & 1u) f = E + (s_cd[1 * C1 + c] & 0x7fffu);
+            else if (f >= E) f = E + (s_cd[(f - E) * C1 + c] & 0x7fffu);
+            else f = s_step[f * C1 + c];
+        }
+    }
+    return f;
+}
+
 __global__ void __launch_bounds__(LX_THREADS, 4) lex3_fold_kernel(Lex3Args a, LexSeg sg) {
     extern __shared__ __align__(16) uint8_t smem[];
-    const int S = a.t.S, C1 = a.t.C1, E = a.t.E;
+    const int S = a.t.S, C1 = a.t.C1;
+    const uint32_t E = (uint32_t)a.t.E;
     uint8_t* s_cls = smem;
     uint16_t* s_cd = reinterpret_cast<uint16_t*>(smem + 256);
     const size_t off_step = (256 + 2 * (size_t)S * C1 + 15) & ~(size_t)15;
     uint16_t* s_step = reinterpret_cast<uint16_t*>(smem + off_step);
-    __shared__ uint32_t s_head[LX_THREADS];
+    __shared__ uint32_t s_head[LX_WIDE / LX_CHUNK];
 
     const int tid = threadIdx.x;
     for (int i = tid; i < 256; i += LX_THREADS) s_cls[i] = a.t.cls[i];
     for (int i = tid; i < S * C1; i += LX_THREADS) s_cd[i] = a.t.cdelta[i];
-    for (int i = tid; i < E * C1; i += LX_THREADS) s_step[i] = a.t.step[i];
+    for (int i = tid; i < (int)E * C1; i += LX_THREADS) s_step[i] = a.t.step[i];
     const long long n = a.n;
-    const uint32_t INIT = 1u;
-    for (unsigned tile = blockIdx.x; tile < a.num_tiles; tile += gridDim.x) {
-        const long long t0 = (long long)tile * LX_TILE;
-        const long long t1 = min(t0 + LX_TILE, n) - 1;
+    for (unsigned ft = blockIdx.x; ft < a.num_wide; ft += gridDim.x) {
+        const long long t0 = (long long)ft * LX_WIDE;
+        const long long t1 = min(t0 + LX_WIDE, n) - 1;
         s_head[tid] = 0;
+        s_head[tid + LX_THREADS] = 0;
         __syncthreads();
-        lx_mark_docs(sg, n, sg.n_docs > 1 ? a.tile_doc[tile] : 0, t0, t1, s_head, nullptr, nullptr);
+        lx_mark_docs(sg, n, sg.n_docs > 1 ? a.tile_doc[2 * (size_t)ft] : 0, t0, t1, s_head, nullptr, nullptr);
         __syncthreads();
-        const long long my = t0 + (long long)tid * LX_ITEMS;
-        const int lim = (int)max(0ll, min((long long)LX_ITEMS, n - my));
+        const long long my = t0 + (long long)tid * (2 * LX_CHUNK);
+        const int lim = (int)max(0ll, min((long long)(2 * LX_CHUNK), n - my));
         if (lim > 0) {
-            uint4 w[2];
-            lx_load(a, my, lim, w);
-            const uint32_t head = s_head[tid];
-            uint32_t f = 0;
-            if (head == 0 && lim == LX_ITEMS) {
+            uint4 w[4];
+            lx_load<4>(a, my, lim, w);
+            const uint32_t ha = s_head[2 * tid], hb = s_head[2 * tid + 1];
+            const long long c = my / LX_CHUNK;
+            if (lim == 2 * LX_CHUNK && (ha | hb) == 0) {
+                uint32_t fa = 0, fb = 0;
 #pragma unroll
-                for (int j = 0; j < LX_ITEMS; ++j) f = s_step[f * C1 + s_cls[byte_of(w, j)]];
-            } else {
-#pragma unroll
-                for (int j = 0; j < LX_ITEMS; ++j) {
-                    if (j < lim) {
-                        const uint32_t c = s_cls[byte_of(w, j)];
-                        if ((head >> j) & 1u) f = E + (s_cd[INIT * C1 + c] & 0x7fffu);
-                        else if (f >= (uint32_t)E) f = E + (s_cd[(f - E) * C1 + c] & 0x7fffu);
-                        else f = s_step[f * C1 + c];
-                    }
+                for (int j = 0; j < LX_CHUNK; ++j) {
+                    fa = s_step[fa * C1 + s_cls[byte_of(w, j)]];
+                    fb = s_step[fb * C1 + s_cls[byte_of(w, LX_CHUNK + j)]];
                 }
+                *reinterpret_cast<uint32_t*>(a.chunk_f + c) = fa | (fb << 16);
+            } else {
+                a.chunk_f[c] = (uint16_t)lx_fold_slow(w, 0, min(lim, LX_CHUNK), ha, s_cls, s_cd, s_step, C1, E);
+                if (lim > LX_CHUNK)
+                    a.chunk_f[c + 1] =
+                        (uint16_t)lx_fold_slow(w, LX_CHUNK, lim - LX_CHUNK, hb, s_cls, s_cd, s_step, C1, E);
             }
-            a.chunk_f[my / LX_ITEMS] = (uint16_t)f;
         }
         __syncthreads();
     }
 }
 
 // ---- kernel 2: states entering the chunks -----------------------------------
-__device__ __forceinline__ uint32_t lx_app(const uint8_t* s_app, uint32_t E, uint32_t f, uint32_t s) {
-    return f >= E ? f - E : s_app[f * 32 + s];
-}
-
 __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
     extern __shared__ __align__(16) uint8_t smem[];
-    const uint32_t E = (uint32_t)a.t.E;
+    const uint32_t rows = (uint32_t)(a.t.E + a.t.S);
     uint8_t* s_app = smem;
     __shared__ uint8_t s_sv[LS_WARPS][32][32];  // [warp][lane segment][start state] -> state
     __shared__ uint8_t s_wagg[LS_WARPS][32];
@@ -210,7 +238,7 @@ __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
     {
         const uint4* src = reinterpret_cast<const uint4*>(a.t.app8);
         uint4* dst = reinterpret_cast<uint4*>(s_app);
-        for (uint32_t i = tid; i < E * 2; i += LS_WARPS * 32) dst[i] = src[i];
+        for (uint32_t i = tid; i < rows * 2; i += LS_WARPS * 32) dst[i] = src[i];
     }
     const uint32_t INIT = 1u;
     const long long M = a.n_chunks;
@@ -244,8 +272,8 @@ __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
 #pragma unroll
             for (int q = 0; q < LS_G / 2; ++q) {
                 const uint32_t v = __shfl_sync(ALP_FULL_MASK, fr[q], l2);
-                cur = lx_app(s_app, E, v & 0xffffu, cur);
-                cur = lx_app(s_app, E, v >> 16, cur);
+                cur = s_app[(v & 0xffffu) * 32 + cur];
+                cur = s_app[(v >> 16) * 32 + cur];
             }
         }
         s_wagg[warp][lane] = (uint8_t)cur;
@@ -259,10 +287,8 @@ __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
                 x = s_wagg[w][x];
             }
             // x = the tile's function: lane s -> state after the tile from s
-            uint32_t sin;
-            if (tile == 0) {
-                sin = INIT;
-            } else {
+            uint32_t sin = INIT;
+            if (tile > 0) {
                 st_volatile32(&a.lb_vec[(size_t)tile * 32 + lane], (ST_A << 30) | x);
                 uint32_t acc = (uint32_t)lane;  // composition of the aggregates passed so far
                 long long j = (long long)tile - 1;
@@ -304,9 +330,9 @@ __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
 #pragma unroll
         for (int q = 0; q < LS_G / 2; ++q) {
             ob[q >> 1] |= st << (16 * (q & 1));
-            st = lx_app(s_app, E, fr[q] & 0xffffu, st);
+            st = s_app[(fr[q] & 0xffffu) * 32 + st];
             ob[q >> 1] |= st << (16 * (q & 1) + 8);
-            st = lx_app(s_app, E, fr[q] >> 16, st);
+            st = s_app[(fr[q] >> 16) * 32 + st];
         }
         if (base + LS_G <= M) {
             *reinterpret_cast<uint4*>(a.chunk_s + base) = make_uint4(ob[0], ob[1], ob[2], ob[3]);
@@ -319,23 +345,175 @@ __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
     }
 }
 
-// ---- kernel 3: tokens ---------------------------------------------------------
+// ---- kernel 3: token counts -------------------------------------------------
+
+// Tokens ending in bytes [b0, b0 + lim) of w from state st, with document
+// heads and last bytes; *lastoff = offset of the last token start or LX_NOOFF.
+__device__ __forceinline__ uint32_t lx_count_slow(const uint4 (&w)[4], int b0, int lim, uint32_t st, uint32_t head,
+                                                  uint32_t last, const uint16_t* s_ent, const uint32_t* s_tok,
+                                                  uint32_t* lastoff) {
+    uint32_t cnt = 0, lo = LX_NOOFF;
+#pragma unroll
+    for (int j = 0; j < LX_CHUNK; ++j) {
+        if (j < lim) {
+            if ((head >> j) & 1u) { st = 1u; lo = (uint32_t)j; }
+            const uint32_t e = s_ent[st * LX_ROW + byte_of(w, b0 + j)];
+            cnt += (e >> 6) & 1u;
+            if (e & LX_START) lo = (uint32_t)j;
+            st = e & LX_NEXT;
+            if (((last >> j) & 1u) && !(s_tok[st] & TOK_IGNORE)) ++cnt;
+        }
+    }
+    *lastoff = lo;
+    return cnt;
+}
+
+// (count, last position) combine over a warp: counts add, the position takes
+// the right operand unless it is NONE.  Lane 0 ends with the total.
+__device__ __forceinline__ void cs_reduce_warp(uint32_t& c, uint32_t& p) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t oc = __shfl_down_sync(ALP_FULL_MASK, c, d);
+        const uint32_t op = __shfl_down_sync(ALP_FULL_MASK, p, d);
+        c += oc;
+        if (op != ALP_NONE32) p = op;
+    }
+}
+
+__global__ void __launch_bounds__(LX_THREADS, 4) lex3_count_kernel(Lex3Args a, LexSeg sg) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int S = a.t.S;
+    uint16_t* s_ent = reinterpret_cast<uint16_t*>(smem);
+    uint32_t* s_tok = reinterpret_cast<uint32_t*>(smem + lex3_tok_off(S));
+    __shared__ uint32_t s_head[LX_WIDE / LX_CHUNK], s_last[LX_WIDE / LX_CHUNK];
+    __shared__ uint32_t s_wc[LX_THREADS / 32], s_wp[LX_THREADS / 32];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(a.t.ent);
+        uint4* dst = reinterpret_cast<uint4*>(s_ent);
+        for (int i = tid; i < (S * LX_ROW * 2 + 15) / 16; i += LX_THREADS) dst[i] = src[i];
+    }
+    for (int i = tid; i < S; i += LX_THREADS) s_tok[i] = a.t.tokinfo[i];
+    const long long n = a.n;
+    for (unsigned ft = blockIdx.x; ft < a.num_wide; ft += gridDim.x) {
+        const long long t0 = (long long)ft * LX_WIDE;
+        const long long t1 = min(t0 + LX_WIDE, n) - 1;
+        s_head[tid] = 0;
+        s_head[tid + LX_THREADS] = 0;
+        s_last[tid] = 0;
+        s_last[tid + LX_THREADS] = 0;
+        __syncthreads();
+        lx_mark_docs(sg, n, sg.n_docs > 1 ? a.tile_doc[2 * (size_t)ft] : 0, t0, t1, s_head, s_last, nullptr);
+        __syncthreads();
+        const long long my = t0 + (long long)tid * (2 * LX_CHUNK);
+        const int lim = (int)max(0ll, min((long long)(2 * LX_CHUNK), n - my));
+        uint32_t cnt = 0, lastp = ALP_NONE32;
+        if (lim > 0) {
+            uint4 w[4];
+            lx_load<4>(a, my, lim, w);
+            const long long c = my / LX_CHUNK;
+            const uint32_t ha = s_head[2 * tid], hb = s_head[2 * tid + 1];
+            const uint32_t la = s_last[2 * tid], lb = s_last[2 * tid + 1];
+            uint32_t ca, cb = 0, oa, ob = LX_NOOFF;
+            if (lim == 2 * LX_CHUNK && (ha | hb | la | lb) == 0) {
+                const uint32_t sab = *reinterpret_cast<const uint16_t*>(a.chunk_s + c);
+                uint32_t sa = sab & 0xffu, sb = sab >> 8;
+                ca = 0;
+                oa = LX_NOOFF;
+#pragma unroll
+                for (int j = 0; j < LX_CHUNK; ++j) {
+                    const uint32_t ea = s_ent[sa * LX_ROW + byte_of(w, j)];
+                    const uint32_t eb = s_ent[sb * LX_ROW + byte_of(w, LX_CHUNK + j)];
+                    ca += (ea >> 6) & 1u;
+                    cb += (eb >> 6) & 1u;
+                    if (ea & LX_START) oa = (uint32_t)j;
+                    if (eb & LX_START) ob = (uint32_t)j;
+                    sa = ea & LX_NEXT;
+                    sb = eb & LX_NEXT;
+                }
+                *reinterpret_cast<uint32_t*>(a.chunk_c + c) = (ca | (oa << 8)) | ((cb | (ob << 8)) << 16);
+            } else {
+                ca = lx_count_slow(w, 0, min(lim, LX_CHUNK), a.chunk_s[c], ha, la, s_ent, s_tok, &oa);
+                a.chunk_c[c] = (uint16_t)(ca | (oa << 8));
+                if (lim > LX_CHUNK) {
+                    cb = lx_count_slow(w, LX_CHUNK, lim - LX_CHUNK, a.chunk_s[c + 1], hb, lb, s_ent, s_tok, &ob);
+                    a.chunk_c[c + 1] = (uint16_t)(cb | (ob << 8));
+                }
+            }
+            cnt = ca + cb;
+            lastp = ob != LX_NOOFF ? (uint32_t)(my + LX_CHUNK + ob)
+                                   : (oa != LX_NOOFF ? (uint32_t)(my + oa) : ALP_NONE32);
+        }
+        // per 8 KiB tile (threads 0..127 and 128..255): count and last start
+        cs_reduce_warp(cnt, lastp);
+        if (lane == 0) { s_wc[warp] = cnt; s_wp[warp] = lastp; }
+        __syncthreads();
+        if (tid == 0 || tid == LX_THREADS / 2) {
+            const int w0 = tid / 32;
+            uint32_t c = 0, p = ALP_NONE32;
+            for (int w2 = w0; w2 < w0 + LX_THREADS / 64; ++w2) {
+                c += s_wc[w2];
+                if (s_wp[w2] != ALP_NONE32) p = s_wp[w2];
+            }
+            const size_t t8 = 2 * (size_t)ft + (tid ? 1 : 0);
+            if (t8 < a.num_tiles) a.tile_cs[t8] = ((unsigned long long)c << 32) | p;
+        }
+        __syncthreads();
+    }
+}
+
+// ---- kernel 4: exclusive (count, last start) over tiles ---------------------
+// One CTA of 1024 threads.  Tile 0 starts from (0, 0).
+__global__ void __launch_bounds__(1024) lex3_tile_scan_kernel(unsigned long long* tile_cs, long long T) {
+    __shared__ uint32_t s_c[32], s_p[32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long per = (T + 1023) / 1024;
+    const long long lo = min(T, (long long)tid * per), hi = min(T, lo + per);
+    uint32_t c = 0, p = ALP_NONE32;
+    for (long long i = lo; i < hi; ++i) {
+        const unsigned long long v = tile_cs[i];
+        c += (uint32_t)(v >> 32);
+        if ((uint32_t)v != ALP_NONE32) p = (uint32_t)v;
+    }
+    uint32_t ic = c, ip = p;
+    warp_scan_cs(ic, ip, lane);
+    if (lane == 31) { s_c[warp] = ic; s_p[warp] = ip; }
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t wc = s_c[lane], wp = s_p[lane];
+        warp_scan_cs(wc, wp, lane);
+        uint32_t xc = __shfl_up_sync(ALP_FULL_MASK, wc, 1), xp = __shfl_up_sync(ALP_FULL_MASK, wp, 1);
+        if (lane == 0) { xc = 0; xp = ALP_NONE32; }
+        s_c[lane] = xc;
+        s_p[lane] = xp;
+    }
+    __syncthreads();
+    uint32_t ec = __shfl_up_sync(ALP_FULL_MASK, ic, 1), ep = __shfl_up_sync(ALP_FULL_MASK, ip, 1);
+    if (lane == 0) { ec = 0; ep = ALP_NONE32; }
+    uint32_t rc = s_c[warp] + ec;
+    uint32_t rp = ep != ALP_NONE32 ? ep : s_p[warp];
+    for (long long i = lo; i < hi; ++i) {
+        const unsigned long long v = tile_cs[i];
+        tile_cs[i] = ((unsigned long long)rc << 32) | (rp != ALP_NONE32 ? rp : 0u);
+        rc += (uint32_t)(v >> 32);
+        if ((uint32_t)v != ALP_NONE32) rp = (uint32_t)v;
+    }
+}
+
+// ---- kernel 5: tokens ---------------------------------------------------------
 template <typename TermT, typename PosT>
 __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, LexSeg sg) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int S = a.t.S;
     uint16_t* s_ent = reinterpret_cast<uint16_t*>(smem);
     uint32_t* s_tok = reinterpret_cast<uint32_t*>(smem + lex3_tok_off(S));
-    uint32_t* s_start = reinterpret_cast<uint32_t*>(smem + lex3_stage_off(S));
-    uint32_t* s_end = s_start + LX_STAGE;
-    uint16_t* s_term = reinterpret_cast<uint16_t*>(s_end + LX_STAGE);
+    uint32_t* s_pk = reinterpret_cast<uint32_t*>(smem + lex3_stage_off(S));  // end - t0 | term << 16
+    uint32_t* s_st = s_pk + LX_STAGE;                                        // start (absolute)
 
-    __shared__ uint32_t s_tile;
-    __shared__ long long s_d0;
     __shared__ unsigned long long s_dmax;
-    __shared__ uint32_t s_head[LX_THREADS], s_last[LX_THREADS];
+    __shared__ uint32_t s_head[LX_TILE / LX_CHUNK], s_last[LX_TILE / LX_CHUNK];
     __shared__ uint32_t s_wc[LX_THREADS / 32], s_wp[LX_THREADS / 32];
-    __shared__ uint32_t s_xc, s_xp, s_bc;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     {
@@ -360,156 +538,92 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
             atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
         }
     };
-    for (;;) {
-        if (tid == 0) {
-            s_tile = atomicAdd(&a.tickets[1], 1u);
-            if (s_tile < a.num_tiles) {
-                s_d0 = ND > 1 ? a.tile_doc[s_tile] : 0;
-                s_dmax = (unsigned long long)s_d0;
-            }
-        }
+    for (unsigned tile = blockIdx.x; tile < a.num_tiles; tile += gridDim.x) {
+        const long long t0 = (long long)tile * LX_TILE;
+        const long long t1 = min(t0 + LX_TILE, n) - 1;
+        const long long d0 = ND > 1 ? a.tile_doc[tile] : 0;
+        if (tid == 0) s_dmax = (unsigned long long)d0;
         s_head[tid] = 0;
         s_last[tid] = 0;
         __syncthreads();
-        const uint32_t tile = s_tile;
-        if (tile >= a.num_tiles) break;
-        const long long t0 = (long long)tile * LX_TILE;
-        const long long t1 = min(t0 + LX_TILE, n) - 1;
-        const long long d0 = s_d0;
         lx_mark_docs(sg, n, d0, t0, t1, s_head, s_last, &s_dmax);
         __syncthreads();
         const long long dmax = (long long)s_dmax;
-        const long long my = t0 + (long long)tid * LX_ITEMS;
-        const int lim = (int)max(0ll, min((long long)LX_ITEMS, n - my));
+        const long long my = t0 + (long long)tid * LX_CHUNK;
+        const int lim = (int)max(0ll, min((long long)LX_CHUNK, n - my));
 
         uint4 w[2];
-        uint32_t s0 = INIT, head = 0, last = 0;
+        uint32_t s0 = INIT, head = 0, last = 0, cnt = 0, lastp = ALP_NONE32;
         long long mydoc = d0;
         if (lim > 0) {
-            lx_load(a, my, lim, w);
-            s0 = a.chunk_s[my / LX_ITEMS];
+            lx_load<2>(a, my, lim, w);
+            s0 = a.chunk_s[my / LX_CHUNK];
+            const uint32_t cc = a.chunk_c[my / LX_CHUNK];
+            cnt = cc & 0xffu;
+            if ((cc >> 8) != LX_NOOFF) lastp = (uint32_t)(my + (cc >> 8));
             head = s_head[tid];
             last = s_last[tid];
             if (dmax > d0) mydoc = doc_upper(sg.doc_off, d0, dmax, my);
         } else {
             w[0] = w[1] = make_uint4(0, 0, 0, 0);
         }
-        const bool plain = (head | last) == 0 && lim == LX_ITEMS;
 
-        // ---- pass 1: tokens ending here and the last start ----------------
-        uint32_t cnt = 0, lastp = ALP_NONE32;
-        {
-            uint32_t st = s0;
-            if (plain) {
-#pragma unroll
-                for (int j = 0; j < LX_ITEMS; ++j) {
-                    const uint32_t e = s_ent[st * LX_ROW + byte_of(w, j)];
-                    cnt += (e >> 5) & 1u;
-                    if (e & LX_START) lastp = (uint32_t)(my + j);
-                    st = e & LX_NEXT;
-                }
-            } else {
-#pragma unroll
-                for (int j = 0; j < LX_ITEMS; ++j) {
-                    if (j < lim) {
-                        if ((head >> j) & 1u) { st = INIT; lastp = (uint32_t)(my + j); }
-                        const uint32_t e = s_ent[st * LX_ROW + byte_of(w, j)];
-                        cnt += (e >> 5) & 1u;
-                        if (e & LX_START) lastp = (uint32_t)(my + j);
-                        st = e & LX_NEXT;
-                        if (((last >> j) & 1u) && !(s_tok[st] & TOK_IGNORE)) ++cnt;
-                    }
-                }
-            }
-        }
-
-        // ---- block scan and look-back of (count, last start) --------------
+        // ---- this thread's place: tile prefix + block scan of stored counts --
+        const unsigned long long X = a.tile_cs[tile];
+        const uint32_t Xc = (uint32_t)(X >> 32), Xp = (uint32_t)X;
         uint32_t ic = cnt, ip = lastp;
         warp_scan_cs(ic, ip, lane);
         uint32_t ec = __shfl_up_sync(ALP_FULL_MASK, ic, 1), ep = __shfl_up_sync(ALP_FULL_MASK, ip, 1);
         if (lane == 0) { ec = 0; ep = ALP_NONE32; }
         if (lane == 31) { s_wc[warp] = ic; s_wp[warp] = ip; }
         __syncthreads();
-        if (warp == 0) {
-            uint32_t wc = lane < LX_THREADS / 32 ? s_wc[lane] : 0u;
-            uint32_t wp = lane < LX_THREADS / 32 ? s_wp[lane] : ALP_NONE32;
-            uint32_t bc = wc, bp = wp;
-            warp_scan_cs(bc, bp, lane);
-            uint32_t xc = __shfl_up_sync(ALP_FULL_MASK, bc, 1), xp = __shfl_up_sync(ALP_FULL_MASK, bp, 1);
-            if (lane == 0) { xc = 0; xp = ALP_NONE32; }
-            if (lane < LX_THREADS / 32) { s_wc[lane] = xc; s_wp[lane] = xp; }
-            const uint32_t Bc = __shfl_sync(ALP_FULL_MASK, bc, LX_THREADS / 32 - 1);
-            const uint32_t Bp = __shfl_sync(ALP_FULL_MASK, bp, LX_THREADS / 32 - 1);
-            uint32_t Xc, Xp;
-            if (tile == 0) {
-                Xc = 0; Xp = 0;
-                if (lane == 0) st_volatile64(&a.lb_cs[0], cs_pack(ST_P, Bc, Bp != ALP_NONE32 ? Bp : 0u));
-            } else {
-                if (lane == 0) st_volatile64(&a.lb_cs[tile], cs_pack(ST_A, Bc, Bp));
-                uint32_t acc_c = 0, acc_p = ALP_NONE32;
-                long long end = tile;
-                while (true) {
-                    const long long idx = end - 32 + lane;
-                    const unsigned long long w2 = idx >= 0 ? wait64(&a.lb_cs[idx], &a.res->error) : cs_pack(ST_P, 0, 0);
-                    const uint32_t flag = (uint32_t)(w2 >> 62);
-                    const uint32_t pm = __ballot_sync(ALP_FULL_MASK, flag == ST_P);
-                    const int p = pm ? 31 - __clz(pm) : -1;
-                    uint32_t vc = lane >= p ? cs_count(w2) : 0u;
-                    uint32_t vp = lane >= p ? cs_pos(w2) : ALP_NONE32;
+        uint32_t wc = 0, wp = ALP_NONE32, Bc = 0;
 #pragma unroll
-                    for (int d = 1; d < 32; d <<= 1) {
-                        const uint32_t oc = __shfl_down_sync(ALP_FULL_MASK, vc, d);
-                        const uint32_t op = __shfl_down_sync(ALP_FULL_MASK, vp, d);
-                        if (lane + d < 32) {
-                            vc += oc;
-                            if (op != ALP_NONE32) vp = op;
-                        }
-                    }
-                    vc = __shfl_sync(ALP_FULL_MASK, vc, 0);
-                    vp = __shfl_sync(ALP_FULL_MASK, vp, 0);
-                    acc_c += vc;
-                    if (acc_p == ALP_NONE32) acc_p = vp;
-                    if (pm) break;
-                    end -= 32;
-                }
-                Xc = acc_c; Xp = acc_p;
-                if (lane == 0) st_volatile64(&a.lb_cs[tile], cs_pack(ST_P, Xc + Bc, Bp != ALP_NONE32 ? Bp : Xp));
+        for (int w2 = 0; w2 < LX_THREADS / 32; ++w2) {
+            if (w2 < warp) {
+                wc += s_wc[w2];
+                if (s_wp[w2] != ALP_NONE32) wp = s_wp[w2];
             }
-            if (lane == 0) { s_xc = Xc; s_xp = Xp; s_bc = Bc; }
+            Bc += s_wc[w2];
         }
-        __syncthreads();
+        const bool staged = Bc <= (uint32_t)LX_STAGE;
+        uint32_t tcount = Xc + wc + ec;
+        uint32_t cur = ep != ALP_NONE32 ? ep : (wp != ALP_NONE32 ? wp : Xp);
 
-        // ---- pass 2: emit ---------------------------------------------------
-        const uint32_t Xc = s_xc;
-        const bool staged = s_bc <= (uint32_t)LX_STAGE;
-        uint32_t tcount = Xc + s_wc[warp] + ec;
-        uint32_t cur = ep != ALP_NONE32 ? ep : (s_wp[warp] != ALP_NONE32 ? s_wp[warp] : s_xp);
-        long long doc = mydoc;
-        long long base = lim > 0 ? sg.doc_off[doc] : 0;
-        auto tok = [&](uint32_t term, uint32_t st_abs, uint32_t en_abs) {
-            if (staged) {
-                const uint32_t k = tcount - Xc;
-                s_term[k] = (uint16_t)term;
-                s_start[k] = st_abs;
-                s_end[k] = en_abs;
-            } else {
-                put((long long)tcount + sent * (2 * doc + 1), term, (long long)st_abs - base, (long long)en_abs - base);
-            }
-            ++tcount;
-        };
+        // ---- emit ---------------------------------------------------------------
         if (lim > 0) {
             uint32_t st = s0;
-            if (plain) {
+            if ((head | last) == 0 && lim == LX_CHUNK && staged) {
+                uint32_t k = tcount - Xc;
+                const uint32_t rel = (uint32_t)(my - t0);
 #pragma unroll
-                for (int j = 0; j < LX_ITEMS; ++j) {
+                for (int j = 0; j < LX_CHUNK; ++j) {
                     const uint32_t e = s_ent[st * LX_ROW + byte_of(w, j)];
-                    if (e & LX_EMIT) tok(s_tok[st] & TOK_TERM_MASK, cur, (uint32_t)(my + j));
+                    if (e & LX_EMIT) {
+                        s_pk[k] = (rel + j) | (s_tok[st] << 16);
+                        s_st[k] = cur;
+                        ++k;
+                    }
                     if (e & LX_START) cur = (uint32_t)(my + j);
                     st = e & LX_NEXT;
                 }
+                tcount = Xc + k;
             } else {
+                long long doc = mydoc;
+                long long base = sg.doc_off[doc];
+                auto tok = [&](uint32_t term, uint32_t st_abs, uint32_t en_abs) {
+                    if (staged) {
+                        const uint32_t k = tcount - Xc;
+                        s_pk[k] = (uint32_t)(en_abs - t0) | (term << 16);
+                        s_st[k] = st_abs;
+                    } else {
+                        put((long long)tcount + sent * (2 * doc + 1), term, (long long)st_abs - base,
+                            (long long)en_abs - base);
+                    }
+                    ++tcount;
+                };
 #pragma unroll
-                for (int j = 0; j < LX_ITEMS; ++j) {
+                for (int j = 0; j < LX_CHUNK; ++j) {
                     if (j < lim) {
                         const long long pos = my + j;
                         if ((head >> j) & 1u) {
@@ -540,11 +654,12 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
                         }
                     }
                 }
+                mydoc = doc;
             }
         }
-        if (my <= n - 1 && n - 1 < my + LX_ITEMS) {
+        if (my <= n - 1 && n - 1 < my + LX_CHUNK) {
             // documents that start at n (empty, at the end) and the closing offset
-            for (long long e2 = doc + 1; e2 < ND; ++e2) {
+            for (long long e2 = mydoc + 1; e2 < ND; ++e2) {
                 sg.tok_off[e2] = tcount;
                 sg.valid[e2] = 0;
                 if (sent) {
@@ -558,14 +673,18 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
         }
         __syncthreads();
 
-        // ---- coalesced copy of the staged tokens -----------------------------
+        // ---- coalesced copy of the staged tokens ---------------------------------
         if (staged) {
-            const uint32_t Bc = s_bc;
+            const long long b0 = sg.doc_off[d0];
             for (uint32_t k = tid; k < Bc; k += LX_THREADS) {
-                const uint32_t en = s_end[k];
-                const long long dk = dmax > d0 ? doc_upper(sg.doc_off, d0, dmax, (long long)en - 1) : d0;
-                const long long bk = sg.doc_off[dk];
-                put((long long)(Xc + k) + sent * (2 * dk + 1), s_term[k], (long long)s_start[k] - bk, (long long)en - bk);
+                const uint32_t pk = s_pk[k];
+                const long long en = t0 + (pk & 0xffffu);
+                long long dk = d0, bk = b0;
+                if (dmax > d0) {
+                    dk = doc_upper(sg.doc_off, d0, dmax, en - 1);
+                    bk = sg.doc_off[dk];
+                }
+                put((long long)(Xc + k) + sent * (2 * dk + 1), pk >> 16, (long long)s_st[k] - bk, en - bk);
             }
         }
         __syncthreads();
