@@ -387,7 +387,8 @@ int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_
     const size_t o_vec = 256, o_cs = o_vec + al(128 * (size_t)stiles), o_f = o_cs + al(8 * (size_t)tiles);
     const size_t o_s = o_f + al(2 * (size_t)chunks + 64), o_c = o_s + al((size_t)chunks + 64);
     const size_t o_td = o_c + al(2 * (size_t)chunks + 64);
-    const size_t sbytes = o_td + al(8 * (size_t)tiles);
+    const size_t o_ccs = o_td + al(8 * (size_t)tiles);
+    const size_t sbytes = o_ccs + al(8 * ((size_t)tiles / LT_CHUNK + 2));
     int rc;
     if ((rc = grow(ctx, ctx->scratch, sbytes))) return rc;
     uint8_t* base = reinterpret_cast<uint8_t*>(ctx->scratch.p);
@@ -461,9 +462,15 @@ int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_
     lex3_count_kernel<<<g3, LX_THREADS, ctx->l3_count_smem, ctx->stream>>>(a, sg);
     CK(cudaGetLastError());
     mark(ctx, "lex3_count_kernel");
-    lex3_tile_scan_kernel<<<1, 1024, 0, ctx->stream>>>(a.tile_cs, tiles);
-    CK(cudaGetLastError());
-    mark(ctx, "lex3_tile_scan_kernel");
+    {
+        const long long lchunks = (tiles + LT_CHUNK - 1) / LT_CHUNK;
+        unsigned long long* ccs = reinterpret_cast<unsigned long long*>(base + o_ccs);
+        lex3_tile_reduce_kernel<<<(unsigned)lchunks, LT_CHUNK, 0, ctx->stream>>>(a.tile_cs, tiles, ccs);
+        CK(cudaGetLastError());
+        lex3_tile_scan_kernel<<<(unsigned)lchunks, LT_CHUNK, 0, ctx->stream>>>(a.tile_cs, tiles, ccs);
+        CK(cudaGetLastError());
+    }
+    mark(ctx, "lex3_tile_reduce+lex3_tile_scan");
     k5<<<g5, LX_THREADS, ctx->l3_emit_smem, ctx->stream>>>(a, sg);
     CK(cudaGetLastError());
     mark(ctx, "lex3_emit_kernel");
@@ -565,7 +572,7 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     *n_node = 0;
     const long long tiles = (L + PP_TILE - 1) / PP_TILE;
     int rc;
-    if ((rc = grow(ctx, ctx->tmp[T_PID], (size_t)L * 2 + 64)) || (rc = grow(ctx, ctx->tmp[T_TSUMS], tiles * sizeof(PosSums))) ||
+    if ((rc = grow(ctx, ctx->tmp[T_PID], (size_t)L * 2 + 64)) || (rc = grow(ctx, ctx->tmp[T_TSUMS], (tiles + tiles / ST_CHUNK + 2) * sizeof(PosSums))) ||
         (rc = grow(ctx, ctx->tmp[T_NODEOFF], (size_t)(nd + 1) * 8)) || (rc = grow(ctx, ctx->tmp[T_BROFF], (size_t)(nd + 1) * 8)) ||
         (rc = grow(ctx, ctx->scratch, 256)))
         return rc;
@@ -591,9 +598,16 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     parse_pairs_kernel<<<(unsigned)tiles, PP_THREADS, sm1, ctx->stream>>>(a);
     CK(cudaGetLastError());
     mark(ctx, "parse_pairs_kernel");
-    scan_tiles_kernel<<<1, 1024, 0, ctx->stream>>>(a.tile_sums, tiles, d_res, a.node_off, a.br_off, nd);
-    CK(cudaGetLastError());
-    mark(ctx, "scan_tiles_kernel");
+    {
+        const long long chunks = (tiles + ST_CHUNK - 1) / ST_CHUNK;
+        PosSums* csum = a.tile_sums + tiles;  // chunk sums after the tile sums
+        scan_tiles_reduce_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum);
+        CK(cudaGetLastError());
+        scan_tiles_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum, d_res, a.node_off,
+                                                                         a.br_off, nd);
+        CK(cudaGetLastError());
+    }
+    mark(ctx, "scan_tiles_reduce+scan_tiles");
     if ((rc = read_result(ctx, d_res))) return rc;
     const long long N = ctx->h_res->aux[0], B = ctx->h_res->aux[1];
     if (N > 0xffffffffLL || B > 0xffffffffLL) return fail(ctx, ALP_ERR_ARG, "tree too large");

@@ -18,7 +18,8 @@
 //                      chunks from their known states with a 256-column table
 //                      whose entries carry the produce/ignore decisions, and
 //                      stores the chunk's token count and last token start.
-//   lex3_tile_scan_kernel  exclusive (count, last start) over 8 KiB tiles, the
+//   lex3_tile_reduce_kernel, lex3_tile_scan_kernel  exclusive (count, last
+//                      start) over 8 KiB tiles, the
 //                      take_right start scan and the compaction offsets
 //                      (futhark/lexer.fut:83-84,108-120) at tile level.
 //   lex3_emit_kernel   the compaction (futhark/lexer.fut:121-133): places each
@@ -464,18 +465,58 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_count_kernel(Lex3Args a, L
 }
 
 // ---- kernel 4: exclusive (count, last start) over tiles ---------------------
-// One CTA of 1024 threads.  Tile 0 starts from (0, 0).
-__global__ void __launch_bounds__(1024) lex3_tile_scan_kernel(unsigned long long* tile_cs, long long T) {
-    __shared__ uint32_t s_c[32], s_p[32];
+// Two launches over chunks of LT_CHUNK tiles: the chunk sums, then one CTA per
+// chunk scans the chunk sums before its own and its own tiles in place.
+// Tile 0 starts from (0, 0).
+constexpr int LT_CHUNK = 1024;
+
+__device__ __forceinline__ void cs_unpack(unsigned long long v, uint32_t& c, uint32_t& p) {
+    c = (uint32_t)(v >> 32);
+    p = (uint32_t)v;
+}
+
+__global__ void __launch_bounds__(LT_CHUNK) lex3_tile_reduce_kernel(const unsigned long long* tile_cs, long long T,
+                                                                    unsigned long long* chunk_cs) {
+    __shared__ uint32_t s_c[LT_CHUNK / 32], s_p[LT_CHUNK / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const long long per = (T + 1023) / 1024;
-    const long long lo = min(T, (long long)tid * per), hi = min(T, lo + per);
+    const long long i = (long long)blockIdx.x * LT_CHUNK + tid;
     uint32_t c = 0, p = ALP_NONE32;
-    for (long long i = lo; i < hi; ++i) {
-        const unsigned long long v = tile_cs[i];
-        c += (uint32_t)(v >> 32);
-        if ((uint32_t)v != ALP_NONE32) p = (uint32_t)v;
+    if (i < T) cs_unpack(tile_cs[i], c, p);
+    cs_reduce_warp(c, p);
+    if (lane == 0) { s_c[warp] = c; s_p[warp] = p; }
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t tc = 0, tp = ALP_NONE32;
+        for (int w = 0; w < LT_CHUNK / 32; ++w) {
+            tc += s_c[w];
+            if (s_p[w] != ALP_NONE32) tp = s_p[w];
+        }
+        chunk_cs[blockIdx.x] = ((unsigned long long)tc << 32) | tp;
     }
+}
+
+__global__ void __launch_bounds__(LT_CHUNK) lex3_tile_scan_kernel(unsigned long long* tile_cs, long long T,
+                                                                  const unsigned long long* chunk_cs) {
+    __shared__ uint32_t s_c[LT_CHUNK / 32], s_p[LT_CHUNK / 32];
+    __shared__ uint32_t s_cc, s_cp;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long chunk = blockIdx.x;
+    if (warp == 0) {
+        uint32_t cc = 0, cp = ALP_NONE32;
+        for (long long b = 0; b < chunk; b += 32) {
+            uint32_t c = 0, p = ALP_NONE32;
+            if (b + lane < chunk) cs_unpack(chunk_cs[b + lane], c, p);
+            cs_reduce_warp(c, p);
+            c = __shfl_sync(ALP_FULL_MASK, c, 0);
+            p = __shfl_sync(ALP_FULL_MASK, p, 0);
+            cc += c;
+            if (p != ALP_NONE32) cp = p;
+        }
+        if (lane == 0) { s_cc = cc; s_cp = cp; }
+    }
+    const long long i = chunk * LT_CHUNK + tid;
+    uint32_t c = 0, p = ALP_NONE32;
+    if (i < T) cs_unpack(tile_cs[i], c, p);
     uint32_t ic = c, ip = p;
     warp_scan_cs(ic, ip, lane);
     if (lane == 31) { s_c[warp] = ic; s_p[warp] = ip; }
@@ -491,14 +532,9 @@ __global__ void __launch_bounds__(1024) lex3_tile_scan_kernel(unsigned long long
     __syncthreads();
     uint32_t ec = __shfl_up_sync(ALP_FULL_MASK, ic, 1), ep = __shfl_up_sync(ALP_FULL_MASK, ip, 1);
     if (lane == 0) { ec = 0; ep = ALP_NONE32; }
-    uint32_t rc = s_c[warp] + ec;
-    uint32_t rp = ep != ALP_NONE32 ? ep : s_p[warp];
-    for (long long i = lo; i < hi; ++i) {
-        const unsigned long long v = tile_cs[i];
-        tile_cs[i] = ((unsigned long long)rc << 32) | (rp != ALP_NONE32 ? rp : 0u);
-        rc += (uint32_t)(v >> 32);
-        if ((uint32_t)v != ALP_NONE32) rp = (uint32_t)v;
-    }
+    const uint32_t rc = s_cc + s_c[warp] + ec;
+    uint32_t rp = ep != ALP_NONE32 ? ep : (s_p[warp] != ALP_NONE32 ? s_p[warp] : s_cp);
+    if (i < T) tile_cs[i] = ((unsigned long long)rc << 32) | (rp != ALP_NONE32 ? rp : 0u);
 }
 
 // ---- kernel 5: tokens ---------------------------------------------------------

@@ -180,7 +180,7 @@ inline int load_parser(ParseTables& pt, ParseHost& ph, const uint8_t* p, const u
 namespace alp {
 
 constexpr int PP_THREADS = 256;
-constexpr int PP_ITEMS = 8;                        // positions per thread
+constexpr int PP_ITEMS = 4;                        // positions per thread
 constexpr int PP_TILE = PP_THREADS * PP_ITEMS;     // positions per tile
 constexpr int PLE_THREADS = 256;
 constexpr int PLE_ITEMS = 16;
@@ -330,13 +330,12 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
         if (i < a.L) acc = ps_combine(acc, ps_elem(s_pi, p, head, i));
     }
     const long long i0 = base + tid * PP_ITEMS;
-    if (i0 + PP_ITEMS <= a.L && ((i0 & 7) == 0)) {
-        uint4 w;
+    if (i0 + PP_ITEMS <= a.L && ((i0 & 3) == 0)) {
+        static_assert(PP_ITEMS == 4, "pair ids are stored as one 8-byte word per thread");
+        uint2 w;
         w.x = ids[0] | ((uint32_t)ids[1] << 16);
         w.y = ids[2] | ((uint32_t)ids[3] << 16);
-        w.z = ids[4] | ((uint32_t)ids[5] << 16);
-        w.w = ids[6] | ((uint32_t)ids[7] << 16);
-        *reinterpret_cast<uint4*>(a.pid + i0) = w;
+        *reinterpret_cast<uint2*>(a.pid + i0) = w;
     } else {
         for (int j = 0; j < PP_ITEMS; ++j)
             if (i0 + j < a.L) a.pid[i0 + j] = ids[j];
@@ -352,97 +351,125 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
     }
 }
 
-// Exclusive segmented scan of the tile sums in place (one block); totals to
-// res->aux (nodes, brackets, final depth, -, -, heads) and the closing entries
-// of node_off / br_off.
-__global__ void __launch_bounds__(1024) scan_tiles_kernel(PosSums* s, long long tiles, AlpResult* res,
-                                                          long long* node_off, long long* br_off,
-                                                          long long n_docs) {
-    __shared__ PosSums s_w[32];
+// Exclusive segmented scan of the tile sums in place, in two launches:
+// scan_tiles_reduce_kernel sums each chunk of ST_CHUNK tiles, then
+// scan_tiles_kernel (one CTA per chunk) scans the chunk sums before its own
+// and its own tiles.  Totals go to res->aux (nodes, brackets, final depth, -,
+// -, heads) and the closing entries of node_off / br_off.
+constexpr int ST_CHUNK = 1024;
+
+__device__ __forceinline__ PosSums ps_block_reduce(PosSums v, PosSums* s_w) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    PosSums inc = ps_warp_scan(v, lane);
+    if (lane == 31) s_w[warp] = inc;
+    __syncthreads();
+    PosSums t = s_w[0];
+    for (int w = 1; w < (int)(blockDim.x / 32); ++w) t = ps_combine(t, s_w[w]);
+    return t;
+}
+
+__global__ void __launch_bounds__(ST_CHUNK) scan_tiles_reduce_kernel(const PosSums* s, long long tiles,
+                                                                     PosSums* chunk_sums) {
+    __shared__ PosSums s_w[ST_CHUNK / 32];
+    const long long idx = (long long)blockIdx.x * ST_CHUNK + threadIdx.x;
+    PosSums v;
+    if (idx < tiles) v = s[idx]; else possums_zero(v);
+    const PosSums t = ps_block_reduce(v, s_w);
+    if (threadIdx.x == 0) chunk_sums[blockIdx.x] = t;
+}
+
+__global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long long tiles, const PosSums* chunk_sums,
+                                                              AlpResult* res, long long* node_off, long long* br_off,
+                                                              long long n_docs) {
+    __shared__ PosSums s_w[ST_CHUNK / 32];
     __shared__ PosSums s_carry;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) possums_zero(s_carry);
-    __syncthreads();
-    for (long long b = 0; b < tiles; b += 1024) {
-        PosSums v;
-        if (b + tid < tiles) v = s[b + tid]; else possums_zero(v);
-        PosSums inc = ps_warp_scan(v, lane);
-        PosSums ex = ps_shfl_up(inc, 1);
-        if (lane == 0) possums_zero(ex);
-        if (lane == 31) s_w[warp] = inc;
-        __syncthreads();
-        if (warp == 0) {
-            PosSums w = s_w[lane];
-            PosSums wi = ps_warp_scan(w, lane);
-            PosSums we = ps_shfl_up(wi, 1);
-            if (lane == 0) possums_zero(we);
-            s_w[lane] = we;
+    const long long chunk = blockIdx.x;
+    if (warp == 0) {
+        PosSums carry;
+        possums_zero(carry);
+        for (long long b = 0; b < chunk; b += 32) {
+            PosSums v;
+            if (b + lane < chunk) v = chunk_sums[b + lane]; else possums_zero(v);
+            const PosSums inc = ps_warp_scan(v, lane);
+            PosSums last;
+            last.nodes = __shfl_sync(ALP_FULL_MASK, inc.nodes, 31);
+            last.brs = __shfl_sync(ALP_FULL_MASK, inc.brs, 31);
+            last.depth = __shfl_sync(ALP_FULL_MASK, inc.depth, 31);
+            last.v = __shfl_sync(ALP_FULL_MASK, inc.v, 31);
+            last.terms = __shfl_sync(ALP_FULL_MASK, inc.terms, 31);
+            last.heads = __shfl_sync(ALP_FULL_MASK, inc.heads, 31);
+            last.hpos = __shfl_sync(ALP_FULL_MASK, inc.hpos, 31);
+            last.pad = 0;
+            carry = ps_combine(carry, last);
         }
-        __syncthreads();
-        const PosSums pre = ps_combine(s_carry, s_w[warp]);
-        if (b + tid < tiles) s[b + tid] = ps_combine(pre, ex);
-        __syncthreads();
-        if (tid == 1023) s_carry = ps_combine(pre, inc);
-        __syncthreads();
+        if (lane == 0) s_carry = carry;
     }
-    if (tid == 0) {
-        res->aux[0] = (long long)s_carry.nodes;
-        res->aux[1] = (long long)s_carry.brs;
-        res->aux[2] = s_carry.depth;
-        res->aux[3] = s_carry.v;
-        res->aux[4] = (long long)s_carry.terms;
-        res->aux[5] = (long long)s_carry.heads;
-        node_off[n_docs] = (long long)s_carry.nodes;
-        br_off[n_docs] = (long long)s_carry.brs;
+    const long long idx = chunk * ST_CHUNK + tid;
+    PosSums v;
+    if (idx < tiles) v = s[idx]; else possums_zero(v);
+    PosSums inc = ps_warp_scan(v, lane);
+    PosSums ex = ps_shfl_up(inc, 1);
+    if (lane == 0) possums_zero(ex);
+    if (lane == 31) s_w[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        PosSums w = s_w[lane];
+        PosSums wi = ps_warp_scan(w, lane);
+        PosSums we = ps_shfl_up(wi, 1);
+        if (lane == 0) possums_zero(we);
+        s_w[lane] = we;
+    }
+    __syncthreads();
+    const PosSums pre = ps_combine(s_carry, s_w[warp]);
+    if (idx < tiles) s[idx] = ps_combine(pre, ex);
+    if (chunk == gridDim.x - 1 && tid == ST_CHUNK - 1) {
+        const PosSums tot = ps_combine(pre, inc);
+        res->aux[0] = (long long)tot.nodes;
+        res->aux[1] = (long long)tot.brs;
+        res->aux[2] = tot.depth;
+        res->aux[3] = tot.v;
+        res->aux[4] = (long long)tot.terms;
+        res->aux[5] = (long long)tot.heads;
+        node_off[n_docs] = (long long)tot.nodes;
+        br_off[n_docs] = (long long)tot.brs;
     }
 }
 
 // ---------------------------------------------------------------------------
 // K2: expand every position's productions and brackets
 //
-// One tile = PP_TILE positions.  The block scans the per-position sums into
-// shared memory, then hands out output elements (nodes, then brackets)
-// round-robin over threads: element e of the tile finds its position by binary
-// search over the scanned offsets, so consecutive threads write consecutive
-// nodes and every output store is coalesced.
+// One tile = PP_TILE positions.  The block scans the per-position sums; each
+// thread then walks its positions and writes their nodes (first pass) and
+// brackets (second pass) into a shared-memory stage at their tile offsets,
+// and the block copies the stage out with coalesced stores.  A tile with
+// more nodes or brackets than the stage holds writes them directly.
 // ---------------------------------------------------------------------------
-constexpr size_t EXPAND_SMEM_POS = (size_t)PP_TILE * (4 * 7 + 2) + 16;
+constexpr int EX_STAGE_BYTES = 33792;
+constexpr int EX_NCAP = EX_STAGE_BYTES / 12;  // nodes: value, tag | kind << 31, token index
+constexpr int EX_BCAP = EX_STAGE_BYTES / 8;   // brackets: symbol, depth value
+constexpr uint32_t EX_NO_TOKEN = 0xffffffffu;
 
 __host__ __device__ inline size_t expand_smem_bytes(int n_pairs, int n_prods) {
-    return ((sizeof(PairInfo) * n_pairs + (size_t)n_prods * 8 + 15) & ~(size_t)15) + EXPAND_SMEM_POS;
+    return ((sizeof(PairInfo) * n_pairs + (size_t)n_prods * 4 + 15) & ~(size_t)15) + EX_STAGE_BYTES;
 }
 
-// largest p in [0, n) with off[p] <= e  (off ascending, off[0] = 0)
-__device__ __forceinline__ int find_pos(const uint32_t* off, int n, uint32_t e) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (off[mid] <= e) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
-__global__ void __launch_bounds__(PP_THREADS) parse_expand_kernel(ParseArgs a) {
+__global__ void __launch_bounds__(PP_THREADS, 4) parse_expand_kernel(ParseArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     PairInfo* s_pi = reinterpret_cast<PairInfo*>(smem);
-    int32_t* s_ar = reinterpret_cast<int32_t*>(smem + sizeof(PairInfo) * a.t.n_pairs);
-    int32_t* s_pt = s_ar + a.t.n_prods;
-    uint8_t* pbase = smem + ((sizeof(PairInfo) * a.t.n_pairs + (size_t)a.t.n_prods * 8 + 15) & ~(size_t)15);
-    uint32_t* s_noff = reinterpret_cast<uint32_t*>(pbase);            // node offset in tile
-    uint32_t* s_boff = s_noff + PP_TILE;                              // bracket offset in tile
-    int32_t* s_dep = reinterpret_cast<int32_t*>(s_boff + PP_TILE);    // depth before position
-    int32_t* s_v = s_dep + PP_TILE;                                   // v before position
-    uint32_t* s_tr = reinterpret_cast<uint32_t*>(s_v + PP_TILE);      // terminal rank before position
-    uint32_t* s_hp = s_tr + PP_TILE;                                  // ⊢ position of its document
-    uint32_t* s_doc = s_hp + PP_TILE;                                 // document index
-    uint16_t* s_pid = reinterpret_cast<uint16_t*>(s_doc + PP_TILE);
+    int32_t* s_pt = reinterpret_cast<int32_t*>(smem + sizeof(PairInfo) * a.t.n_pairs);
+    uint8_t* stage = smem + ((sizeof(PairInfo) * a.t.n_pairs + (size_t)a.t.n_prods * 4 + 15) & ~(size_t)15);
+    int32_t* s_nv = reinterpret_cast<int32_t*>(stage);
+    uint32_t* s_ntag = reinterpret_cast<uint32_t*>(s_nv + EX_NCAP);
+    uint32_t* s_nti = s_ntag + EX_NCAP;
+    uint32_t* s_bsym = reinterpret_cast<uint32_t*>(stage);
+    int32_t* s_bds = reinterpret_cast<int32_t*>(s_bsym + EX_BCAP);
     __shared__ PosSums s_w[PP_THREADS / 32];
     __shared__ uint32_t s_tn, s_tb;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < a.t.n_pairs * (int)(sizeof(PairInfo) / 4); i += PP_THREADS)
         reinterpret_cast<uint32_t*>(s_pi)[i] = reinterpret_cast<const uint32_t*>(a.t.pairs)[i];
-    for (int i = tid; i < a.t.n_prods; i += PP_THREADS) { s_ar[i] = a.t.arity[i]; s_pt[i] = a.t.prod_term[i]; }
-    __syncthreads();
+    for (int i = tid; i < a.t.n_prods; i += PP_THREADS) s_pt[i] = a.t.prod_term[i];
     const uint32_t SL = a.t.start, SR = a.t.end;
     const long long tbase = (long long)blockIdx.x * PP_TILE;
     const long long i0 = tbase + tid * PP_ITEMS;
@@ -458,6 +485,7 @@ __global__ void __launch_bounds__(PP_THREADS) parse_expand_kernel(ParseArgs a) {
             if (c == SR) em |= 1u << j;
         }
     }
+    __syncthreads();
     PosSums mine;
     possums_zero(mine);
 #pragma unroll
@@ -479,89 +507,145 @@ __global__ void __launch_bounds__(PP_THREADS) parse_expand_kernel(ParseArgs a) {
     }
     __syncthreads();
     const PosSums tp = a.tile_sums[blockIdx.x];
+    const PosSums run0 = ps_combine(ps_combine(tp, s_w[warp]), ex);  // before this thread's first position
+    const uint32_t tn = s_tn, tb = s_tb;
+    const bool nst = tn <= (uint32_t)EX_NCAP, bst = tb <= (uint32_t)EX_BCAP;
+
+    // ---- nodes -------------------------------------------------------------------
     {
-        PosSums run = ps_combine(ps_combine(tp, s_w[warp]), ex);  // before this thread's first position
-        const uint32_t nd0 = (uint32_t)(run.nodes - tp.nodes), bi0 = (uint32_t)(run.brs - tp.brs);
-        uint32_t nd = nd0, bi = bi0;
+        PosSums run = run0;
+        uint32_t nd = (uint32_t)(run.nodes - tp.nodes);
 #pragma unroll
         for (int j = 0; j < PP_ITEMS; ++j) {
-            const int o = tid * PP_ITEMS + j;
             const long long i = i0 + j;
-            const bool head = (hm >> j) & 1u;
-            s_noff[o] = nd;
-            s_boff[o] = bi;
-            s_pid[o] = ids[j];
             if (i < a.L) {
+                const bool head = (hm >> j) & 1u;
                 const long long dep = head ? 0 : run.depth;
-                const long long v = head ? 0 : run.v;
-                const unsigned long long tr = head ? 0 : run.terms;
-                const long long hp = head ? i : run.hpos;
+                const int32_t v = head ? 0 : (int32_t)run.v;
+                const uint32_t tr = head ? 0u : (uint32_t)run.terms;
+                const uint32_t hp = (uint32_t)(head ? i : run.hpos);
                 const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
-                s_dep[o] = (int32_t)dep; s_v[o] = (int32_t)v; s_tr[o] = (uint32_t)tr;
-                s_hp[o] = (uint32_t)hp; s_doc[o] = (uint32_t)doc;
-                if (head && doc >= 0 && doc < a.n_docs) {
+                const bool dok = doc >= 0 && doc < a.n_docs;
+                if (head && dok) {
                     a.node_off[doc] = (long long)(tp.nodes + nd);
-                    a.br_off[doc] = (long long)(tp.brs + bi);
+                    a.br_off[doc] = (long long)(run.brs);
                 }
                 int32_t dd = 0;
                 if (ids[j] == NO_PAIR) {
-                    if (doc >= 0 && doc < a.n_docs) a.doc_valid[doc] = 0;  // no admissible pair
+                    if (dok) a.doc_valid[doc] = 0;  // no admissible pair
                 } else {
-                    const PairInfo& pi = s_pi[ids[j]];
-                    nd += pi.n_prod; bi += pi.n_br; dd = pi.d_depth;
+                    const PairInfo pi = s_pi[ids[j]];
+                    dd = pi.d_depth;
+                    for (uint32_t r = 0; r < pi.n_prod; ++r) {
+                        const uint32_t jj = pi.prod_begin + r;
+                        const uint32_t prod = __ldg(&a.t.pseq[jj]);
+                        const int32_t pt = s_pt[prod];
+                        const int32_t vv = v + __ldg(&a.t.pseq_v[jj]);
+                        uint32_t tagk = prod, ti = EX_NO_TOKEN;
+                        if (pt >= 0 && a.subst_terminals) {
+                            // the k-th terminal production of a document takes its k-th token's span
+                            tagk = (uint32_t)pt | 0x80000000u;
+                            ti = hp + 1 + tr + (uint32_t)__ldg(&a.t.pseq_t[jj]);
+                        }
+                        if (nst) {
+                            s_nv[nd] = vv;
+                            s_ntag[nd] = tagk;
+                            s_nti[nd] = ti;
+                        } else {
+                            const unsigned long long ndg = tp.nodes + nd;
+                            if ((long long)ndg < a.cap_nodes) {
+                                a.vbuf[ndg] = vv;
+                                a.tag[ndg] = tagk & 0x7fffffffu;
+                                a.kind[ndg] = (uint8_t)(tagk >> 31);
+                                a.nstart[ndg] = ti < a.L ? (int64_t)__ldg(&a.pstart[ti]) : 0;
+                                a.nend[ndg] = ti < a.L ? (int64_t)__ldg(&a.pend[ti]) : 0;
+                            }
+                        }
+                        ++nd;
+                    }
                 }
-                if (((em >> j) & 1u) && (dep + dd != 0) && doc >= 0 && doc < a.n_docs)
-                    a.doc_valid[doc] = 0;  // unbalanced at the end
+                if (((em >> j) & 1u) && (dep + dd != 0) && dok) a.doc_valid[doc] = 0;  // unbalanced at the end
                 run = ps_combine(run, ps_elem(s_pi, ids[j], head, i));
-            } else {
-                s_dep[o] = 0; s_v[o] = 0; s_tr[o] = 0; s_hp[o] = 0; s_doc[o] = 0;
             }
         }
     }
     __syncthreads();
-    const uint32_t tn = s_tn, tb = s_tb;
-    const unsigned long long nbase = tp.nodes, bbase = tp.brs;
-    for (uint32_t e = tid; e < tn; e += PP_THREADS) {
-        const int p = find_pos(s_noff, PP_TILE, e);
-        if (s_pid[p] == NO_PAIR) continue;
-        const PairInfo& pi = s_pi[s_pid[p]];
-        const uint32_t j = pi.prod_begin + (e - s_noff[p]);
-        const uint32_t prod = __ldg(&a.t.pseq[j]);
-        const int32_t pt = s_pt[prod];
-        const unsigned long long nd = nbase + e;
-        if ((long long)nd >= a.cap_nodes) break;
-        a.vbuf[nd] = s_v[p] + __ldg(&a.t.pseq_v[j]);
-        if (pt >= 0 && a.subst_terminals) {
-            // the k-th terminal production of a document takes its k-th token's span
-            const long long ti = (long long)s_hp[p] + 1 + s_tr[p] + (uint32_t)__ldg(&a.t.pseq_t[j]);
-            a.tag[nd] = (uint32_t)pt;
-            a.kind[nd] = 1;
-            a.nstart[nd] = ti < a.L ? (int64_t)__ldg(&a.pstart[ti]) : 0;
-            a.nend[nd] = ti < a.L ? (int64_t)__ldg(&a.pend[ti]) : 0;
-        } else {
-            a.tag[nd] = prod;
-            a.kind[nd] = 0;
-            a.nstart[nd] = 0;
-            a.nend[nd] = 0;
+    if (nst) {
+        for (uint32_t e0 = tid; e0 < tn; e0 += 2 * PP_THREADS) {
+            uint32_t tk[2], tix[2];
+            int32_t vv[2];
+            int64_t st[2], en[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const uint32_t e = e0 + u * PP_THREADS;
+                tk[u] = 0; tix[u] = EX_NO_TOKEN; vv[u] = 0; st[u] = 0; en[u] = 0;
+                if (e < tn) { vv[u] = s_nv[e]; tk[u] = s_ntag[e]; tix[u] = s_nti[e]; }
+                if (tix[u] < a.L) { st[u] = __ldg(&a.pstart[tix[u]]); en[u] = __ldg(&a.pend[tix[u]]); }
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const uint32_t e = e0 + u * PP_THREADS;
+                const unsigned long long ndg = tp.nodes + e;
+                if (e < tn && (long long)ndg < a.cap_nodes) {
+                    a.vbuf[ndg] = vv[u];
+                    a.tag[ndg] = tk[u] & 0x7fffffffu;
+                    a.kind[ndg] = (uint8_t)(tk[u] >> 31);
+                    a.nstart[ndg] = st[u];
+                    a.nend[ndg] = en[u];
+                }
+            }
         }
     }
-    for (uint32_t e = tid; e < tb; e += PP_THREADS) {
-        const int p = find_pos(s_boff, PP_TILE, e);
-        if (s_pid[p] == NO_PAIR) continue;
-        const PairInfo& pi = s_pi[s_pid[p]];
-        const uint32_t j = pi.stack_begin + (e - s_boff[p]);
-        const uint32_t sym = __ldg(&a.t.stack[j]);
-        const int32_t before = s_dep[p] + __ldg(&a.t.stack_d[j]);
-        int32_t ds;
-        if (sym >> 31) ds = before;
-        else {
-            ds = before - 1;
-            if (ds < 0 && (long long)s_doc[p] < a.n_docs) a.doc_valid[s_doc[p]] = 0;  // depth below zero
+    __syncthreads();
+
+    // ---- brackets ----------------------------------------------------------------
+    {
+        PosSums run = run0;
+        uint32_t bi = (uint32_t)(run.brs - tp.brs);
+#pragma unroll
+        for (int j = 0; j < PP_ITEMS; ++j) {
+            const long long i = i0 + j;
+            if (i < a.L) {
+                const bool head = (hm >> j) & 1u;
+                const int32_t dep = head ? 0 : (int32_t)run.depth;
+                const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
+                if (ids[j] != NO_PAIR) {
+                    const PairInfo pi = s_pi[ids[j]];
+                    for (uint32_t r = 0; r < pi.n_br; ++r) {
+                        const uint32_t jj = pi.stack_begin + r;
+                        const uint32_t sym = __ldg(&a.t.stack[jj]);
+                        const int32_t before = dep + __ldg(&a.t.stack_d[jj]);
+                        int32_t ds;
+                        if (sym >> 31) ds = before;
+                        else {
+                            ds = before - 1;
+                            if (ds < 0 && doc >= 0 && doc < a.n_docs) a.doc_valid[doc] = 0;  // depth below zero
+                        }
+                        if (bst) {
+                            s_bsym[bi] = sym;
+                            s_bds[bi] = ds;
+                        } else {
+                            const unsigned long long big = tp.brs + bi;
+                            if ((long long)big < a.cap_brs) {
+                                a.brbuf[big] = sym;
+                                a.dsbuf[big] = ds;
+                            }
+                        }
+                        ++bi;
+                    }
+                }
+                run = ps_combine(run, ps_elem(s_pi, ids[j], head, i));
+            }
         }
-        const unsigned long long bi = bbase + e;
-        if ((long long)bi >= a.cap_brs) break;
-        a.brbuf[bi] = sym;
-        a.dsbuf[bi] = ds;
+    }
+    __syncthreads();
+    if (bst) {
+        for (uint32_t e = tid; e < tb; e += PP_THREADS) {
+            const unsigned long long big = tp.brs + e;
+            if ((long long)big >= a.cap_brs) break;
+            a.brbuf[big] = s_bsym[e];
+            a.dsbuf[big] = s_bds[e];
+        }
     }
 }
 
@@ -586,9 +670,14 @@ struct PleArgs {
     AlpResult* res;
 };
 
-// Shared memory: a min tree over the tile (leaves at PLE_TILE..2*PLE_TILE-1)
-// and, for brackets, the symbols.
-constexpr size_t PLE_SMEM = (size_t)(2 * PLE_TILE + PLE_TILE) * 4;
+// Shared memory: the tile's values and a second array (bracket symbols, or
+// node results) with one pad word after every thread's PLE_ITEMS, so that a
+// warp reading element k of its threads' chunks hits 32 different banks; the
+// minima of each chunk's four quarters; a min tree over the PLE_THREADS chunk
+// minima (leaves at PLE_THREADS..2*PLE_THREADS-1); a query queue per warp.
+constexpr int PLE_STRIDE = PLE_ITEMS + 1;
+constexpr size_t PLE_SMEM = (size_t)(2 * PLE_THREADS * PLE_STRIDE + 2 * PLE_THREADS) * 4 +
+                            (size_t)PLE_THREADS * 16 + (size_t)PLE_TILE * 2;
 
 // largest d in [lo, hi] with off[d] <= g
 __device__ __forceinline__ long long seg_upper(const long long* off, long long lo, long long hi, long long g) {
@@ -599,95 +688,193 @@ __device__ __forceinline__ long long seg_upper(const long long* off, long long l
     return lo;
 }
 
-// Each thread owns PLE_ITEMS consecutive elements.  It answers them against
-// its own earlier elements in registers first; the rest walk a shared-memory
-// min tree of the tile (up to the nearest left subtree holding a value <= x,
-// then down to its last such leaf).  Elements smaller than everything before
-// them in the tile escape to ple_escape_kernel.
-__global__ void __launch_bounds__(PLE_THREADS) ple_tile_kernel(PleArgs a) {
+__device__ __forceinline__ int ple_pad(int e) { return (e / PLE_ITEMS) * PLE_STRIDE + (e % PLE_ITEMS); }
+
+// Each thread owns PLE_ITEMS consecutive elements.  An element's answer is
+// (1) its thread's last earlier element <= x (branch-free compares in
+// registers), else (2) the last element <= x in the nearest earlier chunk
+// whose minimum is <= x: a per-warp queue of these queries runs 32 at a time
+// through one copy of the search (min tree up and down, then the chunk's
+// quarter minima, then four elements), else (3) in an earlier tile:
+// ple_escape_kernel.  Node parents are staged in shared memory and written
+// with coalesced stores.
+__global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
-    int32_t* tree = reinterpret_cast<int32_t*>(smem);
-    uint32_t* s_sym = reinterpret_cast<uint32_t*>(smem + 2 * PLE_TILE * 4);
+    int32_t* s_val = reinterpret_cast<int32_t*>(smem);                        // [PLE_THREADS * PLE_STRIDE]
+    int32_t* s_aux = s_val + PLE_THREADS * PLE_STRIDE;                         // symbols / results
+    int32_t* tree = s_aux + PLE_THREADS * PLE_STRIDE;                          // [2 * PLE_THREADS]
+    int4* s_sub = reinterpret_cast<int4*>(tree + 2 * PLE_THREADS);             // [PLE_THREADS] quarter minima
+    uint16_t* s_q = reinterpret_cast<uint16_t*>(s_sub + PLE_THREADS);          // [PLE_TILE] query queues
     __shared__ int32_t s_suf[PLE_THREADS];
+    __shared__ int32_t s_wm[PLE_THREADS / 32];
     __shared__ uint32_t s_cnt[PLE_THREADS / 32];
     __shared__ long long s_sd0, s_sd1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long long base = (long long)blockIdx.x * PLE_TILE;
     const bool brackets = a.sym != nullptr;
-    for (int j = tid; j < PLE_TILE; j += PLE_THREADS) {
-        const long long g = base + j;
-        tree[PLE_TILE + j] = g < a.n ? a.val[g] : INT32_MAX;
-        if (brackets) s_sym[j] = g < a.n ? a.sym[g] : 0u;
+    const long long gfirst = base + (long long)tid * PLE_ITEMS;
+    const int lim = (int)max(0ll, min((long long)PLE_ITEMS, a.n - gfirst));  // valid elements of this thread
+
+    // ---- this thread's values (and symbols) --------------------------------
+    int32_t v[PLE_ITEMS];
+    if (lim == PLE_ITEMS) {
+        const int4* src = reinterpret_cast<const int4*>(a.val + gfirst);
+#pragma unroll
+        for (int q = 0; q < PLE_ITEMS / 4; ++q) {
+            const int4 x = __ldg(src + q);
+            v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < PLE_ITEMS; ++i) v[i] = i < lim ? a.val[gfirst + i] : INT32_MAX;
+    }
+#pragma unroll
+    for (int i = 0; i < PLE_ITEMS; ++i) s_val[tid * PLE_STRIDE + i] = v[i];
+    if (brackets) {
+        if (lim == PLE_ITEMS) {
+            const uint4* src = reinterpret_cast<const uint4*>(a.sym + gfirst);
+#pragma unroll
+            for (int q = 0; q < PLE_ITEMS / 4; ++q) {
+                const uint4 x = __ldg(src + q);
+                s_aux[tid * PLE_STRIDE + 4 * q] = (int32_t)x.x;
+                s_aux[tid * PLE_STRIDE + 4 * q + 1] = (int32_t)x.y;
+                s_aux[tid * PLE_STRIDE + 4 * q + 2] = (int32_t)x.z;
+                s_aux[tid * PLE_STRIDE + 4 * q + 3] = (int32_t)x.w;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < PLE_ITEMS; ++i) s_aux[tid * PLE_STRIDE + i] = i < lim ? (int32_t)a.sym[gfirst + i] : 0;
+        }
     }
     if (tid == 0) {
         s_sd0 = seg_upper(a.seg_off, 0, a.n_seg - 1, base);
         s_sd1 = seg_upper(a.seg_off, 0, a.n_seg - 1, min(base + PLE_TILE, a.n) - 1);
     }
-    __syncthreads();
-    for (int width = PLE_TILE / 2; width >= 1; width >>= 1) {
-        for (int i = tid; i < width; i += PLE_THREADS) {
-            const int node = width + i;
-            tree[node] = min(tree[2 * node], tree[2 * node + 1]);
-        }
-        __syncthreads();
-    }
-    int32_t v[PLE_ITEMS];
-#pragma unroll
-    for (int i = 0; i < PLE_ITEMS; ++i) v[i] = tree[PLE_TILE + tid * PLE_ITEMS + i];
+    int4 qm;
+    qm.x = min(min(v[0], v[1]), min(v[2], v[3]));
+    qm.y = min(min(v[4], v[5]), min(v[6], v[7]));
+    qm.z = min(min(v[8], v[9]), min(v[10], v[11]));
+    qm.w = min(min(v[12], v[13]), min(v[14], v[15]));
+    s_sub[tid] = qm;
+    const int32_t cm = min(min(qm.x, qm.y), min(qm.z, qm.w));
 
-    const long long gfirst = base + tid * PLE_ITEMS;
-    long long doc = gfirst < a.n ? seg_upper(a.seg_off, s_sd0, s_sd1, gfirst) : 0;
-    long long dbase = gfirst < a.n ? a.seg_off[doc] : 0;
-    long long dnext = gfirst < a.n ? a.seg_off[doc + 1] : 0;
+    // ---- min tree over chunk minima: warp levels by shuffles, top by thread 0
+    {
+        int32_t m = cm;
+        int node = PLE_THREADS + tid;
+        tree[node] = m;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            m = min(m, __shfl_xor_sync(ALP_FULL_MASK, m, d));
+            node >>= 1;
+            if ((lane & (2 * d - 1)) == 0) tree[node] = m;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int node = PLE_THREADS / 32 - 1; node >= 1; --node) tree[node] = min(tree[2 * node], tree[2 * node + 1]);
+    }
+    __syncthreads();
+    const long long sd0 = s_sd0, sd1 = s_sd1;
+
+    // ---- (1) answers inside the thread ---------------------------------------
+    long long doc = lim > 0 ? seg_upper(a.seg_off, sd0, sd1, gfirst) : 0;
+    long long dbase = lim > 0 ? a.seg_off[doc] : 0;
+    long long dnext = lim > 0 ? a.seg_off[doc + 1] : 0;
+    uint32_t unres = 0;
 #pragma unroll
     for (int j = 0; j < PLE_ITEMS; ++j) {
-        const int lj = tid * PLE_ITEMS + j;
-        const long long g = base + lj;
-        if (g >= a.n) continue;
-        while (g >= dnext && doc + 1 < a.n_seg) {
-            ++doc;
-            dbase = a.seg_off[doc];
-            dnext = a.seg_off[doc + 1];
-        }
-        const uint32_t my_sym = brackets ? s_sym[lj] : 0u;
-        if (brackets && (my_sym >> 31)) continue;  // lefts ask nothing
-        if (!brackets && g == dbase) { a.out_parent[g] = 0; continue; }  // a document's root
-        const int32_t x = v[j];
-        int ans = -1;
+        if (j < lim) {
+            const long long g = gfirst + j;
+            while (g >= dnext && doc + 1 < a.n_seg) {
+                ++doc;
+                dbase = a.seg_off[doc];
+                dnext = a.seg_off[doc + 1];
+            }
+            const int e = tid * PLE_ITEMS + j;
+            int ans = -1;
 #pragma unroll
-        for (int i = j - 1; i >= 0; --i)
-            if (ans < 0 && v[i] <= x) ans = tid * PLE_ITEMS + i;
-        if (ans < 0) {
-            int node = PLE_TILE + tid * PLE_ITEMS;  // search left of this thread's chunk
-            bool found = false;
-            while (node > 1) {
-                if ((node & 1) && tree[node - 1] <= x) { node = node - 1; found = true; break; }
-                node >>= 1;
-            }
-            if (found) {
-                while (node < PLE_TILE) node = (tree[2 * node + 1] <= x) ? 2 * node + 1 : 2 * node;
-                ans = node - PLE_TILE;
-            }
-        }
-        if (ans >= 0) {
-            const long long ag = base + ans;
+            for (int i = 0; i < j; ++i) ans = v[i] <= v[j] ? tid * PLE_ITEMS + i : ans;
             if (brackets) {
-                const uint32_t l = s_sym[ans];
-                if (ag < dbase || (l & 0x7fffffffu) != (my_sym & 0x7fffffffu) || !(l >> 31)) a.seg_valid[doc] = 0;
+                const uint32_t my_sym = (uint32_t)s_aux[tid * PLE_STRIDE + j];
+                if (!(my_sym >> 31)) {  // rights ask; lefts do not
+                    if (ans >= 0) {
+                        const uint32_t l = (uint32_t)s_aux[tid * PLE_STRIDE + (ans - tid * PLE_ITEMS)];
+                        if (base + ans < dbase || (l & 0x7fffffffu) != (my_sym & 0x7fffffffu) || !(l >> 31))
+                            a.seg_valid[doc] = 0;
+                    } else {
+                        unres |= 1u << j;
+                    }
+                }
             } else {
-                a.out_parent[g] = ag - dbase;
+                int32_t r = 0;  // a document's root: parent 0
+                if (g != dbase) {
+                    if (ans >= 0) r = (int32_t)(base + ans - dbase);
+                    else unres |= 1u << j;
+                }
+                s_aux[tid * PLE_STRIDE + j] = r;
+                (void)e;
             }
-        } else {
-            const unsigned int slot = atomicAdd(a.esc_count, 1u);
-            if ((long long)slot < a.esc_cap) a.esc[slot] = ((unsigned long long)g << 32) | (uint32_t)x;
-            else atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
         }
     }
 
-    // tile minimum and staircase of suffix minima (values strictly below every later one)
-    int32_t cm = INT32_MAX;
-#pragma unroll
-    for (int i = 0; i < PLE_ITEMS; ++i) cm = min(cm, v[i]);
+    // ---- (2) the warp's remaining queries, 32 at a time -----------------------
+    {
+        const uint32_t cnt = __popc(unres);
+        const uint32_t incl = warp_scan_add(cnt, lane);
+        const uint32_t total = __shfl_sync(ALP_FULL_MASK, incl, 31);
+        uint16_t* q = s_q + warp * (32 * PLE_ITEMS);
+        uint32_t o = incl - cnt;
+        for (uint32_t m = unres; m; m &= m - 1) q[o++] = (uint16_t)(tid * PLE_ITEMS + __ffs(m) - 1);
+        __syncwarp();
+        for (uint32_t qb = 0; qb < total; qb += 32) {
+            if (qb + lane < total) {
+                const int e = q[qb + lane];
+                const int32_t x = s_val[ple_pad(e)];
+                const long long g = base + e;
+                int node = PLE_THREADS + e / PLE_ITEMS;  // chunks left of the element's
+                bool found = false;
+                while (node > 1) {
+                    if ((node & 1) && tree[node - 1] <= x) { node = node - 1; found = true; break; }
+                    node >>= 1;
+                }
+                const long long dq = sd0 == sd1 ? sd0 : seg_upper(a.seg_off, sd0, sd1, g);
+                const long long dqb = a.seg_off[dq];
+                if (found) {
+                    while (node < PLE_THREADS) node = (tree[2 * node + 1] <= x) ? 2 * node + 1 : 2 * node;
+                    const int c = node - PLE_THREADS;
+                    const int4 sm = s_sub[c];
+                    const int qq = sm.w <= x ? 3 : (sm.z <= x ? 2 : (sm.y <= x ? 1 : 0));
+                    const int32_t* cv = s_val + c * PLE_STRIDE + 4 * qq;
+                    const int k = cv[3] <= x ? 3 : (cv[2] <= x ? 2 : (cv[1] <= x ? 1 : 0));
+                    const int ans = c * PLE_ITEMS + 4 * qq + k;
+                    if (brackets) {
+                        const uint32_t l = (uint32_t)s_aux[ple_pad(ans)];
+                        const uint32_t r = (uint32_t)s_aux[ple_pad(e)];
+                        if (base + ans < dqb || (l & 0x7fffffffu) != (r & 0x7fffffffu) || !(l >> 31))
+                            a.seg_valid[dq] = 0;
+                    } else {
+                        s_aux[ple_pad(e)] = (int32_t)(base + ans - dqb);
+                    }
+                } else {
+                    const unsigned int slot = atomicAdd(a.esc_count, 1u);
+                    if ((long long)slot < a.esc_cap) a.esc[slot] = ((unsigned long long)g << 32) | (uint32_t)x;
+                    else atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- node parents, coalesced --------------------------------------------------
+    if (!brackets) {
+        for (int e = tid; e < PLE_TILE; e += PLE_THREADS) {
+            const long long g = base + e;
+            if (g < a.n) a.out_parent[g] = s_aux[ple_pad(e)];
+        }
+    }
+
+    // ---- tile minimum and staircase of suffix minima (values strictly below every later one)
     s_suf[tid] = cm;
     __syncthreads();
     int32_t after;
@@ -695,10 +882,9 @@ __global__ void __launch_bounds__(PLE_THREADS) ple_tile_kernel(PleArgs a) {
         int32_t y = s_suf[PLE_THREADS - 1 - tid];  // reversed order
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            int32_t o = __shfl_up_sync(ALP_FULL_MASK, y, d);
+            const int32_t o = __shfl_up_sync(ALP_FULL_MASK, y, d);
             if (lane >= d) y = min(y, o);
         }
-        __shared__ int32_t s_wm[PLE_THREADS / 32];
         if (lane == 31) s_wm[warp] = y;
         __syncthreads();
         int32_t pre = INT32_MAX;
@@ -712,8 +898,7 @@ __global__ void __launch_bounds__(PLE_THREADS) ple_tile_kernel(PleArgs a) {
     int32_t run = after;
 #pragma unroll
     for (int i = PLE_ITEMS - 1; i >= 0; --i) {
-        const long long g = base + tid * PLE_ITEMS + i;
-        if (g < a.n && v[i] < run) flags |= 1u << i;
+        if (i < lim && v[i] < run) flags |= 1u << i;
         run = min(run, v[i]);
     }
     const uint32_t cnt = __popc(flags);
@@ -731,7 +916,7 @@ __global__ void __launch_bounds__(PLE_THREADS) ple_tile_kernel(PleArgs a) {
     for (int i = 0; i < PLE_ITEMS; ++i) {
         if (flags & (1u << i)) {
             a.stair_val[sbase + o] = v[i];
-            a.stair_idx[sbase + o] = (uint32_t)(base + tid * PLE_ITEMS + i);
+            a.stair_idx[sbase + o] = (uint32_t)(gfirst + i);
             ++o;
         }
     }
