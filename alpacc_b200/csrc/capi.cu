@@ -570,6 +570,7 @@ int put_doc_off(alp_ctx* ctx, long long n) {
 int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, ParseOut* o, int64_t cap, int ctx_out,
                     int64_t* n_node, int want_tree) {
     *n_node = 0;
+    if (L >= 0x7fffffffLL) return fail(ctx, ALP_ERR_ARG, "too many positions (%lld)", L);
     const long long tiles = (L + PP_TILE - 1) / PP_TILE;
     int rc;
     if ((rc = grow(ctx, ctx->tmp[T_PID], (size_t)L * 2 + 64)) || (rc = grow(ctx, ctx->tmp[T_TSUMS], (tiles + tiles / ST_CHUNK + 2) * sizeof(PosSums))) ||
@@ -638,7 +639,8 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     a.dsbuf = (int32_t*)ctx->tmp[T_DSBUF].p;
     a.cap_nodes = N;
     a.cap_brs = B;
-    const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_prods);
+    const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
+    if (sm2 > 220 * 1024) return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
     CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
     mark(ctx, "start");
     parse_expand_kernel<<<(unsigned)tiles, PP_THREADS, sm2, ctx->stream>>>(a);

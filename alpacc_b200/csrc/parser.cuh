@@ -44,7 +44,12 @@ struct ParseTables {
     const int16_t* pseq_v;      // [n_pseq] sum of (arity-1) over the pair's earlier productions
     const int16_t* pseq_t;      // [n_pseq] terminal productions among the pair's earlier productions
     const int16_t* stack_d;     // [n_stack] depth change before this bracket within its pair
-    int q, k, T, n_pairs, n_prods;
+    // per production-sequence entry: x = production | (terminal + 1) << 16 (0: not a terminal
+    // production), y = (uint16) pseq_v | pseq_t << 16
+    const uint2* pseq_rec;
+    // per stack entry: x = symbol | left << 31, y = (uint16) stack_d
+    const uint2* stack_rec;
+    int q, k, T, n_pairs, n_prods, n_pseq, n_stack;
     uint32_t empty, start, end;
 };
 
@@ -150,6 +155,17 @@ inline int load_parser(ParseTables& pt, ParseHost& ph, const uint8_t* p, const u
             acc_d += (stack[j] >> 31) ? 1 : -1;
         }
     }
+    std::vector<uint2> prec(n_pseq), srec(n_stack);
+    for (uint32_t j = 0; j < n_pseq; ++j) {
+        const int32_t tm = pterm[pseq[j]];
+        if (tm >= 65535) { err = "terminal id too large"; return 4; }
+        prec[j].x = pseq[j] | ((uint32_t)(tm >= 0 ? tm + 1 : 0) << 16);
+        prec[j].y = (uint32_t)(uint16_t)pv[j] | ((uint32_t)(uint16_t)ptm[j] << 16);
+    }
+    for (uint32_t j = 0; j < n_stack; ++j) {
+        srec[j].x = stack[j];
+        srec[j].y = (uint32_t)(uint16_t)sd[j];
+    }
     auto up = [&](const void* h, size_t bytes, const void** d) -> bool {
         void* x = nullptr;
         if (cudaMalloc(&x, bytes < 16 ? 16 : bytes) != cudaSuccess) return false;
@@ -166,9 +182,12 @@ inline int load_parser(ParseTables& pt, ParseHost& ph, const uint8_t* p, const u
               up(pterm.data(), pterm.size() * 4, (const void**)&pt.prod_term) &&
               up(pv.data(), pv.size() * 2, (const void**)&pt.pseq_v) &&
               up(ptm.data(), ptm.size() * 2, (const void**)&pt.pseq_t) &&
-              up(sd.data(), sd.size() * 2, (const void**)&pt.stack_d);
+              up(sd.data(), sd.size() * 2, (const void**)&pt.stack_d) &&
+              up(prec.data(), prec.size() * 8, (const void**)&pt.pseq_rec) &&
+              up(srec.data(), srec.size() * 8, (const void**)&pt.stack_rec);
     if (!ok) { err = "cudaMalloc/cudaMemcpy failed for parser tables"; return 2; }
     pt.q = (int)q; pt.k = (int)k; pt.T = (int)T; pt.n_pairs = (int)n_pairs; pt.n_prods = (int)n_prods;
+    pt.n_pseq = (int)n_pseq; pt.n_stack = (int)n_stack;
     pt.empty = empty; pt.start = start; pt.end = end;
     ph.q = (int)q; ph.k = (int)k; ph.n_terms = (int)n_terms; ph.n_prods = (int)n_prods; ph.n_pairs = (int)n_pairs;
     ph.max_prods = maxp; ph.max_brackets = maxb; ph.key_space = space;
@@ -179,7 +198,7 @@ inline int load_parser(ParseTables& pt, ParseHost& ph, const uint8_t* p, const u
 
 namespace alp {
 
-constexpr int PP_THREADS = 256;
+constexpr int PP_THREADS = 512;
 constexpr int PP_ITEMS = 4;                        // positions per thread
 constexpr int PP_TILE = PP_THREADS * PP_ITEMS;     // positions per tile
 constexpr int PLE_THREADS = 256;
@@ -190,15 +209,17 @@ constexpr uint16_t NO_PAIR = 0xffff;
 // Running sums over positions.  Positions are the documents' ⊢ tokens ⊣
 // sequences back to back; nodes, brackets and heads (⊢ count) run over all
 // documents, depth / v / terminals restart at every ⊢ (a segmented scan).
+// All fields are 32-bit: node and bracket totals are checked below 2^32 and
+// positions below 2^31 before any launch.
 struct __align__(16) PosSums {
-    unsigned long long nodes;   // productions
-    unsigned long long brs;     // brackets
-    long long depth;            // lefts - rights since the last ⊢
-    long long v;                // sum of (arity - 1) since the last ⊢
-    unsigned long long terms;   // terminal productions since the last ⊢
-    unsigned long long heads;   // ⊢ positions
-    long long hpos;             // position of the last ⊢ (-1: none)
-    unsigned long long pad;
+    uint32_t nodes;   // productions
+    uint32_t brs;     // brackets
+    int32_t depth;    // lefts - rights since the last ⊢
+    int32_t v;        // sum of (arity - 1) since the last ⊢
+    uint32_t terms;   // terminal productions since the last ⊢
+    uint32_t heads;   // ⊢ positions
+    int32_t hpos;     // position of the last ⊢ (-1: none)
+    uint32_t pad;
 };
 
 __device__ __forceinline__ void possums_zero(PosSums& s) {
@@ -209,8 +230,11 @@ __device__ __forceinline__ PosSums ps_combine(const PosSums& a, const PosSums& b
     r.nodes = a.nodes + b.nodes;
     r.brs = a.brs + b.brs;
     r.heads = a.heads + b.heads;
-    if (b.heads) { r.depth = b.depth; r.v = b.v; r.terms = b.terms; r.hpos = b.hpos; }
-    else { r.depth = a.depth + b.depth; r.v = a.v + b.v; r.terms = a.terms + b.terms; r.hpos = a.hpos; }
+    const bool h = b.heads != 0;
+    r.depth = h ? b.depth : a.depth + b.depth;
+    r.v = h ? b.v : a.v + b.v;
+    r.terms = h ? b.terms : a.terms + b.terms;
+    r.hpos = h ? b.hpos : a.hpos;
     r.pad = 0;
     return r;
 }
@@ -226,8 +250,20 @@ __device__ __forceinline__ PosSums ps_shfl_up(const PosSums& x, int d) {
     r.pad = 0;
     return r;
 }
-// inclusive warp scan (lanes in order)
+// inclusive warp scan (lanes in order); a warp without a ⊢ needs plain sums
 __device__ __forceinline__ PosSums ps_warp_scan(PosSums x, int lane) {
+    if (!__any_sync(ALP_FULL_MASK, x.heads != 0)) {
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t on = __shfl_up_sync(ALP_FULL_MASK, x.nodes, d);
+            const uint32_t ob = __shfl_up_sync(ALP_FULL_MASK, x.brs, d);
+            const int32_t od = __shfl_up_sync(ALP_FULL_MASK, x.depth, d);
+            const int32_t ov = __shfl_up_sync(ALP_FULL_MASK, x.v, d);
+            const uint32_t ot = __shfl_up_sync(ALP_FULL_MASK, x.terms, d);
+            if (lane >= d) { x.nodes += on; x.brs += ob; x.depth += od; x.v += ov; x.terms += ot; }
+        }
+        return x;
+    }
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         PosSums o = ps_shfl_up(x, d);
@@ -242,7 +278,7 @@ __device__ __forceinline__ PosSums ps_elem(const PairInfo* s_pi, uint16_t p, boo
         const PairInfo& pi = s_pi[p];
         e.nodes = pi.n_prod; e.brs = pi.n_br; e.depth = pi.d_depth; e.v = pi.d_v; e.terms = pi.n_term;
     }
-    if (head) { e.heads = 1; e.hpos = i; }
+    if (head) { e.heads = 1; e.hpos = (int32_t)i; }
     return e;
 }
 
@@ -423,16 +459,35 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
     __syncthreads();
     const PosSums pre = ps_combine(s_carry, s_w[warp]);
     if (idx < tiles) s[idx] = ps_combine(pre, ex);
-    if (chunk == gridDim.x - 1 && tid == ST_CHUNK - 1) {
-        const PosSums tot = ps_combine(pre, inc);
-        res->aux[0] = (long long)tot.nodes;
-        res->aux[1] = (long long)tot.brs;
-        res->aux[2] = tot.depth;
-        res->aux[3] = tot.v;
-        res->aux[4] = (long long)tot.terms;
-        res->aux[5] = (long long)tot.heads;
-        node_off[n_docs] = (long long)tot.nodes;
-        br_off[n_docs] = (long long)tot.brs;
+    if (chunk == gridDim.x - 1) {
+        __syncthreads();
+        if (tid == ST_CHUNK - 1) s_carry = ps_combine(pre, inc);
+        if (warp == 0) {
+            // node and bracket totals in 64 bits, so that a total past 2^32 is seen
+            unsigned long long tn = 0, tb = 0;
+            for (long long b = lane; b <= chunk; b += 32) {
+                if (b < chunk) { tn += chunk_sums[b].nodes; tb += chunk_sums[b].brs; }
+            }
+            for (int d = 16; d >= 1; d >>= 1) {
+                tn += __shfl_down_sync(ALP_FULL_MASK, tn, d);
+                tb += __shfl_down_sync(ALP_FULL_MASK, tb, d);
+            }
+            if (lane == 0) { res->aux[0] = (long long)tn; res->aux[1] = (long long)tb; }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const PosSums tot = s_carry;
+            // the last chunk's own sums on top of the 64-bit totals of the earlier chunks
+            const PosSums own = chunk_sums[chunk];
+            res->aux[0] += own.nodes;
+            res->aux[1] += own.brs;
+            res->aux[2] = tot.depth;
+            res->aux[3] = tot.v;
+            res->aux[4] = (long long)tot.terms;
+            res->aux[5] = (long long)tot.heads;
+            node_off[n_docs] = res->aux[0];
+            br_off[n_docs] = res->aux[1];
+        }
     }
 }
 
@@ -445,20 +500,28 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
 // and the block copies the stage out with coalesced stores.  A tile with
 // more nodes or brackets than the stage holds writes them directly.
 // ---------------------------------------------------------------------------
-constexpr int EX_STAGE_BYTES = 33792;
+constexpr int EX_STAGE_BYTES = 67584;
 constexpr int EX_NCAP = EX_STAGE_BYTES / 12;  // nodes: value, tag | kind << 31, token index
 constexpr int EX_BCAP = EX_STAGE_BYTES / 8;   // brackets: symbol, depth value
 constexpr uint32_t EX_NO_TOKEN = 0xffffffffu;
 
-__host__ __device__ inline size_t expand_smem_bytes(int n_pairs, int n_prods) {
-    return ((sizeof(PairInfo) * n_pairs + (size_t)n_prods * 4 + 15) & ~(size_t)15) + EX_STAGE_BYTES;
+// pair infos (20 bytes each), then the 8-byte records from a 16-byte boundary
+__host__ __device__ inline size_t expand_rec_off(int n_pairs) {
+    return (sizeof(PairInfo) * n_pairs + 15) & ~(size_t)15;
+}
+__host__ __device__ inline size_t expand_tables_bytes(int n_pairs, int n_pseq, int n_stack) {
+    return (expand_rec_off(n_pairs) + 8 * ((size_t)n_pseq + n_stack) + 15) & ~(size_t)15;
+}
+__host__ __device__ inline size_t expand_smem_bytes(int n_pairs, int n_pseq, int n_stack) {
+    return expand_tables_bytes(n_pairs, n_pseq, n_stack) + EX_STAGE_BYTES;
 }
 
-__global__ void __launch_bounds__(PP_THREADS, 4) parse_expand_kernel(ParseArgs a) {
+__global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     PairInfo* s_pi = reinterpret_cast<PairInfo*>(smem);
-    int32_t* s_pt = reinterpret_cast<int32_t*>(smem + sizeof(PairInfo) * a.t.n_pairs);
-    uint8_t* stage = smem + ((sizeof(PairInfo) * a.t.n_pairs + (size_t)a.t.n_prods * 4 + 15) & ~(size_t)15);
+    uint2* s_prec = reinterpret_cast<uint2*>(smem + expand_rec_off(a.t.n_pairs));
+    uint2* s_srec = s_prec + a.t.n_pseq;
+    uint8_t* stage = smem + expand_tables_bytes(a.t.n_pairs, a.t.n_pseq, a.t.n_stack);
     int32_t* s_nv = reinterpret_cast<int32_t*>(stage);
     uint32_t* s_ntag = reinterpret_cast<uint32_t*>(s_nv + EX_NCAP);
     uint32_t* s_nti = s_ntag + EX_NCAP;
@@ -469,7 +532,8 @@ __global__ void __launch_bounds__(PP_THREADS, 4) parse_expand_kernel(ParseArgs a
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < a.t.n_pairs * (int)(sizeof(PairInfo) / 4); i += PP_THREADS)
         reinterpret_cast<uint32_t*>(s_pi)[i] = reinterpret_cast<const uint32_t*>(a.t.pairs)[i];
-    for (int i = tid; i < a.t.n_prods; i += PP_THREADS) s_pt[i] = a.t.prod_term[i];
+    for (int i = tid; i < a.t.n_pseq; i += PP_THREADS) s_prec[i] = a.t.pseq_rec[i];
+    for (int i = tid; i < a.t.n_stack; i += PP_THREADS) s_srec[i] = a.t.stack_rec[i];
     const uint32_t SL = a.t.start, SR = a.t.end;
     const long long tbase = (long long)blockIdx.x * PP_TILE;
     const long long i0 = tbase + tid * PP_ITEMS;
@@ -520,15 +584,15 @@ __global__ void __launch_bounds__(PP_THREADS, 4) parse_expand_kernel(ParseArgs a
             const long long i = i0 + j;
             if (i < a.L) {
                 const bool head = (hm >> j) & 1u;
-                const long long dep = head ? 0 : run.depth;
-                const int32_t v = head ? 0 : (int32_t)run.v;
+                const int32_t dep = head ? 0 : run.depth;
+                const int32_t v = head ? 0 : run.v;
                 const uint32_t tr = head ? 0u : (uint32_t)run.terms;
                 const uint32_t hp = (uint32_t)(head ? i : run.hpos);
                 const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
                 const bool dok = doc >= 0 && doc < a.n_docs;
                 if (head && dok) {
                     a.node_off[doc] = (long long)(tp.nodes + nd);
-                    a.br_off[doc] = (long long)(run.brs);
+                    a.br_off[doc] = (long long)run.brs;
                 }
                 int32_t dd = 0;
                 if (ids[j] == NO_PAIR) {
@@ -537,15 +601,14 @@ __global__ void __launch_bounds__(PP_THREADS, 4) parse_expand_kernel(ParseArgs a
                     const PairInfo pi = s_pi[ids[j]];
                     dd = pi.d_depth;
                     for (uint32_t r = 0; r < pi.n_prod; ++r) {
-                        const uint32_t jj = pi.prod_begin + r;
-                        const uint32_t prod = __ldg(&a.t.pseq[jj]);
-                        const int32_t pt = s_pt[prod];
-                        const int32_t vv = v + __ldg(&a.t.pseq_v[jj]);
-                        uint32_t tagk = prod, ti = EX_NO_TOKEN;
-                        if (pt >= 0 && a.subst_terminals) {
+                        const uint2 rec = s_prec[pi.prod_begin + r];
+                        const uint32_t tm1 = rec.x >> 16;  // terminal + 1, 0: not a terminal production
+                        const int32_t vv = v + (int32_t)(int16_t)(rec.y & 0xffffu);
+                        uint32_t tagk = rec.x & 0xffffu, ti = EX_NO_TOKEN;
+                        if (tm1 && a.subst_terminals) {
                             // the k-th terminal production of a document takes its k-th token's span
-                            tagk = (uint32_t)pt | 0x80000000u;
-                            ti = hp + 1 + tr + (uint32_t)__ldg(&a.t.pseq_t[jj]);
+                            tagk = (tm1 - 1) | 0x80000000u;
+                            ti = hp + 1 + tr + (rec.y >> 16);
                         }
                         if (nst) {
                             s_nv[nd] = vv;
@@ -612,9 +675,9 @@ __global__ void __launch_bounds__(PP_THREADS, 4) parse_expand_kernel(ParseArgs a
                 if (ids[j] != NO_PAIR) {
                     const PairInfo pi = s_pi[ids[j]];
                     for (uint32_t r = 0; r < pi.n_br; ++r) {
-                        const uint32_t jj = pi.stack_begin + r;
-                        const uint32_t sym = __ldg(&a.t.stack[jj]);
-                        const int32_t before = dep + __ldg(&a.t.stack_d[jj]);
+                        const uint2 rec = s_srec[pi.stack_begin + r];
+                        const uint32_t sym = rec.x;
+                        const int32_t before = dep + (int32_t)(int16_t)(rec.y & 0xffffu);
                         int32_t ds;
                         if (sym >> 31) ds = before;
                         else {
