@@ -270,9 +270,14 @@ int launch_lex(alp_ctx* ctx, const uint8_t* d_in, long long n, void* term, void*
     return ALP_OK;
 }
 
-int check_in(alp_ctx* ctx, const void* p, int64_t n) {
+// Input size limit: 2^30 - 1 bytes for paths that can reach the single-pass
+// lexer kernels (30-bit token counts in their look-back words); just under
+// 2^31 where the multi-kernel lexer handles the input (32-bit counts and
+// positions, int32 parser positions).
+int check_in(alp_ctx* ctx, const void* p, int64_t n, bool allow_wide = false) {
     if (!ctx) return ALP_ERR_ARG;
-    if (n < 0 || n > (int64_t)0x3fffffffLL) return fail(ctx, ALP_ERR_ARG, "input size %lld out of range", (long long)n);
+    const int64_t lim = (allow_wide && ctx->lex3) ? (int64_t)0x7ff00000LL : (int64_t)0x3fffffffLL;
+    if (n < 0 || n > lim) return fail(ctx, ALP_ERR_ARG, "input size %lld out of range", (long long)n);
     if (n > 0 && !p) return fail(ctx, ALP_ERR_ARG, "null input");
     return ALP_OK;
 }
@@ -898,7 +903,7 @@ int alp_memcpy(alp_ctx* ctx, void* dst, const void* src, size_t bytes) {
 
 int alp_lex_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_term, int64_t* d_start,
                  int64_t* d_end, int64_t cap, int64_t* n_tok, int* valid) {
-    int rc = check_in(ctx, d_in, n);
+    int rc = check_in(ctx, d_in, n, true);
     if (rc) return rc;
     if (!n_tok || !valid || (cap > 0 && (!d_term || !d_start || !d_end)))
         return fail(ctx, ALP_ERR_ARG, "null output");
@@ -1008,7 +1013,7 @@ int alp_lex_noalloc(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_te
 
 int alp_lex(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t** d_term, int64_t** d_start,
             int64_t** d_end, int64_t* n_tok, int* valid) {
-    int rc = check_in(ctx, d_in, n);
+    int rc = check_in(ctx, d_in, n, true);
     if (rc) return rc;
     if (!d_term || !d_start || !d_end || !n_tok || !valid) return fail(ctx, ALP_ERR_ARG, "null output");
     CK(cudaSetDevice(ctx->device));
@@ -1032,7 +1037,7 @@ int alp_lex(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t** d_term, int
 
 int alp_lex_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, uint32_t* h_term, int64_t* h_start,
                  int64_t* h_end, int64_t cap, int64_t* n_tok, int* valid) {
-    int rc = check_in(ctx, h_in, n);
+    int rc = check_in(ctx, h_in, n, true);
     if (rc) return rc;
     if (!n_tok || !valid) return fail(ctx, ALP_ERR_ARG, "null output");
     CK(cudaSetDevice(ctx->device));
@@ -1056,7 +1061,7 @@ int alp_lex_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, uint32_t* h_term,
 
 int alp_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t** d_parent, uint32_t** d_tag, uint8_t** d_kind,
               int64_t** d_start, int64_t** d_end, int64_t* n_node, int* valid) {
-    int rc = check_in(ctx, d_in, n);
+    int rc = check_in(ctx, d_in, n, true);
     if (rc) return rc;
     if (!d_parent || !d_tag || !d_kind || !d_start || !d_end || !n_node || !valid)
         return fail(ctx, ALP_ERR_ARG, "null output");
@@ -1074,7 +1079,7 @@ int alp_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t** d_parent, 
 
 int alp_parse_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t* d_parent, uint32_t* d_tag, uint8_t* d_kind,
                    int64_t* d_start, int64_t* d_end, int64_t cap, int64_t* n_node, int* valid) {
-    int rc = check_in(ctx, d_in, n);
+    int rc = check_in(ctx, d_in, n, true);
     if (rc) return rc;
     if (!n_node || !valid || (cap > 0 && (!d_parent || !d_tag || !d_kind || !d_start || !d_end)))
         return fail(ctx, ALP_ERR_ARG, "null output");
@@ -1085,7 +1090,7 @@ int alp_parse_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t* d_pare
 
 int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_parent, uint32_t* h_tag, uint8_t* h_kind,
                    int64_t* h_start, int64_t* h_end, int64_t cap, int64_t* n_node, int* valid) {
-    int rc = check_in(ctx, h_in, n);
+    int rc = check_in(ctx, h_in, n, true);
     if (rc) return rc;
     if (!n_node || !valid) return fail(ctx, ALP_ERR_ARG, "null output");
     CK(cudaSetDevice(ctx->device));
@@ -1406,7 +1411,7 @@ int alp_lex_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int64
     CK(cudaMemcpyAsync(ctx->h_stage, d_off + n_docs, 8, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     n = ctx->h_stage[0];
-    int rc = check_in(ctx, d_in, n);
+    int rc = check_in(ctx, d_in, n, true);
     if (rc) return rc;
     if ((rc = grow(ctx, ctx->out[0], (size_t)n * 4 + 16)) || (rc = grow(ctx, ctx->out[1], (size_t)n * 8 + 16)) ||
         (rc = grow(ctx, ctx->out[2], (size_t)n * 8 + 16)) || (rc = grow(ctx, ctx->tmp[T_DVALID], (size_t)n_docs + 16)))
@@ -1437,7 +1442,7 @@ int alp_parse_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int
     CK(cudaMemcpyAsync(ctx->h_stage, d_off + n_docs, 8, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     const int64_t n = ctx->h_stage[0];
-    int rc = check_in(ctx, d_in, n);
+    int rc = check_in(ctx, d_in, n, true);
     if (rc) return rc;
     const size_t tcap = (size_t)n + 2 * (size_t)n_docs + 16;
     if ((rc = grow(ctx, ctx->tmp[T_TTERM], tcap * 2)) || (rc = grow(ctx, ctx->tmp[T_TSTART], tcap * 4)) ||

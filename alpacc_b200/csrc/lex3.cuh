@@ -36,7 +36,7 @@ constexpr int LX_THREADS = 256;
 constexpr int LX_CHUNK = 32;                    // bytes per chunk, the unit of the state scan
 constexpr int LX_TILE = LX_THREADS * LX_CHUNK;  // 8 KiB emit tile: one chunk per thread
 constexpr int LX_WIDE = 2 * LX_TILE;            // 16 KiB fold / count tile: two chunks per thread
-constexpr int LX_STAGE = 2560;                  // tokens one emit tile stages in shared memory
+constexpr int LX_STAGE = 4096;                  // tokens one emit tile stages in shared memory
 constexpr int LS_WARPS = 8;
 constexpr int LS_G = 16;                        // chunks per lane in the state scan
 constexpr int LS_TILE = LS_WARPS * 32 * LS_G;   // 4096 chunks per state-scan tile
@@ -119,11 +119,15 @@ __global__ void lex3_tile_doc_kernel(const long long* off, long long nd, long lo
 // Document heads and last bytes of tile [t0, t1] as per-chunk bit masks
 // (bit j of word c: byte t0 + 32c + j); *s_dmax = the last document with a
 // byte at or before t1.
+// With s_doff, also s_doff[d - d0] = off[d] for the first LX_DOCS documents.
+constexpr int LX_DOCS = 64;
 __device__ __forceinline__ void lx_mark_docs(const LexSeg& sg, long long n, long long d0, long long t0, long long t1,
-                                             uint32_t* s_head, uint32_t* s_last, unsigned long long* s_dmax) {
+                                             uint32_t* s_head, uint32_t* s_last, unsigned long long* s_dmax,
+                                             uint32_t* s_doff = nullptr) {
     for (long long d = d0 + threadIdx.x; d <= sg.n_docs; d += blockDim.x) {
         const long long h = sg.doc_off[d];
         if (h > t1 + 1) break;
+        if (s_doff && d - d0 < LX_DOCS) s_doff[d - d0] = (uint32_t)h;
         if (h >= t0 && h <= t1 && h < n) {
             const long long r = h - t0;
             atomicOr(&s_head[r >> 5], 1u << (r & 31));
@@ -159,15 +163,16 @@ __device__ __forceinline__ void lx_load(const Lex3Args& a, long long my, int lim
 
 // ---- kernel 1: chunk endomorphisms ------------------------------------------
 
-// One chunk's endomorphism from bytes [b0, b0 + lim) of w, with document heads.
-__device__ __forceinline__ uint32_t lx_fold_slow(const uint4 (&w)[4], int b0, int lim, uint32_t head,
+// One chunk's endomorphism from bytes in[0, lim), with document heads (a
+// compact loop: only chunks at document heads or the input's end).
+__device__ __forceinline__ uint32_t lx_fold_slow(const uint8_t* in, int lim, uint32_t head,
                                                  const uint8_t* s_cls, const uint16_t* s_cd, const uint16_t* s_step,
                                                  int C1, uint32_t E) {
     uint32_t f = 0;
-#pragma unroll
-    for (int j = 0; j < LX_CHUNK; ++j) {
-        if (j < lim) {
-            const uint32_t c = s_cls[byte_of(w, b0 + j)];
+#pragma unroll 1
+    for (int j = 0; j < lim; ++j) {
+        {
+            const uint32_t c = s_cls[__ldg(in + j)];
             if ((head >> j) & 1u) f = E + (s_cd[1 * C1 + c] & 0x7fffu);
             else if (f >= E) f = E + (s_cd[(f - E) * C1 + c] & 0x7fffu);
             else f = s_step[f * C1 + c];
@@ -215,10 +220,10 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_fold_kernel(Lex3Args a, Le
                 }
                 *reinterpret_cast<uint32_t*>(a.chunk_f + c) = fa | (fb << 16);
             } else {
-                a.chunk_f[c] = (uint16_t)lx_fold_slow(w, 0, min(lim, LX_CHUNK), ha, s_cls, s_cd, s_step, C1, E);
+                a.chunk_f[c] = (uint16_t)lx_fold_slow(a.in + my, min(lim, LX_CHUNK), ha, s_cls, s_cd, s_step, C1, E);
                 if (lim > LX_CHUNK)
                     a.chunk_f[c + 1] =
-                        (uint16_t)lx_fold_slow(w, LX_CHUNK, lim - LX_CHUNK, hb, s_cls, s_cd, s_step, C1, E);
+                        (uint16_t)lx_fold_slow(a.in + my + LX_CHUNK, lim - LX_CHUNK, hb, s_cls, s_cd, s_step, C1, E);
             }
         }
         __syncthreads();
@@ -348,17 +353,18 @@ __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
 
 // ---- kernel 3: token counts -------------------------------------------------
 
-// Tokens ending in bytes [b0, b0 + lim) of w from state st, with document
-// heads and last bytes; *lastoff = offset of the last token start or LX_NOOFF.
-__device__ __forceinline__ uint32_t lx_count_slow(const uint4 (&w)[4], int b0, int lim, uint32_t st, uint32_t head,
+// Tokens ending in bytes in[0, lim) from state st, with document heads and
+// last bytes; *lastoff = offset of the last token start or LX_NOOFF.  A
+// compact loop: only chunks at document boundaries or the input's end.
+__device__ __forceinline__ uint32_t lx_count_slow(const uint8_t* in, int lim, uint32_t st, uint32_t head,
                                                   uint32_t last, const uint16_t* s_ent, const uint32_t* s_tok,
                                                   uint32_t* lastoff) {
     uint32_t cnt = 0, lo = LX_NOOFF;
-#pragma unroll
-    for (int j = 0; j < LX_CHUNK; ++j) {
-        if (j < lim) {
+#pragma unroll 1
+    for (int j = 0; j < lim; ++j) {
+        {
             if ((head >> j) & 1u) { st = 1u; lo = (uint32_t)j; }
-            const uint32_t e = s_ent[st * LX_ROW + byte_of(w, b0 + j)];
+            const uint32_t e = s_ent[st * LX_ROW + __ldg(in + j)];
             cnt += (e >> 6) & 1u;
             if (e & LX_START) lo = (uint32_t)j;
             st = e & LX_NEXT;
@@ -435,10 +441,11 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_count_kernel(Lex3Args a, L
                 }
                 *reinterpret_cast<uint32_t*>(a.chunk_c + c) = (ca | (oa << 8)) | ((cb | (ob << 8)) << 16);
             } else {
-                ca = lx_count_slow(w, 0, min(lim, LX_CHUNK), a.chunk_s[c], ha, la, s_ent, s_tok, &oa);
+                ca = lx_count_slow(a.in + my, min(lim, LX_CHUNK), a.chunk_s[c], ha, la, s_ent, s_tok, &oa);
                 a.chunk_c[c] = (uint16_t)(ca | (oa << 8));
                 if (lim > LX_CHUNK) {
-                    cb = lx_count_slow(w, LX_CHUNK, lim - LX_CHUNK, a.chunk_s[c + 1], hb, lb, s_ent, s_tok, &ob);
+                    cb = lx_count_slow(a.in + my + LX_CHUNK, lim - LX_CHUNK, a.chunk_s[c + 1], hb, lb, s_ent, s_tok,
+                                       &ob);
                     a.chunk_c[c + 1] = (uint16_t)(cb | (ob << 8));
                 }
             }
@@ -550,6 +557,7 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
     __shared__ unsigned long long s_dmax;
     __shared__ uint32_t s_head[LX_TILE / LX_CHUNK], s_last[LX_TILE / LX_CHUNK];
     __shared__ uint32_t s_wc[LX_THREADS / 32], s_wp[LX_THREADS / 32];
+    __shared__ uint32_t s_doff[LX_DOCS];  // offsets of the tile's documents d0.. (up to LX_DOCS)
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     {
@@ -560,6 +568,23 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
     for (int i = tid; i < S; i += LX_THREADS) s_tok[i] = a.t.tokinfo[i];
     const long long n = a.n;
     const long long ND = sg.n_docs;
+    // document holding position p of this tile: the largest d in [d0, dmax]
+    // with off[d] <= p, from the shared offsets when the tile has few documents
+    auto doc_of = [&](long long d0, long long dmax, long long p) -> long long {
+        if (dmax == d0) return d0;
+        if (dmax - d0 < LX_DOCS) {
+            int lo = 0, hi = (int)(dmax - d0);
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if ((long long)s_doff[mid] <= p) lo = mid; else hi = mid - 1;
+            }
+            return d0 + lo;
+        }
+        return doc_upper(sg.doc_off, d0, dmax, p);
+    };
+    auto base_of = [&](long long d0, long long dmax, long long d) -> long long {
+        return (dmax - d0 < LX_DOCS) ? (long long)s_doff[d - d0] : sg.doc_off[d];
+    };
     const uint32_t INIT = 1u;
     TermT* o_term = reinterpret_cast<TermT*>(a.out_term);
     PosT* o_start = reinterpret_cast<PosT*>(a.out_start);
@@ -582,7 +607,7 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
         s_head[tid] = 0;
         s_last[tid] = 0;
         __syncthreads();
-        lx_mark_docs(sg, n, d0, t0, t1, s_head, s_last, &s_dmax);
+        lx_mark_docs(sg, n, d0, t0, t1, s_head, s_last, &s_dmax, s_doff);
         __syncthreads();
         const long long dmax = (long long)s_dmax;
         const long long my = t0 + (long long)tid * LX_CHUNK;
@@ -599,7 +624,7 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
             if ((cc >> 8) != LX_NOOFF) lastp = (uint32_t)(my + (cc >> 8));
             head = s_head[tid];
             last = s_last[tid];
-            if (dmax > d0) mydoc = doc_upper(sg.doc_off, d0, dmax, my);
+            mydoc = doc_of(d0, dmax, my);
         } else {
             w[0] = w[1] = make_uint4(0, 0, 0, 0);
         }
@@ -646,7 +671,7 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
                 tcount = Xc + k;
             } else {
                 long long doc = mydoc;
-                long long base = sg.doc_off[doc];
+                long long base = base_of(d0, dmax, doc);
                 auto tok = [&](uint32_t term, uint32_t st_abs, uint32_t en_abs) {
                     if (staged) {
                         const uint32_t k = tcount - Xc;
@@ -658,14 +683,17 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
                     }
                     ++tcount;
                 };
-#pragma unroll
-                for (int j = 0; j < LX_CHUNK; ++j) {
-                    if (j < lim) {
+                // a compact loop (bytes through L1): only threads at document
+                // boundaries, partial chunks or overflowing tiles come here
+#pragma unroll 1
+                for (int j = 0; j < lim; ++j) {
+                    {
                         const long long pos = my + j;
                         if ((head >> j) & 1u) {
                             // every document starting here (empty ones first, then the real one)
-                            doc = doc_upper(sg.doc_off, d0, dmax, pos);
-                            const long long dl = doc_lower(sg.doc_off, 0, doc, pos);
+                            doc = doc_of(d0, dmax, pos);
+                            long long dl = doc;  // empty documents that start here too
+                            while (dl > 0 && sg.doc_off[dl - 1] >= pos) --dl;
                             base = pos;
                             for (long long e2 = dl; e2 <= doc; ++e2) {
                                 sg.tok_off[e2] = tcount;
@@ -678,7 +706,7 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
                             cur = (uint32_t)pos;
                             st = INIT;
                         }
-                        const uint32_t e = s_ent[st * LX_ROW + byte_of(w, j)];
+                        const uint32_t e = s_ent[st * LX_ROW + __ldg(a.in + pos)];
                         if (e & LX_EMIT) tok(s_tok[st] & TOK_TERM_MASK, cur, (uint32_t)pos);
                         if (e & LX_START) cur = (uint32_t)pos;
                         st = e & LX_NEXT;
@@ -711,14 +739,14 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
 
         // ---- coalesced copy of the staged tokens ---------------------------------
         if (staged) {
-            const long long b0 = sg.doc_off[d0];
+            const long long b0 = base_of(d0, dmax, d0);
             for (uint32_t k = tid; k < Bc; k += LX_THREADS) {
                 const uint32_t pk = s_pk[k];
                 const long long en = t0 + (pk & 0xffffu);
                 long long dk = d0, bk = b0;
                 if (dmax > d0) {
-                    dk = doc_upper(sg.doc_off, d0, dmax, en - 1);
-                    bk = sg.doc_off[dk];
+                    dk = doc_of(d0, dmax, en - 1);
+                    bk = base_of(d0, dmax, dk);
                 }
                 put((long long)(Xc + k) + sent * (2 * dk + 1), pk >> 16, (long long)s_st[k] - bk, en - bk);
             }

@@ -344,14 +344,6 @@ __device__ __forceinline__ long long doc_upper(const long long* off, long long l
     }
     return lo;
 }
-// smallest d in [lo, hi] with off[d] >= p
-__device__ __forceinline__ long long doc_lower(const long long* off, long long lo, long long hi, long long p) {
-    while (lo < hi) {
-        const long long mid = (lo + hi) >> 1;
-        if (off[mid] >= p) hi = mid; else lo = mid + 1;
-    }
-    return lo;
-}
 
 // Bytes of a thread live in four uint4 registers; byte j of the 64.
 __device__ __forceinline__ uint32_t raw_byte(const uint4 (&w)[4], int j) {
@@ -615,7 +607,8 @@ __global__ void __launch_bounds__(LEX_THREADS, 4) lex_seg_kernel(LexArgs a, LexS
                     if ((head >> j) & 1ull) {
                         // every document starting here (empty ones first, then the real one)
                         doc = doc_upper(sg.doc_off, d0, d1, pos);
-                        const long long dl = doc_lower(sg.doc_off, 0, doc, pos);
+                        long long dl = doc;  // empty documents that start here too
+                        while (dl > 0 && sg.doc_off[dl - 1] >= pos) --dl;
                         base = pos;
                         for (long long e = dl; e <= doc; ++e) {
                             sg.tok_off[e] = tcount;

@@ -498,7 +498,8 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
 // thread then walks its positions and writes their nodes (first pass) and
 // brackets (second pass) into a shared-memory stage at their tile offsets,
 // and the block copies the stage out with coalesced stores.  A tile with
-// more nodes or brackets than the stage holds writes them directly.
+// more nodes or brackets than the stage holds goes through it in rounds over
+// thread ranges.
 // ---------------------------------------------------------------------------
 constexpr int EX_STAGE_BYTES = 67584;
 constexpr int EX_NCAP = EX_STAGE_BYTES / 12;  // nodes: value, tag | kind << 31, token index
@@ -573,142 +574,177 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     const PosSums tp = a.tile_sums[blockIdx.x];
     const PosSums run0 = ps_combine(ps_combine(tp, s_w[warp]), ex);  // before this thread's first position
     const uint32_t tn = s_tn, tb = s_tb;
-    const bool nst = tn <= (uint32_t)EX_NCAP, bst = tb <= (uint32_t)EX_BCAP;
+    // Tile-local first node / bracket of every thread.  A tile with more than
+    // the stage holds is staged in rounds over equal thread ranges; a round
+    // that still does not fit writes directly.
+    __shared__ uint32_t s_n0[PP_THREADS + 1], s_b0[PP_THREADS + 1];
+    __shared__ int s_rn, s_rb;
+    s_n0[tid] = run0.nodes - tp.nodes;
+    s_b0[tid] = run0.brs - tp.brs;
+    if (tid == 0) { s_n0[PP_THREADS] = tn; s_b0[PP_THREADS] = tb; }
+    __syncthreads();
+    if (tid == 0) {
+        auto rounds = [](const uint32_t* o, uint32_t cap) {
+            int R = 1;
+            for (; R < 16; R *= 2) {
+                bool ok = true;
+                for (int r = 0; r < R && ok; ++r)
+                    ok = o[(r + 1) * PP_THREADS / R] - o[r * PP_THREADS / R] <= cap;
+                if (ok) break;
+            }
+            return R;
+        };
+        s_rn = rounds(s_n0, EX_NCAP);
+        s_rb = rounds(s_b0, EX_BCAP);
+    }
+    __syncthreads();
+    const int Rn = s_rn, Rb = s_rb;
 
     // ---- nodes -------------------------------------------------------------------
-    {
-        PosSums run = run0;
-        uint32_t nd = (uint32_t)(run.nodes - tp.nodes);
+    for (int rr = 0; rr < Rn; ++rr) {
+        const int lo = rr * PP_THREADS / Rn, hi = (rr + 1) * PP_THREADS / Rn;
+        const uint32_t nb = s_n0[lo], ncount = s_n0[hi] - nb;
+        const bool nst = ncount <= (uint32_t)EX_NCAP;
+        if (tid >= lo && tid < hi) {
+            PosSums run = run0;
+            uint32_t nd = (uint32_t)(run.nodes - tp.nodes);
 #pragma unroll
-        for (int j = 0; j < PP_ITEMS; ++j) {
-            const long long i = i0 + j;
-            if (i < a.L) {
-                const bool head = (hm >> j) & 1u;
-                const int32_t dep = head ? 0 : run.depth;
-                const int32_t v = head ? 0 : run.v;
-                const uint32_t tr = head ? 0u : (uint32_t)run.terms;
-                const uint32_t hp = (uint32_t)(head ? i : run.hpos);
-                const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
-                const bool dok = doc >= 0 && doc < a.n_docs;
-                if (head && dok) {
-                    a.node_off[doc] = (long long)(tp.nodes + nd);
-                    a.br_off[doc] = (long long)run.brs;
-                }
-                int32_t dd = 0;
-                if (ids[j] == NO_PAIR) {
-                    if (dok) a.doc_valid[doc] = 0;  // no admissible pair
-                } else {
-                    const PairInfo pi = s_pi[ids[j]];
-                    dd = pi.d_depth;
-                    for (uint32_t r = 0; r < pi.n_prod; ++r) {
-                        const uint2 rec = s_prec[pi.prod_begin + r];
-                        const uint32_t tm1 = rec.x >> 16;  // terminal + 1, 0: not a terminal production
-                        const int32_t vv = v + (int32_t)(int16_t)(rec.y & 0xffffu);
-                        uint32_t tagk = rec.x & 0xffffu, ti = EX_NO_TOKEN;
-                        if (tm1 && a.subst_terminals) {
-                            // the k-th terminal production of a document takes its k-th token's span
-                            tagk = (tm1 - 1) | 0x80000000u;
-                            ti = hp + 1 + tr + (rec.y >> 16);
-                        }
-                        if (nst) {
-                            s_nv[nd] = vv;
-                            s_ntag[nd] = tagk;
-                            s_nti[nd] = ti;
-                        } else {
-                            const unsigned long long ndg = tp.nodes + nd;
-                            if ((long long)ndg < a.cap_nodes) {
-                                a.vbuf[ndg] = vv;
-                                a.tag[ndg] = tagk & 0x7fffffffu;
-                                a.kind[ndg] = (uint8_t)(tagk >> 31);
-                                a.nstart[ndg] = ti < a.L ? (int64_t)__ldg(&a.pstart[ti]) : 0;
-                                a.nend[ndg] = ti < a.L ? (int64_t)__ldg(&a.pend[ti]) : 0;
+            for (int j = 0; j < PP_ITEMS; ++j) {
+                const long long i = i0 + j;
+                if (i < a.L) {
+                    const bool head = (hm >> j) & 1u;
+                    const int32_t dep = head ? 0 : run.depth;
+                    const int32_t v = head ? 0 : run.v;
+                    const uint32_t tr = head ? 0u : (uint32_t)run.terms;
+                    const uint32_t hp = (uint32_t)(head ? i : run.hpos);
+                    const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
+                    const bool dok = doc >= 0 && doc < a.n_docs;
+                    if (head && dok) {
+                        a.node_off[doc] = (long long)(tp.nodes + nd);
+                        a.br_off[doc] = (long long)run.brs;
+                    }
+                    int32_t dd = 0;
+                    if (ids[j] == NO_PAIR) {
+                        if (dok) a.doc_valid[doc] = 0;  // no admissible pair
+                    } else {
+                        const PairInfo pi = s_pi[ids[j]];
+                        dd = pi.d_depth;
+                        for (uint32_t r = 0; r < pi.n_prod; ++r) {
+                            const uint2 rec = s_prec[pi.prod_begin + r];
+                            const uint32_t tm1 = rec.x >> 16;  // terminal + 1, 0: not a terminal production
+                            const int32_t vv = v + (int32_t)(int16_t)(rec.y & 0xffffu);
+                            uint32_t tagk = rec.x & 0xffffu, ti = EX_NO_TOKEN;
+                            if (tm1 && a.subst_terminals) {
+                                // the k-th terminal production of a document takes its k-th token's span
+                                tagk = (tm1 - 1) | 0x80000000u;
+                                ti = hp + 1 + tr + (rec.y >> 16);
                             }
+                            if (nst) {
+                                s_nv[nd - nb] = vv;
+                                s_ntag[nd - nb] = tagk;
+                                s_nti[nd - nb] = ti;
+                            } else {
+                                const unsigned long long ndg = tp.nodes + nd;
+                                if ((long long)ndg < a.cap_nodes) {
+                                    a.vbuf[ndg] = vv;
+                                    a.tag[ndg] = tagk & 0x7fffffffu;
+                                    a.kind[ndg] = (uint8_t)(tagk >> 31);
+                                    a.nstart[ndg] = ti < a.L ? (int64_t)__ldg(&a.pstart[ti]) : 0;
+                                    a.nend[ndg] = ti < a.L ? (int64_t)__ldg(&a.pend[ti]) : 0;
+                                }
+                            }
+                            ++nd;
                         }
-                        ++nd;
+                    }
+                    if (((em >> j) & 1u) && (dep + dd != 0) && dok) a.doc_valid[doc] = 0;  // unbalanced at the end
+                    run = ps_combine(run, ps_elem(s_pi, ids[j], head, i));
+                }
+            }
+        }
+        __syncthreads();
+        if (nst) {
+            for (uint32_t e0 = tid; e0 < ncount; e0 += 2 * PP_THREADS) {
+                uint32_t tk[2], tix[2];
+                int32_t vv[2];
+                int64_t st[2], en[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const uint32_t e = e0 + u * PP_THREADS;
+                    tk[u] = 0; tix[u] = EX_NO_TOKEN; vv[u] = 0; st[u] = 0; en[u] = 0;
+                    if (e < ncount) { vv[u] = s_nv[e]; tk[u] = s_ntag[e]; tix[u] = s_nti[e]; }
+                    if (tix[u] < a.L) { st[u] = __ldg(&a.pstart[tix[u]]); en[u] = __ldg(&a.pend[tix[u]]); }
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const uint32_t e = e0 + u * PP_THREADS;
+                    const unsigned long long ndg = tp.nodes + nb + e;
+                    if (e < ncount && (long long)ndg < a.cap_nodes) {
+                        a.vbuf[ndg] = vv[u];
+                        a.tag[ndg] = tk[u] & 0x7fffffffu;
+                        a.kind[ndg] = (uint8_t)(tk[u] >> 31);
+                        a.nstart[ndg] = st[u];
+                        a.nend[ndg] = en[u];
                     }
                 }
-                if (((em >> j) & 1u) && (dep + dd != 0) && dok) a.doc_valid[doc] = 0;  // unbalanced at the end
-                run = ps_combine(run, ps_elem(s_pi, ids[j], head, i));
             }
         }
+        __syncthreads();
     }
-    __syncthreads();
-    if (nst) {
-        for (uint32_t e0 = tid; e0 < tn; e0 += 2 * PP_THREADS) {
-            uint32_t tk[2], tix[2];
-            int32_t vv[2];
-            int64_t st[2], en[2];
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const uint32_t e = e0 + u * PP_THREADS;
-                tk[u] = 0; tix[u] = EX_NO_TOKEN; vv[u] = 0; st[u] = 0; en[u] = 0;
-                if (e < tn) { vv[u] = s_nv[e]; tk[u] = s_ntag[e]; tix[u] = s_nti[e]; }
-                if (tix[u] < a.L) { st[u] = __ldg(&a.pstart[tix[u]]); en[u] = __ldg(&a.pend[tix[u]]); }
-            }
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const uint32_t e = e0 + u * PP_THREADS;
-                const unsigned long long ndg = tp.nodes + e;
-                if (e < tn && (long long)ndg < a.cap_nodes) {
-                    a.vbuf[ndg] = vv[u];
-                    a.tag[ndg] = tk[u] & 0x7fffffffu;
-                    a.kind[ndg] = (uint8_t)(tk[u] >> 31);
-                    a.nstart[ndg] = st[u];
-                    a.nend[ndg] = en[u];
-                }
-            }
-        }
-    }
-    __syncthreads();
 
     // ---- brackets ----------------------------------------------------------------
-    {
-        PosSums run = run0;
-        uint32_t bi = (uint32_t)(run.brs - tp.brs);
+    for (int rr = 0; rr < Rb; ++rr) {
+        const int lo = rr * PP_THREADS / Rb, hi = (rr + 1) * PP_THREADS / Rb;
+        const uint32_t bb = s_b0[lo], bcount = s_b0[hi] - bb;
+        const bool bst = bcount <= (uint32_t)EX_BCAP;
+        if (tid >= lo && tid < hi) {
+            PosSums run = run0;
+            uint32_t bi = (uint32_t)(run.brs - tp.brs);
 #pragma unroll
-        for (int j = 0; j < PP_ITEMS; ++j) {
-            const long long i = i0 + j;
-            if (i < a.L) {
-                const bool head = (hm >> j) & 1u;
-                const int32_t dep = head ? 0 : (int32_t)run.depth;
-                const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
-                if (ids[j] != NO_PAIR) {
-                    const PairInfo pi = s_pi[ids[j]];
-                    for (uint32_t r = 0; r < pi.n_br; ++r) {
-                        const uint2 rec = s_srec[pi.stack_begin + r];
-                        const uint32_t sym = rec.x;
-                        const int32_t before = dep + (int32_t)(int16_t)(rec.y & 0xffffu);
-                        int32_t ds;
-                        if (sym >> 31) ds = before;
-                        else {
-                            ds = before - 1;
-                            if (ds < 0 && doc >= 0 && doc < a.n_docs) a.doc_valid[doc] = 0;  // depth below zero
-                        }
-                        if (bst) {
-                            s_bsym[bi] = sym;
-                            s_bds[bi] = ds;
-                        } else {
-                            const unsigned long long big = tp.brs + bi;
-                            if ((long long)big < a.cap_brs) {
-                                a.brbuf[big] = sym;
-                                a.dsbuf[big] = ds;
+            for (int j = 0; j < PP_ITEMS; ++j) {
+                const long long i = i0 + j;
+                if (i < a.L) {
+                    const bool head = (hm >> j) & 1u;
+                    const int32_t dep = head ? 0 : (int32_t)run.depth;
+                    const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
+                    if (ids[j] != NO_PAIR) {
+                        const PairInfo pi = s_pi[ids[j]];
+                        for (uint32_t r = 0; r < pi.n_br; ++r) {
+                            const uint2 rec = s_srec[pi.stack_begin + r];
+                            const uint32_t sym = rec.x;
+                            const int32_t before = dep + (int32_t)(int16_t)(rec.y & 0xffffu);
+                            int32_t ds;
+                            if (sym >> 31) ds = before;
+                            else {
+                                ds = before - 1;
+                                if (ds < 0 && doc >= 0 && doc < a.n_docs) a.doc_valid[doc] = 0;  // depth below zero
                             }
+                            if (bst) {
+                                s_bsym[bi - bb] = sym;
+                                s_bds[bi - bb] = ds;
+                            } else {
+                                const unsigned long long big = tp.brs + bi;
+                                if ((long long)big < a.cap_brs) {
+                                    a.brbuf[big] = sym;
+                                    a.dsbuf[big] = ds;
+                                }
+                            }
+                            ++bi;
                         }
-                        ++bi;
                     }
+                    run = ps_combine(run, ps_elem(s_pi, ids[j], head, i));
                 }
-                run = ps_combine(run, ps_elem(s_pi, ids[j], head, i));
             }
         }
-    }
-    __syncthreads();
-    if (bst) {
-        for (uint32_t e = tid; e < tb; e += PP_THREADS) {
-            const unsigned long long big = tp.brs + e;
-            if ((long long)big >= a.cap_brs) break;
-            a.brbuf[big] = s_bsym[e];
-            a.dsbuf[big] = s_bds[e];
+        __syncthreads();
+        if (bst) {
+            for (uint32_t e = tid; e < bcount; e += PP_THREADS) {
+                const unsigned long long big = tp.brs + bb + e;
+                if ((long long)big >= a.cap_brs) break;
+                a.brbuf[big] = s_bsym[e];
+                a.dsbuf[big] = s_bds[e];
+            }
         }
+        __syncthreads();
     }
 }
 

@@ -1,10 +1,10 @@
 #!/usr/bin/env python3
 """Benchmark: bit-exact lex+parse of synthetic JSON on B200.
 
-Workload (one step): the full json.alp lex+parse (bytes -> preorder tree
-with parents, tags, kinds and spans) of one 256 MiB synthetic JSON document
-of nesting depth <= 16, through the C ABI (``alp_parse``).  Inputs are larger
-than L2, so no flush is needed between steps.
+Default workload (one step): the full json.alp lex+parse (bytes -> preorder
+tree with parents, tags, kinds and spans) of one 256 MiB synthetic JSON
+document of nesting depth <= 16, through the C ABI (``alp_parse``).  Inputs
+are larger than L2, so no flush is needed between steps.
 
 * ``value``   -- input GB/s with the document resident in HBM (device-timed
                  with CUDA events around the ``alp_parse`` calls).
@@ -19,10 +19,26 @@ than L2, so no flush is needed between steps.
                  reference's generated lexer and parser) on a bounded sample of
                  the same generator, rank 0 only.
 
-``--impl reference`` times that CPU restatement alone (the reference's own
+Other workloads (``--workload``), one JSON line each, same keys:
+
+* ``lex``    -- json.alp lexer only (lexer-mode terminal ids) on one 512 MiB
+                document of nesting depth <= 8 (``alp_lex``); algorithmic bytes
+                input + 20 B per token (u32 id, i64 start, i64 end).
+* ``batch``  -- 100,000 JSON documents and 50,000 sexp documents with
+                log-normal sizes (median 4 KiB, sigma 1.5, capped at 4 MiB),
+                each set in one ``alp_parse_batch`` call per step; algorithmic
+                bytes input + 29 B per node + offsets and validity.
+* ``spec``   -- learned boundary-state speculation for the json.alp and
+                sexp.alp lexers: the MLP trained on the GPU on exact boundary
+                states of documents from other seeds, then
+                ``alp_lex_speculative`` at chunk sizes 256/1024/4096 on 512 MiB
+                inputs against the plain lexer, with hit rate and re-run
+                fraction; the output is compared token for token.
+
+``--impl reference`` times the CPU restatement alone (the reference's own
 Futhark/Haskell toolchain is not available) on the same workload shape.
-Under torchrun each rank parses its own document (weak scaling, replicas,
-no data-path collective); the step time is the max over ranks.
+Under torchrun each rank runs its own inputs (weak scaling, replicas, no
+data-path collective); the step time is the max over ranks.
 """
 
 from __future__ import annotations
@@ -189,20 +205,358 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+
+SEED_LEX = 0xA1FACC00 + 1
+SEED_BATCH = 0xA1FACC00 + 3
+SEED_TRAIN = 0xA1FACC10
+
+
+def _dist_init(world: int):
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def _max_over_ranks(ms: float, dist, local: int) -> float:
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _timed(step, steps: int, local: int, dist):
+    """ms per step of `steps` calls (CUDA events on the current stream,
+    synchronize and barrier on both sides, max over ranks) and the clocks."""
+    import torch
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = _max_over_ranks(ev0.elapsed_time(ev1) / steps, dist, local)
+    return ms, clk.summary()
+
+
+def _kernels(kern):
+    total_k = sum(t for _, t in kern) or 1.0
+    top = max(kern, key=lambda x: x[1]) if kern else ("", 0.0)
+    return ({k: round(t, 4) for k, t in kern}, {k: round(t / total_k, 4) for k, t in kern}, top,
+            sum(1 + k.count("+") for k, _ in kern))
+
+
+def _line(metric, value, world, args, ms, config, alg_bytes, kern, e2e, clocks, extra=None):
+    peak, peak_kind = _peaks()
+    kms, share, top, launches = _kernels(kern)
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    line = {"metric": metric, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic", "config": config,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "dominant_kernel": top[0], "dominant_kernel_ms": top[1],
+                         "kernels_ms": kms, "kernel_share": share},
+            "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clocks}
+    if extra:
+        line.update(extra)
+    return line
+
+
+def run_lex(args, rank: int, world: int, local: int):
+    """json.alp lexer only, one 512 MiB document (lexer-mode ids), alp_lex."""
+    import ctypes
+    import torch
+    from alpacc_b200 import api, synth, tables
+    torch.cuda.set_device(local)
+    dist = _dist_init(world)
+    size = (args.doc_mib << 20) if args.doc_mib_given else 512 << 20
+    doc = synth.json_doc(size, 8, SEED_LEX + 1000 * rank)
+    g = api.Grammar(tables.load("json", "lexer"), device=local)
+    d_in = torch.from_numpy(doc).to(f"cuda:{local}")
+    g._stream()
+    L = api.native()
+    ptrs = [ctypes.c_void_p() for _ in range(3)]
+    n_tok, valid = ctypes.c_int64(0), ctypes.c_int(0)
+
+    def step():
+        rc = L.alp_lex(g.h, ctypes.c_void_p(d_in.data_ptr()), size, *[ctypes.byref(p) for p in ptrs],
+                       ctypes.byref(n_tok), ctypes.byref(valid))
+        if rc != 0 or not valid.value:
+            raise RuntimeError("alp_lex failed rc=%d: %s" % (rc, L.alp_last_error(g.h).decode()))
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    M = n_tok.value
+    ms, clocks = _timed(step, args.steps, local, dist)
+    g.profile(True)
+    step()
+    kern = g.timings()
+    g.profile(False)
+    # end to end: pinned host bytes in, tokens back to pinned host memory
+    h_in = torch.from_numpy(doc).pin_memory()
+    outs = [torch.empty(M, dtype=dt, pin_memory=True) for dt in (torch.int32, torch.int64, torch.int64)]
+    n2, v2 = ctypes.c_int64(0), ctypes.c_int(0)
+
+    def e2e_step():
+        rc = L.alp_lex_host(g.h, ctypes.c_void_p(h_in.data_ptr()), size, *[ctypes.c_void_p(o.data_ptr()) for o in outs],
+                            M, ctypes.byref(n2), ctypes.byref(v2))
+        if rc != 0 or n2.value != M:
+            raise RuntimeError("alp_lex_host failed rc=%d" % rc)
+
+    e2e_step()
+    ms_e2e, _ = _timed(e2e_step, max(1, min(args.steps, 5)), local, dist)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = _line("input GB/s lex (json.alp lexer-only, plain scan, bit-exact)", world * size / (ms * 1e-3) / 1e9,
+                 world, args, ms,
+                 {"workload": "json.alp lexer only, one %d MiB synthetic JSON document per GPU (depth <= 8), "
+                              "bytes -> (u32 id, i64 start, i64 end) tokens" % (size >> 20),
+                  "doc_bytes": size, "tokens": M, "tokens_per_byte": M / size, "parallelism": "replicas",
+                  "l2": "inputs larger than L2 (no flush needed)"},
+                 size + 20 * M, kern,
+                 {"value": world * size / (ms_e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": size,
+                  "d2h_bytes_per_step": 20 * M, "ms_per_step": ms_e2e}, clocks)
+    line["roofline"]["scope"] = "whole alp_lex call: input bytes + 20 B per token, over the step time"
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args, rank: int, world: int, local: int):
+    """100,000 JSON + 50,000 sexp documents, log-normal sizes, alp_parse_batch."""
+    import ctypes
+    import torch
+    from alpacc_b200 import api, synth, tables
+    torch.cuda.set_device(local)
+    dist = _dist_init(world)
+    dev = f"cuda:{local}"
+    L = api.native()
+    sets = []
+    nj = args.batch_docs
+    for name, n_docs, depth, seed in (("json", nj, 8, SEED_BATCH), ("sexp", nj // 2, 20, SEED_BATCH + 1)):
+        seed += 1000 * rank
+        sizes = synth.lognormal_sizes(n_docs, median=4096, sigma=1.5, cap=4 << 20, seed=seed)
+        data, off = synth.batch(name, sizes, depth, seed)
+        g = api.Grammar(tables.load(name, "both"), device=local)
+        sets.append({"name": name, "g": g, "data": data, "off": off, "n_docs": n_docs,
+                     "x": torch.from_numpy(data).to(dev), "o": torch.from_numpy(off).to(dev),
+                     "ptrs": [ctypes.c_void_p() for _ in range(7)], "N": ctypes.c_int64(0)})
+    sets[0]["g"]._stream()
+
+    def call(st, x, o):
+        rc = L.alp_parse_batch(st["g"].h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(o.data_ptr()), st["n_docs"],
+                               *[ctypes.byref(p) for p in st["ptrs"]], ctypes.byref(st["N"]))
+        if rc != 0:
+            raise RuntimeError("alp_parse_batch failed rc=%d: %s" % (rc, L.alp_last_error(st["g"].h).decode()))
+
+    def step():
+        for st in sets:
+            call(st, st["x"], st["o"])
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    ms, clocks = _timed(step, args.steps, local, dist)
+    kern = []
+    for st in sets:
+        st["g"].profile(True)
+        call(st, st["x"], st["o"])
+        kern += [("%s:%s" % (st["name"], k), t) for k, t in st["g"].timings()]
+        st["g"].profile(False)
+        valid = _wrap_valid(st)
+        st["accepted"] = int(valid.sum())
+    # end to end: inputs and offsets from pinned host memory, the trees, node
+    # offsets and validity back to pinned host memory, all inside the timed region
+    h2d = d2h = 0
+    for st in sets:
+        N, D = st["N"].value, st["n_docs"]
+        st["h_x"] = torch.from_numpy(st["data"]).pin_memory()
+        st["h_o"] = torch.from_numpy(st["off"]).pin_memory()
+        st["d_x"] = torch.empty_like(st["x"])
+        st["d_o"] = torch.empty_like(st["o"])
+        st["h_out"] = [torch.empty(N * w, dtype=torch.uint8, pin_memory=True) for w in (8, 4, 1, 8, 8)]
+        st["h_noff"] = torch.empty((D + 1) * 8, dtype=torch.uint8, pin_memory=True)
+        st["h_valid"] = torch.empty(D, dtype=torch.uint8, pin_memory=True)
+        h2d += st["h_x"].numel() + st["h_o"].numel() * 8
+        d2h += N * 29 + (D + 1) * 8 + D
+    def e2e_step():
+        for st in sets:
+            st["d_x"].copy_(st["h_x"], non_blocking=True)
+            st["d_o"].copy_(st["h_o"], non_blocking=True)
+            call(st, st["d_x"], st["d_o"])
+            outs = [p.value for p in st["ptrs"]]
+            for dst, src in zip(st["h_out"] + [st["h_noff"], st["h_valid"]], outs):
+                if dst.numel() and L.alp_memcpy(st["g"].h, ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(src),
+                                                dst.numel()) != 0:
+                    raise RuntimeError("alp_memcpy failed")
+
+    e2e_step()
+    ms_e2e, _ = _timed(e2e_step, max(1, min(args.steps, 3)), local, dist)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    n_bytes = sum(len(st["data"]) for st in sets)
+    alg = sum(len(st["data"]) + 29 * st["N"].value + 17 * (st["n_docs"] + 1) for st in sets)
+    cfg = {"workload": "batched segmented lex+parse: %d json.alp documents (depth <= 8) and %d "
+                       "sexp.alp documents (depth <= 20), log-normal sizes (median 4 KiB, sigma 1.5, cap 4 MiB), "
+                       "one alp_parse_batch call per grammar per step" % (sets[0]["n_docs"], sets[1]["n_docs"]),
+           "parallelism": "replicas", "l2": "inputs larger than L2 (no flush needed)"}
+    for st in sets:
+        cfg[st["name"]] = {"docs": st["n_docs"], "bytes": len(st["data"]), "nodes": st["N"].value,
+                           "accepted": st["accepted"]}
+    line = _line("input GB/s batched lex+parse (json.alp + sexp.alp documents, bit-exact)",
+                 world * n_bytes / (ms * 1e-3) / 1e9, world, args, ms, cfg, alg, kern,
+                 {"value": world * n_bytes / (ms_e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                  "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}, clocks)
+    line["roofline"]["scope"] = ("both alp_parse_batch calls: input bytes + 29 B per node + 17 B per document "
+                                 "(offsets in, node offsets and validity out), over the step time")
+    print(json.dumps(line), flush=True)
+
+
+def _wrap_valid(st):
+    import torch
+    from alpacc_b200 import api
+    return api._wrap(st["g"].h, st["ptrs"][6].value or 0, st["n_docs"], torch.uint8, st["g"].device)
+
+
+def run_spec(args, rank: int, world: int, local: int):
+    """Learned boundary-state speculation against the plain lexer."""
+    import ctypes
+    import torch
+    from alpacc_b200 import api, spec, synth, tables
+    torch.cuda.set_device(local)
+    dist = _dist_init(world)
+    dev = f"cuda:{local}"
+    size = (args.doc_mib << 20) if args.doc_mib_given else 512 << 20
+    L = api.native()
+    results = {}
+    kern_all = []
+    best = None
+    clocks = None
+    for name, depth, eval_seed in (("json", 8, SEED_LEX), ("sexp", 20, SEED_BATCH + 1)):
+        g = api.Grammar(tables.load(name, "lexer"), device=local)
+        g._stream()
+        # training pairs: documents from other seeds, about 10^7 boundaries
+        t0 = time.perf_counter()
+        docs = [synth.json_doc(16 << 20, depth, SEED_TRAIN + k) if name == "json"
+                else synth.sexp_doc(16 << 20, depth, SEED_TRAIN + k) for k in range(10)]
+        win, lab = spec.dataset(g, docs, 1000000, SEED_TRAIN)
+        model = spec.BoundaryModel(g, seed=1)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        hist = model.train(win, lab, epochs=1, batch=4096, lr=2e-3)
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - t1
+        del win, lab
+        doc = synth.json_doc(size, depth, eval_seed) if name == "json" else synth.sexp_doc(size, depth, eval_seed)
+        x = torch.from_numpy(doc).to(dev)
+        ptrs = [ctypes.c_void_p() for _ in range(3)]
+        n_tok, valid = ctypes.c_int64(0), ctypes.c_int(0)
+
+        def plain():
+            rc = L.alp_lex(g.h, ctypes.c_void_p(x.data_ptr()), size, *[ctypes.byref(p) for p in ptrs],
+                           ctypes.byref(n_tok), ctypes.byref(valid))
+            if rc != 0 or not valid.value:
+                raise RuntimeError("alp_lex failed")
+
+        for _ in range(max(3, args.warmup)):
+            plain()
+        ms_plain, clk = _timed(plain, args.steps, local, dist)
+        clocks = clocks or clk
+        M = n_tok.value
+        ref = [api._wrap(g.h, p.value or 0, M, dt, g.device).clone()
+               for p, dt in zip(ptrs, (torch.int32, torch.int64, torch.int64))]
+        res = {"train_pairs": int(hist["steps"]) * 4096, "train_s": t_train, "train_acc": hist["last_acc"],
+               "plain_gbs": size / (ms_plain * 1e-3) / 1e9, "tokens": M, "chunks": {}}
+        Ls = spec._L()
+        sptr = [ctypes.c_void_p() for _ in range(3)]
+        sn, sv = ctypes.c_int64(0), ctypes.c_int(0)
+        stats = (ctypes.c_int64 * 4)()
+        for C in (256, 1024, 4096):
+
+            def sp():
+                rc = Ls.alp_lex_speculative(g.h, ctypes.c_void_p(model.wbf.data_ptr()),
+                                            ctypes.c_void_p(model.params.data_ptr()), model.n_states,
+                                            ctypes.c_void_p(x.data_ptr()), size, C, *[ctypes.byref(p) for p in sptr],
+                                            ctypes.byref(sn), ctypes.byref(sv), stats)
+                if rc != 0:
+                    raise RuntimeError("alp_lex_speculative failed: %s" % L.alp_last_error(g.h).decode())
+
+            for _ in range(max(3, args.warmup)):
+                sp()
+            ms_sp, _ = _timed(sp, args.steps, local, dist)
+            st = list(stats)
+            exact = bool(sv.value) and sn.value == M and all(
+                torch.equal(api._wrap(g.h, p.value or 0, M, r.dtype, g.device), r) for p, r in zip(sptr, ref))
+            res["chunks"][str(C)] = {"gbs": size / (ms_sp * 1e-3) / 1e9, "ms": ms_sp,
+                                     "hit_rate": 1.0 - st[1] / max(1, st[0]), "rerun_fraction": st[2] / max(1, st[0]),
+                                     "rounds": st[3], "bit_exact": bool(exact),
+                                     "vs_plain": ms_plain / ms_sp}
+            if not exact:
+                raise RuntimeError("speculative tokens differ from the plain lexer (%s, C=%d)" % (name, C))
+            if name == "json" and (best is None or ms_sp < best[1]):
+                best = (C, ms_sp, M)
+        g.profile(True)
+        model.lex(x, best[0] if name == "json" else 1024)
+        kern_all += [("%s:%s" % (name, k), t) for k, t in g.timings()]
+        g.profile(False)
+        results[name] = res
+        del x
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    C, ms, M = best
+    line = _line("input GB/s lex, learned boundary-state speculation (json.alp lexer, bit-exact)",
+                 world * size / (ms * 1e-3) / 1e9, world, args, ms,
+                 {"workload": "json.alp lexer on one %d MiB document (depth <= 8) with MLP-predicted chunk "
+                              "start states, best chunk size; sexp.alp in 'results'" % (size >> 20),
+                  "chunk": C, "doc_bytes": size, "results": results, "parallelism": "replicas",
+                  "l2": "inputs larger than L2 (no flush needed)"},
+                 size + 20 * M, kern_all,
+                 {"value": None, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                  "note": "speculation is a device-resident variant of alp_lex; see the lex workload for e2e"},
+                 clocks)
+    line["roofline"]["scope"] = "alp_lex_speculative: input bytes + 20 B per token, over the step time"
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--doc-mib", type=int, default=DOC_BYTES >> 20)
+    ap.add_argument("--doc-mib", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="parse", choices=["parse", "lex", "batch", "spec"])
+    ap.add_argument("--batch-docs", type=int, default=100000, help="JSON documents of the batch workload "
+                    "(half as many sexp documents); smaller values are for profiling")
     args = ap.parse_args()
+    args.doc_mib_given = args.doc_mib is not None
+    if args.doc_mib is None:
+        args.doc_mib = DOC_BYTES >> 20
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload != "parse":
+        return {"lex": run_lex, "batch": run_batch, "spec": run_spec}[args.workload](args, rank, world, local)
 
     import torch
     from alpacc_b200 import api, tables

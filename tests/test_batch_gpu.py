@@ -118,3 +118,62 @@ def test_single_doc_batch_equals_parse(has_gpu):
     assert valid.cpu().numpy()[0] == 1
     np.testing.assert_array_equal(tree.parent.cpu().numpy(), one.parent.cpu().numpy())
     np.testing.assert_array_equal(tree.start.cpu().numpy(), one.start.cpu().numpy())
+
+
+def _stress_layout(name):
+    """Documents that start exactly on 8 KiB and 16 KiB tile boundaries, runs
+    of hundreds of one- and two-byte documents (tiles holding more documents
+    than the shared offset list), empty documents between them, and documents
+    dense in tokens and nodes (a token every other byte)."""
+    o, c, one = (b"[", b"]", b"1") if name == "json" else (b"(", b")", b"a")
+    sep = b"," if name == "json" else b" "
+    dense = o + sep.join([one] * 6000) + c
+    docs, pos = [], 0
+
+    def add(d):
+        nonlocal pos
+        docs.append(d)
+        pos += len(d)
+
+    for boundary in (8192, 16384, 3 * 8192, 4 * 16384):
+        add(dense)
+        pad = (-pos) % boundary
+        if pad >= 2:
+            add(o + b" " * (pad - 2) + c)
+        elif pad == 1:
+            add(one)
+        add(b"")
+        add(o + one + c)
+    for i in range(700):
+        add(one if i % 3 else b"")
+        if i % 50 == 0:
+            add(o + c)
+    add(dense)
+    return docs
+
+
+@pytest.mark.parametrize("name", ["json", "sexp"])
+def test_parse_batch_tile_boundaries_and_dense(has_gpu, name):
+    g, o = _ctx(name, "both")
+    docs = _stress_layout(name)
+    data, off = _pack(docs)
+    tree, node_off, valid = g.parse_batch_int(data, off)
+    par, tag, kind, st, en = (x.cpu().numpy() for x in (tree.parent, tree.tag, tree.kind, tree.start, tree.end))
+    node_off, valid = node_off.cpu().numpy(), valid.cpu().numpy()
+    for i, d in enumerate(docs):
+        want = o.lex_parse(d)
+        assert bool(valid[i]) == (want is not None), (i, d[:40])
+        if want is None:
+            continue
+        a, b = node_off[i], node_off[i + 1]
+        for got, w in zip((par[a:b], tag[a:b].astype(np.uint32), kind[a:b], st[a:b], en[a:b]), want):
+            np.testing.assert_array_equal(got, w)
+    term, start, end, tok_off, lvalid = (x.cpu().numpy() for x in g.lex_batch_int(data, off))
+    for i, d in enumerate(docs):
+        want = o.lex_futhark(d)
+        assert bool(lvalid[i]) == (want is not None)
+        if want is not None:
+            a, b = tok_off[i], tok_off[i + 1]
+            np.testing.assert_array_equal(term[a:b].astype(np.uint32), want[0])
+            np.testing.assert_array_equal(start[a:b], want[1])
+            np.testing.assert_array_equal(end[a:b], want[2])
