@@ -61,6 +61,9 @@ struct alp_ctx {
     int prof = 0;
     std::vector<std::pair<const char*, cudaEvent_t>> marks;
     uint8_t* state_out = nullptr;         // set only inside alp_lex_states
+    long long last_tokens = 0;            // counts of the last call, for alp_ctx_info
+    long long last_positions = 0;
+    long long last_brackets = 0;
     DevBuf mlp[16];                       // MLP training activations
     DevBuf spec[16];                      // speculative lexer chunk arrays
 };
@@ -483,6 +486,7 @@ int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_
     CK(cudaStreamSynchronize(ctx->stream));
     if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
     *total = ctx->h_res->count;
+    ctx->last_tokens = *total;
     if (ctx->h_res->error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
     return ALP_OK;
 }
@@ -555,6 +559,7 @@ int lex_seg(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_o
     CK(cudaStreamSynchronize(ctx->stream));
     if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
     *total = ctx->h_res->count;
+    ctx->last_tokens = *total;
     if (ctx->h_res->error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
     return ALP_OK;
 }
@@ -616,6 +621,8 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     mark(ctx, "scan_tiles_reduce+scan_tiles");
     if ((rc = read_result(ctx, d_res))) return rc;
     const long long N = ctx->h_res->aux[0], B = ctx->h_res->aux[1];
+    ctx->last_positions = L;
+    ctx->last_brackets = B;
     if (N > 0xffffffffLL || B > 0xffffffffLL) return fail(ctx, ALP_ERR_ARG, "tree too large");
     if (ctx_out) {
         if ((rc = grow(ctx, ctx->out[3], N * 8 + 8)) || (rc = grow(ctx, ctx->out[4], N * 4 + 8)) ||
@@ -859,9 +866,10 @@ int alp_set_stream(alp_ctx* ctx, void* stream) {
 
 int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out) {
     if (!ctx || !out) return ALP_ERR_ARG;
-    int64_t v[8] = {ctx->has_lexer, ctx->has_parser, ctx->has_parser ? ctx->ph.n_terms : ctx->n_terms,
-                    ctx->ph.n_prods, ctx->ph.q, ctx->ph.k, ctx->ph.max_prods, ctx->ph.max_brackets};
-    for (int i = 0; i < n_out && i < 8; ++i) out[i] = v[i];
+    int64_t v[11] = {ctx->has_lexer, ctx->has_parser, ctx->has_parser ? ctx->ph.n_terms : ctx->n_terms,
+                     ctx->ph.n_prods, ctx->ph.q, ctx->ph.k, ctx->ph.max_prods, ctx->ph.max_brackets,
+                     ctx->last_tokens, ctx->last_positions, ctx->last_brackets};
+    for (int i = 0; i < n_out && i < 11; ++i) out[i] = v[i];
     return ALP_OK;
 }
 

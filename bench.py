@@ -206,6 +206,95 @@ def run_reference(args, rank: int, world: int):
 
 
 
+def _traffic_table():
+    """Per-unit DRAM bytes per launch of each kernel, from the committed ncu summary."""
+    out = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic_per_unit.txt")) as f:
+            for ln in f:
+                if ln.startswith("#") or not ln.strip():
+                    continue
+                k, unit, v = ln.split()
+                out[k] = (unit, float(v))
+    except OSError:
+        pass
+    return out
+
+
+def _kernel_alg_bytes(name, units, parse_layout=True):
+    """Algorithmic bytes of one launch: the inputs a kernel must read once and
+    the outputs it must write once for its part of the path.  units: n (input
+    bytes), m (tokens), L (parser positions), N (nodes), B (brackets)."""
+    n, m, L, N, B = (units.get(k, 0) for k in ("n", "m", "L", "N", "B"))
+    c = (n + 31) // 32
+    tok = 10 if parse_layout else 20
+    table = {
+        "parse_expand_kernel": 4 * L + 8 * m + 25 * N + 8 * B,   # ids in, spans in, node fields + brackets out
+        "ple_tile_kernel(nodes)": 12 * N,                      # values in, parents out
+        "ple_tile_kernel(brackets)": 8 * B,                    # depth values and symbols in
+        "lex3_emit_kernel": n + 3 * c + tok * m,               # bytes, chunk states and counts in, tokens out
+        "lex3_fold_kernel": n + 2 * c,                         # bytes in, chunk endomorphisms out
+        "lex3_count_kernel": n + 3 * c,                        # bytes, chunk states in, counts out
+        "parse_pairs_kernel": 4 * L,                           # terminal ids in, pair ids out
+    }
+    return table.get(name)
+
+
+def _unit_count(unit, units):
+    return {"node": units.get("N", 0), "bracket": units.get("B", 0), "byte": units.get("n", 0),
+            "position": units.get("L", 0)}.get(unit, 0)
+
+
+def _roofline(kern, units, ms_path, alg_path, parse_layout=True):
+    """roofline of the dominant kernel (achieved = its algorithmic bytes per
+    launch over its CUDA-event duration) and the whole call as path_roofline."""
+    peak, peak_kind = _peaks()
+    kms, share, top, _ = _kernels(kern)
+    name, tms = top
+    base = name.split(":")[-1]
+    alg = _kernel_alg_bytes(base, units, parse_layout)
+    tt = _traffic_table().get(base)
+    roof = {"bound": "hbm", "kernel": name, "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
+            "achieved": None, "frac": None, "traffic": None, "kernel_ms": tms}
+    if alg and tms:
+        roof["achieved"] = alg / (tms * 1e-3) / 1e9
+        roof["frac"] = roof["achieved"] / peak
+        roof["algorithmic_bytes"] = alg
+    if tt:
+        roof["traffic"] = tt[1] * _unit_count(tt[0], units)
+        roof["traffic_source"] = "ncu DRAM read+write per %s (profiles/traffic_per_unit.txt) x units" % tt[0]
+    path = {"achieved": alg_path / (ms_path * 1e-3) / 1e9, "unit": "GB/s"}
+    path["frac"] = path["achieved"] / peak
+    roof["kernels_ms"] = kms
+    roof["kernel_share"] = share
+    return roof, path
+
+
+def _profiled(g, step, reps: int):
+    """Per-kernel milliseconds averaged over `reps` instrumented calls."""
+    acc, order = {}, []
+    for _ in range(reps):
+        g.profile(True)
+        step()
+        for k, t in g.timings():
+            if k not in acc:
+                acc[k] = 0.0
+                order.append(k)
+            acc[k] += t
+        g.profile(False)
+    return [(k, acc[k] / reps) for k in order]
+
+
+def _ctx_counts(g):
+    import ctypes
+    from alpacc_b200 import api
+    L = api.native()
+    out = (ctypes.c_int64 * 11)()
+    L.alp_ctx_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    L.alp_ctx_info(g.h, out, 11)
+    return {"m": int(out[8]), "L": int(out[9]), "B": int(out[10])}
+
+
 SEED_LEX = 0xA1FACC00 + 1
 SEED_BATCH = 0xA1FACC00 + 3
 SEED_TRAIN = 0xA1FACC10
@@ -256,17 +345,14 @@ def _kernels(kern):
             sum(1 + k.count("+") for k, _ in kern))
 
 
-def _line(metric, value, world, args, ms, config, alg_bytes, kern, e2e, clocks, extra=None):
-    peak, peak_kind = _peaks()
-    kms, share, top, launches = _kernels(kern)
-    achieved = alg_bytes / (ms * 1e-3) / 1e9
+def _line(metric, value, world, args, ms, config, alg_bytes, kern, e2e, clocks, extra=None, units=None,
+          parse_layout=True):
+    _, _, _, launches = _kernels(kern)
+    roof, path = _roofline(kern, units or {}, ms, alg_bytes, parse_layout)
     line = {"metric": metric, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic", "config": config,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                         "dominant_kernel": top[0], "dominant_kernel_ms": top[1],
-                         "kernels_ms": kms, "kernel_share": share},
+            "roofline": roof, "path_roofline": path,
             "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clocks}
     if extra:
         line.update(extra)
@@ -299,10 +385,7 @@ def run_lex(args, rank: int, world: int, local: int):
         step()
     M = n_tok.value
     ms, clocks = _timed(step, args.steps, local, dist)
-    g.profile(True)
-    step()
-    kern = g.timings()
-    g.profile(False)
+    kern = _profiled(g, step, 3)
     # end to end: pinned host bytes in, tokens back to pinned host memory
     h_in = torch.from_numpy(doc).pin_memory()
     outs = [torch.empty(M, dtype=dt, pin_memory=True) for dt in (torch.int32, torch.int64, torch.int64)]
@@ -329,8 +412,9 @@ def run_lex(args, rank: int, world: int, local: int):
                   "l2": "inputs larger than L2 (no flush needed)"},
                  size + 20 * M, kern,
                  {"value": world * size / (ms_e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": size,
-                  "d2h_bytes_per_step": 20 * M, "ms_per_step": ms_e2e}, clocks)
-    line["roofline"]["scope"] = "whole alp_lex call: input bytes + 20 B per token, over the step time"
+                  "d2h_bytes_per_step": 20 * M, "ms_per_step": ms_e2e}, clocks,
+                 units={"n": size, "m": M}, parse_layout=False)
+    line["path_roofline"]["scope"] = "whole alp_lex call: input bytes + 20 B per token, over the step time"
     print(json.dumps(line), flush=True)
 
 
@@ -374,6 +458,7 @@ def run_batch(args, rank: int, world: int, local: int):
         call(st, st["x"], st["o"])
         kern += [("%s:%s" % (st["name"], k), t) for k, t in st["g"].timings()]
         st["g"].profile(False)
+        st["counts"] = _ctx_counts(st["g"])
         valid = _wrap_valid(st)
         st["accepted"] = int(valid.sum())
     # end to end: inputs and offsets from pinned host memory, the trees, node
@@ -417,12 +502,15 @@ def run_batch(args, rank: int, world: int, local: int):
     for st in sets:
         cfg[st["name"]] = {"docs": st["n_docs"], "bytes": len(st["data"]), "nodes": st["N"].value,
                            "accepted": st["accepted"]}
+    _, _, top, _ = _kernels(kern)
+    st_top = [st for st in sets if top[0].startswith(st["name"] + ":")][0]
+    units = dict(st_top["counts"], n=len(st_top["data"]), N=st_top["N"].value)
     line = _line("input GB/s batched lex+parse (json.alp + sexp.alp documents, bit-exact)",
                  world * n_bytes / (ms * 1e-3) / 1e9, world, args, ms, cfg, alg, kern,
                  {"value": world * n_bytes / (ms_e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
-                  "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}, clocks)
-    line["roofline"]["scope"] = ("both alp_parse_batch calls: input bytes + 29 B per node + 17 B per document "
-                                 "(offsets in, node offsets and validity out), over the step time")
+                  "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}, clocks, units=units)
+    line["path_roofline"]["scope"] = ("both alp_parse_batch calls: input bytes + 29 B per node + 17 B per "
+                                      "document (offsets in, node offsets and validity out), over the step time")
     print(json.dumps(line), flush=True)
 
 
@@ -530,8 +618,8 @@ def run_spec(args, rank: int, world: int, local: int):
                  size + 20 * M, kern_all,
                  {"value": None, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                   "note": "speculation is a device-resident variant of alp_lex; see the lex workload for e2e"},
-                 clocks)
-    line["roofline"]["scope"] = "alp_lex_speculative: input bytes + 20 B per token, over the step time"
+                 clocks, units={"n": size, "m": M}, parse_layout=False)
+    line["path_roofline"]["scope"] = "alp_lex_speculative: input bytes + 20 B per token, over the step time"
     print(json.dumps(line), flush=True)
 
 
@@ -607,11 +695,10 @@ def main():
         ms = float(t.item())
         dist.barrier()
 
-    # per-kernel breakdown from one instrumented step (outside the timed region)
-    g.profile(True)
-    step()
-    kern = g.timings()
-    g.profile(False)
+    # per-kernel breakdown: CUDA events between the launches of three instrumented
+    # steps right after the timed region, averaged per kernel
+    kern = _profiled(g, step, 3)
+    counts = _ctx_counts(g)
 
     # end to end through the host-buffer entry point
     h_in = torch.from_numpy(doc).pin_memory()
@@ -651,13 +738,11 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
-    peak, peak_kind = _peaks()
     alg_bytes = size + NODE_BYTES * N
-    achieved = alg_bytes / (ms * 1e-3) / 1e9
-    total_k = sum(t for _, t in kern) or 1.0
     # one mark per kernel, except "a+b" marks that cover two launches
     launches_per_step = sum(1 + k.count("+") for k, _ in kern)
-    top = max(kern, key=lambda x: x[1]) if kern else ("", 0.0)
+    roof, path = _roofline(kern, dict(counts, n=size, N=N), ms, alg_bytes)
+    path["scope"] = "whole alp_parse call: %d input bytes + %d B per node, over the step time" % (size, NODE_BYTES)
     line = {
         "metric": METRIC,
         "value": world * size / (ms * 1e-3) / 1e9,
@@ -675,13 +760,8 @@ def main():
                                "(depth <= %d), bytes -> preorder tree" % (args.doc_mib, DEPTH),
                    "doc_bytes": size, "nodes": N, "nodes_per_byte": N / size, "parallelism": "replicas",
                    "l2": "inputs larger than L2 (no flush needed)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                     "scope": "whole alp_parse call: %d input bytes + %d B per node, over the step time"
-                              % (size, NODE_BYTES),
-                     "dominant_kernel": top[0], "dominant_kernel_ms": top[1],
-                     "kernels_ms": {k: round(t, 4) for k, t in kern},
-                     "kernel_share": {k: round(t / total_k, 4) for k, t in kern}},
+        "roofline": roof,
+        "path_roofline": path,
         "e2e": {"value": world * size / (ms_e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": size,
                 "d2h_bytes_per_step": NODE_BYTES * N, "ms_per_step": ms_e2e},
         "gpu_launches": launches_per_step * args.steps,

@@ -60,7 +60,9 @@ const char* alp_last_error(const alp_ctx* ctx);
 int alp_set_stream(alp_ctx* ctx, void* stream);
 /* Grammar facts: out[0] has_lexer, [1] has_parser, [2] n_terminals,
  * [3] n_productions, [4] lookback q, [5] lookahead k, [6] max productions per
- * admissible pair, [7] max brackets per pair. */
+ * admissible pair, [7] max brackets per pair; counts of the last call on this
+ * context: [8] tokens, [9] parser positions (tokens + 2 per document),
+ * [10] brackets.  No reference counterpart (measurement support). */
 int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out);
 
 /* Per-kernel timing (no reference counterpart; measurement support): when on,
