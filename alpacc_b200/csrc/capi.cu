@@ -16,6 +16,7 @@
 #include "parser.cuh"
 #include "mlp.cuh"
 #include "spec.cuh"
+#include "spec3.cuh"
 
 using namespace alp;
 
@@ -383,30 +384,49 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
 
 // Multi-kernel lexer (DFAs of at most 32 states): chunk endomorphisms, the
 // state scan over them, token counts, the tile scan of the counts, and the
-// token pass.  Same contract as lex_seg.
-template <typename TermT, typename PosT>
-int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_off, long long nd, int sentinels,
-             TermT* term, PosT* start, PosT* end, long long cap, uint8_t* valid, long long* total) {
-    const long long tiles = (n + LX_TILE - 1) / LX_TILE;
-    const long long wide = (n + LX_WIDE - 1) / LX_WIDE;
-    const long long chunks = (n + LX_CHUNK - 1) / LX_CHUNK;
-    const long long stiles = (chunks + LS_TILE - 1) / LS_TILE;
+// token pass.  Same contract as lex_seg.  Split in stages so that the
+// speculative lexer can replace the front (states and counts per chunk).
+struct Lex3Run {
+    Lex3Args a;
+    LexSeg sg;
+    uint8_t* base;
+    size_t o_td, o_ccs;
+    long long tiles, wide, chunks, stiles, nd;
+    int sms;
+};
+
+int lex3_grid(alp_ctx* ctx, const Lex3Run& r, const void* k, int threads, size_t smem, long long work, unsigned* g) {
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem));
+    long long x = (long long)(per_sm > 0 ? per_sm : 1) * r.sms;
+    *g = (unsigned)(x < work ? x : work);
+    return ALP_OK;
+}
+
+int lex3_prepare(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_off, long long nd, int sentinels,
+                 void* term, void* start, void* end, long long cap, uint8_t* valid, Lex3Run& r) {
+    r.tiles = (n + LX_TILE - 1) / LX_TILE;
+    r.wide = (n + LX_WIDE - 1) / LX_WIDE;
+    r.chunks = (n + LX_CHUNK - 1) / LX_CHUNK;
+    r.stiles = (r.chunks + LS_TILE - 1) / LS_TILE;
+    r.nd = nd;
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t o_vec = 256, o_cs = o_vec + al(128 * (size_t)stiles), o_f = o_cs + al(8 * (size_t)tiles);
-    const size_t o_s = o_f + al(2 * (size_t)chunks + 64), o_c = o_s + al((size_t)chunks + 64);
-    const size_t o_td = o_c + al(2 * (size_t)chunks + 64);
-    const size_t o_ccs = o_td + al(8 * (size_t)tiles);
-    const size_t sbytes = o_ccs + al(8 * ((size_t)tiles / LT_CHUNK + 2));
+    const size_t o_vec = 256, o_cs = o_vec + al(128 * (size_t)r.stiles), o_f = o_cs + al(8 * (size_t)r.tiles);
+    const size_t o_s = o_f + al(2 * (size_t)r.chunks + 64), o_c = o_s + al((size_t)r.chunks + 64);
+    r.o_td = o_c + al(2 * (size_t)r.chunks + 64);
+    r.o_ccs = r.o_td + al(8 * (size_t)r.tiles);
+    const size_t sbytes = r.o_ccs + al(8 * ((size_t)r.tiles / LT_CHUNK + 2));
     int rc;
     if ((rc = grow(ctx, ctx->scratch, sbytes))) return rc;
     uint8_t* base = reinterpret_cast<uint8_t*>(ctx->scratch.p);
+    r.base = base;
     CK(cudaMemsetAsync(base, 0, o_cs, ctx->stream));  // result, tickets, look-back words
-    Lex3Args a;
+    Lex3Args& a = r.a;
     a.in = d_in;
     a.n = n;
     a.aligned16 = ((reinterpret_cast<uintptr_t>(d_in) & 15u) == 0) ? 1 : 0;
     a.t = ctx->l3;
-    a.n_chunks = chunks;
+    a.n_chunks = r.chunks;
     a.chunk_f = reinterpret_cast<uint16_t*>(base + o_f);
     a.chunk_s = base + o_s;
     a.chunk_c = reinterpret_cast<uint16_t*>(base + o_c);
@@ -414,15 +434,15 @@ int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_
     a.lb_vec = reinterpret_cast<uint32_t*>(base + o_vec);
     a.res = reinterpret_cast<AlpResult*>(base);
     a.tickets = reinterpret_cast<unsigned int*>(base + 128);
-    a.tile_doc = reinterpret_cast<const long long*>(base + o_td);
+    a.tile_doc = reinterpret_cast<const long long*>(base + r.o_td);
     a.out_term = term;
     a.out_start = start;
     a.out_end = end;
     a.cap = cap;
-    a.num_tiles = (unsigned)tiles;
-    a.num_wide = (unsigned)wide;
-    a.num_scan_tiles = (unsigned)stiles;
-    LexSeg sg;
+    a.num_tiles = (unsigned)r.tiles;
+    a.num_wide = (unsigned)r.wide;
+    a.num_scan_tiles = (unsigned)r.stiles;
+    LexSeg& sg = r.sg;
     sg.doc_off = d_off;
     sg.n_docs = nd;
     sg.tok_off = (long long*)ctx->tmp[T_TOKOFF].p;
@@ -430,65 +450,84 @@ int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_
     sg.sentinels = sentinels;
     sg.sent_l = ctx->has_parser ? ctx->pt.start : 0;
     sg.sent_r = ctx->has_parser ? ctx->pt.end : 0;
-    int sms = 0;
-    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    auto grid_of = [&](const void* k, int threads, size_t smem, long long work, unsigned* g) -> int {
-        int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem));
-        long long x = (long long)(per_sm > 0 ? per_sm : 1) * sms;
-        *g = (unsigned)(x < work ? x : work);
-        return ALP_OK;
-    };
-    auto k5 = lex3_emit_kernel<TermT, PosT>;
-    unsigned g1, g2, g3, g5;
+    CK(cudaDeviceGetAttribute(&r.sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    if (nd > 1) {
+        const long long gb = (nd + 255) / 256;
+        CK(cudaMemsetAsync(base + r.o_td, 0, 8 * (size_t)r.tiles, ctx->stream));
+        mark(ctx, "start");
+        lex3_tile_doc_kernel<<<(unsigned)(gb < 4096 ? gb : 4096), 256, 0, ctx->stream>>>(
+            d_off, nd, reinterpret_cast<long long*>(base + r.o_td), r.tiles);
+        CK(cudaGetLastError());
+        mark(ctx, "lex3_tile_doc_kernel");
+    }
+    return ALP_OK;
+}
+
+// chunk endomorphisms -> chunk states -> chunk counts and tile counts
+int lex3_front(alp_ctx* ctx, Lex3Run& r) {
+    unsigned g1, g2, g3;
+    int rc;
     CK(cudaFuncSetAttribute(lex3_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_fold_smem));
     CK(cudaFuncSetAttribute(lex3_fold_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     CK(cudaFuncSetAttribute(lex3_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_scan_smem));
     CK(cudaFuncSetAttribute(lex3_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_count_smem));
-    CK(cudaFuncSetAttribute(k5, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_emit_smem));
-    CK(cudaFuncSetAttribute(k5, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    if ((rc = grid_of((const void*)lex3_fold_kernel, LX_THREADS, ctx->l3_fold_smem, wide, &g1)) ||
-        (rc = grid_of((const void*)lex3_scan_kernel, LS_WARPS * 32, ctx->l3_scan_smem, stiles, &g2)) ||
-        (rc = grid_of((const void*)lex3_count_kernel, LX_THREADS, ctx->l3_count_smem, wide, &g3)) ||
-        (rc = grid_of((const void*)k5, LX_THREADS, ctx->l3_emit_smem, tiles, &g5)))
+    if ((rc = lex3_grid(ctx, r, (const void*)lex3_fold_kernel, LX_THREADS, ctx->l3_fold_smem, r.wide, &g1)) ||
+        (rc = lex3_grid(ctx, r, (const void*)lex3_scan_kernel, LS_WARPS * 32, ctx->l3_scan_smem, r.stiles, &g2)) ||
+        (rc = lex3_grid(ctx, r, (const void*)lex3_count_kernel, LX_THREADS, ctx->l3_count_smem, r.wide, &g3)))
         return rc;
     mark(ctx, "start");
-    if (nd > 1) {
-        const long long gb = (nd + 255) / 256;
-        CK(cudaMemsetAsync(base + o_td, 0, 8 * (size_t)tiles, ctx->stream));
-        lex3_tile_doc_kernel<<<(unsigned)(gb < 4096 ? gb : 4096), 256, 0, ctx->stream>>>(
-            d_off, nd, reinterpret_cast<long long*>(base + o_td), tiles);
-        CK(cudaGetLastError());
-        mark(ctx, "lex3_tile_doc_kernel");
-    }
-    lex3_fold_kernel<<<g1, LX_THREADS, ctx->l3_fold_smem, ctx->stream>>>(a, sg);
+    lex3_fold_kernel<<<g1, LX_THREADS, ctx->l3_fold_smem, ctx->stream>>>(r.a, r.sg);
     CK(cudaGetLastError());
     mark(ctx, "lex3_fold_kernel");
-    lex3_scan_kernel<<<g2, LS_WARPS * 32, ctx->l3_scan_smem, ctx->stream>>>(a);
+    lex3_scan_kernel<<<g2, LS_WARPS * 32, ctx->l3_scan_smem, ctx->stream>>>(r.a);
     CK(cudaGetLastError());
     mark(ctx, "lex3_scan_kernel");
-    lex3_count_kernel<<<g3, LX_THREADS, ctx->l3_count_smem, ctx->stream>>>(a, sg);
+    lex3_count_kernel<<<g3, LX_THREADS, ctx->l3_count_smem, ctx->stream>>>(r.a, r.sg);
     CK(cudaGetLastError());
     mark(ctx, "lex3_count_kernel");
+    return ALP_OK;
+}
+
+// tile scan of the counts -> token pass -> result
+template <typename TermT, typename PosT>
+int lex3_back(alp_ctx* ctx, Lex3Run& r, long long* total) {
+    auto k5 = lex3_emit_kernel<TermT, PosT>;
+    unsigned g5;
+    int rc;
+    CK(cudaFuncSetAttribute(k5, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_emit_smem));
+    CK(cudaFuncSetAttribute(k5, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    if ((rc = lex3_grid(ctx, r, (const void*)k5, LX_THREADS, ctx->l3_emit_smem, r.tiles, &g5))) return rc;
+    mark(ctx, "start");
     {
-        const long long lchunks = (tiles + LT_CHUNK - 1) / LT_CHUNK;
-        unsigned long long* ccs = reinterpret_cast<unsigned long long*>(base + o_ccs);
-        lex3_tile_reduce_kernel<<<(unsigned)lchunks, LT_CHUNK, 0, ctx->stream>>>(a.tile_cs, tiles, ccs);
+        const long long lchunks = (r.tiles + LT_CHUNK - 1) / LT_CHUNK;
+        unsigned long long* ccs = reinterpret_cast<unsigned long long*>(r.base + r.o_ccs);
+        lex3_tile_reduce_kernel<<<(unsigned)lchunks, LT_CHUNK, 0, ctx->stream>>>(r.a.tile_cs, r.tiles, ccs);
         CK(cudaGetLastError());
-        lex3_tile_scan_kernel<<<(unsigned)lchunks, LT_CHUNK, 0, ctx->stream>>>(a.tile_cs, tiles, ccs);
+        lex3_tile_scan_kernel<<<(unsigned)lchunks, LT_CHUNK, 0, ctx->stream>>>(r.a.tile_cs, r.tiles, ccs);
         CK(cudaGetLastError());
     }
     mark(ctx, "lex3_tile_reduce+lex3_tile_scan");
-    k5<<<g5, LX_THREADS, ctx->l3_emit_smem, ctx->stream>>>(a, sg);
+    k5<<<g5, LX_THREADS, ctx->l3_emit_smem, ctx->stream>>>(r.a, r.sg);
     CK(cudaGetLastError());
     mark(ctx, "lex3_emit_kernel");
-    CK(cudaMemcpyAsync(ctx->h_res, a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->h_res, r.a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
     *total = ctx->h_res->count;
     ctx->last_tokens = *total;
     if (ctx->h_res->error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
     return ALP_OK;
+}
+
+template <typename TermT, typename PosT>
+int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_off, long long nd, int sentinels,
+             TermT* term, PosT* start, PosT* end, long long cap, uint8_t* valid, long long* total) {
+    Lex3Run r;
+    int rc;
+    if ((rc = lex3_prepare(ctx, d_in, n, d_off, nd, sentinels, term, start, end, cap, valid, r)) ||
+        (rc = lex3_front(ctx, r)))
+        return rc;
+    return lex3_back<TermT, PosT>(ctx, r, total);
 }
 
 // Segmented lexer over documents at d_off[0..nd] (device).  sentinels: the
@@ -1281,6 +1320,112 @@ int alp_mlp_predict(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_
     return ALP_OK;
 }
 
+// Speculative lexing on the multi-kernel lexer: predicted block states
+// replace the fold and scan kernels (spec3.cuh); the tile scan and the token
+// pass are lex3's.  Block size `chunk` is a multiple of 256.
+static int spec3_lex(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_states, const uint8_t* d_in, int64_t n,
+                     int64_t chunk, uint32_t** d_term, int64_t** d_start, int64_t** d_end, int64_t* n_tok, int* valid,
+                     int64_t* stats) {
+    const long long K = (n + chunk - 1) / chunk;
+    DevBuf* sb = ctx->spec;
+    int rc;
+    if ((rc = grow(ctx, sb[0], K + 16)) || (rc = grow(ctx, sb[1], K + 16)) || (rc = grow(ctx, sb[4], K * 4 + 16)) ||
+        (rc = grow(ctx, sb[5], K * 4 + 16)) || (rc = grow(ctx, sb[10], K * 8 + 16)) || (rc = grow(ctx, sb[11], 64)) ||
+        (rc = grow(ctx, sb[12], K + 16)) || (rc = grow(ctx, ctx->tmp[T_TOKOFF], 16)) ||
+        (rc = grow(ctx, ctx->tmp[T_DVALID], 16)) || (rc = put_doc_off(ctx, n)))
+        return rc;
+    uint8_t* dvalid = (uint8_t*)ctx->tmp[T_DVALID].p;
+    int64_t cap = n / 2 + 1024;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        if ((rc = grow(ctx, ctx->out[0], cap * 4)) || (rc = grow(ctx, ctx->out[1], cap * 8)) ||
+            (rc = grow(ctx, ctx->out[2], cap * 8)))
+            return rc;
+        cap = (int64_t)(ctx->out[1].bytes / 8);
+        Lex3Run r;
+        if ((rc = lex3_prepare(ctx, d_in, n, (const long long*)ctx->tmp[T_DOCOFF].p, 1, 0, ctx->out[0].p,
+                               ctx->out[1].p, ctx->out[2].p, cap, dvalid, r)))
+            return rc;
+        SpecArgs sa;
+        memset(&sa, 0, sizeof sa);
+        sa.in = d_in;
+        sa.n = n;
+        sa.C = chunk;
+        sa.K = K;
+        sa.st = (uint8_t*)sb[0].p;
+        sa.en = (uint8_t*)sb[1].p;
+        uint32_t* lists[2] = {(uint32_t*)sb[4].p, (uint32_t*)sb[5].p};
+        unsigned int* next_n = (unsigned int*)sb[11].p;
+        // 1) predictions at every block boundary; block 0 starts in the initial state
+        CK(cudaMemsetAsync(sa.st, 1, 1, ctx->stream));
+        if (K > 1) {
+            long long* pos = (long long*)sb[10].p;
+            positions_kernel<<<grid_for(K - 1), 256, 0, ctx->stream>>>(pos, K - 1, chunk);
+            if ((rc = alp_mlp_predict(ctx, wbf, wf32, n_states, d_in, n, reinterpret_cast<const int64_t*>(pos), K - 1,
+                                      sa.st + 1)))
+                return rc;
+        }
+        // 2) every block from its predicted state, 3) re-run blocks until every start is exact
+        const size_t smem = ctx->l3_count_smem;
+        CK(cudaFuncSetAttribute(spec3_run_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        mark(ctx, "start");
+        spec3_run_kernel<<<grid_for(K), 256, smem, ctx->stream>>>(sa, r.a);
+        CK(cudaGetLastError());
+        mark(ctx, "spec3_run_kernel");
+        long long reruns = 0, first = -1, rounds = 0;
+        int cur = 0;
+        while (true) {
+            CK(cudaMemsetAsync(next_n, 0, 4, ctx->stream));
+            sa.list = nullptr;
+            sa.next_list = lists[cur];
+            sa.next_n = next_n;
+            spec_flag_kernel<<<grid_for(K), 256, 0, ctx->stream>>>(sa, (uint8_t*)sb[12].p);
+            spec_fix_kernel<<<grid_for(K), 256, 0, ctx->stream>>>(sa, (const uint8_t*)sb[12].p);
+            CK(cudaGetLastError());
+            unsigned int h_next = 0;
+            CK(cudaMemcpyAsync(ctx->h_stage, next_n, 4, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            memcpy(&h_next, ctx->h_stage, 4);
+            if (first < 0) first = h_next;
+            if (h_next == 0) break;
+            ++rounds;
+            reruns += h_next;
+            sa.list = lists[cur];
+            sa.list_n = h_next;
+            spec3_run_kernel<<<grid_for(h_next), 256, smem, ctx->stream>>>(sa, r.a);
+            CK(cudaGetLastError());
+            cur ^= 1;
+            if (rounds > 64) break;  // predictions too poor: the plain lexer decides
+        }
+        mark(ctx, "spec_verify");
+        if (rounds > 64) {
+            rc = alp_lex(ctx, d_in, n, d_term, d_start, d_end, n_tok, valid);
+            if (stats) { stats[0] = K; stats[1] = first; stats[2] = reruns; stats[3] = -1; }
+            return rc;
+        }
+        // 4) tile counts, tile scan, token pass
+        spec3_tiles_kernel<<<(unsigned)(r.tiles < 148 * 16 ? r.tiles : 148 * 16), LX_THREADS, 0, ctx->stream>>>(r.a);
+        CK(cudaGetLastError());
+        mark(ctx, "spec3_tiles_kernel");
+        long long total = 0;
+        rc = lex3_back<uint32_t, int64_t>(ctx, r, &total);
+        if (rc == ALP_ERR_CAPACITY) {
+            cap = total + 1;
+            continue;
+        }
+        if (rc) return rc;
+        int v = 0;
+        if ((rc = read_valid0(ctx, dvalid, &v))) return rc;
+        *valid = v;
+        *n_tok = v ? total : 0;
+        if (stats) { stats[0] = K; stats[1] = first; stats[2] = reruns; stats[3] = rounds; }
+        break;
+    }
+    *d_term = (uint32_t*)ctx->out[0].p;
+    *d_start = (int64_t*)ctx->out[1].p;
+    *d_end = (int64_t*)ctx->out[2].p;
+    return ALP_OK;
+}
+
 int alp_lex_speculative(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_states, const uint8_t* d_in,
                         int64_t n, int64_t chunk, uint32_t** d_term, int64_t** d_start, int64_t** d_end,
                         int64_t* n_tok, int* valid, int64_t* stats) {
@@ -1298,6 +1443,8 @@ int alp_lex_speculative(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, in
         *valid = (ctx->h_tokinfo[1] & TOK_ACCEPT) ? 1 : 0;
         return ALP_OK;
     }
+    if (ctx->lex3 && chunk % 256 == 0 && n <= 0x3fffffffLL)
+        return spec3_lex(ctx, wbf, wf32, n_states, d_in, n, chunk, d_term, d_start, d_end, n_tok, valid, stats);
     const long long K = (n + chunk - 1) / chunk;
     const long long nb = (K + SPEC_SCAN_BLOCK - 1) / SPEC_SCAN_BLOCK;
     DevBuf* sb = ctx->spec;

@@ -69,7 +69,7 @@ def test_mlp_predict_matches_reference(has_gpu):
 
 
 @pytest.mark.parametrize("name", ["json", "sexp"])
-@pytest.mark.parametrize("chunk", [256, 1024, 4096])
+@pytest.mark.parametrize("chunk", [128, 256, 1024, 4096])
 def test_speculative_tokens_exact(has_gpu, name, chunk):
     from alpacc_b200 import spec
     g, o = _g(name)
