@@ -1311,12 +1311,20 @@ int alp_mlp_predict(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_
     w.b2 = wf32 + P_B2;
     w.b3 = wf32 + P_B3;
     w.n_states = n_states;
-    CK(cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM));
+    int rc;
+    if ((rc = grow(ctx, ctx->mlp[15], (size_t)MLP_IN * MLP_H * 2))) return rc;
+    __nv_bfloat16* w1t = reinterpret_cast<__nv_bfloat16*>(ctx->mlp[15].p);
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    CK(cudaFuncSetAttribute(mlp_infer2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I2_SMEM));
+    const long long tiles = (count + I2_ROWS - 1) / I2_ROWS;
+    const long long grid = tiles < 2LL * sms ? tiles : 2LL * sms;
     mark(ctx, "start");
-    mlp_infer_kernel<<<(unsigned)((count + INF_ROWS - 1) / INF_ROWS), 256, INF_SMEM, ctx->stream>>>(
-        w, d_in, n, reinterpret_cast<const long long*>(d_pos), count, d_pred);
+    mlp_w1t_kernel<<<128, 256, 0, ctx->stream>>>(w.w1, w1t);
+    mlp_infer2_kernel<<<(unsigned)grid, I2_WARPS * 32, I2_SMEM, ctx->stream>>>(
+        w, w1t, d_in, n, reinterpret_cast<const long long*>(d_pos), count, d_pred);
     CK(cudaGetLastError());
-    mark(ctx, "mlp_infer_kernel");
+    mark(ctx, "mlp_w1t+mlp_infer2");
     return ALP_OK;
 }
 
@@ -1367,47 +1375,33 @@ static int spec3_lex(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n
         // 2) every block from its predicted state, 3) re-run blocks until every start is exact
         const size_t smem = ctx->l3_count_smem;
         CK(cudaFuncSetAttribute(spec3_run_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaFuncSetAttribute(spec3_fixup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         mark(ctx, "start");
-        spec3_run_kernel<<<grid_for(K), 256, smem, ctx->stream>>>(sa, r.a);
+        spec3_run_kernel<<<grid_for((K + 1) / 2), 256, smem, ctx->stream>>>(sa, r.a);
         CK(cudaGetLastError());
         mark(ctx, "spec3_run_kernel");
-        long long reruns = 0, first = -1, rounds = 0;
-        int cur = 0;
-        while (true) {
-            CK(cudaMemsetAsync(next_n, 0, 4, ctx->stream));
-            sa.list = nullptr;
-            sa.next_list = lists[cur];
-            sa.next_n = next_n;
-            spec_flag_kernel<<<grid_for(K), 256, 0, ctx->stream>>>(sa, (uint8_t*)sb[12].p);
-            spec_fix_kernel<<<grid_for(K), 256, 0, ctx->stream>>>(sa, (const uint8_t*)sb[12].p);
-            CK(cudaGetLastError());
-            unsigned int h_next = 0;
-            CK(cudaMemcpyAsync(ctx->h_stage, next_n, 4, cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
-            memcpy(&h_next, ctx->h_stage, 4);
-            if (first < 0) first = h_next;
-            if (h_next == 0) break;
-            ++rounds;
-            reruns += h_next;
-            sa.list = lists[cur];
-            sa.list_n = h_next;
-            spec3_run_kernel<<<grid_for(h_next), 256, smem, ctx->stream>>>(sa, r.a);
-            CK(cudaGetLastError());
-            cur ^= 1;
-            if (rounds > 64) break;  // predictions too poor: the plain lexer decides
-        }
-        mark(ctx, "spec_verify");
-        if (rounds > 64) {
-            rc = alp_lex(ctx, d_in, n, d_term, d_start, d_end, n_tok, valid);
-            if (stats) { stats[0] = K; stats[1] = first; stats[2] = reruns; stats[3] = -1; }
-            return rc;
-        }
+        CK(cudaMemsetAsync(next_n, 0, 4, ctx->stream));
+        sa.list = nullptr;
+        sa.next_list = lists[0];
+        sa.next_n = next_n;
+        spec_flag_kernel<<<grid_for(K), 256, 0, ctx->stream>>>(sa, (uint8_t*)sb[12].p);
+        spec_fix_kernel<<<grid_for(K), 256, 0, ctx->stream>>>(sa, (const uint8_t*)sb[12].p);
+        spec3_fixup_kernel<<<1, 256, smem, ctx->stream>>>(sa, r.a, lists[0], next_n, (const uint8_t*)sb[12].p, 64);
+        CK(cudaGetLastError());
+        mark(ctx, "spec_flag+spec_fix+spec3_fixup");
         // 4) tile counts, tile scan, token pass
         spec3_tiles_kernel<<<(unsigned)(r.tiles < 148 * 16 ? r.tiles : 148 * 16), LX_THREADS, 0, ctx->stream>>>(r.a);
         CK(cudaGetLastError());
         mark(ctx, "spec3_tiles_kernel");
         long long total = 0;
         rc = lex3_back<uint32_t, int64_t>(ctx, r, &total);
+        const long long rounds = ctx->h_res->aux[0], reruns = ctx->h_res->aux[1], first = ctx->h_res->aux[2];
+        if (rounds < 0) {
+            // predictions too poor for the fix-up rounds: the plain lexer decides
+            rc = alp_lex(ctx, d_in, n, d_term, d_start, d_end, n_tok, valid);
+            if (stats) { stats[0] = K; stats[1] = first; stats[2] = reruns; stats[3] = -1; }
+            return rc;
+        }
         if (rc == ALP_ERR_CAPACITY) {
             cap = total + 1;
             continue;

@@ -395,4 +395,206 @@ __global__ void __launch_bounds__(256) mlp_infer_kernel(MlpWeights w, const uint
     }
 }
 
+// ---------------------------------------------------------------------------
+// Inference, persistent: 128 windows per tile, one warp per 16 of them.
+// W1 comes in pre-transposed ([n][k], mlp_w1t_kernel) and streams through
+// shared memory in slabs of four window positions (k = 64) with cp.async
+// double buffering; the other weights stay in shared memory for the CTA's
+// lifetime.  Layers 2 and 3 take their A fragments straight from the previous
+// layer's accumulators (bias, ReLU, BF16 rounding in registers): an m16n8
+// accumulator pair is exactly an m16k16 A fragment.  Same arithmetic as
+// mlp_infer_kernel (BF16 operands, FP32 accumulation, BF16 activations).
+// ---------------------------------------------------------------------------
+constexpr int I2_WARPS = 8;
+constexpr int I2_ROWS = I2_WARPS * 16;          // windows per tile
+constexpr int I2_KPOS = 4;                      // window positions per W1 slab
+constexpr int I2_SLABS = MLP_WIN / I2_KPOS;
+constexpr int I2_LDK = I2_KPOS * MLP_EMB + 8;   // 72: k stride of a slab row
+constexpr int I2_LDH = MLP_H + 8;               // 136
+constexpr int I2_LDW = 80;                      // window row stride (bytes): 20 words, conflict-free rows
+constexpr size_t I2_SMEM = 256 * MLP_EMB * 2 + MLP_H * I2_LDH * 2 + MLP_OUT * I2_LDH * 2 +
+                           (MLP_H + MLP_H + MLP_OUT) * 4 + 2 * MLP_H * I2_LDK * 2 + I2_ROWS * I2_LDW;
+
+__global__ void mlp_w1t_kernel(const __nv_bfloat16* w1, __nv_bfloat16* w1t) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < MLP_IN * MLP_H; i += gridDim.x * blockDim.x) {
+        const int k = i / MLP_H, c = i % MLP_H;
+        w1t[c * MLP_IN + k] = w1[i];
+    }
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ uint32_t relu_pack(float x, float y) {
+    return pack2(__float2bfloat16(fmaxf(x, 0.f)), __float2bfloat16(fmaxf(y, 0.f)));
+}
+
+__global__ void __launch_bounds__(I2_WARPS * 32, 2) mlp_infer2_kernel(MlpWeights w, const __nv_bfloat16* w1t,
+                                                                      const uint8_t* in, long long n,
+                                                                      const long long* pos, long long count,
+                                                                      uint8_t* pred) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __nv_bfloat16* s_emb = reinterpret_cast<__nv_bfloat16*>(smem);                 // [256][16]
+    __nv_bfloat16* s_w2t = s_emb + 256 * MLP_EMB;                                   // [128][136]
+    __nv_bfloat16* s_w3t = s_w2t + MLP_H * I2_LDH;                                  // [32][136]
+    float* s_b1 = reinterpret_cast<float*>(s_w3t + MLP_OUT * I2_LDH);
+    float* s_b2 = s_b1 + MLP_H;
+    float* s_b3 = s_b2 + MLP_H;
+    __nv_bfloat16* s_w1 = reinterpret_cast<__nv_bfloat16*>(s_b3 + MLP_OUT);         // [2][128][72]
+    uint8_t* s_win = reinterpret_cast<uint8_t*>(s_w1 + 2 * MLP_H * I2_LDK);          // [128][80]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    for (int i = tid; i < 256 * MLP_EMB; i += I2_WARPS * 32) s_emb[i] = w.emb[i];
+    for (int i = tid; i < MLP_H * MLP_H; i += I2_WARPS * 32) s_w2t[(i % MLP_H) * I2_LDH + i / MLP_H] = w.w2[i];
+    for (int i = tid; i < MLP_H * MLP_OUT; i += I2_WARPS * 32) s_w3t[(i % MLP_OUT) * I2_LDH + i / MLP_OUT] = w.w3[i];
+    for (int i = tid; i < MLP_H; i += I2_WARPS * 32) { s_b1[i] = w.b1[i]; s_b2[i] = w.b2[i]; }
+    for (int i = tid; i < MLP_OUT; i += I2_WARPS * 32) s_b3[i] = w.b3[i];
+    const bool in16 = (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
+    const long long tiles = (count + I2_ROWS - 1) / I2_ROWS;
+
+    auto load_slab = [&](int s, int buf) {
+        __nv_bfloat16* dst = s_w1 + buf * MLP_H * I2_LDK;
+#pragma unroll
+        for (int q = 0; q < (MLP_H * 8) / (I2_WARPS * 32); ++q) {
+            const int idx = tid + q * I2_WARPS * 32;
+            const int nn = idx >> 3, c = idx & 7;
+            cp_async16(dst + nn * I2_LDK + c * 8, w1t + (size_t)nn * MLP_IN + s * (I2_KPOS * MLP_EMB) + c * 8);
+        }
+        cp_async_commit();
+    };
+
+    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const long long r0 = tile * I2_ROWS;
+        __syncthreads();  // the previous tile is done with s_win and the slabs
+        load_slab(0, 0);
+        // the tile's windows (spaces before the input's start and past its end)
+        for (int i = tid; i < I2_ROWS * 4; i += I2_WARPS * 32) {
+            const int r = i >> 2, q = i & 3;
+            uint4 v = make_uint4(0x20202020u, 0x20202020u, 0x20202020u, 0x20202020u);
+            if (r0 + r < count) {
+                const long long p0 = pos[r0 + r] - MLP_WIN + 16 * q;
+                if (in16 && p0 >= 0 && p0 + 16 <= n && (p0 & 15) == 0) {
+                    v = __ldg(reinterpret_cast<const uint4*>(in + p0));
+                } else {
+                    uint32_t x[4];
+#pragma unroll
+                    for (int b = 0; b < 16; ++b) {
+                        const long long at = p0 + b;
+                        const uint32_t by = (at >= 0 && at < n) ? in[at] : 0x20u;
+                        if ((b & 3) == 0) x[b >> 2] = 0;
+                        x[b >> 2] |= by << (8 * (b & 3));
+                    }
+                    v = make_uint4(x[0], x[1], x[2], x[3]);
+                }
+            }
+            *reinterpret_cast<uint4*>(s_win + r * I2_LDW + 16 * q) = v;
+        }
+        // ---- layer 1 ----
+        float acc[16][4];
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[j][q] = 0.f;
+        const int row = warp * 16 + g;
+        for (int s = 0; s < I2_SLABS; ++s) {
+            if (s + 1 < I2_SLABS) {
+                load_slab(s + 1, (s + 1) & 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            const __nv_bfloat16* slab = s_w1 + (s & 1) * MLP_H * I2_LDK;
+#pragma unroll
+            for (int kk = 0; kk < I2_KPOS; ++kk) {
+                const int p = s * I2_KPOS + kk;
+                const __nv_bfloat16* e0 = s_emb + s_win[row * I2_LDW + p] * MLP_EMB;
+                const __nv_bfloat16* e1 = s_emb + s_win[(row + 8) * I2_LDW + p] * MLP_EMB;
+                const uint32_t a0 = *reinterpret_cast<const uint32_t*>(e0 + 2 * t);
+                const uint32_t a1 = *reinterpret_cast<const uint32_t*>(e1 + 2 * t);
+                const uint32_t a2 = *reinterpret_cast<const uint32_t*>(e0 + 2 * t + 8);
+                const uint32_t a3 = *reinterpret_cast<const uint32_t*>(e1 + 2 * t + 8);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const __nv_bfloat16* bt = slab + (8 * j + g) * I2_LDK + kk * MLP_EMB + 2 * t;
+                    mma_bf16(acc[j], a0, a1, a2, a3, *reinterpret_cast<const uint32_t*>(bt),
+                             *reinterpret_cast<const uint32_t*>(bt + 8));
+                }
+            }
+            __syncthreads();  // all warps are done with this slab before it is refilled
+        }
+        // ---- layer 2: A fragments from the layer-1 accumulators ----
+        uint32_t ha[8][4];
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            const int c0 = 16 * s + 2 * t, c1 = c0 + 8;
+            ha[s][0] = relu_pack(acc[2 * s][0] + s_b1[c0], acc[2 * s][1] + s_b1[c0 + 1]);
+            ha[s][1] = relu_pack(acc[2 * s][2] + s_b1[c0], acc[2 * s][3] + s_b1[c0 + 1]);
+            ha[s][2] = relu_pack(acc[2 * s + 1][0] + s_b1[c1], acc[2 * s + 1][1] + s_b1[c1 + 1]);
+            ha[s][3] = relu_pack(acc[2 * s + 1][2] + s_b1[c1], acc[2 * s + 1][3] + s_b1[c1 + 1]);
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[j][q] = 0.f;
+#pragma unroll
+        for (int s = 0; s < 8; ++s)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const __nv_bfloat16* bt = s_w2t + (8 * j + g) * I2_LDH + 16 * s + 2 * t;
+                mma_bf16(acc[j], ha[s][0], ha[s][1], ha[s][2], ha[s][3], *reinterpret_cast<const uint32_t*>(bt),
+                         *reinterpret_cast<const uint32_t*>(bt + 8));
+            }
+        // ---- layer 3 ----
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            const int c0 = 16 * s + 2 * t, c1 = c0 + 8;
+            ha[s][0] = relu_pack(acc[2 * s][0] + s_b2[c0], acc[2 * s][1] + s_b2[c0 + 1]);
+            ha[s][1] = relu_pack(acc[2 * s][2] + s_b2[c0], acc[2 * s][3] + s_b2[c0 + 1]);
+            ha[s][2] = relu_pack(acc[2 * s + 1][0] + s_b2[c1], acc[2 * s + 1][1] + s_b2[c1 + 1]);
+            ha[s][3] = relu_pack(acc[2 * s + 1][2] + s_b2[c1], acc[2 * s + 1][3] + s_b2[c1 + 1]);
+        }
+        float z[4][4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) z[j][q] = 0.f;
+#pragma unroll
+        for (int s = 0; s < 8; ++s)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const __nv_bfloat16* bt = s_w3t + (8 * j + g) * I2_LDH + 16 * s + 2 * t;
+                mma_bf16(z[j], ha[s][0], ha[s][1], ha[s][2], ha[s][3], *reinterpret_cast<const uint32_t*>(bt),
+                         *reinterpret_cast<const uint32_t*>(bt + 8));
+            }
+        // argmax over the valid logits of rows g and g + 8 (lowest index on ties)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float bv = -INFINITY;
+            int bi = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int c = j * 8 + t * 2 + q;
+                    const float v = c < w.n_states ? z[j][h * 2 + q] + s_b3[c] : -INFINITY;
+                    if (v > bv) { bv = v; bi = c; }
+                }
+#pragma unroll
+            for (int d = 1; d < 4; d <<= 1) {
+                const float ov = __shfl_xor_sync(ALP_FULL_MASK, bv, d);
+                const int oi = __shfl_xor_sync(ALP_FULL_MASK, bi, d);
+                if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+            }
+            const long long r = r0 + warp * 16 + g + h * 8;
+            if (t == 0 && r < count) pred[r] = (uint8_t)bi;
+        }
+    }
+}
+
 }  // namespace alp
