@@ -645,7 +645,16 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     const size_t sm1 = sizeof(PairInfo) * ctx->pt.n_pairs + (size_t)(PP_TILE + ctx->pt.q + ctx->pt.k) * 4;
     CK(cudaFuncSetAttribute(parse_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
     mark(ctx, "start");
-    parse_pairs_kernel<<<(unsigned)tiles, PP_THREADS, sm1, ctx->stream>>>(a);
+    unsigned g_pairs = 1, g_expand = 1;
+    {
+        int sms = 0, per1 = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, parse_pairs_kernel, PP_THREADS, sm1));
+        const long long x = (long long)(per1 > 0 ? per1 : 1) * sms;
+        g_pairs = (unsigned)(x < tiles ? x : tiles);
+        g_expand = (unsigned)(2LL * sms < tiles ? 2LL * sms : tiles);  // persistent; set below from occupancy
+    }
+    parse_pairs_kernel<<<g_pairs, PP_THREADS, sm1, ctx->stream>>>(a);
     CK(cudaGetLastError());
     mark(ctx, "parse_pairs_kernel");
     {
@@ -694,7 +703,14 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     if (sm2 > 220 * 1024) return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
     CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
     mark(ctx, "start");
-    parse_expand_kernel<<<(unsigned)tiles, PP_THREADS, sm2, ctx->stream>>>(a);
+    {
+        int sms = 0, per2 = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, parse_expand_kernel, PP_THREADS, sm2));
+        const long long x = (long long)(per2 > 0 ? per2 : 1) * sms;
+        g_expand = (unsigned)(x < tiles ? x : tiles);
+    }
+    parse_expand_kernel<<<g_expand, PP_THREADS, sm2, ctx->stream>>>(a);
     CK(cudaGetLastError());
     mark(ctx, "parse_expand_kernel");
     if (want_tree) {

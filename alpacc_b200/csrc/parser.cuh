@@ -329,8 +329,11 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
         uint32_t pw = 1;
         for (int j = 0; j < W; ++j) { s_pow[W - 1 - j] = pw; pw *= (uint32_t)a.t.T; }
     }
-    const long long base = (long long)blockIdx.x * PP_TILE;
+    const long long n_tiles = (a.L + PP_TILE - 1) / PP_TILE;
+    for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const long long base = tile * PP_TILE;
     const int span = PP_TILE + W;  // window [base - q, base + PP_TILE + k)
+    __syncthreads();  // the previous tile is done with s_term and s_w
     for (int i = tid; i < span; i += PP_THREADS) s_term[i] = pos_term(a, base - q + i);
     __syncthreads();
     const uint32_t SL = a.t.start, SR = a.t.end, EMPTY = a.t.empty;
@@ -383,7 +386,8 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
     if (tid == 0) {
         PosSums t = s_w[0];
         for (int w = 1; w < PP_THREADS / 32; ++w) t = ps_combine(t, s_w[w]);
-        a.tile_sums[blockIdx.x] = t;
+        a.tile_sums[tile] = t;
+    }
     }
 }
 
@@ -536,7 +540,10 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     for (int i = tid; i < a.t.n_pseq; i += PP_THREADS) s_prec[i] = a.t.pseq_rec[i];
     for (int i = tid; i < a.t.n_stack; i += PP_THREADS) s_srec[i] = a.t.stack_rec[i];
     const uint32_t SL = a.t.start, SR = a.t.end;
-    const long long tbase = (long long)blockIdx.x * PP_TILE;
+    const long long n_tiles = (a.L + PP_TILE - 1) / PP_TILE;
+    for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    __syncthreads();  // the previous tile is done with the stage and the scan arrays
+    const long long tbase = tile * PP_TILE;
     const long long i0 = tbase + tid * PP_ITEMS;
     uint16_t ids[PP_ITEMS];
     uint32_t hm = 0, em = 0;  // head / end bits of this thread's positions
@@ -571,7 +578,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
         if (lane == PP_THREADS / 32 - 1) { s_tn = (uint32_t)wi.nodes; s_tb = (uint32_t)wi.brs; }
     }
     __syncthreads();
-    const PosSums tp = a.tile_sums[blockIdx.x];
+    const PosSums tp = a.tile_sums[tile];
     const PosSums run0 = ps_combine(ps_combine(tp, s_w[warp]), ex);  // before this thread's first position
     const uint32_t tn = s_tn, tb = s_tb;
     // Tile-local first node / bracket of every thread.  A tile with more than
@@ -745,6 +752,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             }
         }
         __syncthreads();
+    }
     }
 }
 
