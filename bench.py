@@ -300,22 +300,30 @@ SEED_BATCH = 0xA1FACC00 + 3
 SEED_TRAIN = 0xA1FACC10
 
 
-def _dist_init(world: int):
+def _dist_init(world: int, backend: str = "nccl"):
+    """Process group for N > 1 ranks (one per GPU; gloo for the CPU tests),
+    with a short timeout so that ranks waiting for a dead peer fail."""
     if world <= 1:
         return None
     import datetime
     import torch.distributed as dist
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return dist
 
 
-def _max_over_ranks(ms: float, dist, local: int) -> float:
+def _max_over_ranks(ms: float, dist, device) -> float:
+    """The step time of the job: the slowest rank's."""
     if not dist:
         return ms
     import torch
-    t = torch.tensor([ms], device=f"cuda:{local}")
+    t = torch.tensor([ms], dtype=torch.float64, device=device if isinstance(device, str) else f"cuda:{device}")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def _gbs(world: int, bytes_per_rank: int, ms: float) -> float:
+    """Whole-job input GB/s: every rank processes bytes_per_rank (weak scaling)."""
+    return world * bytes_per_rank / (ms * 1e-3) / 1e9
 
 
 def _timed(step, steps: int, local: int, dist):
@@ -404,14 +412,14 @@ def run_lex(args, rank: int, world: int, local: int):
         dist.destroy_process_group()
     if rank != 0:
         return
-    line = _line("input GB/s lex (json.alp lexer-only, plain scan, bit-exact)", world * size / (ms * 1e-3) / 1e9,
+    line = _line("input GB/s lex (json.alp lexer-only, plain scan, bit-exact)", _gbs(world, size, ms),
                  world, args, ms,
                  {"workload": "json.alp lexer only, one %d MiB synthetic JSON document per GPU (depth <= 8), "
                               "bytes -> (u32 id, i64 start, i64 end) tokens" % (size >> 20),
                   "doc_bytes": size, "tokens": M, "tokens_per_byte": M / size, "parallelism": "replicas",
                   "l2": "inputs larger than L2 (no flush needed)"},
                  size + 20 * M, kern,
-                 {"value": world * size / (ms_e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": size,
+                 {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": size,
                   "d2h_bytes_per_step": 20 * M, "ms_per_step": ms_e2e}, clocks,
                  units={"n": size, "m": M}, parse_layout=False)
     line["path_roofline"]["scope"] = "whole alp_lex call: input bytes + 20 B per token, over the step time"
@@ -506,8 +514,8 @@ def run_batch(args, rank: int, world: int, local: int):
     st_top = [st for st in sets if top[0].startswith(st["name"] + ":")][0]
     units = dict(st_top["counts"], n=len(st_top["data"]), N=st_top["N"].value)
     line = _line("input GB/s batched lex+parse (json.alp + sexp.alp documents, bit-exact)",
-                 world * n_bytes / (ms * 1e-3) / 1e9, world, args, ms, cfg, alg, kern,
-                 {"value": world * n_bytes / (ms_e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                 _gbs(world, n_bytes, ms), world, args, ms, cfg, alg, kern,
+                 {"value": _gbs(world, n_bytes, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": h2d,
                   "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}, clocks, units=units)
     line["path_roofline"]["scope"] = ("both alp_parse_batch calls: input bytes + 29 B per node + 17 B per "
                                       "document (offsets in, node offsets and validity out), over the step time")
@@ -610,7 +618,7 @@ def run_spec(args, rank: int, world: int, local: int):
         return
     C, ms, M = best
     line = _line("input GB/s lex, learned boundary-state speculation (json.alp lexer, bit-exact)",
-                 world * size / (ms * 1e-3) / 1e9, world, args, ms,
+                 _gbs(world, size, ms), world, args, ms,
                  {"workload": "json.alp lexer on one %d MiB document (depth <= 8) with MLP-predicted chunk "
                               "start states, best chunk size; sexp.alp in 'results'" % (size >> 20),
                   "chunk": C, "doc_bytes": size, "results": results, "parallelism": "replicas",
@@ -650,11 +658,7 @@ def main():
     from alpacc_b200 import api, tables
 
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = _dist_init(world)
     size = args.doc_mib << 20
     doc = make_doc(SEED + 1000 * rank, size)
     g = api.Grammar(tables.load("json", "both"), device=local)
@@ -688,11 +692,8 @@ def main():
             step()
         ev1.record(stream)
         torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = _max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, local)
     if dist:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
 
     # per-kernel breakdown: CUDA events between the launches of three instrumented
@@ -723,11 +724,7 @@ def main():
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_e2e = e0.elapsed_time(e1) / k_e2e
-    if dist:
-        t = torch.tensor([ms_e2e], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = _max_over_ranks(e0.elapsed_time(e1) / k_e2e, dist, local)
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -745,7 +742,7 @@ def main():
     path["scope"] = "whole alp_parse call: %d input bytes + %d B per node, over the step time" % (size, NODE_BYTES)
     line = {
         "metric": METRIC,
-        "value": world * size / (ms * 1e-3) / 1e9,
+        "value": _gbs(world, size, ms),
         "unit": "GB/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -762,7 +759,7 @@ def main():
                    "l2": "inputs larger than L2 (no flush needed)"},
         "roofline": roof,
         "path_roofline": path,
-        "e2e": {"value": world * size / (ms_e2e * 1e-3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": size,
+        "e2e": {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": size,
                 "d2h_bytes_per_step": NODE_BYTES * N, "ms_per_step": ms_e2e},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
