@@ -939,17 +939,28 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
                 const int e = q[qb + lane];
                 const int32_t x = s_val[ple_pad(e)];
                 const long long g = base + e;
-                int node = PLE_THREADS + e / PLE_ITEMS;  // chunks left of the element's
-                bool found = false;
-                while (node > 1) {
-                    if ((node & 1) && tree[node - 1] <= x) { node = node - 1; found = true; break; }
-                    node >>= 1;
+                // the nearest earlier chunk with minimum <= x: the few chunks just
+                // before the element's first (most answers are near), then the tree
+                const int ce = e / PLE_ITEMS;
+                int c = -1;
+#pragma unroll
+                for (int back = 1; back <= 4; ++back)
+                    if (c < 0 && ce - back >= 0 && tree[PLE_THREADS + ce - back] <= x) c = ce - back;
+                bool found = c >= 0;
+                if (!found && ce > 4) {
+                    int node = PLE_THREADS + ce - 4;  // chunks left of those
+                    while (node > 1) {
+                        if ((node & 1) && tree[node - 1] <= x) { node = node - 1; found = true; break; }
+                        node >>= 1;
+                    }
+                    if (found) {
+                        while (node < PLE_THREADS) node = (tree[2 * node + 1] <= x) ? 2 * node + 1 : 2 * node;
+                        c = node - PLE_THREADS;
+                    }
                 }
                 const long long dq = sd0 == sd1 ? sd0 : seg_upper(a.seg_off, sd0, sd1, g);
                 const long long dqb = a.seg_off[dq];
                 if (found) {
-                    while (node < PLE_THREADS) node = (tree[2 * node + 1] <= x) ? 2 * node + 1 : 2 * node;
-                    const int c = node - PLE_THREADS;
                     const int4 sm = s_sub[c];
                     const int qq = sm.w <= x ? 3 : (sm.z <= x ? 2 : (sm.y <= x ? 1 : 0));
                     const int32_t* cv = s_val + c * PLE_STRIDE + 4 * qq;
