@@ -67,6 +67,14 @@ def native() -> ctypes.CDLL:
         L.alp_pre_productions.argtypes = [vp, vp, i64, P(vp), P(i64), P(i32)]
         L.alp_lex_batch.argtypes = [vp, vp, vp, i64, P(vp), P(vp), P(vp), P(vp), P(vp), P(i64)]
         L.alp_parse_batch.argtypes = [vp, vp, vp, i64, P(vp), P(vp), P(vp), P(vp), P(vp), P(vp), P(vp), P(i64)]
+        L.alp_lex_stream_begin.argtypes = [vp, vp, vp, vp, i64, P(vp)]
+        L.alp_lex_stream_push.argtypes = [vp, vp, i64]
+        L.alp_lex_stream_tokens.argtypes = [vp, P(i64)]
+        L.alp_lex_stream_end.argtypes = [vp, P(i64), P(i32)]
+        L.alp_lex_stream_window.argtypes = [vp, vp, vp, vp, i64, i64]
+        L.alp_lex_stream_free.argtypes = [vp]
+        L.alp_lex_stream_free.restype = None
+        L.alp_lex_host_stream.argtypes = [vp, vp, i64, i64, vp, vp, vp, i64, P(i64), P(i32)]
         _lib = L
     return _lib
 
@@ -219,6 +227,33 @@ class Grammar:
         k = n.value
         return term[:k], start[:k], end[:k]
 
+    def lex_stream(self, cap: int) -> "TokenStream":
+        """A token stream over input pushed in pieces (alp_lex_stream_*),
+        writing up to `cap` tokens into device tensors it owns."""
+        return TokenStream(self, cap)
+
+    def lex_host_stream(self, data: np.ndarray, piece: int = 0, out=None):
+        """alp_lex_host through alp_lex_host_stream: the input in pieces with
+        the copies in and out overlapped with the lexing.  `out`: optional
+        (term uint32, start int64, end int64) host arrays (pinned for overlap)."""
+        arr = np.ascontiguousarray(data, dtype=np.uint8)
+        if out is None:
+            cap = len(arr) + 1
+            out = (np.empty(cap, np.uint32), np.empty(cap, np.int64), np.empty(cap, np.int64))
+        term, start, end = out
+        cap = min(len(term), len(start), len(end))
+        n, valid = ctypes.c_int64(0), ctypes.c_int(0)
+        self._stream()
+        ptr = lambda a: ctypes.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
+        rc = native().alp_lex_host_stream(self.h, ptr(arr), len(arr), piece, ptr(term), ptr(start), ptr(end), cap,
+                                          ctypes.byref(n), ctypes.byref(valid))
+        if rc != ALP_OK:
+            self._err(rc)
+        if not valid.value:
+            return None
+        k = n.value
+        return term[:k], start[:k], end[:k]
+
     # ----------------------------------------------------------------- parser
     def _tree(self, pp, pt, pk, ps, pe, n) -> Tree:
         torch = _torch()
@@ -358,3 +393,80 @@ class Grammar:
         tree = self._tree(*ptrs[:5], k)
         return (tree, _wrap(self.h, ptrs[5].value or 0, nd + 1, torch.int64, self.device),
                 _wrap(self.h, ptrs[6].value or 0, nd, torch.uint8, self.device))
+
+
+class TokenStream:
+    """Input lexed as it arrives: ``push`` pieces (bytes, numpy or uint8
+    tensors), then ``end`` for the tokens of the whole stream, equal to
+    ``Grammar.lex_int`` of the concatenation (None when rejected).  ``tokens``
+    waits for the pushed pieces and gives the count of tokens final so far."""
+
+    def __init__(self, grammar: Grammar, cap: int):
+        torch = _torch()
+        self.g = grammar
+        self.term = torch.empty(max(cap, 1), dtype=torch.int32, device=grammar.device)
+        self.start = torch.empty(max(cap, 1), dtype=torch.int64, device=grammar.device)
+        self.end_ = torch.empty(max(cap, 1), dtype=torch.int64, device=grammar.device)
+        self._pending = []  # pieces the GPU may still read
+        self.first = 0
+        grammar._stream()
+        h = ctypes.c_void_p()
+        rc = native().alp_lex_stream_begin(grammar.h, ctypes.c_void_p(self.term.data_ptr()),
+                                           ctypes.c_void_p(self.start.data_ptr()),
+                                           ctypes.c_void_p(self.end_.data_ptr()), cap, ctypes.byref(h))
+        if rc != ALP_OK:
+            grammar._err(rc)
+        self.h = h
+
+    def push(self, data) -> None:
+        x = self.g._as_device_bytes(data)
+        self.g._stream()
+        rc = native().alp_lex_stream_push(self.h, ctypes.c_void_p(x.data_ptr()), x.numel())
+        if rc != ALP_OK:
+            self.g._err(rc)
+        self._pending.append(x)
+
+    def tokens(self) -> int:
+        n = ctypes.c_int64(0)
+        rc = native().alp_lex_stream_tokens(self.h, ctypes.byref(n))
+        if rc != ALP_OK:
+            self.g._err(rc)
+        self._pending.clear()
+        return n.value
+
+    def window(self, first: int) -> None:
+        """Later tokens go to element ``token index - first`` of this stream's
+        buffers; tokens before ``first`` are not stored."""
+        rc = native().alp_lex_stream_window(self.h, ctypes.c_void_p(self.term.data_ptr()),
+                                            ctypes.c_void_p(self.start.data_ptr()),
+                                            ctypes.c_void_p(self.end_.data_ptr()), self.term.numel(), first)
+        if rc != ALP_OK:
+            self.g._err(rc)
+        self.first = first
+
+    def finish(self) -> Tuple[int, bool]:
+        """Ends the stream: (tokens written in all, accepted)."""
+        n, valid = ctypes.c_int64(0), ctypes.c_int(0)
+        rc = native().alp_lex_stream_end(self.h, ctypes.byref(n), ctypes.byref(valid))
+        self._pending.clear()
+        if rc != ALP_OK:
+            self.g._err(rc)
+        return n.value, bool(valid.value)
+
+    def end(self):
+        k, ok = self.finish()
+        if not ok:
+            return None
+        k -= self.first
+        return self.term[:k], self.start[:k], self.end_[:k]
+
+    def close(self) -> None:
+        if self.h:
+            native().alp_lex_stream_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -67,6 +67,26 @@ struct alp_ctx {
     long long last_brackets = 0;
     DevBuf mlp[16];                       // MLP training activations
     DevBuf spec[16];                      // speculative lexer chunk arrays
+    // host-input token streams (alp_lex_host_stream): copy streams, events,
+    // two slots of piece and token buffers, the carry and its pinned mirrors
+    cudaStream_t cp_in = nullptr, cp_out = nullptr;
+    cudaEvent_t ev_in[2] = {}, ev_done[2] = {}, ev_out[2] = {};
+    DevBuf pipe;
+    DevBuf carry;
+    LexCarry* h_carry = nullptr;          // pinned, [2]
+};
+
+struct alp_lex_stream {
+    alp_ctx* ctx = nullptr;
+    LexCarry* d_carry = nullptr;
+    LexCarry* h_carry = nullptr;          // pinned
+    uint32_t* term = nullptr;
+    int64_t* start = nullptr;
+    int64_t* end = nullptr;
+    long long cap = 0;
+    long long pos = 0;                    // bytes pushed so far
+    long long first = 0;                  // stream token stored at element 0 of the outputs
+    int ended = 0;
 };
 
 namespace {
@@ -442,7 +462,13 @@ int lex3_prepare(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long
     a.num_tiles = (unsigned)r.tiles;
     a.num_wide = (unsigned)r.wide;
     a.num_scan_tiles = (unsigned)r.stiles;
+    a.carry = nullptr;
+    a.pos_base = 0;
+    a.carry_tokens = 0;
+    a.tok_first = 0;
     LexSeg& sg = r.sg;
+    sg.cont = 0;
+    sg.end1 = 0;
     sg.doc_off = d_off;
     sg.n_docs = nd;
     sg.tok_off = (long long*)ctx->tmp[T_TOKOFF].p;
@@ -488,9 +514,9 @@ int lex3_front(alp_ctx* ctx, Lex3Run& r) {
     return ALP_OK;
 }
 
-// tile scan of the counts -> token pass -> result
+// tile scan of the counts -> token pass (stream-ordered, no wait)
 template <typename TermT, typename PosT>
-int lex3_back(alp_ctx* ctx, Lex3Run& r, long long* total) {
+int lex3_emit(alp_ctx* ctx, Lex3Run& r) {
     auto k5 = lex3_emit_kernel<TermT, PosT>;
     unsigned g5;
     int rc;
@@ -510,6 +536,14 @@ int lex3_back(alp_ctx* ctx, Lex3Run& r, long long* total) {
     k5<<<g5, LX_THREADS, ctx->l3_emit_smem, ctx->stream>>>(r.a, r.sg);
     CK(cudaGetLastError());
     mark(ctx, "lex3_emit_kernel");
+    return ALP_OK;
+}
+
+// tile scan of the counts -> token pass -> result
+template <typename TermT, typename PosT>
+int lex3_back(alp_ctx* ctx, Lex3Run& r, long long* total) {
+    int rc;
+    if ((rc = lex3_emit<TermT, PosT>(ctx, r))) return rc;
     CK(cudaMemcpyAsync(ctx->h_res, r.a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
@@ -574,7 +608,7 @@ int lex_seg(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_o
     a.cap = cap;
     a.num_tiles = (unsigned)tiles;
     a.state_out = nullptr;
-    LexSeg sg;
+    LexSeg sg{};
     sg.doc_off = d_off;
     sg.n_docs = nd;
     sg.tok_off = (long long*)ctx->tmp[T_TOKOFF].p;
@@ -908,6 +942,16 @@ void alp_ctx_destroy(alp_ctx* ctx) {
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
     if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     for (auto& m : ctx->marks) cudaEventDestroy(m.second);
+    if (ctx->pipe.p) cudaFree(ctx->pipe.p);
+    if (ctx->carry.p) cudaFree(ctx->carry.p);
+    if (ctx->h_carry) cudaFreeHost(ctx->h_carry);
+    for (int i = 0; i < 2; ++i) {
+        if (ctx->ev_in[i]) cudaEventDestroy(ctx->ev_in[i]);
+        if (ctx->ev_done[i]) cudaEventDestroy(ctx->ev_done[i]);
+        if (ctx->ev_out[i]) cudaEventDestroy(ctx->ev_out[i]);
+    }
+    if (ctx->cp_in) cudaStreamDestroy(ctx->cp_in);
+    if (ctx->cp_out) cudaStreamDestroy(ctx->cp_out);
     delete ctx;
 }
 
@@ -1117,6 +1161,251 @@ int alp_lex_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, uint32_t* h_term,
         CK(cudaMemcpyAsync(h_end, de, (size_t)*n_tok * 8, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
     }
+    return ALP_OK;
+}
+
+
+// ---- token streams ----------------------------------------------------------
+// Input that arrives in pieces, lexed piece by piece with the DFA state and the
+// start of the token in progress carried on the device, so that the tokens are
+// those of alp_lex on the concatenation (the reference's chunk loop:
+// futhark/lexer.fut:148-160, cuda/lexer.cu:452-543).  A piece writes the tokens
+// that end inside it; the last token follows when the stream ends.
+
+// One piece [d_in, d_in + n) at stream position pos: the five lexer kernels
+// with the carry as entry state and no end of input, then the carry update.
+// global: tokens go after carry->tokens, else from index 0.  Stream-ordered.
+static int stream_piece(alp_ctx* ctx, LexCarry* carry, const uint8_t* d_in, long long n, long long pos, int global,
+                        long long first, uint32_t* term, int64_t* start, int64_t* end, long long cap) {
+    int rc;
+    if ((rc = grow(ctx, ctx->tmp[T_TOKOFF], 64))) return rc;
+    Lex3Run r;
+    if ((rc = lex3_prepare(ctx, d_in, n, nullptr, 1, 0, term, start, end, cap,
+                           reinterpret_cast<uint8_t*>(ctx->tmp[T_TOKOFF].p) + 32, r)))
+        return rc;
+    r.sg.cont = 1;
+    r.sg.end1 = n + 1;  // the input does not end in this piece
+    r.a.carry = carry;
+    r.a.pos_base = pos;
+    r.a.carry_tokens = global;
+    r.a.tok_first = first;
+    if ((rc = lex3_front(ctx, r)) || (rc = lex3_emit<uint32_t, int64_t>(ctx, r))) return rc;
+    lex3_stream_tail_kernel<<<1, LX_THREADS, 0, ctx->stream>>>(r.a);
+    CK(cudaGetLastError());
+    mark(ctx, "lex3_stream_tail_kernel");
+    return ALP_OK;
+}
+
+static int stream_end(alp_ctx* ctx, LexCarry* carry, long long total, int global, long long first, uint32_t* term,
+                      int64_t* start, int64_t* end, long long cap) {
+    lex3_stream_end_kernel<<<1, 32, 0, ctx->stream>>>(carry, ctx->l3.tokinfo, total, global, first, term,
+                                                      reinterpret_cast<long long*>(start),
+                                                      reinterpret_cast<long long*>(end), cap);
+    CK(cudaGetLastError());
+    return ALP_OK;
+}
+
+static int stream_ok(alp_ctx* ctx) {
+    if (!ctx) return ALP_ERR_ARG;
+    if (!ctx->has_lexer) return fail(ctx, ALP_ERR_MODE, "tables have no lexer");
+    if (!ctx->lex3) return fail(ctx, ALP_ERR_TABLE, "token streams need a DFA of at most 32 states");
+    return ALP_OK;
+}
+
+static LexCarry carry_init() {
+    LexCarry c{};
+    c.state = 1u;  // the DFA's initial state
+    return c;
+}
+
+int alp_lex_stream_begin(alp_ctx* ctx, uint32_t* d_term, int64_t* d_start, int64_t* d_end, int64_t cap,
+                         alp_lex_stream** out) {
+    int rc;
+    if ((rc = stream_ok(ctx))) return rc;
+    if (!out || cap < 0 || (cap > 0 && (!d_term || !d_start || !d_end))) return fail(ctx, ALP_ERR_ARG, "bad argument");
+    *out = nullptr;
+    CK(cudaSetDevice(ctx->device));
+    alp_lex_stream* s = new alp_lex_stream();
+    s->ctx = ctx;
+    s->term = d_term;
+    s->start = d_start;
+    s->end = d_end;
+    s->cap = cap;
+    const LexCarry c0 = carry_init();
+    cudaError_t e = cudaMalloc(&s->d_carry, sizeof(LexCarry));
+    if (e == cudaSuccess) e = cudaHostAlloc(&s->h_carry, sizeof(LexCarry), cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_carry, &c0, sizeof c0, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        alp_lex_stream_free(s);
+        return fail(ctx, ALP_ERR_CUDA, "stream setup: %s", cudaGetErrorString(e));
+    }
+    *out = s;
+    return ALP_OK;
+}
+
+int alp_lex_stream_push(alp_lex_stream* s, const uint8_t* d_piece, int64_t n) {
+    if (!s) return ALP_ERR_ARG;
+    alp_ctx* ctx = s->ctx;
+    int rc = check_in(ctx, d_piece, n, true);
+    if (rc) return rc;
+    if (s->ended) return fail(ctx, ALP_ERR_ARG, "stream already ended");
+    if (n == 0) return ALP_OK;
+    CK(cudaSetDevice(ctx->device));
+    if ((rc = stream_piece(ctx, s->d_carry, d_piece, n, s->pos, 1, s->first, s->term, s->start, s->end, s->cap)))
+        return rc;
+    s->pos += n;
+    return ALP_OK;
+}
+
+// Waits for the pushed pieces; *n_tok = tokens written so far.
+static int stream_read(alp_lex_stream* s, int64_t* n_tok) {
+    alp_ctx* ctx = s->ctx;
+    CK(cudaMemcpyAsync(s->h_carry, s->d_carry, sizeof(LexCarry), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (s->h_carry->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
+    *n_tok = s->h_carry->tokens;
+    if (s->h_carry->error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
+    return ALP_OK;
+}
+
+int alp_lex_stream_tokens(alp_lex_stream* s, int64_t* n_tok) {
+    if (!s || !n_tok) return s ? fail(s->ctx, ALP_ERR_ARG, "null output") : ALP_ERR_ARG;
+    alp_ctx* ctx = s->ctx;
+    CK(cudaSetDevice(ctx->device));
+    return stream_read(s, n_tok);
+}
+
+int alp_lex_stream_end(alp_lex_stream* s, int64_t* n_tok, int* valid) {
+    if (!s) return ALP_ERR_ARG;
+    alp_ctx* ctx = s->ctx;
+    if (!n_tok || !valid) return fail(ctx, ALP_ERR_ARG, "null output");
+    if (s->ended) return fail(ctx, ALP_ERR_ARG, "stream already ended");
+    CK(cudaSetDevice(ctx->device));
+    int rc;
+    if ((rc = stream_end(ctx, s->d_carry, s->pos, 1, s->first, s->term, s->start, s->end, s->cap))) return rc;
+    s->ended = 1;
+    rc = stream_read(s, n_tok);
+    *valid = s->h_carry->valid;
+    if (!rc && !*valid) *n_tok = 0;  // a rejected input has no tokens
+    ctx->last_tokens = *n_tok;
+    return rc;
+}
+
+int alp_lex_stream_window(alp_lex_stream* s, uint32_t* d_term, int64_t* d_start, int64_t* d_end, int64_t cap,
+                          int64_t first) {
+    if (!s) return ALP_ERR_ARG;
+    alp_ctx* ctx = s->ctx;
+    if (cap < 0 || first < 0 || (cap > 0 && (!d_term || !d_start || !d_end)))
+        return fail(ctx, ALP_ERR_ARG, "bad argument");
+    s->term = d_term;
+    s->start = d_start;
+    s->end = d_end;
+    s->cap = cap;
+    s->first = first;
+    return ALP_OK;
+}
+
+void alp_lex_stream_free(alp_lex_stream* s) {
+    if (!s) return;
+    if (s->ctx) cudaSetDevice(s->ctx->device);
+    if (s->d_carry) cudaFree(s->d_carry);
+    if (s->h_carry) cudaFreeHost(s->h_carry);
+    delete s;
+}
+
+// Host input in pieces of `piece` bytes through two slots: the copy of piece
+// i+1 in, the lexing of piece i and the copy of piece i-1's tokens out run at
+// once on three streams.  Host buffers should be pinned for the copies to
+// overlap.
+int alp_lex_host_stream(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t piece, uint32_t* h_term,
+                        int64_t* h_start, int64_t* h_end, int64_t cap, int64_t* n_tok, int* valid) {
+    int rc;
+    if ((rc = stream_ok(ctx))) return rc;
+    if (n < 0 || (n > 0 && !h_in)) return fail(ctx, ALP_ERR_ARG, "bad input");
+    if (!n_tok || !valid || cap < 0 || (cap > 0 && (!h_term || !h_start || !h_end)))
+        return fail(ctx, ALP_ERR_ARG, "bad argument");
+    if (piece <= 0) piece = 16ll << 20;
+    piece = (piece + 255) & ~255ll;
+    if (piece > 0x40000000ll) return fail(ctx, ALP_ERR_ARG, "piece size %lld out of range", (long long)piece);
+    *n_tok = 0;
+    *valid = 0;
+    if (n == 0) {  // the empty input: accepted iff the initial state accepts, no token
+        *valid = (ctx->h_tokinfo[1] & TOK_ACCEPT) ? 1 : 0;
+        return ALP_OK;
+    }
+    CK(cudaSetDevice(ctx->device));
+    const long long P = piece < n ? piece : ((n + 255) & ~255ll);
+    const long long tcap = P + 1;  // tokens of one piece: one per byte at most, plus the last token
+    const size_t b_in = (size_t)P + 256, b_term = ((size_t)tcap * 4 + 255) & ~(size_t)255,
+                 b_pos = ((size_t)tcap * 8 + 255) & ~(size_t)255;
+    const size_t b_slot = b_in + b_term + 2 * b_pos;
+    if ((rc = grow(ctx, ctx->pipe, 2 * b_slot)) || (rc = grow(ctx, ctx->carry, sizeof(LexCarry)))) return rc;
+    if (!ctx->cp_in) {
+        CK(cudaStreamCreateWithFlags(&ctx->cp_in, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&ctx->cp_out, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; ++i) {
+            CK(cudaEventCreateWithFlags(&ctx->ev_in[i], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ctx->ev_done[i], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ctx->ev_out[i], cudaEventDisableTiming));
+        }
+        CK(cudaHostAlloc(&ctx->h_carry, 2 * sizeof(LexCarry), cudaHostAllocDefault));
+    }
+    // nothing from an earlier call may still use the slots
+    CK(cudaStreamSynchronize(ctx->cp_out));
+    CK(cudaStreamSynchronize(ctx->cp_in));
+    LexCarry* d_carry = reinterpret_cast<LexCarry*>(ctx->carry.p);
+    const LexCarry c0 = carry_init();
+    ctx->h_carry[0] = c0;
+    CK(cudaMemcpyAsync(d_carry, &ctx->h_carry[0], sizeof c0, cudaMemcpyHostToDevice, ctx->stream));
+    uint8_t* slots = reinterpret_cast<uint8_t*>(ctx->pipe.p);
+    auto in_of = [&](int k) { return slots + k * b_slot; };
+    auto term_of = [&](int k) { return reinterpret_cast<uint32_t*>(slots + k * b_slot + b_in); };
+    auto start_of = [&](int k) { return reinterpret_cast<int64_t*>(slots + k * b_slot + b_in + b_term); };
+    auto end_of = [&](int k) { return reinterpret_cast<int64_t*>(slots + k * b_slot + b_in + b_term + b_pos); };
+    const long long np = (n + P - 1) / P;
+    long long copied = 0;  // tokens handed to the host so far
+    bool overflow = false;
+    // piece i-1's tokens out, once its lexing is done
+    auto retire = [&](long long i) -> int {
+        const int k = (int)(i & 1);
+        CK(cudaEventSynchronize(ctx->ev_done[k]));
+        const LexCarry c = ctx->h_carry[k];
+        if (c.error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
+        if (c.error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "piece token buffer too small");
+        const long long m = c.piece;
+        if (copied + m > cap) overflow = true;
+        if (!overflow && m > 0) {
+            CK(cudaMemcpyAsync(h_term + copied, term_of(k), (size_t)m * 4, cudaMemcpyDeviceToHost, ctx->cp_out));
+            CK(cudaMemcpyAsync(h_start + copied, start_of(k), (size_t)m * 8, cudaMemcpyDeviceToHost, ctx->cp_out));
+            CK(cudaMemcpyAsync(h_end + copied, end_of(k), (size_t)m * 8, cudaMemcpyDeviceToHost, ctx->cp_out));
+        }
+        CK(cudaEventRecord(ctx->ev_out[k], ctx->cp_out));
+        copied += m;
+        if (i == np - 1) *valid = c.valid;
+        return ALP_OK;
+    };
+    for (long long i = 0; i < np; ++i) {
+        const int k = (int)(i & 1);
+        const long long off = i * P, len = (n - off < P) ? n - off : P;
+        if (i >= 2) CK(cudaStreamWaitEvent(ctx->cp_in, ctx->ev_done[k], 0));  // slot k's piece i-2 is lexed
+        CK(cudaMemcpyAsync(in_of(k), h_in + off, (size_t)len, cudaMemcpyHostToDevice, ctx->cp_in));
+        CK(cudaEventRecord(ctx->ev_in[k], ctx->cp_in));
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_in[k], 0));
+        if (i >= 2) CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_out[k], 0));  // piece i-2's tokens are out
+        if ((rc = stream_piece(ctx, d_carry, in_of(k), len, off, 0, 0, term_of(k), start_of(k), end_of(k), tcap)))
+            return rc;
+        if (i == np - 1 && (rc = stream_end(ctx, d_carry, n, 0, 0, term_of(k), start_of(k), end_of(k), tcap)))
+            return rc;
+        CK(cudaMemcpyAsync(&ctx->h_carry[k], d_carry, sizeof(LexCarry), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaEventRecord(ctx->ev_done[k], ctx->stream));
+        if (i >= 1 && (rc = retire(i - 1))) return rc;
+    }
+    if ((rc = retire(np - 1))) return rc;
+    CK(cudaStreamSynchronize(ctx->cp_out));
+    *n_tok = *valid ? copied : 0;  // a rejected input has no tokens
+    ctx->last_tokens = *n_tok;
+    if (overflow && *valid) return fail(ctx, ALP_ERR_CAPACITY, "host token buffer too small");
     return ALP_OK;
 }
 

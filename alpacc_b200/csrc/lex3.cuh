@@ -60,6 +60,19 @@ struct Lex3Tables {
     int S, C1, E;
 };
 
+// What one piece of a token stream hands to the next, in device memory (the
+// reference's chunk loop carries (state, last start, size) the same way:
+// futhark/lexer.fut:148-160, cuda/lexer.cu:105-117,397-407).
+struct __align__(16) LexCarry {
+    long long start;    // stream position where the kept token in progress started
+    long long tokens;   // tokens written so far
+    long long piece;    // tokens the last piece wrote
+    uint32_t state;     // DFA state after the bytes so far
+    uint32_t error;     // ALP_DEV_ERR_* bits of all pieces
+    int valid;          // set when the stream ends
+    int pad;
+};
+
 struct Lex3Args {
     const uint8_t* in;
     long long n;
@@ -81,6 +94,10 @@ struct Lex3Args {
     unsigned int num_tiles;        // 8 KiB tiles
     unsigned int num_wide;         // 16 KiB tiles
     unsigned int num_scan_tiles;   // LS_TILE-chunk tiles
+    LexCarry* carry;               // stream piece: entry state and token start (null: plain input)
+    long long pos_base;            // stream position of in[0] (added to output positions)
+    int carry_tokens;              // outputs start at index carry->tokens - tok_first (else 0)
+    long long tok_first;           // stream token stored at element 0 of the outputs
 };
 
 __host__ __device__ inline size_t lex3_fold_smem(int S, int C1, int E) {
@@ -125,10 +142,10 @@ __device__ __forceinline__ void lx_mark_docs(const LexSeg& sg, long long n, long
                                              uint32_t* s_head, uint32_t* s_last, unsigned long long* s_dmax,
                                              uint32_t* s_doff = nullptr) {
     for (long long d = d0 + threadIdx.x; d <= sg.n_docs; d += blockDim.x) {
-        const long long h = sg.doc_off[d];
+        const long long h = seg_off(sg, d);
         if (h > t1 + 1) break;
         if (s_doff && d - d0 < LX_DOCS) s_doff[d - d0] = (uint32_t)h;
-        if (h >= t0 && h <= t1 && h < n) {
+        if (h >= t0 && h <= t1 && h < n && !(sg.cont && d == 0)) {
             const long long r = h - t0;
             atomicOr(&s_head[r >> 5], 1u << (r & 31));
         }
@@ -293,7 +310,7 @@ __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
                 x = s_wagg[w][x];
             }
             // x = the tile's function: lane s -> state after the tile from s
-            uint32_t sin = INIT;
+            uint32_t sin = a.carry ? a.carry->state : INIT;
             if (tile > 0) {
                 st_volatile32(&a.lb_vec[(size_t)tile * 32 + lane], (ST_A << 30) | x);
                 uint32_t acc = (uint32_t)lane;  // composition of the aggregates passed so far
@@ -474,7 +491,7 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_count_kernel(Lex3Args a, L
 // ---- kernel 4: exclusive (count, last start) over tiles ---------------------
 // Two launches over chunks of LT_CHUNK tiles: the chunk sums, then one CTA per
 // chunk scans the chunk sums before its own and its own tiles in place.
-// Tile 0 starts from (0, 0).
+// Tile 0 starts from (0, NONE): no token start before the input.
 constexpr int LT_CHUNK = 1024;
 
 __device__ __forceinline__ void cs_unpack(unsigned long long v, uint32_t& c, uint32_t& p) {
@@ -541,7 +558,7 @@ __global__ void __launch_bounds__(LT_CHUNK) lex3_tile_scan_kernel(unsigned long 
     if (lane == 0) { ec = 0; ep = ALP_NONE32; }
     const uint32_t rc = s_cc + s_c[warp] + ec;
     uint32_t rp = ep != ALP_NONE32 ? ep : (s_p[warp] != ALP_NONE32 ? s_p[warp] : s_cp);
-    if (i < T) tile_cs[i] = ((unsigned long long)rc << 32) | (rp != ALP_NONE32 ? rp : 0u);
+    if (i < T) tile_cs[i] = ((unsigned long long)rc << 32) | rp;
 }
 
 // ---- kernel 5: tokens ---------------------------------------------------------
@@ -590,7 +607,17 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
     PosT* o_start = reinterpret_cast<PosT*>(a.out_start);
     PosT* o_end = reinterpret_cast<PosT*>(a.out_end);
     const long long sent = sg.sentinels ? 1 : 0;
+    // a stream piece places its tokens after the earlier pieces' and maps
+    // positions to the stream; a start of NONE is the carried token start
+    const long long tbase = (a.carry && a.carry_tokens) ? a.carry->tokens - a.tok_first : 0;
+    const long long pb = a.pos_base;
+    const long long snone = a.carry ? a.carry->start : 0;
+    auto spos = [&](uint32_t st_abs, long long bk) -> long long {
+        return st_abs == ALP_NONE32 ? snone : (long long)st_abs - bk + pb;
+    };
     auto put = [&](long long idx, uint32_t term, long long st, long long en) {
+        idx += tbase;
+        if (idx < 0) return;  // before the stream's output window
         if (idx < a.cap) {
             o_term[idx] = (TermT)term;
             o_start[idx] = (PosT)st;
@@ -678,8 +705,8 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
                         s_pk[k] = (uint32_t)(en_abs - t0) | (term << 16);
                         s_st[k] = st_abs;
                     } else {
-                        put((long long)tcount + sent * (2 * doc + 1), term, (long long)st_abs - base,
-                            (long long)en_abs - base);
+                        put((long long)tcount + sent * (2 * doc + 1), term, spos(st_abs, base),
+                            (long long)en_abs - base + pb);
                     }
                     ++tcount;
                 };
@@ -748,11 +775,78 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, Le
                     dk = doc_of(d0, dmax, en - 1);
                     bk = base_of(d0, dmax, dk);
                 }
-                put((long long)(Xc + k) + sent * (2 * dk + 1), pk >> 16, (long long)s_st[k] - bk, en - bk);
+                put((long long)(Xc + k) + sent * (2 * dk + 1), pk >> 16, spos(s_st[k], bk), en - bk + pb);
             }
         }
         __syncthreads();
     }
+}
+
+// ---- streams: the carry after a piece, the last token at the end --------------
+// After the token pass of one piece (launched with the piece's Lex3Args):
+// the DFA state after its last byte, the start of the kept token in progress
+// (the last token start in the piece, else unchanged), and the token count.
+__global__ void __launch_bounds__(LX_THREADS) lex3_stream_tail_kernel(Lex3Args a) {
+    __shared__ long long s_best[LX_THREADS / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long C = a.n_chunks, T = a.num_tiles;
+    long long best = -1;  // last token start in the last tile
+    for (long long c = (T - 1) * (LX_TILE / LX_CHUNK) + tid; c < C; c += LX_THREADS) {
+        const uint32_t off = a.chunk_c[c] >> 8;
+        if (off != LX_NOOFF) best = max(best, c * LX_CHUNK + (long long)off);
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) best = max(best, (long long)__shfl_xor_sync(ALP_FULL_MASK, best, d));
+    if (lane == 0) s_best[warp] = best;
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 0; w < LX_THREADS / 32; ++w) best = max(best, s_best[w]);
+        if (best < 0) {
+            const uint32_t xp = (uint32_t)a.tile_cs[T - 1];  // exclusive: before the last tile
+            if (xp != ALP_NONE32) best = xp;
+        }
+        LexCarry* c = a.carry;
+        if (best >= 0) c->start = a.pos_base + best;
+        uint32_t st = a.chunk_s[C - 1];
+        for (long long p = (C - 1) * LX_CHUNK; p < a.n; ++p) st = a.t.ent[st * LX_ROW + a.in[p]] & LX_NEXT;
+        c->state = st;
+        c->piece = a.res->count;
+        c->tokens += a.res->count;
+        c->error |= a.res->error;
+    }
+}
+
+// End of a stream of `total` bytes: the last token (futhark/lexer.fut:108-115
+// at the input's end) and acceptance, from the carry.  With `global` the token
+// goes after all tokens so far (token `first` at element 0), else after the
+// last piece's.  An empty stream is judged like an empty input.
+__global__ void lex3_stream_end_kernel(LexCarry* c, const uint32_t* tokinfo, long long total, int global,
+                                       long long first, uint32_t* term, long long* start, long long* end,
+                                       long long cap) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t ti = tokinfo[c->state];
+    if (total == 0) {  // the empty input: accepted iff the initial state accepts, no token
+        c->valid = (ti & TOK_ACCEPT) ? 1 : 0;
+        if (global) c->piece = 0;
+        return;
+    }
+    long long k = 0;
+    if (!(ti & TOK_IGNORE)) {
+        const long long idx = global ? c->tokens - first : c->piece;
+        if (idx < 0) {
+            // before the output window: not stored
+        } else if (idx < cap) {
+            term[idx] = ti & TOK_TERM_MASK;
+            start[idx] = c->start;
+            end[idx] = total;
+        } else {
+            c->error |= ALP_DEV_ERR_CAPACITY;
+        }
+        k = 1;
+    }
+    c->piece = global ? k : c->piece + k;
+    c->tokens += k;
+    c->valid = (ti & TOK_ACCEPT) ? 1 : 0;
 }
 
 }  // namespace alp

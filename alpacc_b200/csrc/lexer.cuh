@@ -325,7 +325,14 @@ struct LexSeg {
     uint8_t* valid;            // [n_docs] out
     int sentinels;
     uint32_t sent_l, sent_r;   // ⊢ and ⊣ terminal ids
+    int cont;                  // document 0 continues a stream: no head at byte 0 (lex3 only)
+    long long end1;            // with doc_off null (one document): doc_off[1] (lex3 only)
 };
+
+// doc_off[d], or (0, end1) for a single document given without an offsets array
+__device__ __forceinline__ long long seg_off(const LexSeg& sg, long long d) {
+    return sg.doc_off ? sg.doc_off[d] : (d == 0 ? 0 : sg.end1);
+}
 
 __device__ __forceinline__ uint32_t ext_apply(const LexTables& t, uint32_t f, uint32_t s) {
     return f >= (uint32_t)t.E ? f - t.E : __ldg(&t.apply[f * t.S + s]);

@@ -406,7 +406,23 @@ def run_lex(args, rank: int, world: int, local: int):
             raise RuntimeError("alp_lex_host failed rc=%d" % rc)
 
     e2e_step()
-    ms_e2e, _ = _timed(e2e_step, max(1, min(args.steps, 5)), local, dist)
+    ms_whole, _ = _timed(e2e_step, max(1, min(args.steps, 5)), local, dist)
+    whole = (n2.value, [o[:M].clone() for o in outs])
+    # the same through the token stream: 32 MiB pieces, the copies in and out
+    # overlapped with the lexing
+    piece = 32 << 20
+
+    def e2e_stream():
+        rc = L.alp_lex_host_stream(g.h, ctypes.c_void_p(h_in.data_ptr()), size, piece,
+                                   *[ctypes.c_void_p(o.data_ptr()) for o in outs], M, ctypes.byref(n2),
+                                   ctypes.byref(v2))
+        if rc != 0 or n2.value != M or not v2.value:
+            raise RuntimeError("alp_lex_host_stream failed rc=%d" % rc)
+
+    e2e_stream()
+    if n2.value != whole[0] or not all(torch.equal(o[:M], w) for o, w in zip(outs, whole[1])):
+        raise RuntimeError("alp_lex_host_stream tokens differ from alp_lex_host")
+    ms_e2e, _ = _timed(e2e_stream, max(1, min(args.steps, 5)), local, dist)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -420,7 +436,10 @@ def run_lex(args, rank: int, world: int, local: int):
                   "l2": "inputs larger than L2 (no flush needed)"},
                  size + 20 * M, kern,
                  {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": size,
-                  "d2h_bytes_per_step": 20 * M, "ms_per_step": ms_e2e}, clocks,
+                  "d2h_bytes_per_step": 20 * M, "ms_per_step": ms_e2e,
+                  "api": "alp_lex_host_stream, 32 MiB pieces, pinned host buffers",
+                  "whole_input": {"api": "alp_lex_host", "value": _gbs(world, size, ms_whole),
+                                  "ms_per_step": ms_whole}}, clocks,
                  units={"n": size, "m": M}, parse_layout=False)
     line["path_roofline"]["scope"] = "whole alp_lex call: input bytes + 20 B per token, over the step time"
     print(json.dumps(line), flush=True)

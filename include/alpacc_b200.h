@@ -104,6 +104,45 @@ int alp_lex_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, uint32_t* h_term,
 int alp_lex_noalloc(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_term, int64_t* d_start,
                     int64_t* d_end, int64_t cap, int64_t* n_tok, int* valid);
 
+/* Token streams: input that arrives in pieces, lexed as it comes.  Replaces the
+ * reference's chunk loop, which carries (last state, last start, size) from one
+ * chunk to the next (futhark/lexer.fut:148-160; cuda/lexer.cu:452-543
+ * lexer_stream).  The tokens equal alp_lex on the concatenation of all pieces,
+ * with positions counted from the stream's first byte.
+ *   - begin: tokens will go to the caller's device buffers of `cap` tokens.
+ *   - push: lexes one piece of device bytes (any size, empty included) and
+ *     writes the tokens that end inside it.  Stream-ordered on the context's
+ *     stream, no wait; the piece must stay unchanged until the work is done.
+ *   - tokens: waits for the pushed pieces; *n_tok = tokens written so far.
+ *   - end: writes the last token, waits; *valid and *n_tok as alp_lex (a
+ *     rejected stream: *valid = 0, *n_tok = 0).  With a buffer too small,
+ *     ALP_ERR_CAPACITY and *n_tok = the tokens needed.
+ *   - window: later tokens go to these buffers, stream token `first` at
+ *     element 0 (tokens before it are not stored).  With first = the count
+ *     from alp_lex_stream_tokens, one piece-sized buffer serves a stream of
+ *     any length, as the reference's per-chunk output arrays do.
+ * Tokens are final once written: a stream that turns out rejected at its end
+ * has already written the tokens before the point of rejection.  Needs a DFA
+ * of at most 32 states (ALP_ERR_TABLE otherwise).  One stream per context at
+ * a time. */
+typedef struct alp_lex_stream alp_lex_stream;
+int alp_lex_stream_begin(alp_ctx* ctx, uint32_t* d_term, int64_t* d_start, int64_t* d_end, int64_t cap,
+                         alp_lex_stream** out);
+int alp_lex_stream_push(alp_lex_stream* s, const uint8_t* d_piece, int64_t n);
+int alp_lex_stream_tokens(alp_lex_stream* s, int64_t* n_tok);
+int alp_lex_stream_end(alp_lex_stream* s, int64_t* n_tok, int* valid);
+int alp_lex_stream_window(alp_lex_stream* s, uint32_t* d_term, int64_t* d_start, int64_t* d_end, int64_t cap,
+                          int64_t first);
+void alp_lex_stream_free(alp_lex_stream* s);
+
+/* alp_lex_host over a stream of `piece`-byte pieces (0: 16 MiB): the copy of
+ * one piece in, the lexing of the one before and the copy of the tokens of the
+ * one before that out overlap on three CUDA streams.  Same results as
+ * alp_lex_host, for inputs of any size; host buffers should be pinned
+ * (cudaHostAlloc) for the copies to overlap. */
+int alp_lex_host_stream(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t piece, uint32_t* h_term,
+                        int64_t* h_start, int64_t* h_end, int64_t cap, int64_t* n_tok, int* valid);
+
 /* parse_int of the lexer+parser generator: bytes -> preorder tree
  * (src/Alpacc/Generator/Futhark/Generator.hs:35-44, futhark/parser.fut:316-336). */
 int alp_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t** d_parent, uint32_t** d_tag,
