@@ -31,7 +31,7 @@ struct PairInfo {           // one admissible pair
     int16_t d_depth;        // lefts - rights
     int16_t d_v;            // sum of (arity - 1) over its productions
     uint16_t n_term;        // terminal productions among them
-    uint16_t pad;
+    int16_t min_ds;         // least (depth before it - 1) over its right brackets; 0x7fff without any
 };
 
 struct ParseTables {
@@ -137,7 +137,12 @@ inline int load_parser(ParseTables& pt, ParseHost& ph, const uint8_t* p, const u
         pi.d_depth = (int16_t)dd;
         pi.d_v = (int16_t)dv;
         pi.n_term = (uint16_t)nt;
-        pi.pad = 0;
+        int md = 0x7fff, acc = 0;
+        for (uint32_t j = sb; j < se; ++j) {
+            if (!(stack[j] >> 31) && acc - 1 < md) md = acc - 1;
+            acc += (stack[j] >> 31) ? 1 : -1;
+        }
+        pi.min_ds = (int16_t)md;
         if ((int)pi.n_prod > maxp) maxp = pi.n_prod;
         if ((int)pi.n_br > maxb) maxb = pi.n_br;
     }
@@ -498,17 +503,20 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
 // ---------------------------------------------------------------------------
 // K2: expand every position's productions and brackets
 //
-// One tile = PP_TILE positions.  The block scans the per-position sums; each
-// thread then walks its positions and writes their nodes (first pass) and
-// brackets (second pass) into a shared-memory stage at their tile offsets,
-// and the block copies the stage out with coalesced stores.  A tile with
-// more nodes or brackets than the stage holds goes through it in rounds over
-// thread ranges.
+// One tile = PP_TILE positions.  The block scans the per-position sums and
+// records, per position, its pair, first node, first bracket, depth, value
+// and first token index in shared memory, and checks the document rules that
+// one position decides alone (an admissible pair, a depth that never goes
+// below zero, depth zero at ⊣).  Nodes are then produced in windows of EX_WIN:
+// each thread marks its positions as the owners of their nodes in the window
+// (16-bit position indices), and the block emits the window one node per
+// thread, in order, with coalesced stores.  Brackets the same way.  No thread
+// walks another position's productions, so warps stay converged whatever the
+// sizes of the pairs.
 // ---------------------------------------------------------------------------
-constexpr int EX_STAGE_BYTES = 67584;
-constexpr int EX_NCAP = EX_STAGE_BYTES / 12;  // nodes: value, tag | kind << 31, token index
-constexpr int EX_BCAP = EX_STAGE_BYTES / 8;   // brackets: symbol, depth value
+constexpr int EX_WIN = 8192;                     // nodes or brackets per window
 constexpr uint32_t EX_NO_TOKEN = 0xffffffffu;
+constexpr size_t EX_POS_BYTES = (size_t)PP_TILE * (5 * 4 + 2);  // per position: 5 words and the pair id
 
 // pair infos (20 bytes each), then the 8-byte records from a 16-byte boundary
 __host__ __device__ inline size_t expand_rec_off(int n_pairs) {
@@ -518,7 +526,27 @@ __host__ __device__ inline size_t expand_tables_bytes(int n_pairs, int n_pseq, i
     return (expand_rec_off(n_pairs) + 8 * ((size_t)n_pseq + n_stack) + 15) & ~(size_t)15;
 }
 __host__ __device__ inline size_t expand_smem_bytes(int n_pairs, int n_pseq, int n_stack) {
-    return expand_tables_bytes(n_pairs, n_pseq, n_stack) + EX_STAGE_BYTES;
+    return expand_tables_bytes(n_pairs, n_pseq, n_stack) + EX_POS_BYTES + 2 * (size_t)EX_WIN;
+}
+
+// Pair ids and terminals of the PP_ITEMS positions from i0 as two 8-byte
+// words (one vector load each when all are in range; ids past the end read
+// as no pair).
+__device__ __forceinline__ void ex_words(const ParseArgs& a, long long i0, uint2& w, uint2& t) {
+    static_assert(PP_ITEMS == 4, "a thread's positions are one 8-byte word");
+    if (i0 + PP_ITEMS <= a.L) {
+        w = __ldg(reinterpret_cast<const uint2*>(a.pid + i0));
+        t = __ldg(reinterpret_cast<const uint2*>(a.P + i0));
+    } else {
+        uint32_t x[PP_ITEMS], y[PP_ITEMS];
+#pragma unroll
+        for (int j = 0; j < PP_ITEMS; ++j) {
+            x[j] = i0 + j < a.L ? a.pid[i0 + j] : NO_PAIR;
+            y[j] = i0 + j < a.L ? a.P[i0 + j] : 0xffffu;
+        }
+        w = make_uint2(x[0] | (x[1] << 16), x[2] | (x[3] << 16));
+        t = make_uint2(y[0] | (y[1] << 16), y[2] | (y[3] << 16));
+    }
 }
 
 __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a) {
@@ -526,12 +554,13 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     PairInfo* s_pi = reinterpret_cast<PairInfo*>(smem);
     uint2* s_prec = reinterpret_cast<uint2*>(smem + expand_rec_off(a.t.n_pairs));
     uint2* s_srec = s_prec + a.t.n_pseq;
-    uint8_t* stage = smem + expand_tables_bytes(a.t.n_pairs, a.t.n_pseq, a.t.n_stack);
-    int32_t* s_nv = reinterpret_cast<int32_t*>(stage);
-    uint32_t* s_ntag = reinterpret_cast<uint32_t*>(s_nv + EX_NCAP);
-    uint32_t* s_nti = s_ntag + EX_NCAP;
-    uint32_t* s_bsym = reinterpret_cast<uint32_t*>(stage);
-    int32_t* s_bds = reinterpret_cast<int32_t*>(s_bsym + EX_BCAP);
+    uint32_t* s_noff = reinterpret_cast<uint32_t*>(smem + expand_tables_bytes(a.t.n_pairs, a.t.n_pseq, a.t.n_stack));
+    uint32_t* s_boff = s_noff + PP_TILE;   // tile-local first node / bracket of each position
+    uint32_t* s_ti = s_boff + PP_TILE;     // token index of the position's first terminal production
+    int32_t* s_v = reinterpret_cast<int32_t*>(s_ti + PP_TILE);  // exscan(arity - 1) before the position
+    int32_t* s_dep = s_v + PP_TILE;        // bracket depth before the position
+    uint16_t* s_id = reinterpret_cast<uint16_t*>(s_dep + PP_TILE);
+    uint16_t* s_own = s_id + PP_TILE;      // [EX_WIN] owning position of each node / bracket of a window
     __shared__ PosSums s_w[PP_THREADS / 32];
     __shared__ uint32_t s_tn, s_tb;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -541,218 +570,168 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     for (int i = tid; i < a.t.n_stack; i += PP_THREADS) s_srec[i] = a.t.stack_rec[i];
     const uint32_t SL = a.t.start, SR = a.t.end;
     const long long n_tiles = (a.L + PP_TILE - 1) / PP_TILE;
+    // this thread's pair ids and terminals, one tile ahead (loads in flight
+    // while the block works on the current tile)
+    uint2 nw, nt;
+    ex_words(a, (long long)blockIdx.x * PP_TILE + tid * PP_ITEMS, nw, nt);
     for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-    __syncthreads();  // the previous tile is done with the stage and the scan arrays
-    const long long tbase = tile * PP_TILE;
-    const long long i0 = tbase + tid * PP_ITEMS;
-    uint16_t ids[PP_ITEMS];
-    uint32_t hm = 0, em = 0;  // head / end bits of this thread's positions
+        __syncthreads();  // the previous tile is done with the shared arrays
+        const long long i0 = tile * PP_TILE + tid * PP_ITEMS;
+        const PosSums tp = a.tile_sums[tile];
+        uint16_t ids[PP_ITEMS];
+        uint32_t hm = 0, em = 0;  // head / end bits of this thread's positions
+        {
+            const uint32_t c[PP_ITEMS] = {nt.x & 0xffffu, nt.x >> 16, nt.y & 0xffffu, nt.y >> 16};
+            ids[0] = (uint16_t)nw.x; ids[1] = (uint16_t)(nw.x >> 16); ids[2] = (uint16_t)nw.y; ids[3] = (uint16_t)(nw.y >> 16);
 #pragma unroll
-    for (int j = 0; j < PP_ITEMS; ++j) {
-        ids[j] = NO_PAIR;
-        if (i0 + j < a.L) {
-            ids[j] = a.pid[i0 + j];
-            const uint32_t c = a.P[i0 + j];
-            if (c == SL) hm |= 1u << j;
-            if (c == SR) em |= 1u << j;
-        }
-    }
-    __syncthreads();
-    PosSums mine;
-    possums_zero(mine);
-#pragma unroll
-    for (int j = 0; j < PP_ITEMS; ++j)
-        if (i0 + j < a.L) mine = ps_combine(mine, ps_elem(s_pi, ids[j], (hm >> j) & 1u, i0 + j));
-    PosSums inc = ps_warp_scan(mine, lane);
-    PosSums ex = ps_shfl_up(inc, 1);
-    if (lane == 0) possums_zero(ex);
-    if (lane == 31) s_w[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        PosSums w;
-        if (lane < PP_THREADS / 32) w = s_w[lane]; else possums_zero(w);
-        PosSums wi = ps_warp_scan(w, lane);
-        PosSums we = ps_shfl_up(wi, 1);
-        if (lane == 0) possums_zero(we);
-        if (lane < PP_THREADS / 32) s_w[lane] = we;
-        if (lane == PP_THREADS / 32 - 1) { s_tn = (uint32_t)wi.nodes; s_tb = (uint32_t)wi.brs; }
-    }
-    __syncthreads();
-    const PosSums tp = a.tile_sums[tile];
-    const PosSums run0 = ps_combine(ps_combine(tp, s_w[warp]), ex);  // before this thread's first position
-    const uint32_t tn = s_tn, tb = s_tb;
-    // Tile-local first node / bracket of every thread.  A tile with more than
-    // the stage holds is staged in rounds over equal thread ranges; a round
-    // that still does not fit writes directly.
-    __shared__ uint32_t s_n0[PP_THREADS + 1], s_b0[PP_THREADS + 1];
-    __shared__ int s_rn, s_rb;
-    s_n0[tid] = run0.nodes - tp.nodes;
-    s_b0[tid] = run0.brs - tp.brs;
-    if (tid == 0) { s_n0[PP_THREADS] = tn; s_b0[PP_THREADS] = tb; }
-    __syncthreads();
-    if (tid == 0) {
-        auto rounds = [](const uint32_t* o, uint32_t cap) {
-            int R = 1;
-            for (; R < 16; R *= 2) {
-                bool ok = true;
-                for (int r = 0; r < R && ok; ++r)
-                    ok = o[(r + 1) * PP_THREADS / R] - o[r * PP_THREADS / R] <= cap;
-                if (ok) break;
+            for (int j = 0; j < PP_ITEMS; ++j) {
+                if (i0 + j < a.L) {
+                    if (c[j] == SL) hm |= 1u << j;
+                    if (c[j] == SR) em |= 1u << j;
+                }
             }
-            return R;
-        };
-        s_rn = rounds(s_n0, EX_NCAP);
-        s_rb = rounds(s_b0, EX_BCAP);
-    }
-    __syncthreads();
-    const int Rn = s_rn, Rb = s_rb;
-
-    // ---- nodes -------------------------------------------------------------------
-    for (int rr = 0; rr < Rn; ++rr) {
-        const int lo = rr * PP_THREADS / Rn, hi = (rr + 1) * PP_THREADS / Rn;
-        const uint32_t nb = s_n0[lo], ncount = s_n0[hi] - nb;
-        const bool nst = ncount <= (uint32_t)EX_NCAP;
-        if (tid >= lo && tid < hi) {
-            PosSums run = run0;
-            uint32_t nd = (uint32_t)(run.nodes - tp.nodes);
+        }
+        if (tile + gridDim.x < n_tiles) ex_words(a, i0 + (long long)gridDim.x * PP_TILE, nw, nt);
+        PosSums mine;
+        possums_zero(mine);
+#pragma unroll
+        for (int j = 0; j < PP_ITEMS; ++j)
+            if (i0 + j < a.L) mine = ps_combine(mine, ps_elem(s_pi, ids[j], (hm >> j) & 1u, i0 + j));
+        const PosSums inc = ps_warp_scan(mine, lane);
+        PosSums ex = ps_shfl_up(inc, 1);
+        if (lane == 0) possums_zero(ex);
+        if (lane == 31) s_w[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            PosSums w;
+            if (lane < PP_THREADS / 32) w = s_w[lane]; else possums_zero(w);
+            const PosSums wi = ps_warp_scan(w, lane);
+            PosSums we = ps_shfl_up(wi, 1);
+            if (lane == 0) possums_zero(we);
+            if (lane < PP_THREADS / 32) s_w[lane] = we;
+            if (lane == PP_THREADS / 32 - 1) { s_tn = wi.nodes; s_tb = wi.brs; }
+        }
+        __syncthreads();
+        // ---- per position: records and the one-position document rules --------
+        uint32_t nof[PP_ITEMS], cnt[PP_ITEMS];  // first node / bracket (tile-local), n_prod | n_br << 16
+        {
+            PosSums run = ps_combine(ps_combine(tp, s_w[warp]), ex);  // before this thread's first position
 #pragma unroll
             for (int j = 0; j < PP_ITEMS; ++j) {
                 const long long i = i0 + j;
+                const int pl = tid * PP_ITEMS + j;
+                nof[j] = run.nodes - tp.nodes;
+                cnt[j] = 0;
                 if (i < a.L) {
                     const bool head = (hm >> j) & 1u;
                     const int32_t dep = head ? 0 : run.depth;
-                    const int32_t v = head ? 0 : run.v;
-                    const uint32_t tr = head ? 0u : (uint32_t)run.terms;
-                    const uint32_t hp = (uint32_t)(head ? i : run.hpos);
                     const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
                     const bool dok = doc >= 0 && doc < a.n_docs;
                     if (head && dok) {
-                        a.node_off[doc] = (long long)(tp.nodes + nd);
+                        a.node_off[doc] = (long long)run.nodes;
                         a.br_off[doc] = (long long)run.brs;
                     }
-                    int32_t dd = 0;
+                    s_noff[pl] = nof[j];
+                    s_boff[pl] = run.brs - tp.brs;
+                    s_ti[pl] = (uint32_t)(head ? i : run.hpos) + 1u + (head ? 0u : run.terms);
+                    s_v[pl] = head ? 0 : run.v;
+                    s_dep[pl] = dep;
+                    s_id[pl] = ids[j];
+                    PosSums e;
+                    possums_zero(e);
                     if (ids[j] == NO_PAIR) {
                         if (dok) a.doc_valid[doc] = 0;  // no admissible pair
                     } else {
                         const PairInfo pi = s_pi[ids[j]];
-                        dd = pi.d_depth;
-                        for (uint32_t r = 0; r < pi.n_prod; ++r) {
-                            const uint2 rec = s_prec[pi.prod_begin + r];
-                            const uint32_t tm1 = rec.x >> 16;  // terminal + 1, 0: not a terminal production
-                            const int32_t vv = v + (int32_t)(int16_t)(rec.y & 0xffffu);
-                            uint32_t tagk = rec.x & 0xffffu, ti = EX_NO_TOKEN;
-                            if (tm1 && a.subst_terminals) {
-                                // the k-th terminal production of a document takes its k-th token's span
-                                tagk = (tm1 - 1) | 0x80000000u;
-                                ti = hp + 1 + tr + (rec.y >> 16);
-                            }
-                            if (nst) {
-                                s_nv[nd - nb] = vv;
-                                s_ntag[nd - nb] = tagk;
-                                s_nti[nd - nb] = ti;
-                            } else {
-                                const unsigned long long ndg = tp.nodes + nd;
-                                if ((long long)ndg < a.cap_nodes) {
-                                    a.vbuf[ndg] = vv;
-                                    a.tag[ndg] = tagk & 0x7fffffffu;
-                                    a.kind[ndg] = (uint8_t)(tagk >> 31);
-                                    a.nstart[ndg] = ti < a.L ? (int64_t)__ldg(&a.pstart[ti]) : 0;
-                                    a.nend[ndg] = ti < a.L ? (int64_t)__ldg(&a.pend[ti]) : 0;
-                                }
-                            }
-                            ++nd;
-                        }
+                        if (dep + (int32_t)pi.min_ds < 0 && dok) a.doc_valid[doc] = 0;  // depth below zero
+                        e.nodes = pi.n_prod; e.brs = pi.n_br; e.depth = pi.d_depth; e.v = pi.d_v; e.terms = pi.n_term;
+                        cnt[j] = (uint32_t)pi.n_prod | ((uint32_t)pi.n_br << 16);
                     }
-                    if (((em >> j) & 1u) && (dep + dd != 0) && dok) a.doc_valid[doc] = 0;  // unbalanced at the end
-                    run = ps_combine(run, ps_elem(s_pi, ids[j], head, i));
+                    if (((em >> j) & 1u) && (dep + e.depth != 0) && dok) a.doc_valid[doc] = 0;  // unbalanced at the end
+                    if (head) { e.heads = 1; e.hpos = (int32_t)i; }
+                    run = ps_combine(run, e);
                 }
             }
         }
-        __syncthreads();
-        if (nst) {
-            for (uint32_t e0 = tid; e0 < ncount; e0 += 2 * PP_THREADS) {
-                uint32_t tk[2], tix[2];
+        const uint32_t tn = s_tn, tb = s_tb;
+        // ---- nodes, one window at a time ---------------------------------------------
+        for (uint32_t w0 = 0; w0 < tn; w0 += EX_WIN) {
+            const uint32_t wn = min(tn - w0, (uint32_t)EX_WIN);
+#pragma unroll
+            for (int j = 0; j < PP_ITEMS; ++j) {
+                const uint32_t b = nof[j], n = cnt[j] & 0xffffu;
+                const uint32_t lo = max(b, w0), hi = min(b + n, w0 + wn);
+                for (uint32_t x = lo; x < hi; ++x) s_own[x - w0] = (uint16_t)(tid * PP_ITEMS + j);
+            }
+            __syncthreads();
+            for (uint32_t e0 = tid; e0 < wn; e0 += 2 * PP_THREADS) {
+                uint32_t tg[2], kd[2], gi[2];
                 int32_t vv[2];
                 int64_t st[2], en[2];
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
                     const uint32_t e = e0 + u * PP_THREADS;
-                    tk[u] = 0; tix[u] = EX_NO_TOKEN; vv[u] = 0; st[u] = 0; en[u] = 0;
-                    if (e < ncount) { vv[u] = s_nv[e]; tk[u] = s_ntag[e]; tix[u] = s_nti[e]; }
-                    if (tix[u] < a.L) { st[u] = __ldg(&a.pstart[tix[u]]); en[u] = __ldg(&a.pend[tix[u]]); }
+                    tg[u] = 0; kd[u] = 0; vv[u] = 0; st[u] = 0; en[u] = 0; gi[u] = 0xffffffffu;
+                    if (e < wn) {
+                        const uint32_t g = w0 + e;
+                        const int pl = s_own[e];
+                        const uint32_t r = g - s_noff[pl];
+                        const uint2 rec = s_prec[s_pi[s_id[pl]].prod_begin + r];
+                        const uint32_t tm1 = rec.x >> 16;  // terminal + 1, 0: not a terminal production
+                        vv[u] = s_v[pl] + (int32_t)(int16_t)(rec.y & 0xffffu);
+                        tg[u] = rec.x & 0xffffu;
+                        gi[u] = tp.nodes + g;
+                        if (tm1 && a.subst_terminals) {
+                            // the k-th terminal production of a document takes its k-th token's span
+                            tg[u] = tm1 - 1;
+                            kd[u] = 1;
+                            const uint32_t ti = s_ti[pl] + (rec.y >> 16);
+                            if (ti < a.L) { st[u] = __ldg(&a.pstart[ti]); en[u] = __ldg(&a.pend[ti]); }
+                        }
+                    }
                 }
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
-                    const uint32_t e = e0 + u * PP_THREADS;
-                    const unsigned long long ndg = tp.nodes + nb + e;
-                    if (e < ncount && (long long)ndg < a.cap_nodes) {
-                        a.vbuf[ndg] = vv[u];
-                        a.tag[ndg] = tk[u] & 0x7fffffffu;
-                        a.kind[ndg] = (uint8_t)(tk[u] >> 31);
-                        a.nstart[ndg] = st[u];
-                        a.nend[ndg] = en[u];
+                    if (gi[u] != 0xffffffffu && (long long)gi[u] < a.cap_nodes) {
+                        const size_t g = gi[u];
+                        a.vbuf[g] = vv[u];
+                        a.tag[g] = tg[u];
+                        a.kind[g] = (uint8_t)kd[u];
+                        a.nstart[g] = st[u];
+                        a.nend[g] = en[u];
                     }
                 }
             }
+            __syncthreads();
         }
-        __syncthreads();
-    }
-
-    // ---- brackets ----------------------------------------------------------------
-    for (int rr = 0; rr < Rb; ++rr) {
-        const int lo = rr * PP_THREADS / Rb, hi = (rr + 1) * PP_THREADS / Rb;
-        const uint32_t bb = s_b0[lo], bcount = s_b0[hi] - bb;
-        const bool bst = bcount <= (uint32_t)EX_BCAP;
-        if (tid >= lo && tid < hi) {
-            PosSums run = run0;
-            uint32_t bi = (uint32_t)(run.brs - tp.brs);
+        // ---- brackets, one window at a time ------------------------------------------
+        for (uint32_t w0 = 0; w0 < tb; w0 += EX_WIN) {
+            const uint32_t wn = min(tb - w0, (uint32_t)EX_WIN);
 #pragma unroll
             for (int j = 0; j < PP_ITEMS; ++j) {
-                const long long i = i0 + j;
-                if (i < a.L) {
-                    const bool head = (hm >> j) & 1u;
-                    const int32_t dep = head ? 0 : (int32_t)run.depth;
-                    const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
-                    if (ids[j] != NO_PAIR) {
-                        const PairInfo pi = s_pi[ids[j]];
-                        for (uint32_t r = 0; r < pi.n_br; ++r) {
-                            const uint2 rec = s_srec[pi.stack_begin + r];
-                            const uint32_t sym = rec.x;
-                            const int32_t before = dep + (int32_t)(int16_t)(rec.y & 0xffffu);
-                            int32_t ds;
-                            if (sym >> 31) ds = before;
-                            else {
-                                ds = before - 1;
-                                if (ds < 0 && doc >= 0 && doc < a.n_docs) a.doc_valid[doc] = 0;  // depth below zero
-                            }
-                            if (bst) {
-                                s_bsym[bi - bb] = sym;
-                                s_bds[bi - bb] = ds;
-                            } else {
-                                const unsigned long long big = tp.brs + bi;
-                                if ((long long)big < a.cap_brs) {
-                                    a.brbuf[big] = sym;
-                                    a.dsbuf[big] = ds;
-                                }
-                            }
-                            ++bi;
-                        }
-                    }
-                    run = ps_combine(run, ps_elem(s_pi, ids[j], head, i));
+                const int pl = tid * PP_ITEMS + j;
+                const uint32_t n = cnt[j] >> 16;
+                if (n) {
+                    const uint32_t b = s_boff[pl];
+                    const uint32_t lo = max(b, w0), hi = min(b + n, w0 + wn);
+                    for (uint32_t x = lo; x < hi; ++x) s_own[x - w0] = (uint16_t)pl;
                 }
             }
-        }
-        __syncthreads();
-        if (bst) {
-            for (uint32_t e = tid; e < bcount; e += PP_THREADS) {
-                const unsigned long long big = tp.brs + bb + e;
-                if ((long long)big >= a.cap_brs) break;
-                a.brbuf[big] = s_bsym[e];
-                a.dsbuf[big] = s_bds[e];
+            __syncthreads();
+            for (uint32_t e = tid; e < wn; e += PP_THREADS) {
+                const uint32_t g = w0 + e;
+                const int pl = s_own[e];
+                const uint32_t r = g - s_boff[pl];
+                const uint2 rec = s_srec[s_pi[s_id[pl]].stack_begin + r];
+                const int32_t before = s_dep[pl] + (int32_t)(int16_t)(rec.y & 0xffffu);
+                const uint32_t bg = tp.brs + g;
+                if ((long long)bg < a.cap_brs) {
+                    a.brbuf[bg] = rec.x;
+                    a.dsbuf[bg] = (rec.x >> 31) ? before : before - 1;  // after a right bracket, before a left
+                }
             }
+            __syncthreads();
         }
-        __syncthreads();
-    }
     }
 }
 
