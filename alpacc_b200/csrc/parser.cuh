@@ -515,8 +515,9 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
 // sizes of the pairs.
 // ---------------------------------------------------------------------------
 constexpr int EX_WIN = 8192;                     // nodes or brackets per window
+constexpr int EX_U = 2;                          // nodes a thread emits at once (token span loads in flight)
 constexpr uint32_t EX_NO_TOKEN = 0xffffffffu;
-constexpr size_t EX_POS_BYTES = (size_t)PP_TILE * (5 * 4 + 2);  // per position: 5 words and the pair id
+constexpr size_t EX_POS_BYTES = (size_t)PP_TILE * 20;  // per position: a node record and a bracket base
 
 // pair infos (20 bytes each), then the 8-byte records from a 16-byte boundary
 __host__ __device__ inline size_t expand_rec_off(int n_pairs) {
@@ -554,13 +555,12 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     PairInfo* s_pi = reinterpret_cast<PairInfo*>(smem);
     uint2* s_prec = reinterpret_cast<uint2*>(smem + expand_rec_off(a.t.n_pairs));
     uint2* s_srec = s_prec + a.t.n_pseq;
-    uint32_t* s_noff = reinterpret_cast<uint32_t*>(smem + expand_tables_bytes(a.t.n_pairs, a.t.n_pseq, a.t.n_stack));
-    uint32_t* s_boff = s_noff + PP_TILE;   // tile-local first node / bracket of each position
-    uint32_t* s_ti = s_boff + PP_TILE;     // token index of the position's first terminal production
-    int32_t* s_v = reinterpret_cast<int32_t*>(s_ti + PP_TILE);  // exscan(arity - 1) before the position
-    int32_t* s_dep = s_v + PP_TILE;        // bracket depth before the position
-    uint16_t* s_id = reinterpret_cast<uint16_t*>(s_dep + PP_TILE);
-    uint16_t* s_own = s_id + PP_TILE;      // [EX_WIN] owning position of each node / bracket of a window
+    // per position: x = its first production record minus its first (tile-local)
+    // node, so that node g reads record g + x; y = exscan(arity - 1) before it;
+    // z = token index of its first terminal production; w = bracket depth before it
+    int4* s_pos = reinterpret_cast<int4*>(smem + expand_tables_bytes(a.t.n_pairs, a.t.n_pseq, a.t.n_stack));
+    int32_t* s_sbd = reinterpret_cast<int32_t*>(s_pos + PP_TILE);  // first stack record minus first bracket
+    uint16_t* s_own = reinterpret_cast<uint16_t*>(s_sbd + PP_TILE);  // [EX_WIN] owner of each node / bracket
     __shared__ PosSums s_w[PP_THREADS / 32];
     __shared__ uint32_t s_tn, s_tb;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -613,7 +613,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
         }
         __syncthreads();
         // ---- per position: records and the one-position document rules --------
-        uint32_t nof[PP_ITEMS], cnt[PP_ITEMS];  // first node / bracket (tile-local), n_prod | n_br << 16
+        uint32_t nof[PP_ITEMS], bof[PP_ITEMS], cnt[PP_ITEMS];  // first node, first bracket (tile-local), n_prod | n_br << 16
         {
             PosSums run = ps_combine(ps_combine(tp, s_w[warp]), ex);  // before this thread's first position
 #pragma unroll
@@ -621,6 +621,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                 const long long i = i0 + j;
                 const int pl = tid * PP_ITEMS + j;
                 nof[j] = run.nodes - tp.nodes;
+                bof[j] = 0;
                 cnt[j] = 0;
                 if (i < a.L) {
                     const bool head = (hm >> j) & 1u;
@@ -631,18 +632,17 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                         a.node_off[doc] = (long long)run.nodes;
                         a.br_off[doc] = (long long)run.brs;
                     }
-                    s_noff[pl] = nof[j];
-                    s_boff[pl] = run.brs - tp.brs;
-                    s_ti[pl] = (uint32_t)(head ? i : run.hpos) + 1u + (head ? 0u : run.terms);
-                    s_v[pl] = head ? 0 : run.v;
-                    s_dep[pl] = dep;
-                    s_id[pl] = ids[j];
+                    bof[j] = run.brs - tp.brs;
                     PosSums e;
                     possums_zero(e);
                     if (ids[j] == NO_PAIR) {
                         if (dok) a.doc_valid[doc] = 0;  // no admissible pair
                     } else {
                         const PairInfo pi = s_pi[ids[j]];
+                        s_pos[pl] = make_int4((int32_t)pi.prod_begin - (int32_t)nof[j], head ? 0 : run.v,
+                                              (int32_t)((uint32_t)(head ? i : run.hpos) + 1u + (head ? 0u : run.terms)),
+                                              dep);
+                        s_sbd[pl] = (int32_t)pi.stack_begin - (int32_t)bof[j];
                         if (dep + (int32_t)pi.min_ds < 0 && dok) a.doc_valid[doc] = 0;  // depth below zero
                         e.nodes = pi.n_prod; e.brs = pi.n_br; e.depth = pi.d_depth; e.v = pi.d_v; e.terms = pi.n_term;
                         cnt[j] = (uint32_t)pi.n_prod | ((uint32_t)pi.n_br << 16);
@@ -664,34 +664,33 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                 for (uint32_t x = lo; x < hi; ++x) s_own[x - w0] = (uint16_t)(tid * PP_ITEMS + j);
             }
             __syncthreads();
-            for (uint32_t e0 = tid; e0 < wn; e0 += 2 * PP_THREADS) {
-                uint32_t tg[2], kd[2], gi[2];
-                int32_t vv[2];
-                int64_t st[2], en[2];
+            for (uint32_t e0 = tid; e0 < wn; e0 += EX_U * PP_THREADS) {
+                uint32_t tg[EX_U], kd[EX_U], gi[EX_U];
+                int32_t vv[EX_U];
+                int64_t st[EX_U], en[EX_U];
 #pragma unroll
-                for (int u = 0; u < 2; ++u) {
+                for (int u = 0; u < EX_U; ++u) {
                     const uint32_t e = e0 + u * PP_THREADS;
                     tg[u] = 0; kd[u] = 0; vv[u] = 0; st[u] = 0; en[u] = 0; gi[u] = 0xffffffffu;
                     if (e < wn) {
                         const uint32_t g = w0 + e;
-                        const int pl = s_own[e];
-                        const uint32_t r = g - s_noff[pl];
-                        const uint2 rec = s_prec[s_pi[s_id[pl]].prod_begin + r];
+                        const int4 ps = s_pos[s_own[e]];
+                        const uint2 rec = s_prec[(int32_t)g + ps.x];
                         const uint32_t tm1 = rec.x >> 16;  // terminal + 1, 0: not a terminal production
-                        vv[u] = s_v[pl] + (int32_t)(int16_t)(rec.y & 0xffffu);
+                        vv[u] = ps.y + (int32_t)(int16_t)(rec.y & 0xffffu);
                         tg[u] = rec.x & 0xffffu;
                         gi[u] = tp.nodes + g;
                         if (tm1 && a.subst_terminals) {
                             // the k-th terminal production of a document takes its k-th token's span
                             tg[u] = tm1 - 1;
                             kd[u] = 1;
-                            const uint32_t ti = s_ti[pl] + (rec.y >> 16);
+                            const uint32_t ti = (uint32_t)ps.z + (rec.y >> 16);
                             if (ti < a.L) { st[u] = __ldg(&a.pstart[ti]); en[u] = __ldg(&a.pend[ti]); }
                         }
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < 2; ++u) {
+                for (int u = 0; u < EX_U; ++u) {
                     if (gi[u] != 0xffffffffu && (long long)gi[u] < a.cap_nodes) {
                         const size_t g = gi[u];
                         a.vbuf[g] = vv[u];
@@ -709,21 +708,16 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             const uint32_t wn = min(tb - w0, (uint32_t)EX_WIN);
 #pragma unroll
             for (int j = 0; j < PP_ITEMS; ++j) {
-                const int pl = tid * PP_ITEMS + j;
-                const uint32_t n = cnt[j] >> 16;
-                if (n) {
-                    const uint32_t b = s_boff[pl];
-                    const uint32_t lo = max(b, w0), hi = min(b + n, w0 + wn);
-                    for (uint32_t x = lo; x < hi; ++x) s_own[x - w0] = (uint16_t)pl;
-                }
+                const uint32_t b = bof[j], n = cnt[j] >> 16;
+                const uint32_t lo = max(b, w0), hi = min(b + n, w0 + wn);
+                for (uint32_t x = lo; x < hi; ++x) s_own[x - w0] = (uint16_t)(tid * PP_ITEMS + j);
             }
             __syncthreads();
             for (uint32_t e = tid; e < wn; e += PP_THREADS) {
                 const uint32_t g = w0 + e;
                 const int pl = s_own[e];
-                const uint32_t r = g - s_boff[pl];
-                const uint2 rec = s_srec[s_pi[s_id[pl]].stack_begin + r];
-                const int32_t before = s_dep[pl] + (int32_t)(int16_t)(rec.y & 0xffffu);
+                const uint2 rec = s_srec[(int32_t)g + s_sbd[pl]];
+                const int32_t before = s_pos[pl].w + (int32_t)(int16_t)(rec.y & 0xffffu);
                 const uint32_t bg = tp.brs + g;
                 if ((long long)bg < a.cap_brs) {
                     a.brbuf[bg] = rec.x;
