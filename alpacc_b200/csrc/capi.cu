@@ -196,6 +196,15 @@ int load_lexer(alp_ctx* ctx, Reader& r) {
     }
     for (uint8_t b : vcls)
         if (b >= C1 - 1) return fail(ctx, ALP_ERR_TABLE, "byte class out of range");
+    // every table entry that a kernel uses as an index must be in range
+    for (uint16_t v : vcd)
+        if ((v & 0x7fffu) >= (uint32_t)S) return fail(ctx, ALP_ERR_TABLE, "lexer transition out of range");
+    for (uint16_t v : vstep)
+        if (v >= (uint32_t)E) return fail(ctx, ALP_ERR_TABLE, "endomorphism step out of range");
+    for (uint16_t v : vcomp)
+        if (v >= (uint32_t)E) return fail(ctx, ALP_ERR_TABLE, "endomorphism composition out of range");
+    for (uint16_t v : vapp)
+        if (v >= (uint32_t)S) return fail(ctx, ALP_ERR_TABLE, "endomorphism application out of range");
     int rc;
     if ((rc = upload(ctx, vcls.data(), vcls.size(), &ctx->lt.cls))) return rc;
     if ((rc = upload(ctx, vcd.data(), vcd.size(), &ctx->lt.cdelta))) return rc;
@@ -915,6 +924,14 @@ int alp_ctx_create(const void* blob, size_t len, int device, alp_ctx** out) {
     if (!rc && hl) rc = load_lexer(ctx, r);
     if (!rc && hp) rc = load_parser(ctx->pt, ctx->ph, r.p, r.e, ctx->owned, ctx->err);
     if (!rc && hp) ctx->has_parser = true;
+    if (!rc && hl && hp) {
+        // the parser indexes its key table with the lexer's terminal ids
+        const uint32_t T = (uint32_t)ctx->pt.T;
+        for (uint32_t v : ctx->h_tokinfo)
+            if ((v & TOK_TERM_MASK) >= T) { rc = fail(ctx, ALP_ERR_TABLE, "lexer terminal id outside the parser's"); break; }
+        if (!rc && (ctx->pt.start >= T || ctx->pt.end >= T || ctx->pt.empty >= T))
+            rc = fail(ctx, ALP_ERR_TABLE, "parser sentinel ids out of range");
+    }
     if (!rc && cudaMallocHost(&ctx->h_res, sizeof(AlpResult)) != cudaSuccess)
         rc = fail(ctx, ALP_ERR_CUDA, "cudaMallocHost failed");
     if (!rc && cudaMallocHost(&ctx->h_stage, 256) != cudaSuccess) rc = fail(ctx, ALP_ERR_CUDA, "cudaMallocHost failed");
@@ -996,6 +1013,35 @@ int alp_ctx_timings(alp_ctx* ctx, char* buf, size_t len) {
     ctx->marks.clear();
     snprintf(buf, len, "%s", out.c_str());
     return out.size() < len ? ALP_OK : ALP_ERR_CAPACITY;
+}
+
+// One thread waits, with the kernels' own bounded waits, on a 32-bit and a
+// 64-bit status word that nothing ever sets: each wait gives up after its
+// poll limit and records the timeout, as a look-back wait does when a tile
+// never publishes.
+__global__ void wait_check_kernel(const uint32_t* w32, const unsigned long long* w64, AlpResult* res) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t a = wait32(w32, &res->error);
+    const unsigned long long b = wait64(w64, &res->error);
+    res->aux[0] = (long long)(a >> 30);
+    res->aux[1] = (long long)(b >> 62);
+}
+
+int alp_check_bounded_wait(alp_ctx* ctx) {
+    if (!ctx) return ALP_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    int rc;
+    if ((rc = grow(ctx, ctx->scratch, 256))) return rc;
+    uint8_t* base = reinterpret_cast<uint8_t*>(ctx->scratch.p);
+    AlpResult* res = reinterpret_cast<AlpResult*>(base);
+    CK(cudaMemsetAsync(base, 0, 256, ctx->stream));  // result and two status words in state X
+    wait_check_kernel<<<1, 32, 0, ctx->stream>>>(reinterpret_cast<const uint32_t*>(base + 128),
+                                                  reinterpret_cast<const unsigned long long*>(base + 136), res);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->h_res, res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "bounded wait gave up");
+    return fail(ctx, ALP_ERR_CUDA, "bounded wait returned without giving up");
 }
 
 int alp_memcpy(alp_ctx* ctx, void* dst, const void* src, size_t bytes) {

@@ -112,6 +112,7 @@ inline int load_parser(ParseTables& pt, ParseHost& ph, const uint8_t* p, const u
             if (t >= T) { err = "key symbol out of range"; return 4; }
             x = x * T + t;
         }
+        if (key_pair[i] >= n_pairs) { err = "key names a pair out of range"; return 4; }
         index[(size_t)x] = (uint16_t)key_pair[i];
     }
     std::vector<PairInfo> info(n_pairs);

@@ -71,6 +71,13 @@ int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out);
 int alp_ctx_profile(alp_ctx* ctx, int on);
 int alp_ctx_timings(alp_ctx* ctx, char* buf, size_t len);
 
+/* Failure detection (no reference counterpart): every wait inside a kernel of
+ * this library is bounded, and a wait that runs out records the fact and lets
+ * the call return ALP_ERR_TIMEOUT with the context still usable.  This runs
+ * one such wait on a status word that nothing sets; it returns ALP_ERR_TIMEOUT
+ * after about a second when the bounds work. */
+int alp_check_bounded_wait(alp_ctx* ctx);
+
 /* Copy `bytes` between any two addresses (device or host) on the context's
  * stream and wait for it; lets bindings move context-owned outputs. */
 int alp_memcpy(alp_ctx* ctx, void* dst, const void* src, size_t bytes);
