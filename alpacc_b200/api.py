@@ -72,6 +72,14 @@ def native() -> ctypes.CDLL:
         L.alp_lex_stream_tokens.argtypes = [vp, P(i64)]
         L.alp_lex_stream_end.argtypes = [vp, P(i64), P(i32)]
         L.alp_lex_stream_window.argtypes = [vp, vp, vp, vp, i64, i64]
+        L.alp_parse_graph_create.argtypes = [vp, vp, i64, vp, i64, i64, i64] + [vp] * 8 + [P(vp)]
+        L.alp_parse_graph_launch.argtypes = [vp, vp]
+        L.alp_parse_graph_result.argtypes = [vp, P(i64)]
+        L.alp_parse_graph_error.argtypes = [vp]
+        L.alp_parse_graph_error.restype = ctypes.c_char_p
+        L.alp_parse_graph_destroy.argtypes = [vp]
+        L.alp_parse_graph_destroy.restype = None
+        L.alp_check_bounded_wait.argtypes = [vp]
         L.alp_lex_stream_free.argtypes = [vp]
         L.alp_lex_stream_free.restype = None
         L.alp_lex_host_stream.argtypes = [vp, vp, i64, i64, vp, vp, vp, i64, P(i64), P(i32)]
@@ -376,6 +384,21 @@ class Grammar:
                 _wrap(self.h, ptrs[3].value or 0, nd + 1, torch.int64, self.device),
                 _wrap(self.h, ptrs[4].value or 0, nd, torch.uint8, self.device))
 
+    def parse_batch_graph(self, data, offsets, cap_nodes: Optional[int] = None, cap_brackets: Optional[int] = None,
+                          slack: float = 0.25) -> "ParseGraph":
+        """alp_parse_graph_*: the batched parse of these documents' shape as a
+        CUDA graph.  Without capacities, one alp_parse_batch call measures the
+        batch and the capacities are its node and bracket counts plus `slack`."""
+        if cap_nodes is None or cap_brackets is None:
+            tree, _, _ = self.parse_batch_int(data, offsets)
+            info = (ctypes.c_int64 * 11)()
+            native().alp_ctx_info(self.h, info, 11)
+            if cap_nodes is None:
+                cap_nodes = int(len(tree) * (1 + slack)) + 64
+            if cap_brackets is None:
+                cap_brackets = int(info[10] * (1 + slack)) + 64
+        return ParseGraph(self, data, offsets, cap_nodes, cap_brackets)
+
     def parse_batch_int(self, data, offsets):
         """Documents back to back -> (Tree, node_off[n+1], valid[n]); parents
         and spans are relative to each document."""
@@ -463,6 +486,73 @@ class TokenStream:
     def close(self) -> None:
         if self.h:
             native().alp_lex_stream_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ParseGraph:
+    """A batched parse captured once as a CUDA graph: ``load`` new documents of
+    the same total size and count, ``launch`` (no wait), then ``result`` for
+    (Tree, node_off, valid) as ``Grammar.parse_batch_int`` gives them."""
+
+    def __init__(self, grammar: Grammar, data, offsets, cap_nodes: int, cap_brackets: int):
+        torch = _torch()
+        self.g = grammar
+        x, off = grammar._batch_inputs(data, offsets)
+        self.x, self.off = x.clone(), off.clone()
+        nd = self.off.numel() - 1
+        dev = grammar.device
+        self.parent = torch.empty(max(cap_nodes, 1), dtype=torch.int64, device=dev)
+        self.tag = torch.empty(max(cap_nodes, 1), dtype=torch.int32, device=dev)
+        self.kind = torch.empty(max(cap_nodes, 1), dtype=torch.uint8, device=dev)
+        self.start = torch.empty(max(cap_nodes, 1), dtype=torch.int64, device=dev)
+        self.end = torch.empty(max(cap_nodes, 1), dtype=torch.int64, device=dev)
+        self.node_off = torch.empty(nd + 1, dtype=torch.int64, device=dev)
+        self.valid = torch.empty(nd, dtype=torch.uint8, device=dev)
+        self.counts = torch.zeros(4, dtype=torch.int64, device=dev)
+        torch.cuda.synchronize(dev)
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())
+        h = ctypes.c_void_p()
+        rc = native().alp_parse_graph_create(grammar.h, vp(self.x), self.x.numel(), vp(self.off), nd, cap_nodes,
+                                             cap_brackets, vp(self.parent), vp(self.tag), vp(self.kind),
+                                             vp(self.start), vp(self.end), vp(self.node_off), vp(self.valid),
+                                             vp(self.counts), ctypes.byref(h))
+        if rc != ALP_OK:
+            grammar._err(rc)
+        self.h = h
+
+    def load(self, data, offsets) -> None:
+        """New documents with the same byte total and document count."""
+        x, off = self.g._batch_inputs(data, offsets)
+        if x.numel() != self.x.numel() or off.numel() != self.off.numel():
+            raise ValueError("a graph replays one batch shape: same bytes and documents")
+        self.x.copy_(x)
+        self.off.copy_(off)
+
+    def launch(self) -> None:
+        torch = _torch()
+        s = torch.cuda.current_stream(self.g.device).cuda_stream
+        rc = native().alp_parse_graph_launch(self.h, ctypes.c_void_p(s))
+        if rc != ALP_OK:
+            raise AlpError(rc, native().alp_parse_graph_error(self.h).decode(errors="replace"))
+
+    def result(self):
+        n = ctypes.c_int64(0)
+        rc = native().alp_parse_graph_result(self.h, ctypes.byref(n))
+        if rc != ALP_OK:
+            raise AlpError(rc, native().alp_parse_graph_error(self.h).decode(errors="replace"))
+        k = n.value
+        tree = Tree(self.parent[:k], self.tag[:k], self.kind[:k], self.start[:k], self.end[:k])
+        return tree, self.node_off, self.valid
+
+    def close(self) -> None:
+        if self.h:
+            native().alp_parse_graph_destroy(self.h)
             self.h = None
 
     def __del__(self):

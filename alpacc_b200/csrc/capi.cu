@@ -349,8 +349,11 @@ int read_result(alp_ctx* ctx, AlpResult* d_res) {
 
 // Previous-smaller-or-equal over `n` values (nodes: writes parent; brackets:
 // checks each right bracket against its match and clears res->valid).
+// With dn, n is a capacity and the element count is read from device memory
+// (no host round trip; grids cover the capacity).
 int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, int64_t* parent, int first,
-            const long long* seg_off, long long n_seg, uint8_t* seg_valid, AlpResult* d_res) {
+            const long long* seg_off, long long n_seg, uint8_t* seg_valid, AlpResult* d_res,
+            const long long* dn = nullptr) {
     if (n == 0) return ALP_OK;
     const long long tiles = (n + PLE_TILE - 1) / PLE_TILE;
     const long long n32 = (tiles + 31) / 32, n1024 = (tiles + 1023) / 1024;
@@ -381,13 +384,14 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     a.esc_count = esc_count;
     a.esc_cap = n;
     a.res = d_res;
+    a.dn = dn;
     CK(cudaFuncSetAttribute(ple_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PLE_SMEM));
     mark(ctx, "start");
     ple_tile_kernel<<<(unsigned)tiles, PLE_THREADS, PLE_SMEM, ctx->stream>>>(a);
     CK(cudaGetLastError());
     mark(ctx, sym ? "ple_tile_kernel(brackets)" : "ple_tile_kernel(nodes)");
     tile_min_levels_kernel<<<(unsigned)((n32 + 255) / 256), 256, 0, ctx->stream>>>(
-        a.tile_min, tiles, (int32_t*)ctx->tmp[first + 1].p, (int32_t*)ctx->tmp[first + 2].p);
+        a.tile_min, tiles, (int32_t*)ctx->tmp[first + 1].p, (int32_t*)ctx->tmp[first + 2].p, dn);
     CK(cudaGetLastError());
     EscArgs e;
     e.esc = a.esc;
@@ -703,10 +707,10 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     {
         const long long chunks = (tiles + ST_CHUNK - 1) / ST_CHUNK;
         PosSums* csum = a.tile_sums + tiles;  // chunk sums after the tile sums
-        scan_tiles_reduce_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum);
+        scan_tiles_reduce_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum, nullptr);
         CK(cudaGetLastError());
         scan_tiles_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum, d_res, a.node_off,
-                                                                         a.br_off, nd);
+                                                                         a.br_off, nd, nullptr);
         CK(cudaGetLastError());
     }
     mark(ctx, "scan_tiles_reduce+scan_tiles");
@@ -1968,5 +1972,269 @@ int alp_parse_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int
     *n_node_total = N;
     return ALP_OK;
 }
+
+}  // extern "C"
+
+// ---- batched parse as a CUDA graph ---------------------------------------------
+// The same kernels as alp_parse_batch, sized by capacities known on the host
+// (bytes, documents, nodes, brackets) and reading the actual counts from device
+// memory, so that the whole sequence runs with no host round trip and can be
+// captured once and replayed with one cudaGraphLaunch.
+
+namespace {
+
+// positions of the batch from the token pass; the result block reset for the parser
+__global__ void batch_sizes_kernel(AlpResult* res, long long n_docs, long long* sizes) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    sizes[0] = res->count + 2 * n_docs;
+    sizes[1] = (long long)res->error;
+    res->count = 0;
+    res->valid = 1;
+    res->error = 0;
+    for (int i = 0; i < 6; ++i) res->aux[i] = 0;
+}
+
+// counts[0] nodes, [1] brackets, [2] positions, [3] ALP_DEV_ERR_* bits
+__global__ void batch_status_kernel(const AlpResult* res, const long long* sizes, long long cap_nodes,
+                                    long long cap_brs, long long* counts) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned int err = res->error | (unsigned int)sizes[1];
+    if (res->aux[0] > cap_nodes || res->aux[1] > cap_brs) err |= ALP_DEV_ERR_CAPACITY;
+    counts[0] = res->aux[0];
+    counts[1] = res->aux[1];
+    counts[2] = sizes[0];
+    counts[3] = (long long)err;
+}
+
+// parse_positions with the position count in device memory (dL), L_cap
+// positions at most, and caller capacities for nodes and brackets.
+int parse_positions_dev(alp_ctx* ctx, long long Lcap, const long long* dL, long long nd, uint8_t* dvalid,
+                        const ParseOut& o, long long cap_nodes, long long cap_brs, long long* node_off) {
+    const long long tiles = (Lcap + PP_TILE - 1) / PP_TILE;
+    int rc;
+    if ((rc = grow(ctx, ctx->tmp[T_PID], (size_t)Lcap * 2 + 64)) ||
+        (rc = grow(ctx, ctx->tmp[T_TSUMS], (tiles + tiles / ST_CHUNK + 2) * sizeof(PosSums))) ||
+        (rc = grow(ctx, ctx->tmp[T_BROFF], (size_t)(nd + 1) * 8)) || (rc = grow(ctx, ctx->scratch, 256)) ||
+        (rc = grow(ctx, ctx->tmp[T_VBUF], (size_t)cap_nodes * 4 + 8)) ||
+        (rc = grow(ctx, ctx->tmp[T_BRBUF], (size_t)cap_brs * 4 + 8)) ||
+        (rc = grow(ctx, ctx->tmp[T_DSBUF], (size_t)cap_brs * 4 + 8)))
+        return rc;
+    AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
+    ParseArgs a;
+    memset(&a, 0, sizeof a);
+    a.t = ctx->pt;
+    a.P = (const uint16_t*)ctx->tmp[T_TTERM].p;
+    a.pstart = (const uint32_t*)ctx->tmp[T_TSTART].p;
+    a.pend = (const uint32_t*)ctx->tmp[T_TEND].p;
+    a.L = Lcap;
+    a.dL = dL;
+    a.n_docs = nd;
+    a.pid = (uint16_t*)ctx->tmp[T_PID].p;
+    a.tile_sums = (PosSums*)ctx->tmp[T_TSUMS].p;
+    a.res = d_res;
+    a.node_off = node_off;
+    a.br_off = (long long*)ctx->tmp[T_BROFF].p;
+    a.doc_valid = dvalid;
+    a.tag = o.tag;
+    a.kind = o.kind;
+    a.nstart = o.start;
+    a.nend = o.end;
+    a.subst_terminals = 1;
+    a.vbuf = (int32_t*)ctx->tmp[T_VBUF].p;
+    a.brbuf = (uint32_t*)ctx->tmp[T_BRBUF].p;
+    a.dsbuf = (int32_t*)ctx->tmp[T_DSBUF].p;
+    a.cap_nodes = cap_nodes;
+    a.cap_brs = cap_brs;
+    int sms = 0, per1 = 0, per2 = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    const size_t sm1 = sizeof(PairInfo) * ctx->pt.n_pairs + (size_t)(PP_TILE + ctx->pt.q + ctx->pt.k) * 4;
+    const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
+    if (sm2 > 220 * 1024) return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
+    CK(cudaFuncSetAttribute(parse_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+    CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, parse_pairs_kernel, PP_THREADS, sm1));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, parse_expand_kernel, PP_THREADS, sm2));
+    const long long x1 = (long long)(per1 > 0 ? per1 : 1) * sms, x2 = (long long)(per2 > 0 ? per2 : 1) * sms;
+    parse_pairs_kernel<<<(unsigned)(x1 < tiles ? x1 : tiles), PP_THREADS, sm1, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    {
+        const long long chunks = (tiles + ST_CHUNK - 1) / ST_CHUNK;
+        PosSums* csum = a.tile_sums + tiles;
+        scan_tiles_reduce_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum, dL);
+        CK(cudaGetLastError());
+        scan_tiles_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum, d_res, a.node_off,
+                                                                         a.br_off, nd, dL);
+        CK(cudaGetLastError());
+    }
+    parse_expand_kernel<<<(unsigned)(x2 < tiles ? x2 : tiles), PP_THREADS, sm2, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    if ((rc = run_ple(ctx, a.vbuf, cap_nodes, nullptr, o.parent, T_N_TMIN, a.node_off, nd, dvalid, d_res,
+                      &d_res->aux[0])))
+        return rc;
+    return run_ple(ctx, a.dsbuf, cap_brs, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res, &d_res->aux[1]);
+}
+
+}  // namespace
+
+struct alp_parse_graph {
+    alp_ctx* child = nullptr;        // tables shared with the parent context, buffers of its own
+    cudaStream_t stream = nullptr;   // capture stream
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t last = nullptr;     // stream of the last launch
+    long long* sizes = nullptr;      // device: positions, lexer error bits
+    long long* h_counts = nullptr;   // pinned
+    int64_t* d_counts = nullptr;
+    long long cap_nodes = 0, cap_brs = 0;
+    // the captured call
+    const uint8_t* d_in = nullptr;
+    long long n = 0, nd = 0;
+    const int64_t* d_off = nullptr;
+    ParseOut o{};
+    int64_t* d_node_off = nullptr;
+    uint8_t* d_valid = nullptr;
+};
+
+namespace {
+
+// the whole batched parse, enqueued on child->stream with no host wait
+int graph_enqueue(alp_parse_graph* g) {
+    alp_ctx* ctx = g->child;
+    const long long n = g->n, nd = g->nd;
+    const size_t tcap = (size_t)n + 2 * (size_t)nd + 16;
+    int rc;
+    if ((rc = grow(ctx, ctx->tmp[T_TTERM], tcap * 2)) || (rc = grow(ctx, ctx->tmp[T_TSTART], tcap * 4)) ||
+        (rc = grow(ctx, ctx->tmp[T_TEND], tcap * 4)) || (rc = grow(ctx, ctx->tmp[T_TOKOFF], (size_t)(nd + 1) * 8)))
+        return rc;
+    Lex3Run r;
+    if ((rc = lex3_prepare(ctx, g->d_in, n, (const long long*)g->d_off, nd, 1, ctx->tmp[T_TTERM].p,
+                           ctx->tmp[T_TSTART].p, ctx->tmp[T_TEND].p, (long long)tcap, g->d_valid, r)) ||
+        (rc = lex3_front(ctx, r)) || (rc = lex3_emit<uint16_t, uint32_t>(ctx, r)))
+        return rc;
+    AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
+    batch_sizes_kernel<<<1, 32, 0, ctx->stream>>>(d_res, nd, g->sizes);
+    CK(cudaGetLastError());
+    if ((rc = parse_positions_dev(ctx, n + 2 * nd, g->sizes, nd, g->d_valid, g->o, g->cap_nodes, g->cap_brs,
+                                  (long long*)g->d_node_off)))
+        return rc;
+    batch_status_kernel<<<1, 32, 0, ctx->stream>>>(d_res, g->sizes, g->cap_nodes, g->cap_brs,
+                                                   (long long*)g->d_counts);
+    CK(cudaGetLastError());
+    return ALP_OK;
+}
+
+alp_ctx* child_ctx(const alp_ctx* p) {
+    alp_ctx* c = new alp_ctx();
+    c->device = p->device;
+    c->has_lexer = p->has_lexer;
+    c->S = p->S; c->C = p->C; c->E = p->E;
+    c->ignore_term = p->ignore_term; c->dead_term = p->dead_term; c->n_terms = p->n_terms;
+    c->h_tokinfo = p->h_tokinfo;
+    c->lt = p->lt;
+    c->lex_smem = p->lex_smem;
+    c->lex3 = p->lex3;
+    c->l3 = p->l3;
+    c->l3_fold_smem = p->l3_fold_smem; c->l3_scan_smem = p->l3_scan_smem;
+    c->l3_count_smem = p->l3_count_smem; c->l3_emit_smem = p->l3_emit_smem;
+    c->has_parser = p->has_parser;
+    c->pt = p->pt;
+    c->ph = p->ph;
+    return c;
+}
+
+void graph_free(alp_parse_graph* g) {
+    if (!g) return;
+    if (g->child) cudaSetDevice(g->child->device);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    if (g->sizes) cudaFree(g->sizes);
+    if (g->h_counts) cudaFreeHost(g->h_counts);
+    if (g->child) {
+        g->child->stream = nullptr;
+        alp_ctx_destroy(g->child);  // its own buffers only: the tables belong to the parent
+    }
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+}
+
+}  // namespace
+
+extern "C" {
+
+int alp_parse_graph_create(alp_ctx* ctx, const uint8_t* d_in, int64_t n, const int64_t* d_off, int64_t n_docs,
+                           int64_t cap_nodes, int64_t cap_brackets, int64_t* d_parent, uint32_t* d_tag,
+                           uint8_t* d_kind, int64_t* d_start, int64_t* d_end, int64_t* d_node_off, uint8_t* d_valid,
+                           int64_t* d_counts, alp_parse_graph** out) {
+    if (!ctx || !out) return ALP_ERR_ARG;
+    *out = nullptr;
+    if (!ctx->has_lexer || !ctx->has_parser) return fail(ctx, ALP_ERR_MODE, "these tables are not lexer+parser tables");
+    if (!ctx->lex3) return fail(ctx, ALP_ERR_TABLE, "graphs need a DFA of at most 32 states");
+    if (n < 1 || n > 0x7ff00000LL || n_docs < 1 || n + 2 * n_docs >= 0x7fffffffLL || cap_nodes < 0 ||
+        cap_brackets < 0 || cap_nodes > 0xffffffffLL || cap_brackets > 0xffffffffLL)
+        return fail(ctx, ALP_ERR_ARG, "graph sizes out of range");
+    if (!d_in || !d_off || !d_parent || !d_tag || !d_kind || !d_start || !d_end || !d_node_off || !d_valid ||
+        !d_counts)
+        return fail(ctx, ALP_ERR_ARG, "null buffer");
+    CK(cudaSetDevice(ctx->device));
+    alp_parse_graph* g = new alp_parse_graph();
+    g->child = child_ctx(ctx);
+    g->d_in = d_in; g->n = n; g->d_off = d_off; g->nd = n_docs;
+    g->o.parent = d_parent; g->o.tag = d_tag; g->o.kind = d_kind; g->o.start = d_start; g->o.end = d_end;
+    g->d_node_off = d_node_off; g->d_valid = d_valid; g->d_counts = d_counts;
+    g->cap_nodes = cap_nodes; g->cap_brs = cap_brackets;
+    auto bad = [&](int rc, const char* what) {
+        const std::string m = g->child->err.empty() ? std::string(what) : g->child->err;
+        graph_free(g);
+        return fail(ctx, rc, "%s", m.c_str());
+    };
+    if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&g->sizes, 64) != cudaSuccess || cudaMallocHost(&g->h_counts, 64) != cudaSuccess ||
+        cudaMallocHost(&g->child->h_res, sizeof(AlpResult)) != cudaSuccess ||
+        cudaMallocHost(&g->child->h_stage, 256) != cudaSuccess)
+        return bad(ALP_ERR_CUDA, "graph set-up failed");
+    g->child->stream = g->stream;
+    // one plain run sizes every buffer and sets every kernel attribute, so
+    // that the captured run allocates nothing
+    int rc = graph_enqueue(g);
+    if (rc) return bad(rc, "graph warm-up failed");
+    if (cudaStreamSynchronize(g->stream) != cudaSuccess) return bad(ALP_ERR_CUDA, "graph warm-up failed");
+    if (cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+        return bad(ALP_ERR_CUDA, "stream capture failed to start");
+    rc = graph_enqueue(g);
+    const cudaError_t ec = cudaStreamEndCapture(g->stream, &g->graph);
+    if (rc) return bad(rc, "graph capture failed");
+    if (ec != cudaSuccess) return bad(ALP_ERR_CUDA, cudaGetErrorString(ec));
+    if (cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess) return bad(ALP_ERR_CUDA, "graph instantiation failed");
+    g->last = g->stream;
+    *out = g;
+    return ALP_OK;
+}
+
+int alp_parse_graph_launch(alp_parse_graph* g, void* stream) {
+    if (!g) return ALP_ERR_ARG;
+    cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : g->stream;
+    alp_ctx* ctx = g->child;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaGraphLaunch(g->exec, s));
+    g->last = s;
+    return ALP_OK;
+}
+
+int alp_parse_graph_result(alp_parse_graph* g, int64_t* n_nodes) {
+    if (!g || !n_nodes) return ALP_ERR_ARG;
+    alp_ctx* ctx = g->child;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(g->h_counts, g->d_counts, 32, cudaMemcpyDeviceToHost, g->last));
+    CK(cudaStreamSynchronize(g->last));
+    *n_nodes = g->h_counts[0];
+    const unsigned int err = (unsigned int)g->h_counts[3];
+    if (err & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "kernel wait timed out");
+    if (err & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "node or bracket capacity too small");
+    return ALP_OK;
+}
+
+const char* alp_parse_graph_error(const alp_parse_graph* g) { return g ? g->child->err.c_str() : "null graph"; }
+
+void alp_parse_graph_destroy(alp_parse_graph* g) { graph_free(g); }
 
 }  // extern "C"

@@ -312,6 +312,7 @@ struct ParseArgs {
     int subst_terminals;        // 1: wrapper productions become terminal nodes (parse_int); 0: production ids
     long long cap_nodes;
     long long cap_brs;
+    const long long* dL;        // when set: the position count, in device memory (L is then its capacity)
 };
 
 __device__ __forceinline__ uint32_t pos_term(const ParseArgs& a, long long i) {
@@ -329,6 +330,7 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
     __shared__ uint32_t s_pow[17];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int q = a.t.q, k = a.t.k, W = q + k;
+    if (a.dL) a.L = *a.dL;
     for (int i = tid; i < a.t.n_pairs * (int)(sizeof(PairInfo) / 4); i += PP_THREADS)
         reinterpret_cast<uint32_t*>(s_pi)[i] = reinterpret_cast<const uint32_t*>(a.t.pairs)[i];
     if (tid == 0) {
@@ -415,8 +417,9 @@ __device__ __forceinline__ PosSums ps_block_reduce(PosSums v, PosSums* s_w) {
 }
 
 __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_reduce_kernel(const PosSums* s, long long tiles,
-                                                                     PosSums* chunk_sums) {
+                                                                     PosSums* chunk_sums, const long long* dL) {
     __shared__ PosSums s_w[ST_CHUNK / 32];
+    if (dL) tiles = (*dL + PP_TILE - 1) / PP_TILE;  // the grid covers the capacity
     const long long idx = (long long)blockIdx.x * ST_CHUNK + threadIdx.x;
     PosSums v;
     if (idx < tiles) v = s[idx]; else possums_zero(v);
@@ -426,11 +429,14 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_reduce_kernel(const PosSu
 
 __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long long tiles, const PosSums* chunk_sums,
                                                               AlpResult* res, long long* node_off, long long* br_off,
-                                                              long long n_docs) {
+                                                              long long n_docs, const long long* dL) {
     __shared__ PosSums s_w[ST_CHUNK / 32];
     __shared__ PosSums s_carry;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long long chunk = blockIdx.x;
+    if (dL) tiles = (*dL + PP_TILE - 1) / PP_TILE;  // the grid covers the capacity
+    const long long last = (tiles + ST_CHUNK - 1) / ST_CHUNK - 1;
+    if (chunk > last) return;
     if (warp == 0) {
         PosSums carry;
         possums_zero(carry);
@@ -469,7 +475,7 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
     __syncthreads();
     const PosSums pre = ps_combine(s_carry, s_w[warp]);
     if (idx < tiles) s[idx] = ps_combine(pre, ex);
-    if (chunk == gridDim.x - 1) {
+    if (chunk == last) {
         __syncthreads();
         if (tid == ST_CHUNK - 1) s_carry = ps_combine(pre, inc);
         if (warp == 0) {
@@ -565,6 +571,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     __shared__ PosSums s_w[PP_THREADS / 32];
     __shared__ uint32_t s_tn, s_tb;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (a.dL) a.L = *a.dL;
     for (int i = tid; i < a.t.n_pairs * (int)(sizeof(PairInfo) / 4); i += PP_THREADS)
         reinterpret_cast<uint32_t*>(s_pi)[i] = reinterpret_cast<const uint32_t*>(a.t.pairs)[i];
     for (int i = tid; i < a.t.n_pseq; i += PP_THREADS) s_prec[i] = a.t.pseq_rec[i];
@@ -749,6 +756,7 @@ struct PleArgs {
     unsigned int* esc_count;
     long long esc_cap;
     AlpResult* res;
+    const long long* dn;         // when set: the element count, in device memory (n is then its capacity)
 };
 
 // Shared memory: the tile's values and a second array (bracket symbols, or
@@ -792,6 +800,10 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
     __shared__ long long s_sd0, s_sd1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long long base = (long long)blockIdx.x * PLE_TILE;
+    if (a.dn) {
+        a.n = min(a.n, *a.dn);
+        if (base >= a.n) return;  // the grid covers the capacity
+    }
     const bool brackets = a.sym != nullptr;
     const long long gfirst = base + (long long)tid * PLE_ITEMS;
     const int lim = (int)max(0ll, min((long long)PLE_ITEMS, a.n - gfirst));  // valid elements of this thread
@@ -1019,8 +1031,10 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
 }
 
 // Level-1/2 minima over groups of 32 / 1024 tiles.
-__global__ void tile_min_levels_kernel(const int32_t* tmin, long long tiles, int32_t* m32, int32_t* m1024) {
+__global__ void tile_min_levels_kernel(const int32_t* tmin, long long tiles, int32_t* m32, int32_t* m1024,
+                                       const long long* dn) {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (dn) tiles = min(tiles, (*dn + PLE_TILE - 1) / PLE_TILE);  // tiles is then the capacity
     const long long n32 = (tiles + 31) / 32;
     if (g < n32) {
         int32_t m = INT32_MAX;

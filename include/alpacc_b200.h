@@ -212,6 +212,35 @@ int alp_parse_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int
                     int64_t** d_parent, uint32_t** d_tag, uint8_t** d_kind, int64_t** d_start,
                     int64_t** d_end, int64_t** d_node_off, uint8_t** d_valid, int64_t* n_node_total);
 
+/* The batched parse as a CUDA graph (no reference counterpart).  alp_parse_batch
+ * waits on the host three times (input size, token total, node and bracket
+ * totals) to size its outputs; for a fixed batch shape this set-up captures the
+ * same kernels, sized by the capacities given here and reading the actual
+ * counts from device memory, in one CUDA graph, so that a batch costs one
+ * cudaGraphLaunch and no host round trip.
+ *   - create: the device buffers and sizes are fixed: d_in (n bytes),
+ *     d_off (n_docs + 1 offsets, d_off[n_docs] = n), node outputs of cap_nodes
+ *     elements, d_node_off (n_docs + 1), d_valid (n_docs), d_counts (4 int64:
+ *     nodes, brackets, positions, error bits).  The contents of d_in and d_off
+ *     may change between launches (same n and n_docs).  Runs the batch once
+ *     uncaptured to size the graph's own scratch, then captures it.
+ *   - launch: enqueues one run on `stream` (NULL: the graph's own stream); no wait.
+ *   - result: waits for the last launch; *n_nodes = nodes of the batch;
+ *     ALP_ERR_CAPACITY when cap_nodes or cap_brackets was too small (then the
+ *     outputs are incomplete and *n_nodes is the count needed).
+ * Outputs and their layout are those of alp_parse_batch.  The graph keeps its
+ * own scratch and shares only the tables with `ctx`, which stays usable; the
+ * graph must be destroyed before `ctx`.  Needs a DFA of at most 32 states. */
+typedef struct alp_parse_graph alp_parse_graph;
+int alp_parse_graph_create(alp_ctx* ctx, const uint8_t* d_in, int64_t n, const int64_t* d_off, int64_t n_docs,
+                           int64_t cap_nodes, int64_t cap_brackets, int64_t* d_parent, uint32_t* d_tag,
+                           uint8_t* d_kind, int64_t* d_start, int64_t* d_end, int64_t* d_node_off, uint8_t* d_valid,
+                           int64_t* d_counts, alp_parse_graph** out);
+int alp_parse_graph_launch(alp_parse_graph* g, void* stream);
+int alp_parse_graph_result(alp_parse_graph* g, int64_t* n_nodes);
+const char* alp_parse_graph_error(const alp_parse_graph* g);
+void alp_parse_graph_destroy(alp_parse_graph* g);
+
 #ifdef __cplusplus
 }
 #endif
