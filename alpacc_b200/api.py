@@ -16,7 +16,7 @@ from __future__ import annotations
 import ctypes
 import os
 from dataclasses import dataclass
-from typing import List, Optional, Tuple, Union
+from typing import List, Optional, Sequence, Tuple, Union
 
 import numpy as np
 
@@ -80,6 +80,10 @@ def native() -> ctypes.CDLL:
         L.alp_parse_graph_destroy.argtypes = [vp]
         L.alp_parse_graph_destroy.restype = None
         L.alp_check_bounded_wait.argtypes = [vp]
+        L.alp_tune_parse.argtypes = [vp, vp, i64, i32, ctypes.c_char_p, ctypes.c_size_t]
+        L.alp_tune_get.argtypes = [vp, P(i32), i32]
+        L.alp_tune_set.argtypes = [vp, P(i32), i32]
+        L.alp_tune_shapes.argtypes = [P(i32), i32]
         L.alp_lex_stream_free.argtypes = [vp]
         L.alp_lex_stream_free.restype = None
         L.alp_lex_host_stream.argtypes = [vp, vp, i64, i64, vp, vp, vp, i64, P(i64), P(i32)]
@@ -358,7 +362,10 @@ class Grammar:
     def _batch_inputs(self, data, offsets):
         torch = _torch()
         x = self._as_device_bytes(data)
-        off = torch.as_tensor(np.ascontiguousarray(offsets, dtype=np.int64)).to(self.device)
+        if isinstance(offsets, torch.Tensor):
+            off = offsets.to(device=self.device, dtype=torch.int64).contiguous()
+        else:
+            off = torch.as_tensor(np.ascontiguousarray(offsets, dtype=np.int64)).to(self.device)
         if off.numel() < 2 or int(off[-1]) != x.numel():
             raise ValueError("offsets must run from 0 to len(data)")
         return x, off
@@ -383,6 +390,43 @@ class Grammar:
                 _wrap(self.h, ptrs[2].value or 0, k, torch.int64, self.device),
                 _wrap(self.h, ptrs[3].value or 0, nd + 1, torch.int64, self.device),
                 _wrap(self.h, ptrs[4].value or 0, nd, torch.uint8, self.device))
+
+    # ---------------------------------------------------------------- tuning
+    @staticmethod
+    def tile_shapes() -> List[Tuple[int, int]]:
+        """(threads, elements per thread) of each previous-smaller-or-equal tile shape."""
+        L = native()
+        k = L.alp_tune_shapes(None, 0)
+        out = (ctypes.c_int32 * (2 * k))()
+        L.alp_tune_shapes(out, 2 * k)
+        return [(out[2 * i], out[2 * i + 1]) for i in range(k)]
+
+    def get_tuning(self) -> List[int]:
+        cfg = (ctypes.c_int32 * 3)()
+        native().alp_tune_get(self.h, cfg, 3)
+        return list(cfg)
+
+    def set_tuning(self, cfg: Sequence[int]) -> None:
+        c = (ctypes.c_int32 * 3)(*cfg)
+        rc = native().alp_tune_set(self.h, c, 3)
+        if rc != ALP_OK:
+            self._err(rc)
+
+    def tune(self, sample, reps: int = 3) -> dict:
+        """alp_tune_parse on `sample` (bytes, numpy or a uint8 tensor): the
+        context keeps the fastest launch shapes; returns them with the timings."""
+        x = self._as_device_bytes(sample)
+        self._stream()
+        buf = ctypes.create_string_buffer(1 << 14)
+        rc = native().alp_tune_parse(self.h, ctypes.c_void_p(x.data_ptr()), x.numel(), reps, buf, len(buf))
+        if rc != ALP_OK:
+            self._err(rc)
+        rows = []
+        for ln in buf.value.decode().splitlines():
+            k, v, ms = ln.split()
+            rows.append((k, int(v), float(ms)))
+        cfg = self.get_tuning()
+        return {"config": cfg, "tile_shape": self.tile_shapes()[cfg[0]], "timings": rows}
 
     def parse_batch_graph(self, data, offsets, cap_nodes: Optional[int] = None, cap_brackets: Optional[int] = None,
                           slack: float = 0.25) -> "ParseGraph":

@@ -2,6 +2,7 @@
 // the host side of every entry point.  Kernels live in the .cuh files.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -32,6 +33,13 @@ struct DevBuf {
 };
 
 }  // namespace
+
+// Launch shapes the autotuner picks (alp_tune_parse); zeros are the defaults.
+struct Tuning {
+    int ple = 0;          // index into ple_shapes
+    int pairs_ctas = 0;   // CTAs per SM of the persistent pair kernel (0: as many as fit)
+    int expand_ctas = 0;  // same for the expand kernel
+};
 
 struct alp_ctx {
     int device = 0;
@@ -74,6 +82,7 @@ struct alp_ctx {
     DevBuf pipe;
     DevBuf carry;
     LexCarry* h_carry = nullptr;          // pinned, [2]
+    Tuning tune;
 };
 
 struct alp_lex_stream {
@@ -349,19 +358,41 @@ int read_result(alp_ctx* ctx, AlpResult* d_res) {
 
 // Previous-smaller-or-equal over `n` values (nodes: writes parent; brackets:
 // checks each right bracket against its match and clears res->valid).
+// Tile shapes of the previous-smaller-or-equal kernel (threads x elements per thread).
+struct PleShape {
+    int threads, items;
+    const void* fn;
+    size_t smem;
+};
+const PleShape ple_shapes[] = {
+    {256, 16, (const void*)ple_tile_kernel<256, 16>, ple_smem(256, 16)},
+    {256, 8, (const void*)ple_tile_kernel<256, 8>, ple_smem(256, 8)},
+    {128, 16, (const void*)ple_tile_kernel<128, 16>, ple_smem(128, 16)},
+    {512, 8, (const void*)ple_tile_kernel<512, 8>, ple_smem(512, 8)},
+};
+constexpr int N_PLE_SHAPES = (int)(sizeof(ple_shapes) / sizeof(ple_shapes[0]));
+
+// CTAs per SM of a persistent kernel: the tuned count, at most what fits
+int persistent_ctas(int fit, int tuned) {
+    if (fit < 1) fit = 1;
+    return (tuned > 0 && tuned < fit) ? tuned : fit;
+}
+
 // With dn, n is a capacity and the element count is read from device memory
 // (no host round trip; grids cover the capacity).
 int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, int64_t* parent, int first,
             const long long* seg_off, long long n_seg, uint8_t* seg_valid, AlpResult* d_res,
             const long long* dn = nullptr) {
     if (n == 0) return ALP_OK;
-    const long long tiles = (n + PLE_TILE - 1) / PLE_TILE;
+    const PleShape& sh = ple_shapes[ctx->tune.ple];
+    const int tile = sh.threads * sh.items;
+    const long long tiles = (n + tile - 1) / tile;
     const long long n32 = (tiles + 31) / 32, n1024 = (tiles + 1023) / 1024;
     int rc;
     if ((rc = grow(ctx, ctx->tmp[first + 0], tiles * 4)) || (rc = grow(ctx, ctx->tmp[first + 1], n32 * 4)) ||
         (rc = grow(ctx, ctx->tmp[first + 2], n1024 * 4)) ||
-        (rc = grow(ctx, ctx->tmp[first + 3], (size_t)tiles * PLE_TILE * 4)) ||
-        (rc = grow(ctx, ctx->tmp[first + 4], (size_t)tiles * PLE_TILE * 4)) ||
+        (rc = grow(ctx, ctx->tmp[first + 3], (size_t)tiles * tile * 4)) ||
+        (rc = grow(ctx, ctx->tmp[first + 4], (size_t)tiles * tile * 4)) ||
         (rc = grow(ctx, ctx->tmp[first + 5], tiles * 4)) ||
         (rc = grow(ctx, ctx->tmp[first + 6], (size_t)n * 8 + 64)))
         return rc;
@@ -385,13 +416,15 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     a.esc_cap = n;
     a.res = d_res;
     a.dn = dn;
-    CK(cudaFuncSetAttribute(ple_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PLE_SMEM));
+    CK(cudaFuncSetAttribute(sh.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
     mark(ctx, "start");
-    ple_tile_kernel<<<(unsigned)tiles, PLE_THREADS, PLE_SMEM, ctx->stream>>>(a);
-    CK(cudaGetLastError());
+    {
+        void* args[] = {&a};
+        CK(cudaLaunchKernel(sh.fn, dim3((unsigned)tiles), dim3(sh.threads), args, sh.smem, ctx->stream));
+    }
     mark(ctx, sym ? "ple_tile_kernel(brackets)" : "ple_tile_kernel(nodes)");
     tile_min_levels_kernel<<<(unsigned)((n32 + 255) / 256), 256, 0, ctx->stream>>>(
-        a.tile_min, tiles, (int32_t*)ctx->tmp[first + 1].p, (int32_t*)ctx->tmp[first + 2].p, dn);
+        a.tile_min, tiles, (int32_t*)ctx->tmp[first + 1].p, (int32_t*)ctx->tmp[first + 2].p, dn, tile);
     CK(cudaGetLastError());
     EscArgs e;
     e.esc = a.esc;
@@ -409,6 +442,7 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     e.n_seg = n_seg;
     e.seg_valid = seg_valid;
     e.res = d_res;
+    e.tile = tile;
     ple_escape_kernel<<<148 * 4, 256, 0, ctx->stream>>>(e);
     CK(cudaGetLastError());
     mark(ctx, sym ? "tile_min+ple_escape(brackets)" : "tile_min+ple_escape(nodes)");
@@ -697,7 +731,7 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
         int sms = 0, per1 = 0;
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, parse_pairs_kernel, PP_THREADS, sm1));
-        const long long x = (long long)(per1 > 0 ? per1 : 1) * sms;
+        const long long x = (long long)persistent_ctas(per1, ctx->tune.pairs_ctas) * sms;
         g_pairs = (unsigned)(x < tiles ? x : tiles);
         g_expand = (unsigned)(2LL * sms < tiles ? 2LL * sms : tiles);  // persistent; set below from occupancy
     }
@@ -754,7 +788,7 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
         int sms = 0, per2 = 0;
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, parse_expand_kernel, PP_THREADS, sm2));
-        const long long x = (long long)(per2 > 0 ? per2 : 1) * sms;
+        const long long x = (long long)persistent_ctas(per2, ctx->tune.expand_ctas) * sms;
         g_expand = (unsigned)(x < tiles ? x : tiles);
     }
     parse_expand_kernel<<<g_expand, PP_THREADS, sm2, ctx->stream>>>(a);
@@ -1046,6 +1080,130 @@ int alp_check_bounded_wait(alp_ctx* ctx) {
     CK(cudaStreamSynchronize(ctx->stream));
     if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "bounded wait gave up");
     return fail(ctx, ALP_ERR_CUDA, "bounded wait returned without giving up");
+}
+
+int alp_tune_get(const alp_ctx* ctx, int32_t* cfg, int n) {
+    if (!ctx || !cfg || n < 3) return ALP_ERR_ARG;
+    cfg[0] = ctx->tune.ple;
+    cfg[1] = ctx->tune.pairs_ctas;
+    cfg[2] = ctx->tune.expand_ctas;
+    return ALP_OK;
+}
+
+int alp_tune_set(alp_ctx* ctx, const int32_t* cfg, int n) {
+    if (!ctx || !cfg || n < 3) return ALP_ERR_ARG;
+    if (cfg[0] < 0 || cfg[0] >= N_PLE_SHAPES || cfg[1] < 0 || cfg[1] > 32 || cfg[2] < 0 || cfg[2] > 32)
+        return fail(ctx, ALP_ERR_ARG, "tuning values out of range");
+    ctx->tune.ple = cfg[0];
+    ctx->tune.pairs_ctas = cfg[1];
+    ctx->tune.expand_ctas = cfg[2];
+    return ALP_OK;
+}
+
+int alp_tune_shapes(int32_t* out, int n) {
+    if (!out) return N_PLE_SHAPES;
+    for (int i = 0; i < N_PLE_SHAPES && 2 * i + 1 < n; ++i) {
+        out[2 * i] = ple_shapes[i].threads;
+        out[2 * i + 1] = ple_shapes[i].items;
+    }
+    return N_PLE_SHAPES;
+}
+
+int alp_tune_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int reps, char* report, size_t report_len) {
+    if (!ctx) return ALP_ERR_ARG;
+    if (!ctx->has_lexer || !ctx->has_parser) return fail(ctx, ALP_ERR_MODE, "these tables are not lexer+parser tables");
+    if (reps < 1 || reps > 100) return fail(ctx, ALP_ERR_ARG, "reps out of range");
+    int rc = check_in(ctx, d_in, n, true);
+    if (rc) return rc;
+    CK(cudaSetDevice(ctx->device));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    std::string rep;
+    long long nodes0 = -1;
+    // median ms of `reps` calls with the context's current tuning
+    auto measure = [&](double* ms) -> int {
+        int64_t *pp, *ps, *pe;
+        uint32_t* pt;
+        uint8_t* pk;
+        int64_t nn = 0;
+        int valid = 0;
+        int r = alp_parse(ctx, d_in, n, &pp, &pt, &pk, &ps, &pe, &nn, &valid);  // warm-up
+        if (r) return r;
+        if (nodes0 < 0) nodes0 = nn;
+        if (nn != nodes0) return fail(ctx, ALP_ERR_CUDA, "tuning variants disagree on the node count");
+        std::vector<float> t;
+        for (int i = 0; i < reps; ++i) {
+            if (cudaEventRecord(e0, ctx->stream) != cudaSuccess) return fail(ctx, ALP_ERR_CUDA, "event record failed");
+            if ((r = alp_parse(ctx, d_in, n, &pp, &pt, &pk, &ps, &pe, &nn, &valid))) return r;
+            if (cudaEventRecord(e1, ctx->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess)
+                return fail(ctx, ALP_ERR_CUDA, "event record failed");
+            float x = 0;
+            cudaEventElapsedTime(&x, e0, e1);
+            t.push_back(x);
+        }
+        std::sort(t.begin(), t.end());
+        *ms = t[t.size() / 2];
+        return ALP_OK;
+    };
+    auto line = [&](const char* what, int v, double ms) {
+        char b[96];
+        snprintf(b, sizeof b, "%s %d %.4f\n", what, v, ms);
+        rep += b;
+    };
+    const Tuning saved = ctx->tune;
+    auto done = [&](int r) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (r) ctx->tune = saved;
+        if (report && report_len) {
+            const size_t k = rep.size() < report_len - 1 ? rep.size() : report_len - 1;
+            memcpy(report, rep.data(), k);
+            report[k] = 0;
+        }
+        return r;
+    };
+    // one knob at a time, the others held at their best so far
+    int fit_pairs = 1, fit_expand = 1;
+    {
+        const size_t sm1 = sizeof(PairInfo) * ctx->pt.n_pairs + (size_t)(PP_TILE + ctx->pt.q + ctx->pt.k) * 4;
+        const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
+        CK(cudaFuncSetAttribute(parse_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+        CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit_pairs, parse_pairs_kernel, PP_THREADS, sm1));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit_expand, parse_expand_kernel, PP_THREADS, sm2));
+    }
+    double best = 1e30, ms = 0;
+    int arg = 0;
+    for (int i = 0; i < N_PLE_SHAPES; ++i) {
+        ctx->tune.ple = i;
+        if ((rc = measure(&ms))) return done(rc);
+        char what[48];
+        snprintf(what, sizeof what, "ple_shape_%dx%d", ple_shapes[i].threads, ple_shapes[i].items);
+        line(what, i, ms);
+        if (ms < best) { best = ms; arg = i; }
+    }
+    ctx->tune.ple = arg;
+    best = 1e30;
+    arg = 0;
+    for (int c = 1; c <= fit_expand; ++c) {
+        ctx->tune.expand_ctas = c;
+        if ((rc = measure(&ms))) return done(rc);
+        line("expand_ctas_per_sm", c, ms);
+        if (ms < best) { best = ms; arg = c; }
+    }
+    ctx->tune.expand_ctas = arg;
+    best = 1e30;
+    arg = 0;
+    for (int c = 1; c <= fit_pairs; ++c) {
+        ctx->tune.pairs_ctas = c;
+        if ((rc = measure(&ms))) return done(rc);
+        line("pairs_ctas_per_sm", c, ms);
+        if (ms < best) { best = ms; arg = c; }
+    }
+    ctx->tune.pairs_ctas = arg;
+    line("best_ms", 0, best);
+    return done(ALP_OK);
 }
 
 int alp_memcpy(alp_ctx* ctx, void* dst, const void* src, size_t bytes) {
@@ -2054,7 +2212,8 @@ int parse_positions_dev(alp_ctx* ctx, long long Lcap, const long long* dL, long 
     CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, parse_pairs_kernel, PP_THREADS, sm1));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, parse_expand_kernel, PP_THREADS, sm2));
-    const long long x1 = (long long)(per1 > 0 ? per1 : 1) * sms, x2 = (long long)(per2 > 0 ? per2 : 1) * sms;
+    const long long x1 = (long long)persistent_ctas(per1, ctx->tune.pairs_ctas) * sms,
+                    x2 = (long long)persistent_ctas(per2, ctx->tune.expand_ctas) * sms;
     parse_pairs_kernel<<<(unsigned)(x1 < tiles ? x1 : tiles), PP_THREADS, sm1, ctx->stream>>>(a);
     CK(cudaGetLastError());
     {
@@ -2139,6 +2298,7 @@ alp_ctx* child_ctx(const alp_ctx* p) {
     c->has_parser = p->has_parser;
     c->pt = p->pt;
     c->ph = p->ph;
+    c->tune = p->tune;
     return c;
 }
 

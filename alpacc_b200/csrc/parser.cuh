@@ -207,6 +207,8 @@ namespace alp {
 constexpr int PP_THREADS = 512;
 constexpr int PP_ITEMS = 4;                        // positions per thread
 constexpr int PP_TILE = PP_THREADS * PP_ITEMS;     // positions per tile
+// previous-smaller-or-equal tiles: the default shape (threads x elements per
+// thread); ple_tile_kernel is instantiated for the shapes ple_shapes lists
 constexpr int PLE_THREADS = 256;
 constexpr int PLE_ITEMS = 16;
 constexpr int PLE_TILE = PLE_THREADS * PLE_ITEMS;  // elements per tile
@@ -749,8 +751,8 @@ struct PleArgs {
     long long n_seg;
     uint8_t* seg_valid;          // brackets: cleared for a document with a mismatch
     int32_t* tile_min;           // [tiles]
-    int32_t* stair_val;          // [tiles * PLE_TILE]
-    uint32_t* stair_idx;         // [tiles * PLE_TILE] global index
+    int32_t* stair_val;          // [tiles * tile elements]
+    uint32_t* stair_idx;         // [tiles * tile elements] global index
     int32_t* stair_len;          // [tiles]
     unsigned long long* esc;     // escapees: index << 32 | (uint32)value
     unsigned int* esc_count;
@@ -760,13 +762,14 @@ struct PleArgs {
 };
 
 // Shared memory: the tile's values and a second array (bracket symbols, or
-// node results) with one pad word after every thread's PLE_ITEMS, so that a
+// node results) with one pad word after every thread's PI elements, so that a
 // warp reading element k of its threads' chunks hits 32 different banks; the
-// minima of each chunk's four quarters; a min tree over the PLE_THREADS chunk
-// minima (leaves at PLE_THREADS..2*PLE_THREADS-1); a query queue per warp.
-constexpr int PLE_STRIDE = PLE_ITEMS + 1;
-constexpr size_t PLE_SMEM = (size_t)(2 * PLE_THREADS * PLE_STRIDE + 2 * PLE_THREADS) * 4 +
-                            (size_t)PLE_THREADS * 16 + (size_t)PLE_TILE * 2;
+// minima of each chunk's quarters; a min tree over the PT chunk minima (leaves
+// at PT..2*PT-1); a query queue per warp.
+// PT threads with PI elements each (PI a multiple of 4): one tile of PT * PI.
+__host__ __device__ constexpr size_t ple_smem(int PT, int PI) {
+    return (size_t)(2 * PT * (PI + 1) + 2 * PT) * 4 + (size_t)PT * (PI / 4) * 4 + (size_t)PT * PI * 2;
+}
 
 // largest d in [lo, hi] with off[d] <= g
 __device__ __forceinline__ long long seg_upper(const long long* off, long long lo, long long hi, long long g) {
@@ -777,9 +780,10 @@ __device__ __forceinline__ long long seg_upper(const long long* off, long long l
     return lo;
 }
 
-__device__ __forceinline__ int ple_pad(int e) { return (e / PLE_ITEMS) * PLE_STRIDE + (e % PLE_ITEMS); }
+template <int PI>
+__device__ __forceinline__ int ple_pad(int e) { return (e / PI) * (PI + 1) + (e % PI); }
 
-// Each thread owns PLE_ITEMS consecutive elements.  An element's answer is
+// Each thread owns PI consecutive elements.  An element's answer is
 // (1) its thread's last earlier element <= x (branch-free compares in
 // registers), else (2) the last element <= x in the nearest earlier chunk
 // whose minimum is <= x: a per-warp queue of these queries runs 32 at a time
@@ -787,74 +791,77 @@ __device__ __forceinline__ int ple_pad(int e) { return (e / PLE_ITEMS) * PLE_STR
 // quarter minima, then four elements), else (3) in an earlier tile:
 // ple_escape_kernel.  Node parents are staged in shared memory and written
 // with coalesced stores.
-__global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
+template <int PT, int PI>
+__global__ void __launch_bounds__(PT, 1024 / PT) ple_tile_kernel(PleArgs a) {
+    static_assert(PI % 4 == 0 && PT % 32 == 0 && PT * PI <= 65536, "tile shape");
+    constexpr int NQ = PI / 4;  // quarters of four elements
     extern __shared__ __align__(16) uint8_t smem[];
-    int32_t* s_val = reinterpret_cast<int32_t*>(smem);                        // [PLE_THREADS * PLE_STRIDE]
-    int32_t* s_aux = s_val + PLE_THREADS * PLE_STRIDE;                         // symbols / results
-    int32_t* tree = s_aux + PLE_THREADS * PLE_STRIDE;                          // [2 * PLE_THREADS]
-    int4* s_sub = reinterpret_cast<int4*>(tree + 2 * PLE_THREADS);             // [PLE_THREADS] quarter minima
-    uint16_t* s_q = reinterpret_cast<uint16_t*>(s_sub + PLE_THREADS);          // [PLE_TILE] query queues
-    __shared__ int32_t s_suf[PLE_THREADS];
-    __shared__ int32_t s_wm[PLE_THREADS / 32];
-    __shared__ uint32_t s_cnt[PLE_THREADS / 32];
+    int32_t* s_val = reinterpret_cast<int32_t*>(smem);                        // [PT * (PI + 1)]
+    int32_t* s_aux = s_val + PT * (PI + 1);                         // symbols / results
+    int32_t* tree = s_aux + PT * (PI + 1);                          // [2 * PT]
+    int32_t* s_sub = tree + 2 * PT;                                   // [PT][NQ] quarter minima
+    uint16_t* s_q = reinterpret_cast<uint16_t*>(s_sub + PT * NQ);     // [(PT * PI)] query queues
+    __shared__ int32_t s_suf[PT];
+    __shared__ int32_t s_wm[PT / 32];
+    __shared__ uint32_t s_cnt[PT / 32];
     __shared__ long long s_sd0, s_sd1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const long long base = (long long)blockIdx.x * PLE_TILE;
+    const long long base = (long long)blockIdx.x * (PT * PI);
     if (a.dn) {
         a.n = min(a.n, *a.dn);
         if (base >= a.n) return;  // the grid covers the capacity
     }
     const bool brackets = a.sym != nullptr;
-    const long long gfirst = base + (long long)tid * PLE_ITEMS;
-    const int lim = (int)max(0ll, min((long long)PLE_ITEMS, a.n - gfirst));  // valid elements of this thread
+    const long long gfirst = base + (long long)tid * PI;
+    const int lim = (int)max(0ll, min((long long)PI, a.n - gfirst));  // valid elements of this thread
 
     // ---- this thread's values (and symbols) --------------------------------
-    int32_t v[PLE_ITEMS];
-    if (lim == PLE_ITEMS) {
+    int32_t v[PI];
+    if (lim == PI) {
         const int4* src = reinterpret_cast<const int4*>(a.val + gfirst);
 #pragma unroll
-        for (int q = 0; q < PLE_ITEMS / 4; ++q) {
+        for (int q = 0; q < PI / 4; ++q) {
             const int4 x = __ldg(src + q);
             v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
         }
     } else {
 #pragma unroll
-        for (int i = 0; i < PLE_ITEMS; ++i) v[i] = i < lim ? a.val[gfirst + i] : INT32_MAX;
+        for (int i = 0; i < PI; ++i) v[i] = i < lim ? a.val[gfirst + i] : INT32_MAX;
     }
 #pragma unroll
-    for (int i = 0; i < PLE_ITEMS; ++i) s_val[tid * PLE_STRIDE + i] = v[i];
+    for (int i = 0; i < PI; ++i) s_val[tid * (PI + 1) + i] = v[i];
     if (brackets) {
-        if (lim == PLE_ITEMS) {
+        if (lim == PI) {
             const uint4* src = reinterpret_cast<const uint4*>(a.sym + gfirst);
 #pragma unroll
-            for (int q = 0; q < PLE_ITEMS / 4; ++q) {
+            for (int q = 0; q < PI / 4; ++q) {
                 const uint4 x = __ldg(src + q);
-                s_aux[tid * PLE_STRIDE + 4 * q] = (int32_t)x.x;
-                s_aux[tid * PLE_STRIDE + 4 * q + 1] = (int32_t)x.y;
-                s_aux[tid * PLE_STRIDE + 4 * q + 2] = (int32_t)x.z;
-                s_aux[tid * PLE_STRIDE + 4 * q + 3] = (int32_t)x.w;
+                s_aux[tid * (PI + 1) + 4 * q] = (int32_t)x.x;
+                s_aux[tid * (PI + 1) + 4 * q + 1] = (int32_t)x.y;
+                s_aux[tid * (PI + 1) + 4 * q + 2] = (int32_t)x.z;
+                s_aux[tid * (PI + 1) + 4 * q + 3] = (int32_t)x.w;
             }
         } else {
 #pragma unroll
-            for (int i = 0; i < PLE_ITEMS; ++i) s_aux[tid * PLE_STRIDE + i] = i < lim ? (int32_t)a.sym[gfirst + i] : 0;
+            for (int i = 0; i < PI; ++i) s_aux[tid * (PI + 1) + i] = i < lim ? (int32_t)a.sym[gfirst + i] : 0;
         }
     }
     if (tid == 0) {
         s_sd0 = seg_upper(a.seg_off, 0, a.n_seg - 1, base);
-        s_sd1 = seg_upper(a.seg_off, 0, a.n_seg - 1, min(base + PLE_TILE, a.n) - 1);
+        s_sd1 = seg_upper(a.seg_off, 0, a.n_seg - 1, min(base + (PT * PI), a.n) - 1);
     }
-    int4 qm;
-    qm.x = min(min(v[0], v[1]), min(v[2], v[3]));
-    qm.y = min(min(v[4], v[5]), min(v[6], v[7]));
-    qm.z = min(min(v[8], v[9]), min(v[10], v[11]));
-    qm.w = min(min(v[12], v[13]), min(v[14], v[15]));
-    s_sub[tid] = qm;
-    const int32_t cm = min(min(qm.x, qm.y), min(qm.z, qm.w));
+    int32_t cm = INT32_MAX;
+#pragma unroll
+    for (int qq = 0; qq < NQ; ++qq) {
+        const int32_t m = min(min(v[4 * qq], v[4 * qq + 1]), min(v[4 * qq + 2], v[4 * qq + 3]));
+        s_sub[tid * NQ + qq] = m;
+        cm = min(cm, m);
+    }
 
     // ---- min tree over chunk minima: warp levels by shuffles, top by thread 0
     {
         int32_t m = cm;
-        int node = PLE_THREADS + tid;
+        int node = PT + tid;
         tree[node] = m;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -865,7 +872,7 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
     }
     __syncthreads();
     if (tid == 0) {
-        for (int node = PLE_THREADS / 32 - 1; node >= 1; --node) tree[node] = min(tree[2 * node], tree[2 * node + 1]);
+        for (int node = PT / 32 - 1; node >= 1; --node) tree[node] = min(tree[2 * node], tree[2 * node + 1]);
     }
     __syncthreads();
     const long long sd0 = s_sd0, sd1 = s_sd1;
@@ -876,7 +883,7 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
     long long dnext = lim > 0 ? a.seg_off[doc + 1] : 0;
     uint32_t unres = 0;
 #pragma unroll
-    for (int j = 0; j < PLE_ITEMS; ++j) {
+    for (int j = 0; j < PI; ++j) {
         if (j < lim) {
             const long long g = gfirst + j;
             while (g >= dnext && doc + 1 < a.n_seg) {
@@ -884,15 +891,15 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
                 dbase = a.seg_off[doc];
                 dnext = a.seg_off[doc + 1];
             }
-            const int e = tid * PLE_ITEMS + j;
+            const int e = tid * PI + j;
             int ans = -1;
 #pragma unroll
-            for (int i = 0; i < j; ++i) ans = v[i] <= v[j] ? tid * PLE_ITEMS + i : ans;
+            for (int i = 0; i < j; ++i) ans = v[i] <= v[j] ? tid * PI + i : ans;
             if (brackets) {
-                const uint32_t my_sym = (uint32_t)s_aux[tid * PLE_STRIDE + j];
+                const uint32_t my_sym = (uint32_t)s_aux[tid * (PI + 1) + j];
                 if (!(my_sym >> 31)) {  // rights ask; lefts do not
                     if (ans >= 0) {
-                        const uint32_t l = (uint32_t)s_aux[tid * PLE_STRIDE + (ans - tid * PLE_ITEMS)];
+                        const uint32_t l = (uint32_t)s_aux[tid * (PI + 1) + (ans - tid * PI)];
                         if (base + ans < dbase || (l & 0x7fffffffu) != (my_sym & 0x7fffffffu) || !(l >> 31))
                             a.seg_valid[doc] = 0;
                     } else {
@@ -905,7 +912,7 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
                     if (ans >= 0) r = (int32_t)(base + ans - dbase);
                     else unres |= 1u << j;
                 }
-                s_aux[tid * PLE_STRIDE + j] = r;
+                s_aux[tid * (PI + 1) + j] = r;
                 (void)e;
             }
         }
@@ -916,49 +923,51 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
         const uint32_t cnt = __popc(unres);
         const uint32_t incl = warp_scan_add(cnt, lane);
         const uint32_t total = __shfl_sync(ALP_FULL_MASK, incl, 31);
-        uint16_t* q = s_q + warp * (32 * PLE_ITEMS);
+        uint16_t* q = s_q + warp * (32 * PI);
         uint32_t o = incl - cnt;
-        for (uint32_t m = unres; m; m &= m - 1) q[o++] = (uint16_t)(tid * PLE_ITEMS + __ffs(m) - 1);
+        for (uint32_t m = unres; m; m &= m - 1) q[o++] = (uint16_t)(tid * PI + __ffs(m) - 1);
         __syncwarp();
         for (uint32_t qb = 0; qb < total; qb += 32) {
             if (qb + lane < total) {
                 const int e = q[qb + lane];
-                const int32_t x = s_val[ple_pad(e)];
+                const int32_t x = s_val[ple_pad<PI>(e)];
                 const long long g = base + e;
                 // the nearest earlier chunk with minimum <= x: the few chunks just
                 // before the element's first (most answers are near), then the tree
-                const int ce = e / PLE_ITEMS;
+                const int ce = e / PI;
                 int c = -1;
 #pragma unroll
                 for (int back = 1; back <= 4; ++back)
-                    if (c < 0 && ce - back >= 0 && tree[PLE_THREADS + ce - back] <= x) c = ce - back;
+                    if (c < 0 && ce - back >= 0 && tree[PT + ce - back] <= x) c = ce - back;
                 bool found = c >= 0;
                 if (!found && ce > 4) {
-                    int node = PLE_THREADS + ce - 4;  // chunks left of those
+                    int node = PT + ce - 4;  // chunks left of those
                     while (node > 1) {
                         if ((node & 1) && tree[node - 1] <= x) { node = node - 1; found = true; break; }
                         node >>= 1;
                     }
                     if (found) {
-                        while (node < PLE_THREADS) node = (tree[2 * node + 1] <= x) ? 2 * node + 1 : 2 * node;
-                        c = node - PLE_THREADS;
+                        while (node < PT) node = (tree[2 * node + 1] <= x) ? 2 * node + 1 : 2 * node;
+                        c = node - PT;
                     }
                 }
                 const long long dq = sd0 == sd1 ? sd0 : seg_upper(a.seg_off, sd0, sd1, g);
                 const long long dqb = a.seg_off[dq];
                 if (found) {
-                    const int4 sm = s_sub[c];
-                    const int qq = sm.w <= x ? 3 : (sm.z <= x ? 2 : (sm.y <= x ? 1 : 0));
-                    const int32_t* cv = s_val + c * PLE_STRIDE + 4 * qq;
+                    int qq = 0;
+#pragma unroll
+                    for (int t2 = 1; t2 < NQ; ++t2)
+                        if (s_sub[c * NQ + t2] <= x) qq = t2;
+                    const int32_t* cv = s_val + c * (PI + 1) + 4 * qq;
                     const int k = cv[3] <= x ? 3 : (cv[2] <= x ? 2 : (cv[1] <= x ? 1 : 0));
-                    const int ans = c * PLE_ITEMS + 4 * qq + k;
+                    const int ans = c * PI + 4 * qq + k;
                     if (brackets) {
-                        const uint32_t l = (uint32_t)s_aux[ple_pad(ans)];
-                        const uint32_t r = (uint32_t)s_aux[ple_pad(e)];
+                        const uint32_t l = (uint32_t)s_aux[ple_pad<PI>(ans)];
+                        const uint32_t r = (uint32_t)s_aux[ple_pad<PI>(e)];
                         if (base + ans < dqb || (l & 0x7fffffffu) != (r & 0x7fffffffu) || !(l >> 31))
                             a.seg_valid[dq] = 0;
                     } else {
-                        s_aux[ple_pad(e)] = (int32_t)(base + ans - dqb);
+                        s_aux[ple_pad<PI>(e)] = (int32_t)(base + ans - dqb);
                     }
                 } else {
                     const unsigned int slot = atomicAdd(a.esc_count, 1u);
@@ -972,9 +981,9 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
 
     // ---- node parents, coalesced --------------------------------------------------
     if (!brackets) {
-        for (int e = tid; e < PLE_TILE; e += PLE_THREADS) {
+        for (int e = tid; e < (PT * PI); e += PT) {
             const long long g = base + e;
-            if (g < a.n) a.out_parent[g] = s_aux[ple_pad(e)];
+            if (g < a.n) a.out_parent[g] = s_aux[ple_pad<PI>(e)];
         }
     }
 
@@ -983,7 +992,7 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
     __syncthreads();
     int32_t after;
     {
-        int32_t y = s_suf[PLE_THREADS - 1 - tid];  // reversed order
+        int32_t y = s_suf[PT - 1 - tid];  // reversed order
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
             const int32_t o = __shfl_up_sync(ALP_FULL_MASK, y, d);
@@ -994,14 +1003,14 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
         int32_t pre = INT32_MAX;
         for (int w = 0; w < warp; ++w) pre = min(pre, s_wm[w]);
         y = min(y, pre);
-        s_suf[PLE_THREADS - 1 - tid] = y;  // s_suf[t] = min over threads t..end
+        s_suf[PT - 1 - tid] = y;  // s_suf[t] = min over threads t..end
         __syncthreads();
-        after = tid + 1 < PLE_THREADS ? s_suf[tid + 1] : INT32_MAX;
+        after = tid + 1 < PT ? s_suf[tid + 1] : INT32_MAX;
     }
     uint32_t flags = 0;
     int32_t run = after;
 #pragma unroll
-    for (int i = PLE_ITEMS - 1; i >= 0; --i) {
+    for (int i = PI - 1; i >= 0; --i) {
         if (i < lim && v[i] < run) flags |= 1u << i;
         run = min(run, v[i]);
     }
@@ -1010,14 +1019,14 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
     if (lane == 31) s_cnt[warp] = incl;
     __syncthreads();
     uint32_t wpre = 0, total = 0;
-    for (int w = 0; w < PLE_THREADS / 32; ++w) {
+    for (int w = 0; w < PT / 32; ++w) {
         if (w < warp) wpre += s_cnt[w];
         total += s_cnt[w];
     }
     uint32_t o = wpre + incl - cnt;
-    const long long sbase = (long long)blockIdx.x * PLE_TILE;
+    const long long sbase = (long long)blockIdx.x * (PT * PI);
 #pragma unroll
-    for (int i = 0; i < PLE_ITEMS; ++i) {
+    for (int i = 0; i < PI; ++i) {
         if (flags & (1u << i)) {
             a.stair_val[sbase + o] = v[i];
             a.stair_idx[sbase + o] = (uint32_t)(gfirst + i);
@@ -1032,9 +1041,9 @@ __global__ void __launch_bounds__(PLE_THREADS, 4) ple_tile_kernel(PleArgs a) {
 
 // Level-1/2 minima over groups of 32 / 1024 tiles.
 __global__ void tile_min_levels_kernel(const int32_t* tmin, long long tiles, int32_t* m32, int32_t* m1024,
-                                       const long long* dn) {
+                                       const long long* dn, int tile) {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (dn) tiles = min(tiles, (*dn + PLE_TILE - 1) / PLE_TILE);  // tiles is then the capacity
+    if (dn) tiles = min(tiles, (*dn + tile - 1) / tile);  // tiles is then the capacity
     const long long n32 = (tiles + 31) / 32;
     if (g < n32) {
         int32_t m = INT32_MAX;
@@ -1094,6 +1103,7 @@ struct EscArgs {
     long long n_seg;
     uint8_t* seg_valid;
     AlpResult* res;
+    int tile;                    // elements per tile
 };
 
 __global__ void ple_escape_kernel(EscArgs a) {
@@ -1102,17 +1112,17 @@ __global__ void ple_escape_kernel(EscArgs a) {
         const unsigned long long r = a.esc[e];
         const long long g = (long long)(r >> 32);
         const int32_t x = (int32_t)(uint32_t)r;
-        const long long t = g / PLE_TILE;
+        const long long t = g / a.tile;
         const long long u = prev_tile_leq(a.tile_min, a.m32, a.m1024, t, x);
         long long ans = -1;
         if (u >= 0) {
-            const int32_t* sv = a.stair_val + u * PLE_TILE;
+            const int32_t* sv = a.stair_val + u * a.tile;
             int lo = 0, hi = a.stair_len[u] - 1;  // largest k with sv[k] <= x (values ascend)
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
                 if (sv[mid] <= x) lo = mid; else hi = mid - 1;
             }
-            ans = a.stair_idx[u * PLE_TILE + lo];
+            ans = a.stair_idx[u * a.tile + lo];
         }
         const long long doc = seg_upper(a.seg_off, 0, a.n_seg - 1, g);
         const long long dbase = a.seg_off[doc];

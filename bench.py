@@ -541,6 +541,98 @@ def run_batch(args, rank: int, world: int, local: int):
     print(json.dumps(line), flush=True)
 
 
+def run_graph(args, rank: int, world: int, local: int):
+    """Small batches of json.alp documents through the captured CUDA graph
+    (alp_parse_graph_*), beside alp_parse_batch on the same documents."""
+    import ctypes
+    import torch
+    from alpacc_b200 import api, synth, tables
+    torch.cuda.set_device(local)
+    dist = _dist_init(world)
+    dev = f"cuda:{local}"
+    L = api.native()
+    g = api.Grammar(tables.load("json", "both"), device=local)
+    g._stream()
+    shapes = [(64, 1024), (256, 4096), (2048, 8192)]  # documents, median bytes
+    head = 1  # the shape the line's value is quoted on
+    res = {}
+    for si, (n_docs, med) in enumerate(shapes):
+        seed = SEED_BATCH + 100 + si + 1000 * rank
+        sizes = synth.lognormal_sizes(n_docs, median=med, sigma=1.0, cap=16 * med, seed=seed)
+        data, off = synth.batch("json", sizes, 8, seed)
+        x, o = torch.from_numpy(data).to(dev), torch.from_numpy(off).to(dev)
+        ptrs = [ctypes.c_void_p() for _ in range(7)]
+        N = ctypes.c_int64(0)
+
+        def plain():
+            rc = L.alp_parse_batch(g.h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(o.data_ptr()), n_docs,
+                                   *[ctypes.byref(p) for p in ptrs], ctypes.byref(N))
+            if rc != 0:
+                raise RuntimeError("alp_parse_batch failed rc=%d" % rc)
+
+        want = g.parse_batch_int(x, o)
+        pg = g.parse_batch_graph(x, o)
+        pg.launch()
+        got = pg.result()
+        exact = (len(got[0]) == len(want[0]) and torch.equal(got[1], want[1]) and torch.equal(got[2], want[2]) and
+                 all(torch.equal(getattr(got[0], f), getattr(want[0], f))
+                     for f in ("parent", "tag", "kind", "start", "end")))
+        if not exact:
+            raise RuntimeError("graph replay differs from alp_parse_batch")
+        for _ in range(max(3, args.warmup)):
+            plain()
+            pg.launch()
+        steps = max(args.steps, 20)
+        ms_plain, _ = _timed(plain, steps, local, dist)
+        ms_graph, clocks = _timed(pg.launch, steps, local, dist)
+        pg.result()
+        r = {"docs": n_docs, "bytes": len(data), "nodes": len(want[0]), "graph_ms": ms_graph, "batch_ms": ms_plain,
+             "graph_gbs": _gbs(world, len(data), ms_graph), "batch_gbs": _gbs(world, len(data), ms_plain),
+             "speedup": ms_plain / ms_graph, "bit_exact": True}
+        if si == head:
+            kern = _profiled(g, plain, 3)
+            counts = _ctx_counts(g)
+            # end to end through the graph: pinned input in, the tree out
+            hx = torch.from_numpy(data).pin_memory()
+            nb = len(want[0])
+            hout = [torch.empty(nb * w, dtype=torch.uint8, pin_memory=True) for w in (8, 4, 1, 8, 8)]
+            srcs = [pg.parent, pg.tag, pg.kind, pg.start, pg.end]
+
+            def e2e():
+                pg.x.copy_(hx, non_blocking=True)
+                pg.launch()
+                pg.result()
+                for dst, src in zip(hout, srcs):
+                    dst.copy_(src.view(torch.uint8)[:dst.numel()], non_blocking=True)
+
+            e2e()
+            ms_e2e, _ = _timed(e2e, steps, local, dist)
+            hd = {"x": data, "N": nb, "counts": counts, "ms": ms_graph, "kern": kern, "clocks": clocks,
+                  "e2e": ms_e2e, "h2d": len(data), "d2h": 29 * nb}
+        pg.close()
+        res["%d docs, median %d B" % (n_docs, med)] = r
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    n_bytes = len(hd["x"])
+    cfg = {"workload": "small batches of json.alp documents (depth <= 8, log-normal sizes, sigma 1.0) through "
+                       "one captured CUDA graph per batch shape (alp_parse_graph_launch), beside alp_parse_batch "
+                       "on the same documents; the value is the %d-document batch" % shapes[head][0],
+           "parallelism": "replicas", "l2": "batches fit in L2; every replay re-reads them (no flush)",
+           "shapes": res}
+    alg = n_bytes + 29 * hd["N"]
+    line = _line("input GB/s batched lex+parse, CUDA graph replay (json.alp documents, bit-exact)",
+                 _gbs(world, n_bytes, hd["ms"]), world, args, hd["ms"], cfg, alg, hd["kern"],
+                 {"value": _gbs(world, n_bytes, hd["e2e"]), "unit": "GB/s", "h2d_bytes_per_step": hd["h2d"],
+                  "d2h_bytes_per_step": hd["d2h"], "ms_per_step": hd["e2e"],
+                  "api": "alp_parse_graph_launch + alp_parse_graph_result, pinned host buffers"},
+                 hd["clocks"], units=dict(hd["counts"], n=n_bytes, N=hd["N"]))
+    line["path_roofline"]["scope"] = "one replay: input bytes + 29 B per node, over the replay time"
+    print(json.dumps(line), flush=True)
+
+
 def _wrap_valid(st):
     import torch
     from alpacc_b200 import api
@@ -658,7 +750,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--doc-mib", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="parse", choices=["parse", "lex", "batch", "spec"])
+    ap.add_argument("--workload", default="parse", choices=["parse", "lex", "batch", "spec", "graph"])
     ap.add_argument("--batch-docs", type=int, default=100000, help="JSON documents of the batch workload "
                     "(half as many sexp documents); smaller values are for profiling")
     args = ap.parse_args()
@@ -671,7 +763,8 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.workload != "parse":
-        return {"lex": run_lex, "batch": run_batch, "spec": run_spec}[args.workload](args, rank, world, local)
+        return {"lex": run_lex, "batch": run_batch, "spec": run_spec,
+                "graph": run_graph}[args.workload](args, rank, world, local)
 
     import torch
     from alpacc_b200 import api, tables

@@ -78,6 +78,19 @@ int alp_ctx_timings(alp_ctx* ctx, char* buf, size_t len);
  * after about a second when the bounds work. */
 int alp_check_bounded_wait(alp_ctx* ctx);
 
+/* Autotuning (no reference counterpart).  A context carries launch shapes:
+ * cfg[0] the tile shape of the previous-smaller-or-equal kernel (an index into
+ * the list alp_tune_shapes writes as (threads, elements per thread) pairs),
+ * cfg[1] and cfg[2] the CTAs per SM of the persistent pair and expand kernels
+ * (0: as many as fit).  alp_tune_parse times alp_parse on a sample (the median
+ * of `reps` calls per candidate, CUDA events), one knob at a time, keeps the
+ * fastest setting in the context and writes "knob value ms" lines to
+ * `report`.  Every setting gives the same outputs; only speed differs. */
+int alp_tune_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int reps, char* report, size_t report_len);
+int alp_tune_get(const alp_ctx* ctx, int32_t* cfg, int n);
+int alp_tune_set(alp_ctx* ctx, const int32_t* cfg, int n);
+int alp_tune_shapes(int32_t* out, int n);
+
 /* Copy `bytes` between any two addresses (device or host) on the context's
  * stream and wait for it; lets bindings move context-owned outputs. */
 int alp_memcpy(alp_ctx* ctx, void* dst, const void* src, size_t bytes);
