@@ -2372,7 +2372,7 @@ int alp_parse_graph_create(alp_ctx* ctx, const uint8_t* d_in, int64_t n, const i
 
 int alp_parse_graph_launch(alp_parse_graph* g, void* stream) {
     if (!g) return ALP_ERR_ARG;
-    cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : g->stream;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
     alp_ctx* ctx = g->child;
     CK(cudaSetDevice(ctx->device));
     CK(cudaGraphLaunch(g->exec, s));

@@ -790,6 +790,9 @@ def main():
             raise RuntimeError("alp_parse failed rc=%d valid=%d: %s" % (rc, valid.value,
                                                                        L.alp_last_error(g.h).decode()))
 
+    # launch shapes from the autotuner, timed on this document (outside the timed region)
+    tuning = g.tune(d_in, reps=3)
+    g._stream()
     for _ in range(max(3, args.warmup)):
         step()
     N = n_node.value
@@ -868,7 +871,9 @@ def main():
         "config": {"workload": "json.alp full lex+parse, one %d MiB synthetic JSON document per GPU "
                                "(depth <= %d), bytes -> preorder tree" % (args.doc_mib, DEPTH),
                    "doc_bytes": size, "nodes": N, "nodes_per_byte": N / size, "parallelism": "replicas",
-                   "l2": "inputs larger than L2 (no flush needed)"},
+                   "l2": "inputs larger than L2 (no flush needed)",
+                   "tuning": {"config": tuning["config"], "tile_shape": list(tuning["tile_shape"]),
+                              "candidates_ms": [[k, v, round(t, 4)] for k, v, t in tuning["timings"]]}},
         "roofline": roof,
         "path_roofline": path,
         "e2e": {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": size,

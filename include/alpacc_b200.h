@@ -237,7 +237,8 @@ int alp_parse_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int
  *     nodes, brackets, positions, error bits).  The contents of d_in and d_off
  *     may change between launches (same n and n_docs).  Runs the batch once
  *     uncaptured to size the graph's own scratch, then captures it.
- *   - launch: enqueues one run on `stream` (NULL: the graph's own stream); no wait.
+ *   - launch: enqueues one run on `stream` (a cudaStream_t; NULL: the legacy
+ *     default stream), ordered after the work already on it; no wait.
  *   - result: waits for the last launch; *n_nodes = nodes of the batch;
  *     ALP_ERR_CAPACITY when cap_nodes or cap_brackets was too small (then the
  *     outputs are incomplete and *n_nodes is the count needed).
