@@ -723,7 +723,7 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     a.node_off = (long long*)ctx->tmp[T_NODEOFF].p;
     a.br_off = (long long*)ctx->tmp[T_BROFF].p;
     a.doc_valid = dvalid;
-    const size_t sm1 = sizeof(PairInfo) * ctx->pt.n_pairs + (size_t)(PP_TILE + ctx->pt.q + ctx->pt.k) * 4;
+    const size_t sm1 = pairs_smem_bytes(ctx->pt.n_pairs, ctx->pt.q + ctx->pt.k);
     CK(cudaFuncSetAttribute(parse_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
     mark(ctx, "start");
     unsigned g_pairs = 1, g_expand = 1;
@@ -1166,7 +1166,7 @@ int alp_tune_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int reps, char*
     // one knob at a time, the others held at their best so far
     int fit_pairs = 1, fit_expand = 1;
     {
-        const size_t sm1 = sizeof(PairInfo) * ctx->pt.n_pairs + (size_t)(PP_TILE + ctx->pt.q + ctx->pt.k) * 4;
+        const size_t sm1 = pairs_smem_bytes(ctx->pt.n_pairs, ctx->pt.q + ctx->pt.k);
         const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
         CK(cudaFuncSetAttribute(parse_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
         CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
@@ -2205,7 +2205,7 @@ int parse_positions_dev(alp_ctx* ctx, long long Lcap, const long long* dL, long 
     a.cap_brs = cap_brs;
     int sms = 0, per1 = 0, per2 = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    const size_t sm1 = sizeof(PairInfo) * ctx->pt.n_pairs + (size_t)(PP_TILE + ctx->pt.q + ctx->pt.k) * 4;
+    const size_t sm1 = pairs_smem_bytes(ctx->pt.n_pairs, ctx->pt.q + ctx->pt.k);
     const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
     if (sm2 > 220 * 1024) return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
     CK(cudaFuncSetAttribute(parse_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));

@@ -324,6 +324,11 @@ __device__ __forceinline__ uint32_t pos_term(const ParseArgs& a, long long i) {
 // ---------------------------------------------------------------------------
 // K1: pair ids and per-tile (segmented) sums
 // ---------------------------------------------------------------------------
+// The pair kernel's shared memory: the pair infos, then the window of terminals.
+__host__ __device__ inline size_t pairs_smem_bytes(int n_pairs, int window) {
+    return sizeof(PairInfo) * (size_t)n_pairs + ((size_t)PP_TILE + window) * 4;
+}
+
 __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     PairInfo* s_pi = reinterpret_cast<PairInfo*>(smem);
@@ -526,7 +531,11 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
 constexpr int EX_WIN = 8192;                     // nodes or brackets per window
 constexpr int EX_U = 2;                          // nodes a thread emits at once (token span loads in flight)
 constexpr uint32_t EX_NO_TOKEN = 0xffffffffu;
-constexpr size_t EX_POS_BYTES = (size_t)PP_TILE * 20;  // per position: a node record and a bracket base
+// per position: a node record and a bracket base, one unused slot after every
+// thread's four positions, so that the 32 lanes of a warp writing their first
+// position (64 bytes apart without the pad) hit distinct banks
+constexpr size_t EX_POS_BYTES = (size_t)PP_TILE * 5 / 4 * 20;
+__device__ __forceinline__ int ex_slot(int pl) { return pl + (pl >> 2); }
 
 // pair infos (20 bytes each), then the 8-byte records from a 16-byte boundary
 __host__ __device__ inline size_t expand_rec_off(int n_pairs) {
@@ -568,8 +577,8 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     // node, so that node g reads record g + x; y = exscan(arity - 1) before it;
     // z = token index of its first terminal production; w = bracket depth before it
     int4* s_pos = reinterpret_cast<int4*>(smem + expand_tables_bytes(a.t.n_pairs, a.t.n_pseq, a.t.n_stack));
-    int32_t* s_sbd = reinterpret_cast<int32_t*>(s_pos + PP_TILE);  // first stack record minus first bracket
-    uint16_t* s_own = reinterpret_cast<uint16_t*>(s_sbd + PP_TILE);  // [EX_WIN] owner of each node / bracket
+    int32_t* s_sbd = reinterpret_cast<int32_t*>(s_pos + PP_TILE * 5 / 4);  // first stack record minus first bracket
+    uint16_t* s_own = reinterpret_cast<uint16_t*>(s_sbd + PP_TILE * 5 / 4);  // [EX_WIN] owner of each node / bracket
     __shared__ PosSums s_w[PP_THREADS / 32];
     __shared__ uint32_t s_tn, s_tb;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -649,10 +658,10 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                         if (dok) a.doc_valid[doc] = 0;  // no admissible pair
                     } else {
                         const PairInfo pi = s_pi[ids[j]];
-                        s_pos[pl] = make_int4((int32_t)pi.prod_begin - (int32_t)nof[j], head ? 0 : run.v,
+                        s_pos[ex_slot(pl)] = make_int4((int32_t)pi.prod_begin - (int32_t)nof[j], head ? 0 : run.v,
                                               (int32_t)((uint32_t)(head ? i : run.hpos) + 1u + (head ? 0u : run.terms)),
                                               dep);
-                        s_sbd[pl] = (int32_t)pi.stack_begin - (int32_t)bof[j];
+                        s_sbd[ex_slot(pl)] = (int32_t)pi.stack_begin - (int32_t)bof[j];
                         if (dep + (int32_t)pi.min_ds < 0 && dok) a.doc_valid[doc] = 0;  // depth below zero
                         e.nodes = pi.n_prod; e.brs = pi.n_br; e.depth = pi.d_depth; e.v = pi.d_v; e.terms = pi.n_term;
                         cnt[j] = (uint32_t)pi.n_prod | ((uint32_t)pi.n_br << 16);
@@ -684,7 +693,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                     tg[u] = 0; kd[u] = 0; vv[u] = 0; st[u] = 0; en[u] = 0; gi[u] = 0xffffffffu;
                     if (e < wn) {
                         const uint32_t g = w0 + e;
-                        const int4 ps = s_pos[s_own[e]];
+                        const int4 ps = s_pos[ex_slot(s_own[e])];
                         const uint2 rec = s_prec[(int32_t)g + ps.x];
                         const uint32_t tm1 = rec.x >> 16;  // terminal + 1, 0: not a terminal production
                         vv[u] = ps.y + (int32_t)(int16_t)(rec.y & 0xffffu);
@@ -726,8 +735,8 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             for (uint32_t e = tid; e < wn; e += PP_THREADS) {
                 const uint32_t g = w0 + e;
                 const int pl = s_own[e];
-                const uint2 rec = s_srec[(int32_t)g + s_sbd[pl]];
-                const int32_t before = s_pos[pl].w + (int32_t)(int16_t)(rec.y & 0xffffu);
+                const uint2 rec = s_srec[(int32_t)g + s_sbd[ex_slot(pl)]];
+                const int32_t before = s_pos[ex_slot(pl)].w + (int32_t)(int16_t)(rec.y & 0xffffu);
                 const uint32_t bg = tp.brs + g;
                 if ((long long)bg < a.cap_brs) {
                     a.brbuf[bg] = rec.x;
