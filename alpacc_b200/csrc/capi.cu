@@ -536,22 +536,31 @@ int lex3_prepare(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long
     return ALP_OK;
 }
 
-// chunk endomorphisms -> chunk states -> chunk counts and tile counts
-int lex3_front(alp_ctx* ctx, Lex3Run& r) {
-    unsigned g1, g2, g3;
+// chunk endomorphisms
+int lex3_fold(alp_ctx* ctx, Lex3Run& r) {
+    unsigned g1;
     int rc;
     CK(cudaFuncSetAttribute(lex3_fold_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_fold_smem));
     CK(cudaFuncSetAttribute(lex3_fold_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    CK(cudaFuncSetAttribute(lex3_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_scan_smem));
-    CK(cudaFuncSetAttribute(lex3_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_count_smem));
-    if ((rc = lex3_grid(ctx, r, (const void*)lex3_fold_kernel, LX_THREADS, ctx->l3_fold_smem, r.wide, &g1)) ||
-        (rc = lex3_grid(ctx, r, (const void*)lex3_scan_kernel, LS_WARPS * 32, ctx->l3_scan_smem, r.stiles, &g2)) ||
-        (rc = lex3_grid(ctx, r, (const void*)lex3_count_kernel, LX_THREADS, ctx->l3_count_smem, r.wide, &g3)))
-        return rc;
+    if ((rc = lex3_grid(ctx, r, (const void*)lex3_fold_kernel, LX_THREADS, ctx->l3_fold_smem, r.wide, &g1))) return rc;
     mark(ctx, "start");
     lex3_fold_kernel<<<g1, LX_THREADS, ctx->l3_fold_smem, ctx->stream>>>(r.a, r.sg);
     CK(cudaGetLastError());
     mark(ctx, "lex3_fold_kernel");
+    return ALP_OK;
+}
+
+// chunk endomorphisms -> chunk states -> chunk counts and tile counts
+int lex3_front(alp_ctx* ctx, Lex3Run& r, bool folded = false) {
+    unsigned g2, g3;
+    int rc;
+    if (!folded && (rc = lex3_fold(ctx, r))) return rc;
+    CK(cudaFuncSetAttribute(lex3_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_scan_smem));
+    CK(cudaFuncSetAttribute(lex3_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_count_smem));
+    if ((rc = lex3_grid(ctx, r, (const void*)lex3_scan_kernel, LS_WARPS * 32, ctx->l3_scan_smem, r.stiles, &g2)) ||
+        (rc = lex3_grid(ctx, r, (const void*)lex3_count_kernel, LX_THREADS, ctx->l3_count_smem, r.wide, &g3)))
+        return rc;
+    mark(ctx, "start");
     lex3_scan_kernel<<<g2, LS_WARPS * 32, ctx->l3_scan_smem, ctx->stream>>>(r.a);
     CK(cudaGetLastError());
     mark(ctx, "lex3_scan_kernel");
@@ -562,8 +571,19 @@ int lex3_front(alp_ctx* ctx, Lex3Run& r) {
 }
 
 // tile scan of the counts -> token pass (stream-ordered, no wait)
+// exclusive (count, last start) over the tiles
+int lex3_tiles(alp_ctx* ctx, Lex3Run& r) {
+    const long long lchunks = (r.tiles + LT_CHUNK - 1) / LT_CHUNK;
+    unsigned long long* ccs = reinterpret_cast<unsigned long long*>(r.base + r.o_ccs);
+    lex3_tile_reduce_kernel<<<(unsigned)lchunks, LT_CHUNK, 0, ctx->stream>>>(r.a.tile_cs, r.tiles, ccs);
+    CK(cudaGetLastError());
+    lex3_tile_scan_kernel<<<(unsigned)lchunks, LT_CHUNK, 0, ctx->stream>>>(r.a.tile_cs, r.tiles, ccs);
+    CK(cudaGetLastError());
+    return ALP_OK;
+}
+
 template <typename TermT, typename PosT>
-int lex3_emit(alp_ctx* ctx, Lex3Run& r) {
+int lex3_emit(alp_ctx* ctx, Lex3Run& r, bool tiles_done = false) {
     auto k5 = lex3_emit_kernel<TermT, PosT>;
     unsigned g5;
     int rc;
@@ -571,14 +591,7 @@ int lex3_emit(alp_ctx* ctx, Lex3Run& r) {
     CK(cudaFuncSetAttribute(k5, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     if ((rc = lex3_grid(ctx, r, (const void*)k5, LX_THREADS, ctx->l3_emit_smem, r.tiles, &g5))) return rc;
     mark(ctx, "start");
-    {
-        const long long lchunks = (r.tiles + LT_CHUNK - 1) / LT_CHUNK;
-        unsigned long long* ccs = reinterpret_cast<unsigned long long*>(r.base + r.o_ccs);
-        lex3_tile_reduce_kernel<<<(unsigned)lchunks, LT_CHUNK, 0, ctx->stream>>>(r.a.tile_cs, r.tiles, ccs);
-        CK(cudaGetLastError());
-        lex3_tile_scan_kernel<<<(unsigned)lchunks, LT_CHUNK, 0, ctx->stream>>>(r.a.tile_cs, r.tiles, ccs);
-        CK(cudaGetLastError());
-    }
+    if (!tiles_done && (rc = lex3_tiles(ctx, r))) return rc;
     mark(ctx, "lex3_tile_reduce+lex3_tile_scan");
     k5<<<g5, LX_THREADS, ctx->l3_emit_smem, ctx->stream>>>(r.a, r.sg);
     CK(cudaGetLastError());
@@ -1618,6 +1631,155 @@ int alp_lex_host_stream(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t pi
 }
 
 
+
+// ---- shards: one document lexed by several GPUs ---------------------------------
+// Each GPU holds one byte range.  begin: the range's state function (32 bytes);
+// the ranks exchange functions and compose the prefix to get each range's
+// entry state; count: the range's token count and last token start from that
+// state; the ranks exchange those to get each range's first token index and
+// carried token start; emit: the range's tokens with document positions.
+struct alp_lex_shard {
+    alp_ctx* ctx = nullptr;
+    const uint8_t* d_in = nullptr;
+    long long n = 0, pos = 0;
+    int last = 0;
+    int stage = 0;                 // 1 after begin, 2 after count, 3 after emit
+    LexCarry* d_carry = nullptr;   // device: carry in, [2] totals
+    long long* d_tot = nullptr;
+    uint8_t* d_fn = nullptr;       // [blocks + 1][32]
+    uint8_t* d_valid = nullptr;
+    long long* h = nullptr;        // pinned staging
+    Lex3Run r;
+};
+
+static int shard_prepare(alp_lex_shard* s) {
+    alp_ctx* ctx = s->ctx;
+    int rc;
+    if ((rc = grow(ctx, ctx->tmp[T_TOKOFF], 64))) return rc;
+    if ((rc = lex3_prepare(ctx, s->d_in, s->n, nullptr, 1, 0, nullptr, nullptr, nullptr, 0, s->d_valid, s->r)))
+        return rc;
+    s->r.sg.cont = 1;
+    s->r.sg.end1 = s->last ? s->n : s->n + 1;  // only the last range ends the document
+    s->r.a.carry = s->d_carry;
+    s->r.a.pos_base = s->pos;
+    s->r.a.carry_tokens = 1;
+    s->r.a.tok_first = 0;
+    return ALP_OK;
+}
+
+int alp_lex_shard_begin(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t pos, int is_last, uint8_t* h_fn,
+                        alp_lex_shard** out) {
+    int rc;
+    if ((rc = stream_ok(ctx))) return rc;
+    if (!out || !h_fn || pos < 0) return fail(ctx, ALP_ERR_ARG, "bad argument");
+    *out = nullptr;
+    if ((rc = check_in(ctx, d_in, n, true))) return rc;
+    if (n < 1) return fail(ctx, ALP_ERR_ARG, "a shard holds at least one byte");
+    CK(cudaSetDevice(ctx->device));
+    alp_lex_shard* s = new alp_lex_shard();
+    s->ctx = ctx;
+    s->d_in = d_in;
+    s->n = n;
+    s->pos = pos;
+    s->last = is_last ? 1 : 0;
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    const int blocks = sms;
+    cudaError_t e = cudaMalloc(&s->d_carry, sizeof(LexCarry) + 64);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_fn, (size_t)(blocks + 1) * 32 + 64);
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h, 64);
+    if (e != cudaSuccess) {
+        alp_lex_shard_free(s);
+        return fail(ctx, ALP_ERR_CUDA, "shard set-up: %s", cudaGetErrorString(e));
+    }
+    s->d_tot = reinterpret_cast<long long*>(reinterpret_cast<uint8_t*>(s->d_carry) + sizeof(LexCarry));
+    s->d_valid = reinterpret_cast<uint8_t*>(s->d_tot + 4);
+    if ((rc = shard_prepare(s))) { alp_lex_shard_free(s); return rc; }
+    if ((rc = lex3_fold(ctx, s->r))) { alp_lex_shard_free(s); return rc; }
+    const int rows = ctx->E + ctx->S;
+    const size_t fsm = (size_t)rows * 32;
+    CK(cudaFuncSetAttribute(lex3_fn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+    lex3_fn_kernel<<<blocks, LF_WARPS * 32, fsm, ctx->stream>>>(s->r.a.chunk_f, s->r.chunks, ctx->l3.app8, rows,
+                                                                 s->d_fn);
+    CK(cudaGetLastError());
+    lex3_fn_final_kernel<<<1, 32, 0, ctx->stream>>>(s->d_fn, blocks, s->d_fn + (size_t)blocks * 32);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(s->h, s->d_fn + (size_t)blocks * 32, 32, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    memcpy(h_fn, s->h, 32);
+    s->stage = 1;
+    *out = s;
+    return ALP_OK;
+}
+
+int alp_lex_shard_count(alp_lex_shard* s, uint32_t entry_state, int64_t* n_tok, int64_t* last_start) {
+    if (!s || !n_tok || !last_start) return ALP_ERR_ARG;
+    alp_ctx* ctx = s->ctx;
+    if (s->stage != 1) return fail(ctx, ALP_ERR_ARG, "count follows begin, once");
+    if (entry_state >= (uint32_t)ctx->S) return fail(ctx, ALP_ERR_ARG, "entry state out of range");
+    CK(cudaSetDevice(ctx->device));
+    LexCarry c{};
+    c.state = entry_state;
+    memcpy(s->h, &c, sizeof c);
+    CK(cudaMemcpyAsync(s->d_carry, s->h, sizeof c, cudaMemcpyHostToDevice, ctx->stream));
+    int rc;
+    if ((rc = lex3_front(ctx, s->r, true)) || (rc = lex3_tiles(ctx, s->r))) return rc;
+    lex3_shard_totals_kernel<<<1, LX_THREADS, 0, ctx->stream>>>(s->r.a, s->d_tot);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(s->h, s->d_tot, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(s->h + 2, &s->r.a.res->error, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if ((unsigned int)s->h[2] & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
+    *n_tok = s->h[0];
+    *last_start = s->h[1] < 0 ? -1 : s->pos + s->h[1];
+    s->stage = 2;
+    return ALP_OK;
+}
+
+int alp_lex_shard_emit(alp_lex_shard* s, int64_t carried_start, uint32_t* d_term, int64_t* d_start, int64_t* d_end,
+                       int64_t cap, int64_t* n_tok, int* valid) {
+    if (!s || !n_tok || !valid) return ALP_ERR_ARG;
+    alp_ctx* ctx = s->ctx;
+    if (s->stage != 2) return fail(ctx, ALP_ERR_ARG, "emit follows count, once");
+    if (cap < 0 || (cap > 0 && (!d_term || !d_start || !d_end)) || carried_start < 0)
+        return fail(ctx, ALP_ERR_ARG, "bad argument");
+    CK(cudaSetDevice(ctx->device));
+    // the carry's state stays (the scan already used it); tokens from 0, the carried start
+    LexCarry c{};
+    CK(cudaMemcpyAsync(&c, s->d_carry, sizeof c, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    c.start = carried_start;
+    c.tokens = 0;
+    memcpy(s->h, &c, sizeof c);
+    CK(cudaMemcpyAsync(s->d_carry, s->h, sizeof c, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(s->d_valid, 0, 1, ctx->stream));
+    s->r.a.out_term = d_term;
+    s->r.a.out_start = d_start;
+    s->r.a.out_end = d_end;
+    s->r.a.cap = cap;
+    int rc;
+    if ((rc = lex3_emit<uint32_t, int64_t>(ctx, s->r, true))) return rc;
+    CK(cudaMemcpyAsync(ctx->h_res, s->r.a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
+    uint8_t v = 0;
+    CK(cudaMemcpyAsync(s->h, s->d_valid, 1, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    v = *reinterpret_cast<uint8_t*>(s->h);
+    s->stage = 3;
+    if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
+    *n_tok = ctx->h_res->count;
+    *valid = s->last ? (int)v : 1;
+    if (ctx->h_res->error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
+    return ALP_OK;
+}
+
+void alp_lex_shard_free(alp_lex_shard* s) {
+    if (!s) return;
+    if (s->ctx) cudaSetDevice(s->ctx->device);
+    if (s->d_carry) cudaFree(s->d_carry);
+    if (s->d_fn) cudaFree(s->d_fn);
+    if (s->h) cudaFreeHost(s->h);
+    delete s;
+}
 
 int alp_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t** d_parent, uint32_t** d_tag, uint8_t** d_kind,
               int64_t** d_start, int64_t** d_end, int64_t* n_node, int* valid) {

@@ -849,4 +849,79 @@ __global__ void lex3_stream_end_kernel(LexCarry* c, const uint32_t* tokinfo, lon
     c->valid = (ti & TOK_ACCEPT) ? 1 : 0;
 }
 
+// ---- shards: one byte range of a document lexed on one GPU of several --------
+// The state function of a shard: lane s of the result holds the state after
+// the shard's bytes from entry state s.  Each block composes a contiguous run
+// of chunk endomorphisms (lane-per-state walks through the apply table, one
+// warp per sub-run, then the warps in order); lex3_fn_final_kernel composes
+// the blocks in order.
+constexpr int LF_WARPS = 8;
+__global__ void __launch_bounds__(LF_WARPS * 32) lex3_fn_kernel(const uint16_t* chunk_f, long long C,
+                                                                const uint8_t* app8, int rows, uint8_t* fn) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint8_t s_w[LF_WARPS][32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(app8);
+        uint4* dst = reinterpret_cast<uint4*>(smem);
+        for (int i = tid; i < rows * 2; i += LF_WARPS * 32) dst[i] = src[i];
+    }
+    __syncthreads();
+    const long long per_block = (C + gridDim.x - 1) / gridDim.x;
+    const long long b0 = (long long)blockIdx.x * per_block, b1 = min(C, b0 + per_block);
+    const long long per_warp = (b1 - b0 + LF_WARPS - 1) / LF_WARPS;
+    const long long w0 = b0 + (long long)warp * per_warp, w1 = min(b1, w0 + per_warp);
+    uint32_t cur = (uint32_t)lane;
+    for (long long c = w0; c < w1; ++c) cur = smem[(uint32_t)chunk_f[c] * 32 + cur];
+    s_w[warp][lane] = (uint8_t)cur;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t x = (uint32_t)lane;
+        for (int w = 0; w < LF_WARPS; ++w) x = s_w[w][x];
+        fn[(size_t)blockIdx.x * 32 + lane] = (uint8_t)x;
+    }
+}
+
+__global__ void lex3_fn_final_kernel(const uint8_t* fn, int blocks, uint8_t* out) {
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x >= 32) return;
+    uint32_t x = (uint32_t)lane;
+    for (int b = 0; b < blocks; ++b) x = fn[(size_t)b * 32 + x];
+    out[lane] = (uint8_t)x;
+}
+
+// After the tile scan of a shard's counts: out[0] = tokens that end in the
+// shard, out[1] = position (shard-relative) of its last token start, -1 if none.
+__global__ void __launch_bounds__(LX_THREADS) lex3_shard_totals_kernel(Lex3Args a, long long* out) {
+    __shared__ long long s_best[LX_THREADS / 32];
+    __shared__ unsigned long long s_cnt[LX_THREADS / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long C = a.n_chunks, T = a.num_tiles;
+    long long best = -1;
+    unsigned long long cnt = 0;
+    for (long long c = (T - 1) * (LX_TILE / LX_CHUNK) + tid; c < C; c += LX_THREADS) {
+        const uint32_t cc = a.chunk_c[c];
+        cnt += cc & 0xffu;
+        if ((cc >> 8) != LX_NOOFF) best = max(best, c * LX_CHUNK + (long long)(cc >> 8));
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+        best = max(best, (long long)__shfl_xor_sync(ALP_FULL_MASK, best, d));
+        cnt += __shfl_xor_sync(ALP_FULL_MASK, cnt, d);
+    }
+    if (lane == 0) { s_best[warp] = best; s_cnt[warp] = cnt; }
+    __syncthreads();
+    if (tid == 0) {
+        cnt = 0;
+        for (int w = 0; w < LX_THREADS / 32; ++w) {
+            best = max(best, s_best[w]);
+            cnt += s_cnt[w];
+        }
+        const unsigned long long X = a.tile_cs[T - 1];  // exclusive: before the last tile
+        if (best < 0 && (uint32_t)X != ALP_NONE32) best = (uint32_t)X;
+        out[0] = (long long)(X >> 32) + (long long)cnt;
+        out[1] = best;
+    }
+}
+
 }  // namespace alp

@@ -155,6 +155,31 @@ int alp_lex_stream_window(alp_lex_stream* s, uint32_t* d_term, int64_t* d_start,
                           int64_t first);
 void alp_lex_stream_free(alp_lex_stream* s);
 
+/* One document lexed by several GPUs (no reference counterpart: the
+ * reference's chunk loop runs its chunks one after another).  Each GPU holds
+ * one byte range; the ranks exchange two small records (by any collective)
+ * and each writes the tokens that end in its range, with document positions.
+ * The union over the ranges equals alp_lex on the whole document.
+ *   - begin: `pos` = the range's first byte in the document, is_last for the
+ *     range that ends it; writes the range's state function to h_fn[32]
+ *     (h_fn[s] = state after the range from entry state s).  Entry state of
+ *     range r: start from 1 (the initial state) and apply h_fn of ranges
+ *     0 .. r-1 in order.
+ *   - count: from that entry state, *n_tok = tokens that end in the range and
+ *     *last_start = document position of its last token start (-1: none).
+ *     Range r's first token index is the sum of n_tok over ranges before it;
+ *     its carried start is the last last_start >= 0 among them, else 0.
+ *   - emit: writes the range's *n_tok tokens (token k of the range at element
+ *     k); on the last range *valid as alp_lex (1 elsewhere).
+ * Needs a DFA of at most 32 states.  One shard per context at a time. */
+typedef struct alp_lex_shard alp_lex_shard;
+int alp_lex_shard_begin(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t pos, int is_last, uint8_t* h_fn,
+                        alp_lex_shard** out);
+int alp_lex_shard_count(alp_lex_shard* s, uint32_t entry_state, int64_t* n_tok, int64_t* last_start);
+int alp_lex_shard_emit(alp_lex_shard* s, int64_t carried_start, uint32_t* d_term, int64_t* d_start,
+                       int64_t* d_end, int64_t cap, int64_t* n_tok, int* valid);
+void alp_lex_shard_free(alp_lex_shard* s);
+
 /* alp_lex_host over a stream of `piece`-byte pieces (0: 16 MiB): the copy of
  * one piece in, the lexing of the one before and the copy of the tokens of the
  * one before that out overlap on three CUDA streams.  Same results as
