@@ -1684,7 +1684,7 @@ int alp_lex_shard_begin(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t po
     s->last = is_last ? 1 : 0;
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    const int blocks = sms;
+    const int blocks = sms * 16;  // short sequential runs per warp; the final kernel composes the blocks
     cudaError_t e = cudaMalloc(&s->d_carry, sizeof(LexCarry) + 64);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_fn, (size_t)(blocks + 1) * 32 + 64);
     if (e == cudaSuccess) e = cudaMallocHost(&s->h, 64);
@@ -1702,8 +1702,9 @@ int alp_lex_shard_begin(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t po
     lex3_fn_kernel<<<blocks, LF_WARPS * 32, fsm, ctx->stream>>>(s->r.a.chunk_f, s->r.chunks, ctx->l3.app8, rows,
                                                                  s->d_fn);
     CK(cudaGetLastError());
-    lex3_fn_final_kernel<<<1, 32, 0, ctx->stream>>>(s->d_fn, blocks, s->d_fn + (size_t)blocks * 32);
+    lex3_fn_final_kernel<<<1, 1024, 0, ctx->stream>>>(s->d_fn, blocks, s->d_fn + (size_t)blocks * 32);
     CK(cudaGetLastError());
+    mark(ctx, "lex3_fn_kernel+lex3_fn_final_kernel");
     CK(cudaMemcpyAsync(s->h, s->d_fn + (size_t)blocks * 32, 32, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     memcpy(h_fn, s->h, 32);
@@ -1726,6 +1727,7 @@ int alp_lex_shard_count(alp_lex_shard* s, uint32_t entry_state, int64_t* n_tok, 
     if ((rc = lex3_front(ctx, s->r, true)) || (rc = lex3_tiles(ctx, s->r))) return rc;
     lex3_shard_totals_kernel<<<1, LX_THREADS, 0, ctx->stream>>>(s->r.a, s->d_tot);
     CK(cudaGetLastError());
+    mark(ctx, "lex3_tile_reduce+lex3_tile_scan+lex3_shard_totals_kernel");
     CK(cudaMemcpyAsync(s->h, s->d_tot, 16, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(s->h + 2, &s->r.a.res->error, 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));

@@ -882,12 +882,22 @@ __global__ void __launch_bounds__(LF_WARPS * 32) lex3_fn_kernel(const uint16_t* 
     }
 }
 
-__global__ void lex3_fn_final_kernel(const uint8_t* fn, int blocks, uint8_t* out) {
-    const int lane = threadIdx.x & 31;
-    if (threadIdx.x >= 32) return;
+// 32 warps: warp w composes a contiguous run of the block functions, then
+// warp 0 composes the 32 runs in order.
+__global__ void __launch_bounds__(1024) lex3_fn_final_kernel(const uint8_t* fn, int blocks, uint8_t* out) {
+    __shared__ uint8_t s_w[32][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int per = (blocks + 31) / 32;
+    const int b0 = warp * per, b1 = min(blocks, b0 + per);
     uint32_t x = (uint32_t)lane;
-    for (int b = 0; b < blocks; ++b) x = fn[(size_t)b * 32 + x];
-    out[lane] = (uint8_t)x;
+    for (int b = b0; b < b1; ++b) x = fn[(size_t)b * 32 + x];
+    s_w[warp][lane] = (uint8_t)x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t y = (uint32_t)lane;
+        for (int w = 0; w < 32; ++w) y = s_w[w][y];
+        out[lane] = (uint8_t)y;
+    }
 }
 
 // After the tile scan of a shard's counts: out[0] = tokens that end in the

@@ -633,6 +633,66 @@ def run_graph(args, rank: int, world: int, local: int):
     print(json.dumps(line), flush=True)
 
 
+def run_shard(args, rank: int, world: int, local: int):
+    """One 512 MiB json.alp document lexed by all ranks together: rank r holds
+    the r-th byte range; two all-gathers of a few bytes per rank (state
+    functions, then token counts and last starts) place every range's tokens.
+    Strong scaling: the document is the same for every N."""
+    import torch
+    from alpacc_b200 import api, shard, synth, tables
+    torch.cuda.set_device(local)
+    dist = _dist_init(world)
+    size = (args.doc_mib << 20) if args.doc_mib_given else 512 << 20
+    doc = synth.json_doc(size, 8, SEED_LEX)
+    a, b = size * rank // world, size * (rank + 1) // world
+    g = api.Grammar(tables.load("json", "lexer"), device=local)
+    x = torch.from_numpy(doc[a:b]).to(f"cuda:{local}")
+    g._stream()
+
+    def gather(obj):
+        if not dist:
+            return [obj]
+        out = [None] * world
+        dist.all_gather_object(out, obj)
+        return out
+
+    res = {}
+
+    def step():
+        res["t"] = shard.lex_shard(g, x, a, rank == world - 1, rank, gather)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    ms, clocks = _timed(step, args.steps, local, dist)
+    kern = _profiled(g, step, 3)
+    toks, base, valid = res["t"]
+    n_local = int(toks[0].numel())
+    total = gather(n_local)
+    if world == 1:
+        whole = g.lex_int(x)
+        if whole is None or not all(torch.equal(u.to(v.dtype), v) for u, v in zip(toks, whole)):
+            raise RuntimeError("sharded lexing differs from alp_lex")
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    M = int(sum(total))
+    cfg = {"workload": "json.alp lexer, one %d MiB synthetic document (depth <= 8) split into %d contiguous byte "
+                       "ranges, one per GPU; two all-gathers per step (state functions; token counts and last "
+                       "starts)" % (size >> 20, world),
+           "doc_bytes": size, "tokens": M, "parallelism": "byte ranges of one document",
+           "l2": "inputs larger than L2 (no flush needed)"}
+    line = _line("input GB/s lex of one document across GPUs (json.alp lexer-only, bit-exact)",
+                 size / (ms * 1e-3) / 1e9, world, args, ms, cfg, size + 20 * M, kern,
+                 {"value": None, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                  "note": "device-resident ranges; see the lex workload for host buffers"}, clocks,
+                 units={"n": b - a, "m": n_local}, parse_layout=False)
+    line["scaling"] = "strong"
+    line["path_roofline"]["scope"] = "whole job: document bytes + 20 B per token over the step time, all GPUs"
+    print(json.dumps(line), flush=True)
+
+
 def _wrap_valid(st):
     import torch
     from alpacc_b200 import api
@@ -750,7 +810,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--doc-mib", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="parse", choices=["parse", "lex", "batch", "spec", "graph"])
+    ap.add_argument("--workload", default="parse", choices=["parse", "lex", "batch", "spec", "graph", "shard"])
     ap.add_argument("--batch-docs", type=int, default=100000, help="JSON documents of the batch workload "
                     "(half as many sexp documents); smaller values are for profiling")
     args = ap.parse_args()
@@ -764,7 +824,7 @@ def main():
         return run_reference(args, rank, world)
     if args.workload != "parse":
         return {"lex": run_lex, "batch": run_batch, "spec": run_spec,
-                "graph": run_graph}[args.workload](args, rank, world, local)
+                "graph": run_graph, "shard": run_shard}[args.workload](args, rank, world, local)
 
     import torch
     from alpacc_b200 import api, tables
