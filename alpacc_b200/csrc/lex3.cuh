@@ -36,7 +36,7 @@ constexpr int LX_THREADS = 256;
 constexpr int LX_CHUNK = 32;                    // bytes per chunk, the unit of the state scan
 constexpr int LX_TILE = LX_THREADS * LX_CHUNK;  // 8 KiB emit tile: one chunk per thread
 constexpr int LX_WIDE = 2 * LX_TILE;            // 16 KiB fold / count tile: two chunks per thread
-constexpr int LX_STAGE = 4096;                  // tokens one emit tile stages in shared memory
+constexpr int LX_STAGE = 2048;                  // tokens one emit tile stages in shared memory
 constexpr int LS_WARPS = 8;
 constexpr int LS_G = 16;                        // chunks per lane in the state scan
 constexpr int LS_TILE = LS_WARPS * 32 * LS_G;   // 4096 chunks per state-scan tile
@@ -404,7 +404,7 @@ __device__ __forceinline__ void cs_reduce_warp(uint32_t& c, uint32_t& p) {
     }
 }
 
-__global__ void __launch_bounds__(LX_THREADS, 4) lex3_count_kernel(Lex3Args a, LexSeg sg) {
+__global__ void __launch_bounds__(LX_THREADS, 6) lex3_count_kernel(Lex3Args a, LexSeg sg) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int S = a.t.S;
     uint16_t* s_ent = reinterpret_cast<uint16_t*>(smem);
@@ -563,7 +563,7 @@ __global__ void __launch_bounds__(LT_CHUNK) lex3_tile_scan_kernel(unsigned long 
 
 // ---- kernel 5: tokens ---------------------------------------------------------
 template <typename TermT, typename PosT>
-__global__ void __launch_bounds__(LX_THREADS, 4) lex3_emit_kernel(Lex3Args a, LexSeg sg) {
+__global__ void __launch_bounds__(LX_THREADS, 6) lex3_emit_kernel(Lex3Args a, LexSeg sg) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int S = a.t.S;
     uint16_t* s_ent = reinterpret_cast<uint16_t*>(smem);
