@@ -233,7 +233,7 @@ int load_lexer(alp_ctx* ctx, Reader& r) {
     bool small = S <= 32 && E + S <= 65535 && lex3_fold_smem(S, C1, E) <= 200 * 1024 &&
                  lex3_scan_smem(S, E) <= 160 * 1024 && lex3_emit_smem(S) <= 200 * 1024;
     for (int s = 0; s < S && small; ++s)
-        if ((ctx->h_tokinfo[s] & TOK_TERM_MASK) > 0xffffu) small = false;
+        if ((ctx->h_tokinfo[s] & TOK_TERM_MASK) >= (1u << (16 - LX_TERM_SHIFT))) small = false;
     if (small) {
         std::vector<uint8_t> app8(((size_t)E + S) * 32);
         for (int e = 0; e < E; ++e)
@@ -247,7 +247,8 @@ int load_lexer(alp_ctx* ctx, Reader& r) {
                 const uint32_t nx = e & 0x7fffu;
                 uint32_t v = nx;
                 if (e & 0x8000u) {
-                    if (!(ctx->h_tokinfo[s] & TOK_IGNORE)) v |= LX_EMIT;
+                    if (!(ctx->h_tokinfo[s] & TOK_IGNORE))
+                        v |= LX_EMIT | ((ctx->h_tokinfo[s] & TOK_TERM_MASK) << LX_TERM_SHIFT);
                     if (!(ctx->h_tokinfo[nx] & TOK_IGNORE)) v |= LX_START;
                 }
                 ent[(size_t)s * LX_ROW + b] = (uint16_t)v;

@@ -47,6 +47,7 @@ constexpr int LX_ROW = 258;
 constexpr uint32_t LX_NEXT = 0x1fu;
 constexpr uint32_t LX_START = 1u << 5;  // a kept token starts at this byte
 constexpr uint32_t LX_EMIT = 1u << 6;   // a kept token of term(st) ends before this byte
+constexpr int LX_TERM_SHIFT = 7;        // with LX_EMIT: term(st), the ended token's terminal (< 512)
 constexpr uint32_t LX_NOOFF = 0xffu;    // chunk_c: no token start in the chunk
 
 struct Lex3Tables {
@@ -55,7 +56,7 @@ struct Lex3Tables {
     const uint16_t* step;     // [E][C1] endo after one more byte of the class
     const uint8_t* app8;      // [E+S][32] state after endo f from state s; rows E+s are constant s;
                               // identity beyond S in rows < E
-    const uint16_t* ent;      // [S][LX_ROW] next | LX_START | LX_EMIT (columns 256.. unused)
+    const uint16_t* ent;      // [S][LX_ROW] next | LX_START | LX_EMIT | term << LX_TERM_SHIFT (columns 256.. unused)
     const uint32_t* tokinfo;  // [S] terminal | TOK_ACCEPT | TOK_IGNORE
     int S, C1, E;
 };
@@ -688,7 +689,7 @@ __global__ void __launch_bounds__(LX_THREADS, 6) lex3_emit_kernel(Lex3Args a, Le
                 for (int j = 0; j < LX_CHUNK; ++j) {
                     const uint32_t e = s_ent[st * LX_ROW + byte_of(w, j)];
                     if (e & LX_EMIT) {
-                        s_pk[k] = (rel + j) | (s_tok[st] << 16);
+                        s_pk[k] = (rel + j) | ((e >> LX_TERM_SHIFT) << 16);
                         s_st[k] = cur;
                         ++k;
                     }
@@ -734,7 +735,7 @@ __global__ void __launch_bounds__(LX_THREADS, 6) lex3_emit_kernel(Lex3Args a, Le
                             st = INIT;
                         }
                         const uint32_t e = s_ent[st * LX_ROW + __ldg(a.in + pos)];
-                        if (e & LX_EMIT) tok(s_tok[st] & TOK_TERM_MASK, cur, (uint32_t)pos);
+                        if (e & LX_EMIT) tok(e >> LX_TERM_SHIFT, cur, (uint32_t)pos);
                         if (e & LX_START) cur = (uint32_t)pos;
                         st = e & LX_NEXT;
                         if ((last >> j) & 1u) {
@@ -765,7 +766,23 @@ __global__ void __launch_bounds__(LX_THREADS, 6) lex3_emit_kernel(Lex3Args a, Le
         __syncthreads();
 
         // ---- coalesced copy of the staged tokens ---------------------------------
-        if (staged) {
+        if (staged && dmax == d0) {
+            // one document in the tile: every token's index and positions shift alike
+            const long long ib = (long long)Xc + sent * (2 * d0 + 1) + tbase;
+            const long long off = pb - base_of(d0, dmax, d0);
+            for (uint32_t k = tid; k < Bc; k += LX_THREADS) {
+                const uint32_t pk = s_pk[k], sv = s_st[k];
+                const long long idx = ib + k;
+                if (idx < 0) continue;
+                if (idx < a.cap) {
+                    o_term[idx] = (TermT)(pk >> 16);
+                    o_start[idx] = (PosT)(sv == ALP_NONE32 ? snone : (long long)sv + off);
+                    o_end[idx] = (PosT)(t0 + (pk & 0xffffu) + off);
+                } else {
+                    atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
+                }
+            }
+        } else if (staged) {
             const long long b0 = base_of(d0, dmax, d0);
             for (uint32_t k = tid; k < Bc; k += LX_THREADS) {
                 const uint32_t pk = s_pk[k];
