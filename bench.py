@@ -823,6 +823,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--doc-mib", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="default launch shapes (no autotuner run): for "
+                    "launch lists whose first launches should be the measured ones")
     ap.add_argument("--workload", default="parse", choices=["parse", "lex", "batch", "spec", "graph", "shard"])
     ap.add_argument("--batch-docs", type=int, default=100000, help="JSON documents of the batch workload "
                     "(half as many sexp documents); smaller values are for profiling")
@@ -864,7 +866,10 @@ def main():
                                                                        L.alp_last_error(g.h).decode()))
 
     # launch shapes from the autotuner, timed on this document (outside the timed region)
-    tuning = g.tune(d_in, reps=3)
+    if args.no_tune:
+        tuning = {"config": g.get_tuning(), "tile_shape": g.tile_shapes()[g.get_tuning()[0]], "timings": []}
+    else:
+        tuning = g.tune(d_in, reps=3)
     g._stream()
     for _ in range(max(3, args.warmup)):
         step()
