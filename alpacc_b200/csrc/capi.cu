@@ -738,19 +738,22 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     a.br_off = (long long*)ctx->tmp[T_BROFF].p;
     a.doc_valid = dvalid;
     const size_t sm1 = pairs_smem_bytes(ctx->pt.n_pairs, ctx->pt.q + ctx->pt.k);
-    CK(cudaFuncSetAttribute(parse_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+    CK(cudaFuncSetAttribute(pairs_kernel_for(ctx->pt.q, ctx->pt.k), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
     mark(ctx, "start");
     unsigned g_pairs = 1, g_expand = 1;
     {
         int sms = 0, per1 = 0;
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, parse_pairs_kernel, PP_THREADS, sm1));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, pairs_kernel_for(ctx->pt.q, ctx->pt.k), PP_THREADS, sm1));
         const long long x = (long long)persistent_ctas(per1, ctx->tune.pairs_ctas) * sms;
         g_pairs = (unsigned)(x < tiles ? x : tiles);
         g_expand = (unsigned)(2LL * sms < tiles ? 2LL * sms : tiles);  // persistent; set below from occupancy
     }
-    parse_pairs_kernel<<<g_pairs, PP_THREADS, sm1, ctx->stream>>>(a);
-    CK(cudaGetLastError());
+    {
+        void* args[] = {&a};
+        CK(cudaLaunchKernel(pairs_kernel_for(ctx->pt.q, ctx->pt.k), dim3(g_pairs), dim3(PP_THREADS), args, sm1,
+                            ctx->stream));
+    }
     mark(ctx, "parse_pairs_kernel");
     {
         const long long chunks = (tiles + ST_CHUNK - 1) / ST_CHUNK;
@@ -1182,9 +1185,9 @@ int alp_tune_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int reps, char*
     {
         const size_t sm1 = pairs_smem_bytes(ctx->pt.n_pairs, ctx->pt.q + ctx->pt.k);
         const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
-        CK(cudaFuncSetAttribute(parse_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+        CK(cudaFuncSetAttribute(pairs_kernel_for(ctx->pt.q, ctx->pt.k), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
         CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit_pairs, parse_pairs_kernel, PP_THREADS, sm1));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit_pairs, pairs_kernel_for(ctx->pt.q, ctx->pt.k), PP_THREADS, sm1));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit_expand, parse_expand_kernel, PP_THREADS, sm2));
     }
     double best = 1e30, ms = 0;
@@ -2373,14 +2376,17 @@ int parse_positions_dev(alp_ctx* ctx, long long Lcap, const long long* dL, long 
     const size_t sm1 = pairs_smem_bytes(ctx->pt.n_pairs, ctx->pt.q + ctx->pt.k);
     const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
     if (sm2 > 220 * 1024) return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
-    CK(cudaFuncSetAttribute(parse_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+    CK(cudaFuncSetAttribute(pairs_kernel_for(ctx->pt.q, ctx->pt.k), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
     CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, parse_pairs_kernel, PP_THREADS, sm1));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, pairs_kernel_for(ctx->pt.q, ctx->pt.k), PP_THREADS, sm1));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, parse_expand_kernel, PP_THREADS, sm2));
     const long long x1 = (long long)persistent_ctas(per1, ctx->tune.pairs_ctas) * sms,
                     x2 = (long long)persistent_ctas(per2, ctx->tune.expand_ctas) * sms;
-    parse_pairs_kernel<<<(unsigned)(x1 < tiles ? x1 : tiles), PP_THREADS, sm1, ctx->stream>>>(a);
-    CK(cudaGetLastError());
+    {
+        void* args[] = {&a};
+        CK(cudaLaunchKernel(pairs_kernel_for(ctx->pt.q, ctx->pt.k), dim3((unsigned)(x1 < tiles ? x1 : tiles)),
+                            dim3(PP_THREADS), args, sm1, ctx->stream));
+    }
     {
         const long long chunks = (tiles + ST_CHUNK - 1) / ST_CHUNK;
         PosSums* csum = a.tile_sums + tiles;

@@ -329,6 +329,9 @@ __host__ __device__ inline size_t pairs_smem_bytes(int n_pairs, int window) {
     return sizeof(PairInfo) * (size_t)n_pairs + ((size_t)PP_TILE + window) * 4;
 }
 
+// QT, KT > 0: the lookback and lookahead fixed at compile time (window loops
+// unrolled); 0: read from the tables.
+template <int QT, int KT>
 __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     PairInfo* s_pi = reinterpret_cast<PairInfo*>(smem);
@@ -336,7 +339,7 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
     __shared__ PosSums s_w[PP_THREADS / 32];
     __shared__ uint32_t s_pow[17];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int q = a.t.q, k = a.t.k, W = q + k;
+    const int q = QT > 0 ? QT : a.t.q, k = KT > 0 ? KT : a.t.k, W = q + k;
     if (a.dL) a.L = *a.dL;
     for (int i = tid; i < a.t.n_pairs * (int)(sizeof(PairInfo) / 4); i += PP_THREADS)
         reinterpret_cast<uint32_t*>(s_pi)[i] = reinterpret_cast<const uint32_t*>(a.t.pairs)[i];
@@ -367,12 +370,14 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
             // a window never reaches past its document's ⊢ (left) or ⊣ (right)
             uint32_t x = c * s_pow[q];
             bool ok = c != SL;
+#pragma unroll
             for (int jj = q - 1; jj >= 0; --jj) {
                 const uint32_t t = s_term[o + jj];
                 x += (ok ? t : EMPTY) * s_pow[jj];
                 ok = ok && t != SL;
             }
             ok = c != SR;
+#pragma unroll
             for (int jj = q + 1; jj < W; ++jj) {
                 const uint32_t t = s_term[o + jj];
                 x += (ok ? t : EMPTY) * s_pow[jj];
@@ -394,16 +399,28 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
         for (int j = 0; j < PP_ITEMS; ++j)
             if (i0 + j < a.L) a.pid[i0 + j] = ids[j];
     }
-    // ordered block reduce
+    // ordered block reduce: the warps' totals, then warp 0 over them
     PosSums inc = ps_warp_scan(acc, lane);
     if (lane == 31) s_w[warp] = inc;
     __syncthreads();
-    if (tid == 0) {
-        PosSums t = s_w[0];
-        for (int w = 1; w < PP_THREADS / 32; ++w) t = ps_combine(t, s_w[w]);
-        a.tile_sums[tile] = t;
+    if (warp == 0) {
+        PosSums w;
+        if (lane < PP_THREADS / 32) w = s_w[lane]; else possums_zero(w);
+        const PosSums t = ps_warp_scan(w, lane);
+        if (lane == PP_THREADS / 32 - 1) a.tile_sums[tile] = t;
     }
     }
+}
+
+// The pair kernel for a grammar's (q, k): an unrolled instantiation for the
+// small ones, the generic kernel otherwise.
+inline const void* pairs_kernel_for(int q, int k) {
+    if (q == 1 && k == 1) return (const void*)parse_pairs_kernel<1, 1>;
+    if (q == 1 && k == 2) return (const void*)parse_pairs_kernel<1, 2>;
+    if (q == 1 && k == 3) return (const void*)parse_pairs_kernel<1, 3>;
+    if (q == 2 && k == 1) return (const void*)parse_pairs_kernel<2, 1>;
+    if (q == 2 && k == 2) return (const void*)parse_pairs_kernel<2, 2>;
+    return (const void*)parse_pairs_kernel<0, 0>;
 }
 
 // Exclusive segmented scan of the tile sums in place, in two launches:
