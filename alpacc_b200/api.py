@@ -402,13 +402,17 @@ class Grammar:
         return [(out[2 * i], out[2 * i + 1]) for i in range(k)]
 
     def get_tuning(self) -> List[int]:
-        cfg = (ctypes.c_int32 * 3)()
-        native().alp_tune_get(self.h, cfg, 3)
+        """[tile shape, pair CTAs per SM, expand CTAs per SM, MLP kernel (0 tcgen05, 1 mma.sync)]."""
+        cfg = (ctypes.c_int32 * 4)()
+        native().alp_tune_get(self.h, cfg, 4)
         return list(cfg)
 
     def set_tuning(self, cfg: Sequence[int]) -> None:
-        c = (ctypes.c_int32 * 3)(*cfg)
-        rc = native().alp_tune_set(self.h, c, 3)
+        """Three values (launch shapes) or four (and the MLP inference kernel)."""
+        if len(cfg) not in (3, 4):
+            raise ValueError("tuning takes 3 or 4 values")
+        c = (ctypes.c_int32 * len(cfg))(*cfg)
+        rc = native().alp_tune_set(self.h, c, len(cfg))
         if rc != ALP_OK:
             self._err(rc)
 

@@ -39,6 +39,7 @@ struct Tuning {
     int ple = 0;          // index into ple_shapes
     int pairs_ctas = 0;   // CTAs per SM of the persistent pair kernel (0: as many as fit)
     int expand_ctas = 0;  // same for the expand kernel
+    int mlp = 0;          // boundary-MLP inference: 0 tcgen05 kernel, 1 mma.sync kernel
 };
 
 struct alp_ctx {
@@ -1104,6 +1105,7 @@ int alp_tune_get(const alp_ctx* ctx, int32_t* cfg, int n) {
     cfg[0] = ctx->tune.ple;
     cfg[1] = ctx->tune.pairs_ctas;
     cfg[2] = ctx->tune.expand_ctas;
+    if (n > 3) cfg[3] = ctx->tune.mlp;
     return ALP_OK;
 }
 
@@ -1111,6 +1113,8 @@ int alp_tune_set(alp_ctx* ctx, const int32_t* cfg, int n) {
     if (!ctx || !cfg || n < 3) return ALP_ERR_ARG;
     if (cfg[0] < 0 || cfg[0] >= N_PLE_SHAPES || cfg[1] < 0 || cfg[1] > 32 || cfg[2] < 0 || cfg[2] > 32)
         return fail(ctx, ALP_ERR_ARG, "tuning values out of range");
+    if (n > 3 && (cfg[3] < 0 || cfg[3] > 1)) return fail(ctx, ALP_ERR_ARG, "MLP kernel choice out of range");
+    if (n > 3) ctx->tune.mlp = cfg[3];
     ctx->tune.ple = cfg[0];
     ctx->tune.pairs_ctas = cfg[1];
     ctx->tune.expand_ctas = cfg[2];
@@ -1976,8 +1980,10 @@ int alp_mlp_train_step(alp_ctx* ctx, float* params, uint16_t* wbf, float* grads,
     return ALP_OK;
 }
 
-int alp_mlp_predict(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_states, const uint8_t* d_in, int64_t n,
-                    const int64_t* d_pos, int64_t count, uint8_t* d_pred) {
+// Boundary-state predictions.  d_err: a device word for the tcgen05 kernel's
+// timeout bit, read later by the caller; null = a word of its own, checked here.
+static int mlp_predict(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_states, const uint8_t* d_in,
+                       int64_t n, const int64_t* d_pos, int64_t count, uint8_t* d_pred, unsigned int* d_err) {
     if (!ctx) return ALP_ERR_ARG;
     if (!wbf || !wf32 || n_states < 1 || n_states > MLP_OUT || count < 0 || (count > 0 && (!d_pos || !d_pred)))
         return fail(ctx, ALP_ERR_ARG, "bad MLP arguments");
@@ -1993,20 +1999,52 @@ int alp_mlp_predict(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_
     w.b3 = wf32 + P_B3;
     w.n_states = n_states;
     int rc;
-    if ((rc = grow(ctx, ctx->mlp[15], (size_t)MLP_IN * MLP_H * 2))) return rc;
-    __nv_bfloat16* w1t = reinterpret_cast<__nv_bfloat16*>(ctx->mlp[15].p);
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    CK(cudaFuncSetAttribute(mlp_infer2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I2_SMEM));
-    const long long tiles = (count + I2_ROWS - 1) / I2_ROWS;
-    const long long grid = tiles < 2LL * sms ? tiles : 2LL * sms;
+    if (ctx->tune.mlp == 1) {  // mma.sync kernel
+        if ((rc = grow(ctx, ctx->mlp[15], (size_t)MLP_IN * MLP_H * 2))) return rc;
+        __nv_bfloat16* w1t = reinterpret_cast<__nv_bfloat16*>(ctx->mlp[15].p);
+        CK(cudaFuncSetAttribute(mlp_infer2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I2_SMEM));
+        const long long tiles = (count + I2_ROWS - 1) / I2_ROWS;
+        const long long grid = tiles < 2LL * sms ? tiles : 2LL * sms;
+        mark(ctx, "start");
+        mlp_w1t_kernel<<<128, 256, 0, ctx->stream>>>(w.w1, w1t);
+        mlp_infer2_kernel<<<(unsigned)grid, I2_WARPS * 32, I2_SMEM, ctx->stream>>>(
+            w, w1t, d_in, n, reinterpret_cast<const long long*>(d_pos), count, d_pred);
+        CK(cudaGetLastError());
+        mark(ctx, "mlp_w1t+mlp_infer2");
+        return ALP_OK;
+    }
+    // tcgen05 kernel: weight image in the swizzled operand layout, one CTA per SM
+    if ((rc = grow(ctx, ctx->mlp[14], (size_t)WIMG_BYTES)) || (rc = grow(ctx, ctx->mlp[13], 16))) return rc;
+    unsigned int* own_err = reinterpret_cast<unsigned int*>(ctx->mlp[13].p);
+    if (!d_err) {
+        d_err = own_err;
+        CK(cudaMemsetAsync(d_err, 0, 4, ctx->stream));
+    }
+    CK(cudaFuncSetAttribute(mlp_infer3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)I3_SMEM));
+    const long long tiles = (count + I3_ROWS - 1) / I3_ROWS;
+    const long long grid = tiles < (long long)sms ? tiles : (long long)sms;
     mark(ctx, "start");
-    mlp_w1t_kernel<<<128, 256, 0, ctx->stream>>>(w.w1, w1t);
-    mlp_infer2_kernel<<<(unsigned)grid, I2_WARPS * 32, I2_SMEM, ctx->stream>>>(
-        w, w1t, d_in, n, reinterpret_cast<const long long*>(d_pos), count, d_pred);
+    mlp_wimg_kernel<<<148, 256, 0, ctx->stream>>>(w, reinterpret_cast<__nv_bfloat16*>(ctx->mlp[14].p));
+    mlp_infer3_kernel<<<(unsigned)grid, I3_THREADS, I3_SMEM, ctx->stream>>>(
+        w, reinterpret_cast<const uint8_t*>(ctx->mlp[14].p), d_in, n, reinterpret_cast<const long long*>(d_pos),
+        count, d_pred, d_err);
     CK(cudaGetLastError());
-    mark(ctx, "mlp_w1t+mlp_infer2");
+    mark(ctx, "mlp_wimg+mlp_infer3");
+    if (d_err == own_err) {
+        CK(cudaMemcpyAsync(ctx->h_stage, d_err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        unsigned int e = 0;
+        memcpy(&e, ctx->h_stage, 4);
+        if (e & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "MLP inference wait timed out");
+    }
     return ALP_OK;
+}
+
+int alp_mlp_predict(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n_states, const uint8_t* d_in, int64_t n,
+                    const int64_t* d_pos, int64_t count, uint8_t* d_pred) {
+    return mlp_predict(ctx, wbf, wf32, n_states, d_in, n, d_pos, count, d_pred, nullptr);
 }
 
 // Speculative lexing on the multi-kernel lexer: predicted block states
@@ -2049,8 +2087,8 @@ static int spec3_lex(alp_ctx* ctx, const uint16_t* wbf, const float* wf32, int n
         if (K > 1) {
             long long* pos = (long long*)sb[10].p;
             positions_kernel<<<grid_for(K - 1), 256, 0, ctx->stream>>>(pos, K - 1, chunk);
-            if ((rc = alp_mlp_predict(ctx, wbf, wf32, n_states, d_in, n, reinterpret_cast<const int64_t*>(pos), K - 1,
-                                      sa.st + 1)))
+            if ((rc = mlp_predict(ctx, wbf, wf32, n_states, d_in, n, reinterpret_cast<const int64_t*>(pos), K - 1,
+                                  sa.st + 1, &r.a.res->error)))
                 return rc;
         }
         // 2) every block from its predicted state, 3) re-run blocks until every start is exact

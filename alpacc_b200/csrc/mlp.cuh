@@ -12,6 +12,7 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "umma.cuh"
 
 namespace alp {
 
@@ -595,6 +596,396 @@ __global__ void __launch_bounds__(I2_WARPS * 32, 2) mlp_infer2_kernel(MlpWeights
             if (t == 0 && r < count) pred[r] = (uint8_t)bi;
         }
     }
+}
+
+
+// ---------------------------------------------------------------------------
+// Inference on the fifth-generation tensor cores (tcgen05), warp-specialised.
+// A CTA takes 128 windows at a time (M = 128).  Layer 1 (K = 1024) runs as 8
+// stages of K = 128 (two swizzled K-slabs of 64) through a ring of I3_NS
+// stage buffers.  The K order is permuted so that K-slab s (0..15) holds window
+// positions s, s + 16, s + 32, s + 48 (16 embedding values each): chunk c (16
+// bytes) of a row is half c & 1 of the embedding of the byte at position
+// s + 16 (c >> 1).  Then a thread that owns 16 consecutive window bytes of a
+// row (a quarter) writes two chunks of every K-slab from registers.  Roles:
+//   * 16 builder warps: thread (row tid / 4, quarter tid % 4) keeps its
+//     window bytes in registers (the next tile's are loaded while this one
+//     is built), writes its chunks of the stage's A operand in the 128-byte
+//     swizzled K-major layout and arrives on the stage's `full` mbarrier (one
+//     arrival per warp);
+//   * a producer warp: one bulk copy per stage of the W1 rows, already in that
+//     layout and K order in a weight image (mlp_wimg_kernel), onto the same
+//     `full` mbarrier (an arrival plus the byte count), running ahead as
+//     stages come free;
+//   * an MMA warp: one thread waits for a stage, issues eight 128x128x16 MMAs
+//     into tensor memory and commits them to the stage's `freed` mbarrier,
+//     which hands the stage back; halfway through a tile's layer 1 it issues
+//     layer 2 of the previous tile, and after it that tile's layer 3;
+//   * 8 epilogue warps (warp w owns tensor-memory lanes / rows 32 (w % 4) ..
+//     +31 and half of the columns): bias + ReLU + BF16 of the layer-1 and
+//     layer-2 accumulators into the next layer's A operand (s_h, two swizzled
+//     K-slabs), then the argmax of the layer-3 logits.
+// A stage of K = 128 gives the MMA thread 512 tensor-core cycles of work per
+// mbarrier wait (a wait costs a few hundred cycles even when the phase is
+// already complete).  Tensor memory holds two tiles' accumulators (512
+// columns): tile buffer b has layer 1 in columns 256 b + 0..127, layer 2 in
+// 256 b + 128..255 and layer 3 in 256 b + 0..31, so the epilogue of one tile
+// overlaps layer 1 of the next.  Same rounding points as mlp_infer2_kernel
+// (BF16 operands, FP32 accumulation, BF16 hidden activations).
+//
+// Every mbarrier wait is bounded: one that gives up records
+// ALP_DEV_ERR_TIMEOUT and raises the CTA's abort flag, which every role
+// checks before each wait; each role then leaves its loop, the CTA waits
+// (bounded) for its copies and MMAs in flight and frees its tensor memory.
+// ---------------------------------------------------------------------------
+constexpr int I3_NS = 2;                          // stage buffers of layer 1
+constexpr int I3_BUILDERS = 16;                   // builder warps
+constexpr int I3_EPI = 8;                         // epilogue warps
+constexpr int I3_W_PROD = I3_BUILDERS + I3_EPI;   // producer warp index
+constexpr int I3_W_MMA = I3_W_PROD + 1;           // MMA warp index
+constexpr int I3_THREADS = (I3_W_MMA + 1) * 32;
+constexpr int I3_ROWS = 128;                      // windows per tile (MMA M)
+constexpr int I3_SLAB = 128 * 128;                // bytes of a 128-row x 64 BF16 swizzled K-slab
+constexpr int I3_KSLABS = MLP_IN / 64;            // 16
+constexpr int I3_STAGE = 2 * I3_SLAB;             // a stage: two K-slabs (K = 128)
+constexpr int I3_STAGES = I3_KSLABS / 2;          // 8 stages per tile
+constexpr int I3_W3SLAB = MLP_OUT * 128;          // 32 rows x 64 BF16
+static_assert(I3_BUILDERS * 32 == I3_ROWS * 4, "one builder thread per (row, quarter)");
+// weight image (bytes): W1^T slabs (permuted K), W2^T slabs, W3^T slabs
+constexpr int WIMG_W2 = I3_KSLABS * I3_SLAB;
+constexpr int WIMG_W3 = WIMG_W2 + 2 * I3_SLAB;
+constexpr int WIMG_BYTES = WIMG_W3 + 2 * I3_W3SLAB;
+// shared memory (from a 1024-byte aligned base)
+constexpr int I3_OFF_A = 0;
+constexpr int I3_OFF_B = I3_NS * I3_STAGE;
+constexpr int I3_OFF_H = 2 * I3_NS * I3_STAGE;
+constexpr int I3_OFF_W2 = I3_OFF_H + 2 * I3_SLAB;
+constexpr int I3_OFF_W3 = I3_OFF_W2 + 2 * I3_SLAB;
+constexpr int I3_OFF_EMB = I3_OFF_W3 + 2 * I3_W3SLAB;
+constexpr int I3_OFF_BIAS = I3_OFF_EMB + 256 * MLP_EMB * 2;
+constexpr int I3_OFF_BAR = I3_OFF_BIAS + (2 * MLP_H + MLP_OUT) * 4;
+// full[NS], freed[NS], weights, acc[2], d_free[2], h_full, final
+constexpr int I3_NBAR = 2 * I3_NS + 7;
+constexpr int I3_OFF_TMEM = I3_OFF_BAR + I3_NBAR * 8;
+constexpr size_t I3_SMEM = (size_t)I3_OFF_TMEM + 16 + 1024;  // + alignment slack
+constexpr uint32_t I3_TMEM_COLS = 512;
+static_assert(I3_OFF_BAR % 8 == 0 && I3_OFF_H % 1024 == 0 && I3_OFF_W2 % 1024 == 0 && I3_OFF_W3 % 1024 == 0,
+              "layout");
+static_assert(I3_SMEM + 1024 <= 227 * 1024, "shared memory");
+
+// The weight image: element j (0..63) of row n of a K-slab sits at byte
+// n * 128 + ((j / 8) ^ (n % 8)) * 16 + (j % 8) * 2 of the slab.  For W1, j of
+// slab s is input k = 16 (s + 16 (j / 16)) + j % 16 (the permuted K order);
+// for W2 and W3, k = 64 s + j.
+__global__ void mlp_wimg_kernel(MlpWeights w, __nv_bfloat16* img) {
+    constexpr int total = WIMG_BYTES / 2;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        const int b = 2 * e;
+        int region_off, slab_bytes, N;
+        const __nv_bfloat16* src;
+        if (b < WIMG_W2) {
+            region_off = 0; slab_bytes = I3_SLAB; N = MLP_H; src = w.w1;
+        } else if (b < WIMG_W3) {
+            region_off = WIMG_W2; slab_bytes = I3_SLAB; N = MLP_H; src = w.w2;
+        } else {
+            region_off = WIMG_W3; slab_bytes = I3_W3SLAB; N = MLP_OUT; src = w.w3;
+        }
+        const int slab = (b - region_off) / slab_bytes, o = (b - region_off) % slab_bytes;
+        const int row = o >> 7, chunk = ((o >> 4) & 7) ^ (row & 7), j = chunk * 8 + ((o & 15) >> 1);
+        const int k = region_off == 0 ? 16 * (slab + 16 * (j >> 4)) + (j & 15) : 64 * slab + j;
+        img[e] = src[(size_t)k * N + row];  // the matrices are stored [k][n]
+    }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(mbar);
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+
+// The 16 window bytes [16 qq, 16 qq + 16) of the window ending before pos[row]
+// (spaces before the input's start, past its end and for rows past count).
+__device__ __forceinline__ uint4 window_quarter(const uint8_t* in, long long n, bool in16, long long p_end,
+                                                bool live, int qq) {
+    uint4 v = make_uint4(0x20202020u, 0x20202020u, 0x20202020u, 0x20202020u);
+    if (!live) return v;
+    const long long p0 = p_end - MLP_WIN + 16 * qq;
+    if (in16 && p0 >= 0 && p0 + 16 <= n && (p0 & 15) == 0) return __ldg(reinterpret_cast<const uint4*>(in + p0));
+    uint32_t x[4];
+#pragma unroll
+    for (int b = 0; b < 16; ++b) {
+        const long long at = p0 + b;
+        const uint32_t by = (at >= 0 && at < n) ? in[at] : 0x20u;
+        if ((b & 3) == 0) x[b >> 2] = 0;
+        x[b >> 2] |= by << (8 * (b & 3));
+    }
+    return make_uint4(x[0], x[1], x[2], x[3]);
+}
+
+__device__ __forceinline__ uint32_t quarter_byte(const uint4& v, int s) {
+    const uint32_t wv = s < 4 ? v.x : s < 8 ? v.y : s < 12 ? v.z : v.w;
+    return (wv >> (8 * (s & 3))) & 0xffu;
+}
+
+__global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w, const uint8_t* wimg,
+                                                                    const uint8_t* in, long long n,
+                                                                    const long long* pos, long long count,
+                                                                    uint8_t* pred, unsigned int* err) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    __shared__ int s_abort;
+    uint8_t* sm = smem_raw + ((1024u - ((uint32_t)__cvta_generic_to_shared(smem_raw) & 1023u)) & 1023u);
+    const uint32_t sb = (uint32_t)__cvta_generic_to_shared(sm);
+    __nv_bfloat16* s_emb = reinterpret_cast<__nv_bfloat16*>(sm + I3_OFF_EMB);
+    float* s_b1 = reinterpret_cast<float*>(sm + I3_OFF_BIAS);
+    float* s_b2 = s_b1 + MLP_H;
+    float* s_b3 = s_b2 + MLP_H;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sm + I3_OFF_BAR);
+    uint64_t* freed = full + I3_NS;
+    uint64_t* wbar = freed + I3_NS;
+    uint64_t* acc = wbar + 1;       // [2]: per accumulator buffer, layers 1, 2, 3 of its tile
+    uint64_t* d_free = acc + 2;     // [2]: the epilogue is done with the buffer
+    uint64_t* h_full = d_free + 2;  // the epilogue wrote the next layer's A operand
+    uint64_t* fin = h_full + 1;
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + I3_OFF_TMEM);
+    volatile int* abort_flag = &s_abort;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long tiles = (count + I3_ROWS - 1) / I3_ROWS;
+
+    if (tid == 0) {
+        for (int i = 0; i < I3_NS; ++i) {
+            mbar_init(full + i, I3_BUILDERS + 1);  // builder warps + the producer's copy
+            mbar_init(freed + i, 1);
+        }
+        mbar_init(wbar, 1);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(acc + i, 1);
+            mbar_init(d_free + i, I3_EPI);
+        }
+        mbar_init(h_full, I3_EPI);
+        mbar_init(fin, 1);
+        mbar_fence_init();
+        s_abort = 0;
+    }
+    __syncwarp();
+    if (warp == 0) tmem_alloc(s_tmem, I3_TMEM_COLS);
+    for (int i = tid; i < 256 * MLP_EMB; i += I3_THREADS) s_emb[i] = w.emb[i];
+    for (int i = tid; i < MLP_H; i += I3_THREADS) { s_b1[i] = w.b1[i]; s_b2[i] = w.b2[i]; }
+    for (int i = tid; i < MLP_OUT; i += I3_THREADS) s_b3[i] = w.b3[i];
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = *s_tmem;
+    // a wait that gives up raises the abort flag; after it no role waits again
+    auto wait_ok = [&](uint64_t* bar, uint32_t parity) -> bool {
+        if (*abort_flag) return false;
+        if (mbar_wait(bar, parity, err)) return true;
+        *abort_flag = 1;
+        return false;
+    };
+    // the same for a whole warp: lane 0 waits (few threads polling the
+    // mbarrier unit), the warp goes on or leaves together
+    auto warp_wait_ok = [&](uint64_t* bar, uint32_t parity) -> bool {
+        bool ok = true;
+        if (lane == 0) ok = wait_ok(bar, parity);
+        __syncwarp();
+        return __shfl_sync(ALP_FULL_MASK, ok ? 1 : 0, 0) != 0;
+    };
+
+    if (warp < I3_BUILDERS) {
+        // ---------------- builders: layer-1 A operands ----------------
+        const bool in16 = (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
+        const int qq = tid & 3, rr = tid >> 2;
+        long long tile = blockIdx.x;
+        uint4 cur, nxt = make_uint4(0, 0, 0, 0);
+        {
+            const long long r = tile * I3_ROWS + rr;
+            const bool live = tile < tiles && r < count;
+            cur = window_quarter(in, n, in16, live ? pos[r] : 0, live, qq);
+        }
+        for (uint32_t t = 0; tile < tiles; tile += gridDim.x, ++t) {
+            const long long nt = tile + gridDim.x, nr = nt * I3_ROWS + rr;
+            const bool nlive = nt < tiles && nr < count;
+            long long np = 0;
+            bool ok = true;
+#pragma unroll
+            for (int S = 0; S < I3_STAGES; ++S) {
+                if (S == 0 && nlive) np = pos[nr];  // the next tile's window position ...
+                if (S == I3_STAGES / 2) nxt = window_quarter(in, n, in16, np, nlive, qq);  // ... and bytes
+                const uint32_t g = t * I3_STAGES + S, st = g % I3_NS, u = g / I3_NS;
+                if (u > 0 && !warp_wait_ok(freed + st, (u - 1) & 1u)) { ok = false; break; }
+                uint8_t* A = sm + I3_OFF_A + st * I3_STAGE;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint4* e = reinterpret_cast<const uint4*>(s_emb + quarter_byte(cur, 2 * S + h) * MLP_EMB);
+                    const uint4 lo = e[0], hi = e[1];
+                    *reinterpret_cast<uint4*>(A + h * I3_SLAB + sw128_offset(rr, 2 * qq)) = lo;
+                    *reinterpret_cast<uint4*>(A + h * I3_SLAB + sw128_offset(rr, 2 * qq + 1)) = hi;
+                }
+                fence_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(full + st);
+            }
+            if (!ok) break;
+            cur = nxt;
+        }
+    } else if (warp < I3_W_PROD) {
+        // ---------------- epilogue: rows 32 q + lane, columns half hc ----------------
+        const int q = warp & 3, hc = (warp - I3_BUILDERS) >> 2;
+        const int r = 32 * q + lane;
+        const uint32_t t_row = tbase + ((uint32_t)(32 * q) << 16);
+        // bias + ReLU + BF16 of accumulator columns [col0 + 64 hc, +64): K-slab hc of the next layer's A
+        auto hidden_out = [&](uint32_t col0, const float* bias) {
+            uint8_t* H = sm + I3_OFF_H + hc * I3_SLAB;
+#pragma unroll 1
+            for (int j = 0; j < 2; ++j) {  // 32 columns at a time: chunks 4 j .. 4 j + 3
+                float v[32];
+                tmem_ld32(t_row + col0 + 64 * hc + 32 * j, v);
+                const float4* b4 = reinterpret_cast<const float4*>(bias + 64 * hc + 32 * j);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const float4 p = b4[2 * c], q4 = b4[2 * c + 1];
+                    const float bb[8] = {p.x, p.y, p.z, p.w, q4.x, q4.y, q4.z, q4.w};
+                    uint32_t pk[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        pk[e] = relu_pack(v[8 * c + 2 * e] + bb[2 * e], v[8 * c + 2 * e + 1] + bb[2 * e + 1]);
+                    *reinterpret_cast<uint4*>(H + sw128_offset(r, 4 * j + c)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                }
+            }
+        };
+        auto publish = [&](uint64_t* bar) {
+            fence_async_smem();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar);
+        };
+        for (uint32_t t = 0; (long long)blockIdx.x + (long long)t * gridDim.x < tiles; ++t) {
+            const uint32_t b = t & 1u, k3 = 3u * (t >> 1);
+            const uint32_t col = 256u * b;
+            if (!warp_wait_ok(acc + b, k3 & 1u)) break;
+            tc_fence_after();
+            hidden_out(col, s_b1);
+            publish(h_full);
+            if (!warp_wait_ok(acc + b, (k3 + 1) & 1u)) break;
+            tc_fence_after();
+            hidden_out(col + 128, s_b2);
+            publish(h_full);
+            if (!warp_wait_ok(acc + b, (k3 + 2) & 1u)) break;
+            tc_fence_after();
+            if (hc == 0) {
+                float z[32];
+                tmem_ld32(t_row + col, z);
+                float bv = -INFINITY;
+                int bi = 0;
+#pragma unroll
+                for (int c = 0; c < MLP_OUT; ++c) {
+                    const float v = c < w.n_states ? z[c] + s_b3[c] : -INFINITY;
+                    if (v > bv) { bv = v; bi = c; }
+                }
+                const long long row = ((long long)blockIdx.x + (long long)t * gridDim.x) * I3_ROWS + r;
+                if (row < count) pred[row] = (uint8_t)bi;
+            }
+            publish(d_free + b);
+        }
+    } else if (warp == I3_W_PROD) {
+        // ---------------- producer: W2 / W3 once, then W1 slabs ahead of the MMAs ----------------
+        if (lane == 0) {
+            mbar_expect_tx(wbar, 2 * I3_SLAB + 2 * I3_W3SLAB);
+            bulk_g2s(sb + I3_OFF_W2, wimg + WIMG_W2, 2 * I3_SLAB, wbar);
+            bulk_g2s(sb + I3_OFF_W3, wimg + WIMG_W3, 2 * I3_W3SLAB, wbar);
+            uint32_t issued = 0, ppar = 0;  // stages with a copy issued, and its phase parity
+            uint32_t g = 0;
+            bool ok = true;
+            for (long long tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+                for (int S = 0; S < I3_STAGES; ++S, ++g) {
+                    const uint32_t st = g % I3_NS, u = g / I3_NS;
+                    if (u > 0 && !wait_ok(freed + st, (u - 1) & 1u)) { ok = false; break; }
+                    mbar_expect_tx(full + st, I3_STAGE);
+                    bulk_g2s(sb + I3_OFF_B + st * I3_STAGE, wimg + (size_t)S * I3_STAGE, I3_STAGE, full + st);
+                    issued |= 1u << st;
+                    ppar = (ppar & ~(1u << st)) | ((u & 1u) << st);
+                }
+            }
+            // every copy has landed before the CTA's shared memory goes away (the
+            // phase completes once the copy and this stage's builders are done;
+            // on an abort the wait may give up, bounded)
+            mbar_wait(wbar, 0, err);
+            for (uint32_t st = 0; st < (uint32_t)I3_NS; ++st)
+                if (issued & (1u << st)) mbar_wait(full + st, (ppar >> st) & 1u, err);
+        }
+        __syncwarp();
+    } else {
+        // ---------------- MMA issue: one thread ----------------
+        if (lane == 0) {
+            constexpr uint32_t ID_H = umma_idesc_bf16_f32(I3_ROWS, MLP_H);
+            constexpr uint32_t ID_O = umma_idesc_bf16_f32(I3_ROWS, MLP_OUT);
+            uint32_t g = 0, nh = 0;
+            bool wready = false, ok = true;
+            // layer 2 / layer 3 of the tile in accumulator buffer pb (after the epilogue's operand)
+            auto layer2 = [&](uint32_t pb) -> bool {
+                if (!wait_ok(h_full, nh & 1u)) return false;
+                ++nh;
+                if (!wready) {
+                    if (!wait_ok(wbar, 0)) return false;
+                    wready = true;
+                }
+                tc_fence_after();
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk) {
+                    const uint32_t off = (kk >> 2) * I3_SLAB;
+                    umma_bf16(tbase + 256 * pb + 128, umma_desc_sw128(sb + I3_OFF_H + off) + 2 * (kk & 3),
+                              umma_desc_sw128(sb + I3_OFF_W2 + off) + 2 * (kk & 3), ID_H, kk != 0);
+                }
+                umma_commit(acc + pb);
+                return true;
+            };
+            auto layer3 = [&](uint32_t pb) -> bool {
+                if (!wait_ok(h_full, nh & 1u)) return false;
+                ++nh;
+                tc_fence_after();
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk)
+                    umma_bf16(tbase + 256 * pb, umma_desc_sw128(sb + I3_OFF_H + (kk >> 2) * I3_SLAB) + 2 * (kk & 3),
+                              umma_desc_sw128(sb + I3_OFF_W3 + (kk >> 2) * I3_W3SLAB) + 2 * (kk & 3), ID_O,
+                              kk != 0);
+                umma_commit(acc + pb);
+                return true;
+            };
+            uint32_t t = 0;
+            for (long long tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++t) {
+                const uint32_t b = t & 1u;
+                // the epilogue is done with this buffer's previous tile
+                if (t >= 2 && !wait_ok(d_free + b, ((t >> 1) - 1) & 1u)) { ok = false; break; }
+                for (int S = 0; S < I3_STAGES; ++S, ++g) {
+                    const uint32_t st = g % I3_NS, par = (g / I3_NS) & 1u;
+                    if (!wait_ok(full + st, par)) { ok = false; break; }
+                    tc_fence_after();
+#pragma unroll
+                    for (int kk = 0; kk < 8; ++kk) {
+                        const uint32_t off = st * I3_STAGE + (kk >> 2) * I3_SLAB;
+                        umma_bf16(tbase + 256 * b, umma_desc_sw128(sb + I3_OFF_A + off) + 2 * (kk & 3),
+                                  umma_desc_sw128(sb + I3_OFF_B + off) + 2 * (kk & 3), ID_H, (S | kk) != 0);
+                    }
+                    umma_commit(freed + st);
+                    if (S == I3_STAGES / 2 - 1 && t > 0 && !layer2(b ^ 1u)) { ok = false; break; }
+                }
+                if (!ok) break;
+                umma_commit(acc + b);  // layer 1 of this tile
+                if (t > 0 && !layer3(b ^ 1u)) { ok = false; break; }
+            }
+            if (ok && t > 0) {  // the last tile's layers 2 and 3
+                const uint32_t pb = (t - 1) & 1u;
+                if (layer2(pb)) layer3(pb);
+            }
+            // every MMA has completed before the tensor memory is freed
+            umma_commit(fin);
+            mbar_wait(fin, 0, err);
+        }
+        __syncwarp();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_free(tbase, I3_TMEM_COLS);
 }
 
 }  // namespace alp

@@ -82,7 +82,10 @@ int alp_check_bounded_wait(alp_ctx* ctx);
  * cfg[0] the tile shape of the previous-smaller-or-equal kernel (an index into
  * the list alp_tune_shapes writes as (threads, elements per thread) pairs),
  * cfg[1] and cfg[2] the CTAs per SM of the persistent pair and expand kernels
- * (0: as many as fit).  alp_tune_parse times alp_parse on a sample (the median
+ * (0: as many as fit); with n >= 4, cfg[3] the boundary-MLP inference kernel
+ * (0: tcgen05 tensor-memory kernel, the default; 1: mma.sync kernel, whose
+ * predictions may differ where two logits are within rounding).
+ * alp_tune_parse times alp_parse on a sample (the median
  * of `reps` calls per candidate, CUDA events), one knob at a time, keeps the
  * fastest setting in the context and writes "knob value ms" lines to
  * `report`.  Every setting gives the same outputs; only speed differs. */

@@ -50,22 +50,64 @@ def test_mlp_gradients_match_float64_reference(has_gpu):
         assert err < 2e-2, (name, err)
 
 
-def test_mlp_predict_matches_reference(has_gpu):
-    """The fused inference kernel's argmax against the float64 forward pass
-    (>= 99% agreement: rows whose top two logits are closer than the
-    FP32/BF16 rounding may differ)."""
-    import torch
-    from alpacc_b200 import spec
-    g, _ = _g("json")
-    m = spec.BoundaryModel(g, seed=5)
-    d = _doc("json", 200000, 21)
-    pos = np.arange(1, 1000) * 160
-    pred = m.predict(d, pos).cpu().numpy()
+def _with_mlp_kernel(g, which):
+    cfg = g.get_tuning()
+    g.set_tuning(cfg[:3] + [which])
+    return cfg
+
+
+def _ref_argmax(m, d, pos):
     x = np.frombuffer(d, np.uint8)
     idx = pos[:, None] - 64 + np.arange(64)[None, :]
-    win = np.where(idx >= 0, x[np.clip(idx, 0, None)], 0x20).astype(np.uint8)
+    win = np.where((idx >= 0) & (idx < len(x)), x[np.clip(idx, 0, len(x) - 1)], 0x20).astype(np.uint8)
     _, _, logits = mref.forward_backward(m.params.cpu().numpy(), win, np.zeros(len(pos), np.int64), m.n_states)
-    assert np.mean(pred == logits.argmax(axis=1)) >= 0.99
+    return logits.argmax(axis=1)
+
+
+@pytest.mark.parametrize("kernel", [0, 1], ids=["tcgen05", "mma_sync"])
+def test_mlp_predict_matches_reference(has_gpu, kernel):
+    """Each inference kernel's argmax against the float64 forward pass
+    (>= 99% agreement: rows whose top two logits are closer than the
+    FP32/BF16 rounding may differ)."""
+    from alpacc_b200 import spec
+    g, _ = _g("json")
+    saved = _with_mlp_kernel(g, kernel)
+    try:
+        m = spec.BoundaryModel(g, seed=5)
+        d = _doc("json", 200000, 21)
+        pos = np.arange(1, 1000) * 160
+        pred = m.predict(d, pos).cpu().numpy()
+        assert np.mean(pred == _ref_argmax(m, d, pos)) >= 0.99
+    finally:
+        g.set_tuning(saved)
+
+
+def test_mlp_tcgen05_kernel_agrees_with_mma_sync(has_gpu):
+    """The tcgen05 kernel (tensor-memory accumulators, swizzled shared-memory
+    operands) against the mma.sync kernel: same rounding points, different
+    summation order, so the argmax agrees except on near ties.  Ragged tile
+    counts, windows reaching before the input's start and past its end, and
+    more tiles than SMs (several tiles per CTA, the stage ring wrapping)."""
+    from alpacc_b200 import spec
+    g, _ = _g("json")
+    saved = g.get_tuning()
+    try:
+        m = spec.BoundaryModel(g, seed=7)
+        d = _doc("json", 3 << 20, 23)
+        rng = np.random.default_rng(8)
+        for count in (1, 127, 128, 129, 1000, 19000, 60000):
+            pos = np.sort(rng.integers(0, len(d) + 100, count))
+            pos[:min(count, 3)] = [0, 5, 63][:min(count, 3)]
+            got = {}
+            for k in (0, 1):
+                g.set_tuning(saved[:3] + [k])
+                got[k] = m.predict(d, pos).cpu().numpy()
+            assert got[0].max() < m.n_states
+            assert np.mean(got[0] == got[1]) >= 0.995, count
+            if count <= 1000:
+                assert np.mean(got[0] == _ref_argmax(m, d, pos)) >= 0.99, count
+    finally:
+        g.set_tuning(saved)
 
 
 @pytest.mark.parametrize("name", ["json", "sexp"])
