@@ -602,43 +602,44 @@ __global__ void __launch_bounds__(I2_WARPS * 32, 2) mlp_infer2_kernel(MlpWeights
 // ---------------------------------------------------------------------------
 // Inference on the fifth-generation tensor cores (tcgen05), warp-specialised.
 // A CTA takes 128 windows at a time (M = 128).  Layer 1 (K = 1024) runs as 8
-// stages of K = 128 (two swizzled K-slabs of 64) through a ring of I3_NS
-// stage buffers.  The K order is permuted so that K-slab s (0..15) holds window
-// positions s, s + 16, s + 32, s + 48 (16 embedding values each): chunk c (16
-// bytes) of a row is half c & 1 of the embedding of the byte at position
-// s + 16 (c >> 1).  Then a thread that owns 16 consecutive window bytes of a
-// row (a quarter) writes two chunks of every K-slab from registers.  Roles:
-//   * 16 builder warps: thread (row tid / 4, quarter tid % 4) keeps its
-//     window bytes in registers (the next tile's are loaded while this one
-//     is built), writes its chunks of the stage's A operand in the 128-byte
-//     swizzled K-major layout and arrives on the stage's `full` mbarrier (one
-//     arrival per warp);
-//   * a producer warp: one bulk copy per stage of the W1 rows, already in that
-//     layout and K order in a weight image (mlp_wimg_kernel), onto the same
-//     `full` mbarrier (an arrival plus the byte count), running ahead as
-//     stages come free;
+// stages of K = 128 through a ring of I3_NS stages; a stage's A operand (the
+// gathered embeddings, 128 rows x 128) lives in tensor memory and its B
+// operand (W1 rows) in shared memory.  The K order is permuted so that K-slab
+// s (0..15, 64 wide) holds window positions s, s + 16, s + 32, s + 48 (16
+// embedding values each): a thread that owns 16 consecutive window bytes of a
+// row (a quarter) supplies 16 K values of every slab from registers.  Roles:
+//   * 16 builder warps: thread (row 32 (w % 4) + lane, quarter w / 4) keeps
+//     its window bytes in registers (the next tile's are loaded while this
+//     one is built), looks up the embeddings in shared memory and stores
+//     them into its own tensor-memory lane (tcgen05.st: lane m = row m, two
+//     BF16 K values per 32-bit column), then arrives on the stage's `full`
+//     mbarrier (one arrival per warp);
+//   * a producer warp: one bulk copy per stage of the W1 rows, already in the
+//     128-byte swizzled K-major layout and permuted K order in a weight image
+//     (mlp_wimg_kernel), onto the same `full` mbarrier (an arrival plus the
+//     byte count), running ahead as stages come free;
 //   * an MMA warp: one thread waits for a stage, issues eight 128x128x16 MMAs
-//     into tensor memory and commits them to the stage's `freed` mbarrier,
-//     which hands the stage back; halfway through a tile's layer 1 it issues
-//     layer 2 of the previous tile, and after it that tile's layer 3;
-//   * 8 epilogue warps (warp w owns tensor-memory lanes / rows 32 (w % 4) ..
-//     +31 and half of the columns): bias + ReLU + BF16 of the layer-1 and
-//     layer-2 accumulators into the next layer's A operand (s_h, two swizzled
-//     K-slabs), then the argmax of the layer-3 logits.
-// A stage of K = 128 gives the MMA thread 512 tensor-core cycles of work per
-// mbarrier wait (a wait costs a few hundred cycles even when the phase is
-// already complete).  Tensor memory holds two tiles' accumulators (512
-// columns): tile buffer b has layer 1 in columns 256 b + 0..127, layer 2 in
-// 256 b + 128..255 and layer 3 in 256 b + 0..31, so the epilogue of one tile
-// overlaps layer 1 of the next.  Same rounding points as mlp_infer2_kernel
-// (BF16 operands, FP32 accumulation, BF16 hidden activations).
+//     (A from tensor memory, B from shared memory) and commits them to the
+//     stage's `freed` mbarrier, which hands the stage back; during a tile's
+//     layer 1 it also issues layers 2 and 3 of the previous tile;
+//   * 8 epilogue warps (warp w owns rows 32 (w % 4) .. +31 and half of the
+//     columns): bias + ReLU + BF16 of the layer-1 and layer-2 accumulators
+//     into the next layer's A operand (s_h, two swizzled K-slabs in shared
+//     memory), then the argmax of the layer-3 logits.
+// Tensor memory (512 columns): the A ring in columns 0..255 (stage st at
+// 64 st, K-slab h of it at + 32 h); two accumulator buffers of 128 columns
+// at 256 + 128 b, each holding a tile's layer 1, then layer 2 (once the
+// epilogue has read layer 1), then layer 3 (32 columns), so the epilogue of
+// one tile overlaps layer 1 of the next.  Same rounding points as
+// mlp_infer2_kernel (BF16 operands, FP32 accumulation, BF16 hidden
+// activations).
 //
 // Every mbarrier wait is bounded: one that gives up records
 // ALP_DEV_ERR_TIMEOUT and raises the CTA's abort flag, which every role
 // checks before each wait; each role then leaves its loop, the CTA waits
 // (bounded) for its copies and MMAs in flight and frees its tensor memory.
 // ---------------------------------------------------------------------------
-constexpr int I3_NS = 2;                          // stage buffers of layer 1
+constexpr int I3_NS = 4;                          // stages of layer 1 in flight
 constexpr int I3_BUILDERS = 16;                   // builder warps
 constexpr int I3_EPI = 8;                         // epilogue warps
 constexpr int I3_W_PROD = I3_BUILDERS + I3_EPI;   // producer warp index
@@ -647,18 +648,19 @@ constexpr int I3_THREADS = (I3_W_MMA + 1) * 32;
 constexpr int I3_ROWS = 128;                      // windows per tile (MMA M)
 constexpr int I3_SLAB = 128 * 128;                // bytes of a 128-row x 64 BF16 swizzled K-slab
 constexpr int I3_KSLABS = MLP_IN / 64;            // 16
-constexpr int I3_STAGE = 2 * I3_SLAB;             // a stage: two K-slabs (K = 128)
+constexpr int I3_STAGE = 2 * I3_SLAB;             // W1 bytes of a stage: two K-slabs (K = 128)
 constexpr int I3_STAGES = I3_KSLABS / 2;          // 8 stages per tile
 constexpr int I3_W3SLAB = MLP_OUT * 128;          // 32 rows x 64 BF16
+constexpr uint32_t I3_TCOL_ACC = 256;             // first accumulator column
 static_assert(I3_BUILDERS * 32 == I3_ROWS * 4, "one builder thread per (row, quarter)");
+static_assert(I3_NS * 64 <= (int)I3_TCOL_ACC, "A ring in tensor memory");
 // weight image (bytes): W1^T slabs (permuted K), W2^T slabs, W3^T slabs
 constexpr int WIMG_W2 = I3_KSLABS * I3_SLAB;
 constexpr int WIMG_W3 = WIMG_W2 + 2 * I3_SLAB;
 constexpr int WIMG_BYTES = WIMG_W3 + 2 * I3_W3SLAB;
 // shared memory (from a 1024-byte aligned base)
-constexpr int I3_OFF_A = 0;
-constexpr int I3_OFF_B = I3_NS * I3_STAGE;
-constexpr int I3_OFF_H = 2 * I3_NS * I3_STAGE;
+constexpr int I3_OFF_B = 0;
+constexpr int I3_OFF_H = I3_NS * I3_STAGE;
 constexpr int I3_OFF_W2 = I3_OFF_H + 2 * I3_SLAB;
 constexpr int I3_OFF_W3 = I3_OFF_W2 + 2 * I3_SLAB;
 constexpr int I3_OFF_EMB = I3_OFF_W3 + 2 * I3_W3SLAB;
@@ -743,7 +745,7 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
     uint64_t* wbar = freed + I3_NS;
     uint64_t* acc = wbar + 1;       // [2]: per accumulator buffer, layers 1, 2, 3 of its tile
     uint64_t* d_free = acc + 2;     // [2]: the epilogue is done with the buffer
-    uint64_t* h_full = d_free + 2;  // the epilogue wrote the next layer's A operand
+    uint64_t* h_full = d_free + 2;  // the epilogue read the accumulator and wrote the next layer's A operand
     uint64_t* fin = h_full + 1;
     uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + I3_OFF_TMEM);
     volatile int* abort_flag = &s_abort;
@@ -789,11 +791,13 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
         __syncwarp();
         return __shfl_sync(ALP_FULL_MASK, ok ? 1 : 0, 0) != 0;
     };
+    // this thread's tensor-memory lane (row): warps access lanes 32 (w % 4) .. +31
+    const uint32_t t_lane = tbase + ((uint32_t)(32 * (warp & 3)) << 16);
 
     if (warp < I3_BUILDERS) {
-        // ---------------- builders: layer-1 A operands ----------------
+        // ---------------- builders: layer-1 A operands into tensor memory ----------------
         const bool in16 = (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
-        const int qq = tid & 3, rr = tid >> 2;
+        const int qq = warp >> 2, rr = 32 * (warp & 3) + lane;
         long long tile = blockIdx.x;
         uint4 cur, nxt = make_uint4(0, 0, 0, 0);
         {
@@ -812,15 +816,17 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
                 if (S == I3_STAGES / 2) nxt = window_quarter(in, n, in16, np, nlive, qq);  // ... and bytes
                 const uint32_t g = t * I3_STAGES + S, st = g % I3_NS, u = g / I3_NS;
                 if (u > 0 && !warp_wait_ok(freed + st, (u - 1) & 1u)) { ok = false; break; }
-                uint8_t* A = sm + I3_OFF_A + st * I3_STAGE;
+                tc_fence_after();
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
+                    // K values 16 qq .. 16 qq + 15 of K-slab 2 S + h: columns 8 qq .. 8 qq + 7
                     const uint4* e = reinterpret_cast<const uint4*>(s_emb + quarter_byte(cur, 2 * S + h) * MLP_EMB);
                     const uint4 lo = e[0], hi = e[1];
-                    *reinterpret_cast<uint4*>(A + h * I3_SLAB + sw128_offset(rr, 2 * qq)) = lo;
-                    *reinterpret_cast<uint4*>(A + h * I3_SLAB + sw128_offset(rr, 2 * qq + 1)) = hi;
+                    const uint32_t v[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+                    tmem_st8(t_lane + 64 * st + 32 * h + 8 * qq, v);
                 }
-                fence_async_smem();
+                tmem_wait_st();
+                tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(full + st);
             }
@@ -828,17 +834,16 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
             cur = nxt;
         }
     } else if (warp < I3_W_PROD) {
-        // ---------------- epilogue: rows 32 q + lane, columns half hc ----------------
-        const int q = warp & 3, hc = (warp - I3_BUILDERS) >> 2;
-        const int r = 32 * q + lane;
-        const uint32_t t_row = tbase + ((uint32_t)(32 * q) << 16);
-        // bias + ReLU + BF16 of accumulator columns [col0 + 64 hc, +64): K-slab hc of the next layer's A
+        // ---------------- epilogue: rows 32 (w % 4) + lane, columns half hc ----------------
+        const int hc = (warp - I3_BUILDERS) >> 2;
+        const int r = 32 * (warp & 3) + lane;
+        // bias + ReLU + BF16 of accumulator columns [64 hc, +64): K-slab hc of the next layer's A
         auto hidden_out = [&](uint32_t col0, const float* bias) {
             uint8_t* H = sm + I3_OFF_H + hc * I3_SLAB;
 #pragma unroll 1
             for (int j = 0; j < 2; ++j) {  // 32 columns at a time: chunks 4 j .. 4 j + 3
                 float v[32];
-                tmem_ld32(t_row + col0 + 64 * hc + 32 * j, v);
+                tmem_ld32(t_lane + col0 + 64 * hc + 32 * j, v);
                 const float4* b4 = reinterpret_cast<const float4*>(bias + 64 * hc + 32 * j);
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
@@ -860,20 +865,20 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
         };
         for (uint32_t t = 0; (long long)blockIdx.x + (long long)t * gridDim.x < tiles; ++t) {
             const uint32_t b = t & 1u, k3 = 3u * (t >> 1);
-            const uint32_t col = 256u * b;
+            const uint32_t col = I3_TCOL_ACC + 128u * b;
             if (!warp_wait_ok(acc + b, k3 & 1u)) break;
             tc_fence_after();
             hidden_out(col, s_b1);
             publish(h_full);
             if (!warp_wait_ok(acc + b, (k3 + 1) & 1u)) break;
             tc_fence_after();
-            hidden_out(col + 128, s_b2);
+            hidden_out(col, s_b2);
             publish(h_full);
             if (!warp_wait_ok(acc + b, (k3 + 2) & 1u)) break;
             tc_fence_after();
             if (hc == 0) {
                 float z[32];
-                tmem_ld32(t_row + col, z);
+                tmem_ld32(t_lane + col, z);
                 float bv = -INFINITY;
                 int bi = 0;
 #pragma unroll
@@ -887,7 +892,7 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
             publish(d_free + b);
         }
     } else if (warp == I3_W_PROD) {
-        // ---------------- producer: W2 / W3 once, then W1 slabs ahead of the MMAs ----------------
+        // ---------------- producer: W2 / W3 once, then W1 stages ahead of the MMAs ----------------
         if (lane == 0) {
             mbar_expect_tx(wbar, 2 * I3_SLAB + 2 * I3_W3SLAB);
             bulk_g2s(sb + I3_OFF_W2, wimg + WIMG_W2, 2 * I3_SLAB, wbar);
@@ -919,8 +924,9 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
             constexpr uint32_t ID_H = umma_idesc_bf16_f32(I3_ROWS, MLP_H);
             constexpr uint32_t ID_O = umma_idesc_bf16_f32(I3_ROWS, MLP_OUT);
             uint32_t g = 0, nh = 0;
-            bool wready = false, ok = true;
-            // layer 2 / layer 3 of the tile in accumulator buffer pb (after the epilogue's operand)
+            bool wready = false, ok = true, ready = false;
+            // layer 2 / layer 3 of the tile in accumulator buffer pb, into the same
+            // columns, once the epilogue has read them and written the A operand
             auto layer2 = [&](uint32_t pb) -> bool {
                 if (!wait_ok(h_full, nh & 1u)) return false;
                 ++nh;
@@ -932,7 +938,7 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
 #pragma unroll
                 for (int kk = 0; kk < 8; ++kk) {
                     const uint32_t off = (kk >> 2) * I3_SLAB;
-                    umma_bf16(tbase + 256 * pb + 128, umma_desc_sw128(sb + I3_OFF_H + off) + 2 * (kk & 3),
+                    umma_bf16(tbase + I3_TCOL_ACC + 128 * pb, umma_desc_sw128(sb + I3_OFF_H + off) + 2 * (kk & 3),
                               umma_desc_sw128(sb + I3_OFF_W2 + off) + 2 * (kk & 3), ID_H, kk != 0);
                 }
                 umma_commit(acc + pb);
@@ -944,7 +950,8 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
                 tc_fence_after();
 #pragma unroll
                 for (int kk = 0; kk < 8; ++kk)
-                    umma_bf16(tbase + 256 * pb, umma_desc_sw128(sb + I3_OFF_H + (kk >> 2) * I3_SLAB) + 2 * (kk & 3),
+                    umma_bf16(tbase + I3_TCOL_ACC + 128 * pb,
+                              umma_desc_sw128(sb + I3_OFF_H + (kk >> 2) * I3_SLAB) + 2 * (kk & 3),
                               umma_desc_sw128(sb + I3_OFF_W3 + (kk >> 2) * I3_W3SLAB) + 2 * (kk & 3), ID_O,
                               kk != 0);
                 umma_commit(acc + pb);
@@ -957,20 +964,23 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
                 if (t >= 2 && !wait_ok(d_free + b, ((t >> 1) - 1) & 1u)) { ok = false; break; }
                 for (int S = 0; S < I3_STAGES; ++S, ++g) {
                     const uint32_t st = g % I3_NS, par = (g / I3_NS) & 1u;
-                    if (!wait_ok(full + st, par)) { ok = false; break; }
+                    if (!ready && !wait_ok(full + st, par)) { ok = false; break; }
+                    // test the next stage now: the query's latency hides behind this stage's issue
+                    ready = mbar_test(full + (g + 1) % I3_NS, ((g + 1) / I3_NS) & 1u);
                     tc_fence_after();
 #pragma unroll
-                    for (int kk = 0; kk < 8; ++kk) {
-                        const uint32_t off = st * I3_STAGE + (kk >> 2) * I3_SLAB;
-                        umma_bf16(tbase + 256 * b, umma_desc_sw128(sb + I3_OFF_A + off) + 2 * (kk & 3),
-                                  umma_desc_sw128(sb + I3_OFF_B + off) + 2 * (kk & 3), ID_H, (S | kk) != 0);
-                    }
+                    for (int kk = 0; kk < 8; ++kk)
+                        umma_bf16_ts(tbase + I3_TCOL_ACC + 128 * b, tbase + 64 * st + 8 * kk,
+                                     umma_desc_sw128(sb + I3_OFF_B + st * I3_STAGE + (kk >> 2) * I3_SLAB) +
+                                         2 * (kk & 3),
+                                     ID_H, (S | kk) != 0);
                     umma_commit(freed + st);
-                    if (S == I3_STAGES / 2 - 1 && t > 0 && !layer2(b ^ 1u)) { ok = false; break; }
+                    // the previous tile's layers 2 and 3, once its epilogue has had time for each
+                    if (S == 2 && t > 0 && !layer2(b ^ 1u)) { ok = false; break; }
+                    if (S == 5 && t > 0 && !layer3(b ^ 1u)) { ok = false; break; }
                 }
                 if (!ok) break;
                 umma_commit(acc + b);  // layer 1 of this tile
-                if (t > 0 && !layer3(b ^ 1u)) { ok = false; break; }
             }
             if (ok && t > 0) {  // the last tile's layers 2 and 3
                 const uint32_t pb = (t - 1) & 1u;

@@ -55,6 +55,19 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t desc_a, uint
         "l"(desc_a), "l"(desc_b), "r"(idesc), "r"(accumulate));
 }
 
+// The same with A from tensor memory: lane m holds row m, 32-bit column c
+// holds K elements 2c and 2c + 1 (low half first).
+__device__ __forceinline__ void umma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t desc_b, uint32_t idesc,
+                                             uint32_t accumulate) {
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(desc_b), "r"(idesc), "r"(accumulate));
+}
+
 // The mbarrier arrives once every MMA this thread issued before has completed.
 __device__ __forceinline__ void umma_commit(uint64_t* mbar) {
     const uint32_t a = (uint32_t)__cvta_generic_to_shared(mbar);
@@ -86,6 +99,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, unsig
     }
     atomicOr(err, ALP_DEV_ERR_TIMEOUT);
     return false;
+}
+
+// Non-blocking test of the phase with parity `parity`.
+__device__ __forceinline__ bool mbar_test(uint64_t* mbar, uint32_t parity) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(mbar);
+    uint32_t done;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t"
+        "}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return done != 0;
 }
 
 // mbarrier initialisation becomes visible to the async proxy (bulk copies, tensor core).
@@ -140,5 +169,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 #pragma unroll
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
+
+// 8 consecutive 32-bit columns of this thread's lane, from registers
+// (lane 32 * (warp % 4) + laneid, columns [col, col + 8)); tmem_wait_st waits
+// for this thread's stores.
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 }  // namespace alp
