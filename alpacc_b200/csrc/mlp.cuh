@@ -769,7 +769,12 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
     }
     __syncwarp();
     if (warp == 0) tmem_alloc(s_tmem, I3_TMEM_COLS);
-    for (int i = tid; i < 256 * MLP_EMB; i += I3_THREADS) s_emb[i] = w.emb[i];
+    // embedding row b as two 16-byte halves, swapped when bit 2 of b is set, so
+    // that eight gathers of random rows spread over all eight 16-byte bank groups
+    for (int i = tid; i < 256 * MLP_EMB; i += I3_THREADS) {
+        const int eb = i >> 4, d = i & 15;
+        s_emb[(2 * eb + ((d >> 3) ^ ((eb >> 2) & 1))) * 8 + (d & 7)] = w.emb[i];
+    }
     for (int i = tid; i < MLP_H; i += I3_THREADS) { s_b1[i] = w.b1[i]; s_b2[i] = w.b2[i]; }
     for (int i = tid; i < MLP_OUT; i += I3_THREADS) s_b3[i] = w.b3[i];
     tc_fence_before();
@@ -820,8 +825,9 @@ __global__ void __launch_bounds__(I3_THREADS, 1) mlp_infer3_kernel(MlpWeights w,
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     // K values 16 qq .. 16 qq + 15 of K-slab 2 S + h: columns 8 qq .. 8 qq + 7
-                    const uint4* e = reinterpret_cast<const uint4*>(s_emb + quarter_byte(cur, 2 * S + h) * MLP_EMB);
-                    const uint4 lo = e[0], hi = e[1];
+                    const uint32_t eb = quarter_byte(cur, 2 * S + h), sw = (eb >> 2) & 1u;
+                    const uint4* e = reinterpret_cast<const uint4*>(s_emb + eb * MLP_EMB);
+                    const uint4 lo = e[sw], hi = e[sw ^ 1u];
                     const uint32_t v[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
                     tmem_st8(t_lane + 64 * st + 32 * h + 8 * qq, v);
                 }
