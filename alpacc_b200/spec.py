@@ -200,3 +200,37 @@ class BoundaryModel:
         m.params[P_B3 + state] = 1.0
         m.sync_bf16()
         return m
+
+
+def main(argv=None) -> None:
+    """``python -m alpacc_b200.spec --predict N [--kernel 0|1]``: N boundary
+    predictions (random-init weights, json lexer) at evenly spaced positions
+    of a synthetic 64 MiB json document, three calls, and the inference time
+    of the last one (CUDA events).  Kernel 0 is the tcgen05 kernel, 1 the
+    mma.sync kernel; a small fixed workload for profiling either."""
+    import argparse
+    import torch
+    from . import synth, tables
+    ap = argparse.ArgumentParser(prog="python -m alpacc_b200.spec")
+    ap.add_argument("--predict", type=int, required=True)
+    ap.add_argument("--kernel", type=int, default=0, choices=[0, 1])
+    args = ap.parse_args(argv)
+    g = api.Grammar(tables.load("json", "lexer"))
+    g.set_tuning(g.get_tuning()[:3] + [args.kernel])
+    m = BoundaryModel(g, seed=5)
+    size = 64 << 20
+    x = torch.from_numpy(synth.json_doc(size, 8, 3)).to(g.device)
+    pos = torch.arange(1, args.predict + 1, dtype=torch.int64, device=g.device) * (size // (args.predict + 1))
+    for _ in range(2):
+        m.predict(x, pos)
+    g.profile(True)
+    p = m.predict(x, pos)
+    ms = sum(t for k, t in g.timings() if "mlp" in k)
+    g.profile(False)
+    print("predictions %d  kernel %s  %.4f ms  %.1f TFLOP/s  checksum %d" % (
+        args.predict, "tcgen05" if args.kernel == 0 else "mma.sync", ms,
+        args.predict * 2 * (1024 * 128 + 128 * 128 + 128 * 32) / (ms * 1e-3) / 1e12, int(p.sum())))
+
+
+if __name__ == "__main__":
+    main()

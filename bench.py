@@ -60,6 +60,7 @@ sys.path.insert(0, ROOT)
 DOC_BYTES = 256 << 20
 DEPTH = 16
 NODE_BYTES = 8 + 4 + 1 + 8 + 8
+MLP_FLOPS = 2 * (64 * 16 * 128 + 128 * 128 + 128 * 32)  # boundary MLP, per prediction
 SEED = 0xA1FACC00 + 2
 METRIC = "input GB/s lex+parse (json.alp, plain scan, bit-exact)"
 
@@ -71,6 +72,15 @@ def _peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def _bf16_peak():
+    """Dense BF16 tensor-core peak (burst, cuBLAS) in TFLOP/s and its source."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
 
 
 class ClockSampler:
@@ -725,6 +735,7 @@ def run_spec(args, rank: int, world: int, local: int):
     results = {}
     kern_all = []
     best = None
+    mlp_line = None
     clocks = None
     for name, depth, eval_seed in (("json", 8, SEED_LEX), ("sexp", 20, SEED_BATCH + 1)):
         g = api.Grammar(tables.load(name, "lexer"), device=local)
@@ -793,6 +804,22 @@ def run_spec(args, rank: int, world: int, local: int):
         model.lex(x, best[0] if name == "json" else 1024)
         kern_all += [("%s:%s" % (name, k), t) for k, t in g.timings()]
         g.profile(False)
+        if name == "json":
+            # the boundary MLP alone (tcgen05 kernel): one prediction per 1 KiB chunk start
+            P = size // 1024 - 1
+            cpos = torch.arange(1, P + 1, dtype=torch.int64, device=dev) * 1024
+            ts = []
+            for _ in range(5):
+                g.profile(True)
+                model.predict(x, cpos)
+                ts.append(sum(t for k, t in g.timings() if "mlp" in k))
+                g.profile(False)
+            mlp_ms = sorted(ts)[len(ts) // 2]
+            peak, kind = _bf16_peak()
+            tflops = P * MLP_FLOPS / (mlp_ms * 1e-3) / 1e12
+            mlp_line = {"kernel": "mlp_wimg+mlp_infer3 (tcgen05)", "bound": "tensor", "predictions": P,
+                        "flops_per_prediction": MLP_FLOPS, "ms": mlp_ms, "achieved": tflops, "peak": peak,
+                        "peak_kind": kind + " bf16 burst", "unit": "TFLOP/s", "frac": tflops / peak}
         results[name] = res
         del x
     if dist:
@@ -812,6 +839,7 @@ def run_spec(args, rank: int, world: int, local: int):
                   "note": "speculation is a device-resident variant of alp_lex; see the lex workload for e2e"},
                  clocks, units={"n": size, "m": M}, parse_layout=False)
     line["path_roofline"]["scope"] = "alp_lex_speculative: input bytes + 20 B per token, over the step time"
+    line["mlp_roofline"] = mlp_line
     print(json.dumps(line), flush=True)
 
 
