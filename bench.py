@@ -162,6 +162,13 @@ def make_doc(seed: int, size: int) -> np.ndarray:
     return synth.json_doc(size, DEPTH, seed)
 
 
+def _sha256(a: np.ndarray) -> str:
+    """SHA-256 of a generated input (outside the timed region), so that a run's
+    synthetic workload can be reproduced and compared byte for byte."""
+    import hashlib
+    return hashlib.sha256(memoryview(np.ascontiguousarray(a)).cast("B")).hexdigest()
+
+
 def _host_threads() -> int:
     try:
         n = len(os.sched_getaffinity(0))
@@ -456,7 +463,8 @@ def run_lex(args, rank: int, world: int, local: int):
                  {"workload": "json.alp lexer only, one %d MiB synthetic JSON document per GPU (depth <= 8), "
                               "bytes -> (u32 id, i64 start, i64 end) tokens" % (size >> 20),
                   "doc_bytes": size, "tokens": M, "tokens_per_byte": M / size, "parallelism": "replicas",
-                  "l2": "inputs larger than L2 (no flush needed)"},
+                  "l2": "inputs larger than L2 (no flush needed)", "seed": SEED_LEX,
+                  "input_sha256": _sha256(doc)},
                  size + 20 * M, kern,
                  {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": size,
                   "d2h_bytes_per_step": 20 * M, "ms_per_step": ms_e2e,
@@ -977,7 +985,8 @@ def main():
         "config": {"workload": "json.alp full lex+parse, one %d MiB synthetic JSON document per GPU "
                                "(depth <= %d), bytes -> preorder tree" % (args.doc_mib, DEPTH),
                    "doc_bytes": size, "nodes": N, "nodes_per_byte": N / size, "parallelism": "replicas",
-                   "l2": "inputs larger than L2 (no flush needed)",
+                   "l2": "inputs larger than L2 (no flush needed)", "seed": SEED,
+                   "input_sha256": _sha256(doc),
                    "tuning": {"config": tuning["config"], "tile_shape": list(tuning["tile_shape"]),
                               "candidates_ms": [[k, v, round(t, 4)] for k, v, t in tuning["timings"]]}},
         "roofline": roof,
