@@ -74,6 +74,7 @@ struct alp_ctx {
     long long last_tokens = 0;            // counts of the last call, for alp_ctx_info
     long long last_positions = 0;
     long long last_brackets = 0;
+    long long last_kept = 0;              // brackets left for the search after closing adjacent pairs
     DevBuf mlp[16];                       // MLP training activations
     DevBuf spec[16];                      // speculative lexer chunk arrays
     // host-input token streams (alp_lex_host_stream): copy streams, events,
@@ -767,9 +768,11 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     }
     mark(ctx, "scan_tiles_reduce+scan_tiles");
     if ((rc = read_result(ctx, d_res))) return rc;
-    const long long N = ctx->h_res->aux[0], B = ctx->h_res->aux[1];
+    // nodes, brackets, and brackets left after closing adjacent pairs
+    const long long N = ctx->h_res->aux[0], B = ctx->h_res->aux[1], K = ctx->h_res->aux[6];
     ctx->last_positions = L;
     ctx->last_brackets = B;
+    ctx->last_kept = K;
     if (N > 0xffffffffLL || B > 0xffffffffLL) return fail(ctx, ALP_ERR_ARG, "tree too large");
     if (ctx_out) {
         if ((rc = grow(ctx, ctx->out[3], N * 8 + 8)) || (rc = grow(ctx, ctx->out[4], N * 4 + 8)) ||
@@ -785,8 +788,8 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
         *n_node = N;
         return fail(ctx, ALP_ERR_CAPACITY, "node buffer too small (%lld needed)", (long long)N);
     }
-    if ((rc = grow(ctx, ctx->tmp[T_VBUF], N * 4 + 8)) || (rc = grow(ctx, ctx->tmp[T_BRBUF], B * 4 + 8)) ||
-        (rc = grow(ctx, ctx->tmp[T_DSBUF], B * 4 + 8)))
+    if ((rc = grow(ctx, ctx->tmp[T_VBUF], N * 4 + 8)) || (rc = grow(ctx, ctx->tmp[T_BRBUF], K * 4 + 8)) ||
+        (rc = grow(ctx, ctx->tmp[T_DSBUF], K * 4 + 8)))
         return rc;
     a.tag = o->tag;
     a.kind = o->kind;
@@ -797,7 +800,7 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     a.brbuf = (uint32_t*)ctx->tmp[T_BRBUF].p;
     a.dsbuf = (int32_t*)ctx->tmp[T_DSBUF].p;
     a.cap_nodes = N;
-    a.cap_brs = B;
+    a.cap_brs = K;
     const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
     if (sm2 > 220 * 1024) return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
     CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
@@ -815,7 +818,7 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     if (want_tree) {
         if ((rc = run_ple(ctx, a.vbuf, N, nullptr, o->parent, T_N_TMIN, a.node_off, nd, dvalid, d_res))) return rc;
     }
-    if ((rc = run_ple(ctx, a.dsbuf, B, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res))) return rc;
+    if ((rc = run_ple(ctx, a.dsbuf, K, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res))) return rc;
     if ((rc = read_result(ctx, d_res))) return rc;
     *n_node = N;
     return ALP_OK;
@@ -1038,10 +1041,10 @@ int alp_set_stream(alp_ctx* ctx, void* stream) {
 
 int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out) {
     if (!ctx || !out) return ALP_ERR_ARG;
-    int64_t v[11] = {ctx->has_lexer, ctx->has_parser, ctx->has_parser ? ctx->ph.n_terms : ctx->n_terms,
+    int64_t v[12] = {ctx->has_lexer, ctx->has_parser, ctx->has_parser ? ctx->ph.n_terms : ctx->n_terms,
                      ctx->ph.n_prods, ctx->ph.q, ctx->ph.k, ctx->ph.max_prods, ctx->ph.max_brackets,
-                     ctx->last_tokens, ctx->last_positions, ctx->last_brackets};
-    for (int i = 0; i < n_out && i < 11; ++i) out[i] = v[i];
+                     ctx->last_tokens, ctx->last_positions, ctx->last_brackets, ctx->last_kept};
+    for (int i = 0; i < n_out && i < 12; ++i) out[i] = v[i];
     return ALP_OK;
 }
 
@@ -2355,7 +2358,7 @@ __global__ void batch_sizes_kernel(AlpResult* res, long long n_docs, long long* 
     res->count = 0;
     res->valid = 1;
     res->error = 0;
-    for (int i = 0; i < 6; ++i) res->aux[i] = 0;
+    for (int i = 0; i < 8; ++i) res->aux[i] = 0;
 }
 
 // counts[0] nodes, [1] brackets, [2] positions, [3] ALP_DEV_ERR_* bits
@@ -2439,7 +2442,7 @@ int parse_positions_dev(alp_ctx* ctx, long long Lcap, const long long* dL, long 
     if ((rc = run_ple(ctx, a.vbuf, cap_nodes, nullptr, o.parent, T_N_TMIN, a.node_off, nd, dvalid, d_res,
                       &d_res->aux[0])))
         return rc;
-    return run_ple(ctx, a.dsbuf, cap_brs, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res, &d_res->aux[1]);
+    return run_ple(ctx, a.dsbuf, cap_brs, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res, &d_res->aux[6]);
 }
 
 }  // namespace

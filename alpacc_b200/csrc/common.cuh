@@ -23,7 +23,7 @@ struct __align__(16) AlpResult {
     long long count;        // tokens or nodes written
     int valid;              // 1 accepted, 0 rejected
     unsigned int error;     // ALP_DEV_ERR_* bits
-    long long aux[6];       // kernel-specific extras (counts for sizing, etc.)
+    long long aux[8];       // kernel-specific extras (counts for sizing, etc.)
 };
 
 // ---- status words ---------------------------------------------------------

@@ -227,11 +227,11 @@ struct __align__(16) PosSums {
     uint32_t terms;   // terminal productions since the last ⊢
     uint32_t heads;   // ⊢ positions
     int32_t hpos;     // position of the last ⊢ (-1: none)
-    uint32_t pad;
+    uint32_t cls;     // bracket pairs closed between a position and the one before it
 };
 
 __device__ __forceinline__ void possums_zero(PosSums& s) {
-    s.nodes = 0; s.brs = 0; s.depth = 0; s.v = 0; s.terms = 0; s.heads = 0; s.hpos = -1; s.pad = 0;
+    s.nodes = 0; s.brs = 0; s.depth = 0; s.v = 0; s.terms = 0; s.heads = 0; s.hpos = -1; s.cls = 0;
 }
 __device__ __forceinline__ PosSums ps_combine(const PosSums& a, const PosSums& b) {
     PosSums r;
@@ -243,7 +243,7 @@ __device__ __forceinline__ PosSums ps_combine(const PosSums& a, const PosSums& b
     r.v = h ? b.v : a.v + b.v;
     r.terms = h ? b.terms : a.terms + b.terms;
     r.hpos = h ? b.hpos : a.hpos;
-    r.pad = 0;
+    r.cls = a.cls + b.cls;
     return r;
 }
 __device__ __forceinline__ PosSums ps_shfl_up(const PosSums& x, int d) {
@@ -255,7 +255,7 @@ __device__ __forceinline__ PosSums ps_shfl_up(const PosSums& x, int d) {
     r.terms = __shfl_up_sync(ALP_FULL_MASK, x.terms, d);
     r.heads = __shfl_up_sync(ALP_FULL_MASK, x.heads, d);
     r.hpos = __shfl_up_sync(ALP_FULL_MASK, x.hpos, d);
-    r.pad = 0;
+    r.cls = __shfl_up_sync(ALP_FULL_MASK, x.cls, d);
     return r;
 }
 // inclusive warp scan (lanes in order); a warp without a ⊢ needs plain sums
@@ -268,7 +268,8 @@ __device__ __forceinline__ PosSums ps_warp_scan(PosSums x, int lane) {
             const int32_t od = __shfl_up_sync(ALP_FULL_MASK, x.depth, d);
             const int32_t ov = __shfl_up_sync(ALP_FULL_MASK, x.v, d);
             const uint32_t ot = __shfl_up_sync(ALP_FULL_MASK, x.terms, d);
-            if (lane >= d) { x.nodes += on; x.brs += ob; x.depth += od; x.v += ov; x.terms += ot; }
+            const uint32_t oc = __shfl_up_sync(ALP_FULL_MASK, x.cls, d);
+            if (lane >= d) { x.nodes += on; x.brs += ob; x.depth += od; x.v += ov; x.terms += ot; x.cls += oc; }
         }
         return x;
     }
@@ -290,6 +291,19 @@ __device__ __forceinline__ PosSums ps_elem(const PairInfo* s_pi, uint16_t p, boo
     return e;
 }
 
+// Brackets closed between adjacent positions: a pair's brackets are its
+// rights, then its lefts, so position p's first rights close position p-1's
+// top lefts, min(lefts of p-1, rights of p) of them, unless p starts a
+// document or either has no pair.
+__device__ __forceinline__ uint32_t pair_lefts(const PairInfo& p) {
+    return (uint32_t)(((int32_t)p.n_br + (int32_t)p.d_depth) >> 1);
+}
+__device__ __forceinline__ uint32_t adj_closed(const PairInfo* s_pi, uint32_t prev, uint32_t cur, bool head) {
+    if (head || prev == NO_PAIR || cur == NO_PAIR) return 0;
+    const PairInfo& b = s_pi[cur];
+    return min(pair_lefts(s_pi[prev]), (uint32_t)b.n_br - pair_lefts(b));
+}
+
 struct ParseArgs {
     ParseTables t;
     const uint16_t* P;          // [L] ⊢ tokens ⊣ per document: terminal ids
@@ -299,7 +313,7 @@ struct ParseArgs {
     long long n_docs;
     uint16_t* pid;              // [L] pair id per position
     PosSums* tile_sums;         // [tiles] K1 output, scanned in place to exclusive prefixes
-    AlpResult* res;             // aux[0..5] totals
+    AlpResult* res;             // aux: totals (0 nodes, 1 brackets, 6 brackets kept, 7 adjacent pairs closed)
     // K2 outputs
     uint32_t* tag;
     uint8_t* kind;
@@ -308,8 +322,9 @@ struct ParseArgs {
     int32_t* vbuf;              // node values exscan(arity-1), per document
     uint32_t* brbuf;            // bracket symbol | left<<31
     int32_t* dsbuf;             // bracket depth value (before a left, after a right), per document
+                                //   (the brackets kept after closing adjacent pairs, aux[6] of them)
     long long* node_off;        // [n_docs + 1] first node of each document
-    long long* br_off;          // [n_docs + 1] first bracket of each document
+    long long* br_off;          // [n_docs + 1] first kept bracket of each document
     uint8_t* doc_valid;         // [n_docs] cleared on rejection
     int subst_terminals;        // 1: wrapper productions become terminal nodes (parse_int); 0: production ids
     long long cap_nodes;
@@ -326,7 +341,7 @@ __device__ __forceinline__ uint32_t pos_term(const ParseArgs& a, long long i) {
 // ---------------------------------------------------------------------------
 // The pair kernel's shared memory: the pair infos, then the window of terminals.
 __host__ __device__ inline size_t pairs_smem_bytes(int n_pairs, int window) {
-    return sizeof(PairInfo) * (size_t)n_pairs + ((size_t)PP_TILE + window) * 4;
+    return sizeof(PairInfo) * (size_t)n_pairs + ((size_t)PP_TILE + window + 1) * 4;
 }
 
 // QT, KT > 0: the lookback and lookahead fixed at compile time (window loops
@@ -350,43 +365,79 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
     const long long n_tiles = (a.L + PP_TILE - 1) / PP_TILE;
     for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const long long base = tile * PP_TILE;
-    const int span = PP_TILE + W;  // window [base - q, base + PP_TILE + k)
+    const int span = PP_TILE + W + 1;  // window [base - q - 1, base + PP_TILE + k)
     __syncthreads();  // the previous tile is done with s_term and s_w
-    for (int i = tid; i < span; i += PP_THREADS) s_term[i] = pos_term(a, base - q + i);
+    for (int i = tid; i < span; i += PP_THREADS) s_term[i] = pos_term(a, base - q - 1 + i);
     __syncthreads();
     const uint32_t SL = a.t.start, SR = a.t.end, EMPTY = a.t.empty;
-    PosSums acc;
-    possums_zero(acc);
+    // the pair id at tile-local position pl (-1: the position before the tile);
+    // s_term[pl + 1 + jj] is position base + pl - q + jj
+    auto pair_at = [&](int pl, bool& head) -> uint16_t {
+        const int o = pl + 1;
+        const uint32_t c = s_term[o + q];
+        head = c == SL;
+        // a window never reaches past its document's ⊢ (left) or ⊣ (right)
+        uint32_t x = c * s_pow[q];
+        bool ok = c != SL;
+#pragma unroll
+        for (int jj = q - 1; jj >= 0; --jj) {
+            const uint32_t t = s_term[o + jj];
+            x += (ok ? t : EMPTY) * s_pow[jj];
+            ok = ok && t != SL;
+        }
+        ok = c != SR;
+#pragma unroll
+        for (int jj = q + 1; jj < W; ++jj) {
+            const uint32_t t = s_term[o + jj];
+            x += (ok ? t : EMPTY) * s_pow[jj];
+            ok = ok && t != SR;
+        }
+        return __ldg(&a.t.key_index[x]);
+    };
     uint16_t ids[PP_ITEMS];
+    uint32_t hb = 0;
 #pragma unroll
     for (int j = 0; j < PP_ITEMS; ++j) {
         const long long i = base + tid * PP_ITEMS + j;
         uint16_t p = NO_PAIR;
         bool head = false;
-        if (i < a.L) {
-            const int o = tid * PP_ITEMS + j;  // s_term[o + jj] is position i - q + jj
-            const uint32_t c = s_term[o + q];
-            head = c == SL;
-            // a window never reaches past its document's ⊢ (left) or ⊣ (right)
-            uint32_t x = c * s_pow[q];
-            bool ok = c != SL;
-#pragma unroll
-            for (int jj = q - 1; jj >= 0; --jj) {
-                const uint32_t t = s_term[o + jj];
-                x += (ok ? t : EMPTY) * s_pow[jj];
-                ok = ok && t != SL;
-            }
-            ok = c != SR;
-#pragma unroll
-            for (int jj = q + 1; jj < W; ++jj) {
-                const uint32_t t = s_term[o + jj];
-                x += (ok ? t : EMPTY) * s_pow[jj];
-                ok = ok && t != SR;
-            }
-            p = __ldg(&a.t.key_index[x]);
-        }
+        if (i < a.L) p = pair_at(tid * PP_ITEMS + j, head);
         ids[j] = p;
-        if (i < a.L) acc = ps_combine(acc, ps_elem(s_pi, p, head, i));
+        if (head) hb |= 1u << j;
+    }
+    // the pair before this thread's first position: the previous lane's last,
+    // or (a warp's first lane) computed from the window, which starts one early
+    uint32_t prev = __shfl_up_sync(ALP_FULL_MASK, (uint32_t)ids[PP_ITEMS - 1], 1);
+    if (lane == 0) {
+        const long long ip = base + (long long)tid * PP_ITEMS - 1;
+        bool h;
+        prev = (ip >= 0 && ip < a.L) ? (uint32_t)pair_at(tid * PP_ITEMS - 1, h) : (uint32_t)NO_PAIR;
+    }
+    PosSums acc;
+    possums_zero(acc);
+    {
+        uint32_t lprev = prev != NO_PAIR ? pair_lefts(s_pi[prev]) : 0u;  // the previous position's lefts
+        bool pv = prev != NO_PAIR;
+#pragma unroll
+        for (int j = 0; j < PP_ITEMS; ++j) {
+            const long long i = base + tid * PP_ITEMS + j;
+            if (i < a.L) {
+                const bool head = (hb >> j) & 1u;
+                PosSums e;
+                possums_zero(e);
+                uint32_t nl = 0;
+                if (ids[j] != NO_PAIR) {
+                    const PairInfo& pi = s_pi[ids[j]];
+                    e.nodes = pi.n_prod; e.brs = pi.n_br; e.depth = pi.d_depth; e.v = pi.d_v; e.terms = pi.n_term;
+                    nl = pair_lefts(pi);
+                    if (!head && pv) e.cls = min(lprev, (uint32_t)pi.n_br - nl);  // adj_closed
+                }
+                if (head) { e.heads = 1; e.hpos = (int32_t)i; }
+                acc = ps_combine(acc, e);
+                lprev = nl;
+                pv = ids[j] != NO_PAIR;
+            }
+        }
     }
     const long long i0 = base + tid * PP_ITEMS;
     if (i0 + PP_ITEMS <= a.L && ((i0 & 3) == 0)) {
@@ -476,7 +527,7 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
             last.terms = __shfl_sync(ALP_FULL_MASK, inc.terms, 31);
             last.heads = __shfl_sync(ALP_FULL_MASK, inc.heads, 31);
             last.hpos = __shfl_sync(ALP_FULL_MASK, inc.hpos, 31);
-            last.pad = 0;
+            last.cls = __shfl_sync(ALP_FULL_MASK, inc.cls, 31);
             carry = ps_combine(carry, last);
         }
         if (lane == 0) s_carry = carry;
@@ -503,16 +554,17 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
         __syncthreads();
         if (tid == ST_CHUNK - 1) s_carry = ps_combine(pre, inc);
         if (warp == 0) {
-            // node and bracket totals in 64 bits, so that a total past 2^32 is seen
-            unsigned long long tn = 0, tb = 0;
+            // node, bracket and closed-pair totals in 64 bits, so that a total past 2^32 is seen
+            unsigned long long tn = 0, tb = 0, tc = 0;
             for (long long b = lane; b <= chunk; b += 32) {
-                if (b < chunk) { tn += chunk_sums[b].nodes; tb += chunk_sums[b].brs; }
+                if (b < chunk) { tn += chunk_sums[b].nodes; tb += chunk_sums[b].brs; tc += chunk_sums[b].cls; }
             }
             for (int d = 16; d >= 1; d >>= 1) {
                 tn += __shfl_down_sync(ALP_FULL_MASK, tn, d);
                 tb += __shfl_down_sync(ALP_FULL_MASK, tb, d);
+                tc += __shfl_down_sync(ALP_FULL_MASK, tc, d);
             }
-            if (lane == 0) { res->aux[0] = (long long)tn; res->aux[1] = (long long)tb; }
+            if (lane == 0) { res->aux[0] = (long long)tn; res->aux[1] = (long long)tb; res->aux[7] = (long long)tc; }
         }
         __syncthreads();
         if (tid == 0) {
@@ -521,12 +573,14 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
             const PosSums own = chunk_sums[chunk];
             res->aux[0] += own.nodes;
             res->aux[1] += own.brs;
+            res->aux[7] += own.cls;
             res->aux[2] = tot.depth;
             res->aux[3] = tot.v;
             res->aux[4] = (long long)tot.terms;
             res->aux[5] = (long long)tot.heads;
+            res->aux[6] = res->aux[1] - 2 * res->aux[7];  // brackets left for the search
             node_off[n_docs] = res->aux[0];
-            br_off[n_docs] = res->aux[1];
+            br_off[n_docs] = res->aux[6];
         }
     }
 }
@@ -541,17 +595,27 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
 // below zero, depth zero at ⊣).  Nodes are then produced in windows of EX_WIN:
 // each thread marks its positions as the owners of their nodes in the window
 // (16-bit position indices), and the block emits the window one node per
-// thread, in order, with coalesced stores.  Brackets the same way.  No thread
-// walks another position's productions, so warps stay converged whatever the
-// sizes of the pairs.
+// thread, in order, with coalesced stores.  No thread walks another
+// position's productions, so warps stay converged whatever the sizes of the
+// pairs.
+//
+// Brackets: a pair's brackets are its rights, then its lefts (the stack it
+// pops, then the one it pushes), so a position's first rights close the
+// previous position's top lefts, min(lefts before, rights here) of them, in
+// the same document.  Those pairs are checked here (equal symbols) and
+// dropped: removing matched adjacent pairs leaves every other bracket's
+// match (the previous smaller-or-equal of futhark/parser.fut:153-184) as it
+// was.  The rest -- about half of json's brackets -- is written by the
+// position's own thread, at the front of the tile's bracket range, for the
+// search that follows.
 // ---------------------------------------------------------------------------
-constexpr int EX_WIN = 8192;                     // nodes or brackets per window
+constexpr int EX_WIN = 8192;                     // nodes per window
 constexpr int EX_U = 2;                          // nodes a thread emits at once (token span loads in flight)
 constexpr uint32_t EX_NO_TOKEN = 0xffffffffu;
-// per position: a node record and a bracket base, one unused slot after every
-// thread's four positions, so that the 32 lanes of a warp writing their first
-// position (64 bytes apart without the pad) hit distinct banks
-constexpr size_t EX_POS_BYTES = (size_t)PP_TILE * 5 / 4 * 20;
+// per position: a node record, one unused slot after every thread's four
+// positions, so that the 32 lanes of a warp writing their first position
+// (64 bytes apart without the pad) hit distinct banks
+constexpr size_t EX_POS_BYTES = (size_t)PP_TILE * 5 / 4 * 16;
 __device__ __forceinline__ int ex_slot(int pl) { return pl + (pl >> 2); }
 
 // pair infos (20 bytes each), then the 8-byte records from a 16-byte boundary
@@ -594,10 +658,9 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     // node, so that node g reads record g + x; y = exscan(arity - 1) before it;
     // z = token index of its first terminal production; w = bracket depth before it
     int4* s_pos = reinterpret_cast<int4*>(smem + expand_tables_bytes(a.t.n_pairs, a.t.n_pseq, a.t.n_stack));
-    int32_t* s_sbd = reinterpret_cast<int32_t*>(s_pos + PP_TILE * 5 / 4);  // first stack record minus first bracket
-    uint16_t* s_own = reinterpret_cast<uint16_t*>(s_sbd + PP_TILE * 5 / 4);  // [EX_WIN] owner of each node / bracket
+    uint16_t* s_own = reinterpret_cast<uint16_t*>(s_pos + PP_TILE * 5 / 4);  // [EX_WIN] owner of each node
     __shared__ PosSums s_w[PP_THREADS / 32];
-    __shared__ uint32_t s_tn, s_tb;
+    __shared__ uint32_t s_tn;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (a.dL) a.L = *a.dL;
     for (int i = tid; i < a.t.n_pairs * (int)(sizeof(PairInfo) / 4); i += PP_THREADS)
@@ -628,11 +691,44 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             }
         }
         if (tile + gridDim.x < n_tiles) ex_words(a, i0 + (long long)gridDim.x * PP_TILE, nw, nt);
+        // ---- pairs closed between each position and the one before it (adj_closed),
+        // with the previous lefts carried along; cl[PP_ITEMS] is the next thread's cl[0]
+        const uint32_t up = __shfl_up_sync(ALP_FULL_MASK, (uint32_t)ids[PP_ITEMS - 1], 1);
+        const uint32_t prev_id = lane > 0 ? up : (i0 > 0 && i0 - 1 < a.L ? (uint32_t)a.pid[i0 - 1] : NO_PAIR);
+        uint32_t cl[PP_ITEMS + 1];
         PosSums mine;
         possums_zero(mine);
+        {
+            uint32_t lprev = prev_id != NO_PAIR ? pair_lefts(s_pi[prev_id]) : 0u;
+            bool pv = prev_id != NO_PAIR;
 #pragma unroll
-        for (int j = 0; j < PP_ITEMS; ++j)
-            if (i0 + j < a.L) mine = ps_combine(mine, ps_elem(s_pi, ids[j], (hm >> j) & 1u, i0 + j));
+            for (int j = 0; j < PP_ITEMS; ++j) {
+                cl[j] = 0;
+                if (i0 + j < a.L) {
+                    const bool head = (hm >> j) & 1u;
+                    PosSums e;
+                    possums_zero(e);
+                    uint32_t nl = 0;
+                    if (ids[j] != NO_PAIR) {
+                        const PairInfo& pi = s_pi[ids[j]];
+                        e.nodes = pi.n_prod; e.brs = pi.n_br; e.depth = pi.d_depth; e.v = pi.d_v; e.terms = pi.n_term;
+                        nl = pair_lefts(pi);
+                        if (!head && pv) e.cls = min(lprev, (uint32_t)pi.n_br - nl);
+                    }
+                    if (head) { e.heads = 1; e.hpos = (int32_t)(i0 + j); }
+                    cl[j] = e.cls;
+                    mine = ps_combine(mine, e);
+                    lprev = nl;
+                    pv = ids[j] != NO_PAIR;
+                }
+            }
+            const uint32_t dn = __shfl_down_sync(ALP_FULL_MASK, cl[0], 1);
+            cl[PP_ITEMS] = dn;
+            if (lane == 31) {  // the next warp's first position
+                const long long n0 = i0 + PP_ITEMS;
+                cl[PP_ITEMS] = n0 < a.L ? adj_closed(s_pi, ids[PP_ITEMS - 1], a.pid[n0], (uint32_t)a.P[n0] == SL) : 0u;
+            }
+        }
         const PosSums inc = ps_warp_scan(mine, lane);
         PosSums ex = ps_shfl_up(inc, 1);
         if (lane == 0) possums_zero(ex);
@@ -645,11 +741,14 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             PosSums we = ps_shfl_up(wi, 1);
             if (lane == 0) possums_zero(we);
             if (lane < PP_THREADS / 32) s_w[lane] = we;
-            if (lane == PP_THREADS / 32 - 1) { s_tn = wi.nodes; s_tb = wi.brs; }
+            if (lane == PP_THREADS / 32 - 1) s_tn = wi.nodes;
         }
         __syncthreads();
         // ---- per position: records and the one-position document rules --------
-        uint32_t nof[PP_ITEMS], bof[PP_ITEMS], cnt[PP_ITEMS];  // first node, first bracket (tile-local), n_prod | n_br << 16
+        uint32_t nof[PP_ITEMS], cnt[PP_ITEMS];  // first node (tile-local), n_prod
+        // brackets: the depth before each position and where its kept brackets go
+        uint32_t kof[PP_ITEMS];
+        int32_t depj[PP_ITEMS];
         {
             PosSums run = ps_combine(ps_combine(tp, s_w[warp]), ex);  // before this thread's first position
 #pragma unroll
@@ -657,18 +756,33 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                 const long long i = i0 + j;
                 const int pl = tid * PP_ITEMS + j;
                 nof[j] = run.nodes - tp.nodes;
-                bof[j] = 0;
                 cnt[j] = 0;
+                kof[j] = 0;
+                depj[j] = 0;
                 if (i < a.L) {
                     const bool head = (hm >> j) & 1u;
                     const int32_t dep = head ? 0 : run.depth;
                     const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
                     const bool dok = doc >= 0 && doc < a.n_docs;
+                    depj[j] = dep;
+                    // the previous position's top lefts against this position's first rights
+                    const uint32_t pid_prev = j == 0 ? prev_id : (uint32_t)ids[j - 1];
+                    const uint32_t m = cl[j];
+                    if (m) {
+                        const PairInfo pa = s_pi[pid_prev], pb = s_pi[ids[j]];
+                        bool bad = false;
+                        for (uint32_t t = 0; t < m; ++t)
+                            bad |= ((s_srec[pa.stack_begin + pa.n_br - 1 - t].x ^ s_srec[pb.stack_begin + t].x) &
+                                    0x7fffffffu) != 0;
+                        if (bad && dok) a.doc_valid[doc] = 0;  // a right and its left differ
+                    }
+                    // brackets kept before this position's: all before it, less both sides of
+                    // every closed pair before it, less the lefts it closes here
+                    kof[j] = run.brs - 2u * run.cls - m;
                     if (head && dok) {
                         a.node_off[doc] = (long long)run.nodes;
-                        a.br_off[doc] = (long long)run.brs;
+                        a.br_off[doc] = (long long)kof[j];
                     }
-                    bof[j] = run.brs - tp.brs;
                     PosSums e;
                     possums_zero(e);
                     if (ids[j] == NO_PAIR) {
@@ -678,18 +792,36 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                         s_pos[ex_slot(pl)] = make_int4((int32_t)pi.prod_begin - (int32_t)nof[j], head ? 0 : run.v,
                                               (int32_t)((uint32_t)(head ? i : run.hpos) + 1u + (head ? 0u : run.terms)),
                                               dep);
-                        s_sbd[ex_slot(pl)] = (int32_t)pi.stack_begin - (int32_t)bof[j];
                         if (dep + (int32_t)pi.min_ds < 0 && dok) a.doc_valid[doc] = 0;  // depth below zero
                         e.nodes = pi.n_prod; e.brs = pi.n_br; e.depth = pi.d_depth; e.v = pi.d_v; e.terms = pi.n_term;
                         cnt[j] = (uint32_t)pi.n_prod | ((uint32_t)pi.n_br << 16);
                     }
                     if (((em >> j) & 1u) && (dep + e.depth != 0) && dok) a.doc_valid[doc] = 0;  // unbalanced at the end
                     if (head) { e.heads = 1; e.hpos = (int32_t)i; }
+                    e.cls = m;
                     run = ps_combine(run, e);
                 }
             }
         }
-        const uint32_t tn = s_tn, tb = s_tb;
+        // ---- the kept brackets, each position's by its own thread
+#pragma unroll
+        for (int j = 0; j < PP_ITEMS; ++j) {
+            const uint32_t nb = cnt[j] >> 16;
+            if (nb) {
+                const PairInfo pi = s_pi[ids[j]];
+                const uint32_t hi = nb - cl[j + 1];
+                for (uint32_t r = cl[j]; r < hi; ++r) {
+                    const uint2 rec = s_srec[pi.stack_begin + r];
+                    const int32_t before = depj[j] + (int32_t)(int16_t)(rec.y & 0xffffu);
+                    const unsigned long long g = (unsigned long long)kof[j] + (r - cl[j]);
+                    if (g < (unsigned long long)a.cap_brs) {
+                        a.brbuf[g] = rec.x;
+                        a.dsbuf[g] = (rec.x >> 31) ? before : before - 1;  // after a right bracket, before a left
+                    }
+                }
+            }
+        }
+        const uint32_t tn = s_tn;
         // ---- nodes, one window at a time ---------------------------------------------
         for (uint32_t w0 = 0; w0 < tn; w0 += EX_WIN) {
             const uint32_t wn = min(tn - w0, (uint32_t)EX_WIN);
@@ -735,29 +867,6 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                         a.nstart[g] = st[u];
                         a.nend[g] = en[u];
                     }
-                }
-            }
-            __syncthreads();
-        }
-        // ---- brackets, one window at a time ------------------------------------------
-        for (uint32_t w0 = 0; w0 < tb; w0 += EX_WIN) {
-            const uint32_t wn = min(tb - w0, (uint32_t)EX_WIN);
-#pragma unroll
-            for (int j = 0; j < PP_ITEMS; ++j) {
-                const uint32_t b = bof[j], n = cnt[j] >> 16;
-                const uint32_t lo = max(b, w0), hi = min(b + n, w0 + wn);
-                for (uint32_t x = lo; x < hi; ++x) s_own[x - w0] = (uint16_t)(tid * PP_ITEMS + j);
-            }
-            __syncthreads();
-            for (uint32_t e = tid; e < wn; e += PP_THREADS) {
-                const uint32_t g = w0 + e;
-                const int pl = s_own[e];
-                const uint2 rec = s_srec[(int32_t)g + s_sbd[ex_slot(pl)]];
-                const int32_t before = s_pos[ex_slot(pl)].w + (int32_t)(int16_t)(rec.y & 0xffffu);
-                const uint32_t bg = tp.brs + g;
-                if ((long long)bg < a.cap_brs) {
-                    a.brbuf[bg] = rec.x;
-                    a.dsbuf[bg] = (rec.x >> 31) ? before : before - 1;  // after a right bracket, before a left
                 }
             }
             __syncthreads();
@@ -926,8 +1035,9 @@ __global__ void __launch_bounds__(PT, 1024 / PT) ple_tile_kernel(PleArgs a) {
                 if (!(my_sym >> 31)) {  // rights ask; lefts do not
                     if (ans >= 0) {
                         const uint32_t l = (uint32_t)s_aux[tid * (PI + 1) + (ans - tid * PI)];
-                        if (base + ans < dbase || (l & 0x7fffffffu) != (my_sym & 0x7fffffffu) || !(l >> 31))
+                        if (base + ans < dbase || (l & 0x7fffffffu) != (my_sym & 0x7fffffffu) || !(l >> 31)) {
                             a.seg_valid[doc] = 0;
+                        }
                     } else {
                         unres |= 1u << j;
                     }
@@ -990,8 +1100,9 @@ __global__ void __launch_bounds__(PT, 1024 / PT) ple_tile_kernel(PleArgs a) {
                     if (brackets) {
                         const uint32_t l = (uint32_t)s_aux[ple_pad<PI>(ans)];
                         const uint32_t r = (uint32_t)s_aux[ple_pad<PI>(e)];
-                        if (base + ans < dqb || (l & 0x7fffffffu) != (r & 0x7fffffffu) || !(l >> 31))
+                        if (base + ans < dqb || (l & 0x7fffffffu) != (r & 0x7fffffffu) || !(l >> 31)) {
                             a.seg_valid[dq] = 0;
+                        }
                     } else {
                         s_aux[ple_pad<PI>(e)] = (int32_t)(base + ans - dqb);
                     }
@@ -1153,7 +1264,9 @@ __global__ void ple_escape_kernel(EscArgs a) {
         const long long doc = seg_upper(a.seg_off, 0, a.n_seg - 1, g);
         const long long dbase = a.seg_off[doc];
         if (a.sym) {
-            if (ans < dbase) a.seg_valid[doc] = 0;
+            if (ans < dbase) {
+                a.seg_valid[doc] = 0;
+            }
             else {
                 const uint32_t l = a.sym[ans], rr = a.sym[g];
                 if (!(l >> 31) || (l & 0x7fffffffu) != (rr & 0x7fffffffu)) a.seg_valid[doc] = 0;

@@ -254,14 +254,16 @@ def _traffic_table():
 def _kernel_alg_bytes(name, units, parse_layout=True):
     """Algorithmic bytes of one launch: the inputs a kernel must read once and
     the outputs it must write once for its part of the path.  units: n (input
-    bytes), m (tokens), L (parser positions), N (nodes), B (brackets)."""
+    bytes), m (tokens), L (parser positions), N (nodes), B (brackets), K
+    (brackets left after the pairs closed between adjacent positions)."""
     n, m, L, N, B = (units.get(k, 0) for k in ("n", "m", "L", "N", "B"))
+    K = units.get("K", B)
     c = (n + 31) // 32
     tok = 10 if parse_layout else 20
     table = {
-        "parse_expand_kernel": 4 * L + 8 * m + 25 * N + 8 * B,   # ids in, spans in, node fields + brackets out
+        "parse_expand_kernel": 4 * L + 8 * m + 25 * N + 8 * K,   # ids in, spans in, node fields + kept brackets out
         "ple_tile_kernel(nodes)": 12 * N,                      # values in, parents out
-        "ple_tile_kernel(brackets)": 8 * B,                    # depth values and symbols in
+        "ple_tile_kernel(brackets)": 8 * K,                    # kept brackets' depth values and symbols in
         "lex3_emit_kernel": n + 3 * c + tok * m,               # bytes, chunk states and counts in, tokens out
         "lex3_fold_kernel": n + 2 * c,                         # bytes in, chunk endomorphisms out
         "lex3_count_kernel": n + 3 * c,                        # bytes, chunk states in, counts out
@@ -271,7 +273,7 @@ def _kernel_alg_bytes(name, units, parse_layout=True):
 
 
 def _unit_count(unit, units):
-    return {"node": units.get("N", 0), "bracket": units.get("B", 0), "byte": units.get("n", 0),
+    return {"node": units.get("N", 0), "bracket": units.get("K", units.get("B", 0)), "byte": units.get("n", 0),
             "position": units.get("L", 0)}.get(unit, 0)
 
 
@@ -319,10 +321,10 @@ def _ctx_counts(g):
     import ctypes
     from alpacc_b200 import api
     L = api.native()
-    out = (ctypes.c_int64 * 11)()
+    out = (ctypes.c_int64 * 12)()
     L.alp_ctx_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
-    L.alp_ctx_info(g.h, out, 11)
-    return {"m": int(out[8]), "L": int(out[9]), "B": int(out[10])}
+    L.alp_ctx_info(g.h, out, 12)
+    return {"m": int(out[8]), "L": int(out[9]), "B": int(out[10]), "K": int(out[11])}
 
 
 SEED_LEX = 0xA1FACC00 + 1
@@ -985,6 +987,8 @@ def main():
         "config": {"workload": "json.alp full lex+parse, one %d MiB synthetic JSON document per GPU "
                                "(depth <= %d), bytes -> preorder tree" % (args.doc_mib, DEPTH),
                    "doc_bytes": size, "nodes": N, "nodes_per_byte": N / size, "parallelism": "replicas",
+                   "tokens": counts["m"], "positions": counts["L"], "brackets": counts["B"],
+                   "brackets_searched": counts["K"],
                    "l2": "inputs larger than L2 (no flush needed)", "seed": SEED,
                    "input_sha256": _sha256(doc),
                    "tuning": {"config": tuning["config"], "tile_shape": list(tuning["tile_shape"]),

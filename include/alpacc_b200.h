@@ -62,7 +62,9 @@ int alp_set_stream(alp_ctx* ctx, void* stream);
  * [3] n_productions, [4] lookback q, [5] lookahead k, [6] max productions per
  * admissible pair, [7] max brackets per pair; counts of the last call on this
  * context: [8] tokens, [9] parser positions (tokens + 2 per document),
- * [10] brackets.  No reference counterpart (measurement support). */
+ * [10] brackets, [11] brackets left for the bracket-matching search after
+ * the pairs closed between adjacent positions are removed.  No reference
+ * counterpart (measurement support). */
 int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out);
 
 /* Per-kernel timing (no reference counterpart; measurement support): when on,

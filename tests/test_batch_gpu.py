@@ -177,3 +177,45 @@ def test_parse_batch_tile_boundaries_and_dense(has_gpu, name):
             np.testing.assert_array_equal(term[a:b].astype(np.uint32), want[0])
             np.testing.assert_array_equal(start[a:b], want[1])
             np.testing.assert_array_equal(end[a:b], want[2])
+
+
+@pytest.mark.parametrize("name", ["json", "sexp"])
+def test_parse_batch_bracket_mismatches(has_gpu, name):
+    """Brackets are matched inside threads and warps, and only the rest crosses
+    tiles: documents whose one flaw is a closer of the wrong kind (depth
+    intact) at the start, the middle or the end, documents that end open
+    followed by documents that start with closers, and many small documents
+    per warp, each document's validity against the oracle."""
+    g, o = _ctx(name, "both")
+    rng = np.random.default_rng(23)
+    docs = _docs(name, 600, 47, median=120, cap=60000)
+    closers = b"]}" if name == "json" else b")"
+    for i in range(0, len(docs), 3):
+        d = bytearray(docs[i])
+        pos = [k for k, c in enumerate(d) if c in closers]
+        if not pos:
+            continue
+        j = pos[[0, len(pos) // 2, len(pos) - 1, int(rng.integers(0, len(pos)))][i % 4]]
+        if name == "json":
+            d[j] = closers[(closers.index(d[j]) + 1) % 2]
+        else:
+            del d[j]
+        docs[i] = bytes(d)
+    opener, closer = (b"[", b"]") if name == "json" else (b"(", b")")
+    extra = []
+    for k in range(1, 40):
+        extra += [opener * k + (b"1" if name == "json" else b"a"), closer * k, opener * k + closer * k]
+    docs = docs[:300] + extra + docs[300:]
+    data, off = _pack(docs)
+    tree, node_off, valid = g.parse_batch_int(data, off)
+    par = tree.parent.cpu().numpy()
+    node_off, valid = node_off.cpu().numpy(), valid.cpu().numpy()
+    n_bad = 0
+    for i, d in enumerate(docs):
+        want = o.lex_parse(d)
+        assert bool(valid[i]) == (want is not None), (i, d[:60])
+        if want is None:
+            n_bad += 1
+            continue
+        np.testing.assert_array_equal(par[node_off[i]:node_off[i + 1]], want[0])
+    assert n_bad > 100
