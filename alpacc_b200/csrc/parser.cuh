@@ -394,6 +394,15 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
         }
         return __ldg(&a.t.key_index[x]);
     };
+    // the pair before this thread's first position: a warp's first lane computes it
+    // from the window (which starts one position early), first, so that its table
+    // load is in flight with the four below; the other lanes take the previous lane's last
+    uint32_t before = NO_PAIR;
+    if (lane == 0) {
+        const long long ip = base + (long long)tid * PP_ITEMS - 1;
+        bool h;
+        if (ip >= 0 && ip < a.L) before = pair_at(tid * PP_ITEMS - 1, h);
+    }
     uint16_t ids[PP_ITEMS];
     uint32_t hb = 0;
 #pragma unroll
@@ -405,14 +414,8 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
         ids[j] = p;
         if (head) hb |= 1u << j;
     }
-    // the pair before this thread's first position: the previous lane's last,
-    // or (a warp's first lane) computed from the window, which starts one early
-    uint32_t prev = __shfl_up_sync(ALP_FULL_MASK, (uint32_t)ids[PP_ITEMS - 1], 1);
-    if (lane == 0) {
-        const long long ip = base + (long long)tid * PP_ITEMS - 1;
-        bool h;
-        prev = (ip >= 0 && ip < a.L) ? (uint32_t)pair_at(tid * PP_ITEMS - 1, h) : (uint32_t)NO_PAIR;
-    }
+    const uint32_t up = __shfl_up_sync(ALP_FULL_MASK, (uint32_t)ids[PP_ITEMS - 1], 1);
+    const uint32_t prev = lane == 0 ? before : up;
     PosSums acc;
     possums_zero(acc);
     {

@@ -137,3 +137,40 @@ def test_host_buffers(has_gpu):
     want = o.lex_parse(d.tobytes())
     for a, b in zip(got, want):
         np.testing.assert_array_equal(a, b)
+
+
+def _bracket_counts(tb, data: bytes):
+    """Brackets of the LLP pair sequence and the pairs closed between adjacent
+    positions (a position's first rights against the previous position's top
+    lefts, none across a document start), computed on the CPU from the
+    oracle's tokens and the pair table."""
+    o = oracle.Oracle(tb.blob())
+    p = tb.parser
+    terms = o.lex_futhark(data)[0]
+    arr = [p.start] + [int(t) for t in terms] + [p.end]
+    kmap = dict(zip(p.keys, p.key_pair))
+    n = len(arr)
+    pids = [kmap[tuple(arr[j] if 0 <= j < n else p.empty for j in range(i - p.q, i + p.k))] for i in range(n)]
+    nbr = [b - a for a, b, _, _ in p.pairs]
+    nl = [sum(1 for x in p.stack[a:b] if x >> 31) for a, b, _, _ in p.pairs]
+    brackets = sum(nbr[x] for x in pids)
+    closed = sum(min(nl[a], nbr[b] - nl[b]) for a, b in zip(pids, pids[1:]))
+    return brackets, closed
+
+
+@pytest.mark.parametrize("name", ["json", "arithmetic", "sexp"])
+def test_adjacent_bracket_pairs_counted(has_gpu, name):
+    """The parser closes the bracket pairs between adjacent positions before the
+    bracket search; the counts it reports equal the CPU's."""
+    import ctypes
+    from alpacc_b200 import api
+    g, o, tb = _ctx(name)
+    for i, size in enumerate([100, 5000, 300000]):
+        d = _gen(name, size, 900 + i).tobytes()
+        assert g.parse_int(d) is not None
+        info = (ctypes.c_int64 * 12)()
+        assert api.native().alp_ctx_info(g.h, info, 12) == 0
+        brackets, closed = _bracket_counts(tb, d)
+        assert info[10] == brackets
+        assert info[11] == brackets - 2 * closed
+        assert 0 < info[11] < brackets or brackets == 0
