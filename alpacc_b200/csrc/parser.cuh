@@ -659,7 +659,8 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     uint2* s_srec = s_prec + a.t.n_pseq;
     // per position: x = its first production record minus its first (tile-local)
     // node, so that node g reads record g + x; y = exscan(arity - 1) before it;
-    // z = token index of its first terminal production; w = bracket depth before it
+    // z = token index of its first terminal production; w = depth before it (not read by
+    // the node windows; a record stays one 16-byte store)
     int4* s_pos = reinterpret_cast<int4*>(smem + expand_tables_bytes(a.t.n_pairs, a.t.n_pseq, a.t.n_stack));
     uint16_t* s_own = reinterpret_cast<uint16_t*>(s_pos + PP_TILE * 5 / 4);  // [EX_WIN] owner of each node
     __shared__ PosSums s_w[PP_THREADS / 32];
