@@ -6,7 +6,6 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -75,6 +74,7 @@ struct alp_ctx {
     long long last_positions = 0;
     long long last_brackets = 0;
     long long last_kept = 0;              // brackets left for the search after closing adjacent pairs
+    long long dev_allocs = 0;             // cudaMalloc calls made for this context's buffers
     DevBuf mlp[16];                       // MLP training activations
     DevBuf spec[16];                      // speculative lexer chunk arrays
     // host-input token streams (alp_lex_host_stream): copy streams, events,
@@ -135,6 +135,7 @@ int grow(alp_ctx* ctx, DevBuf& b, size_t bytes) {
     b.bytes = 0;
     size_t want = bytes < 256 ? 256 : bytes;
     CK(cudaMalloc(&b.p, want));
+    ++ctx->dev_allocs;
     b.bytes = want;
     return ALP_OK;
 }
@@ -144,6 +145,7 @@ int upload(alp_ctx* ctx, const T* h, size_t count, const T** d) {
     void* p = nullptr;
     size_t bytes = count * sizeof(T);
     CK(cudaMalloc(&p, bytes < 16 ? 16 : bytes));
+    ++ctx->dev_allocs;
     if (bytes) CK(cudaMemcpy(p, h, bytes, cudaMemcpyHostToDevice));
     ctx->owned.push_back(p);
     *d = reinterpret_cast<const T*>(p);
@@ -1041,10 +1043,10 @@ int alp_set_stream(alp_ctx* ctx, void* stream) {
 
 int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out) {
     if (!ctx || !out) return ALP_ERR_ARG;
-    int64_t v[12] = {ctx->has_lexer, ctx->has_parser, ctx->has_parser ? ctx->ph.n_terms : ctx->n_terms,
+    int64_t v[13] = {ctx->has_lexer, ctx->has_parser, ctx->has_parser ? ctx->ph.n_terms : ctx->n_terms,
                      ctx->ph.n_prods, ctx->ph.q, ctx->ph.k, ctx->ph.max_prods, ctx->ph.max_brackets,
-                     ctx->last_tokens, ctx->last_positions, ctx->last_brackets, ctx->last_kept};
-    for (int i = 0; i < n_out && i < 12; ++i) out[i] = v[i];
+                     ctx->last_tokens, ctx->last_positions, ctx->last_brackets, ctx->last_kept, ctx->dev_allocs};
+    for (int i = 0; i < n_out && i < 13; ++i) out[i] = v[i];
     return ALP_OK;
 }
 
@@ -1256,12 +1258,13 @@ int alp_lex_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_term,
 // Scratch-free lexing: alp_lex_noalloc
 //
 // Some callers cannot allocate device memory at the moment they lex: code that
-// owns every byte of the device through its own pool, code on a latency-bound
-// path where cudaMalloc/cudaFree would synchronise the device, or a host
-// callback that must not enter the allocator.  alp_lex_noalloc serves them:
+// owns every byte of the device through its own pool (a serving framework that
+// reserved the GPU up front), or a path where cudaMalloc/cudaFree would
+// synchronise the device and stall other streams.  alp_lex_noalloc serves them:
 // the look-back status words and the result block live in the fixed array
 // below, compiled into the library, instead of in context scratch that grows
 // with cudaMalloc.  The caller still passes the input and the output buffers.
+// The call blocks on the context stream until the token count is read back.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -1272,25 +1275,10 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = 256 + 12 * (size_t)NOALLOC_MAX_TILES;  
 // Every GPU that loads this library holds one copy until the process exits.
 // Host code must not pass `g_noalloc_scratch` itself to a kernel: on the host
 // the name is only a stand-in, so its device address comes from
-// cudaGetSymbolAddress below.
+// cudaGetSymbolAddress, asked again on every call.  The lookup allocates
+// nothing, and asking each time keeps the address right when the device's
+// primary context was reset and the module reloaded at another address.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
-
-constexpr int NOALLOC_MAX_DEVICES = 64;
-std::once_flag g_noalloc_once[NOALLOC_MAX_DEVICES];
-void* g_noalloc_ptr[NOALLOC_MAX_DEVICES];
-cudaError_t g_noalloc_err[NOALLOC_MAX_DEVICES];
-
-// Device address of the fixed scratch on `device` (which must be current),
-// looked up once per device.
-void* noalloc_scratch(int device, cudaError_t* err) {
-    std::call_once(g_noalloc_once[device], [device] {
-        void* p = nullptr;
-        g_noalloc_err[device] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        g_noalloc_ptr[device] = g_noalloc_err[device] == cudaSuccess ? p : nullptr;
-    });
-    *err = g_noalloc_err[device];
-    return g_noalloc_ptr[device];
-}
 
 }  // namespace
 
@@ -1306,7 +1294,6 @@ int alp_lex_noalloc(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_te
     if (!n_tok || !valid || (cap > 0 && (!d_term || !d_start || !d_end)))
         return fail(ctx, ALP_ERR_ARG, "alp_lex_noalloc: null output");
     if (!ctx->has_lexer) return fail(ctx, ALP_ERR_MODE, "these tables have no lexer");
-    if (ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES) return fail(ctx, ALP_ERR_ARG, "device id too large");
     *n_tok = 0;
     *valid = 0;
     CK(cudaSetDevice(ctx->device));
@@ -1314,9 +1301,10 @@ int alp_lex_noalloc(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_te
         *valid = (ctx->h_tokinfo[1] & TOK_ACCEPT) ? 1 : 0;
         return ALP_OK;
     }
-    cudaError_t se;
-    uint8_t* base = reinterpret_cast<uint8_t*>(noalloc_scratch(ctx->device, &se));
-    if (!base) return fail(ctx, ALP_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(se));
+    void* sym = nullptr;
+    const cudaError_t se = cudaGetSymbolAddress(&sym, g_noalloc_scratch);
+    if (se != cudaSuccess || !sym) return fail(ctx, ALP_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(se));
+    uint8_t* base = reinterpret_cast<uint8_t*>(sym);
     const long long tiles = (n + LEX_TILE - 1) / LEX_TILE;
     const size_t used = 256 + 12 * (size_t)tiles;
     // the array keeps the previous call's words: clear the part this call uses
@@ -1338,7 +1326,13 @@ int alp_lex_noalloc(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_te
     a.state_out = nullptr;
     auto k = lex_kernel<LEX_ITEMS, uint32_t, int64_t>;
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->lex_smem));
-    k<<<(unsigned)tiles, LEX_THREADS, ctx->lex_smem, ctx->stream>>>(a);
+    // persistent like launch_lex: as many CTAs as fit at once, each taking tile tickets
+    int per_sm = 0, sms = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, LEX_THREADS, ctx->lex_smem));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    long long grid = (long long)(per_sm > 0 ? per_sm : 1) * sms;
+    if (grid > tiles) grid = tiles;
+    k<<<(unsigned)grid, LEX_THREADS, ctx->lex_smem, ctx->stream>>>(a);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(ctx->h_res, a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));

@@ -15,9 +15,11 @@ are larger than L2, so no flush is needed between steps.
                  u32 tag, u8 kind, i64 start, i64 end) over the step time,
                  against the measured HBM copy bandwidth; plus a per-kernel
                  breakdown from one instrumented step.
-* ``cpu_baseline`` -- the CPU oracle (sequential C restatement of the
-                 reference's generated lexer and parser) on a bounded sample of
-                 the same generator, rank 0 only.
+* ``cpu_baseline`` -- the data-parallel CPU restatement of the
+                 reference's generated lexer and parser (oracle/par.c, OpenMP,
+                 every host thread) on the same document, rank 0 only.
+* ``parity``  -- SHA-256 of each output array of the e2e call's tree against
+                 the sequential oracle's, at full size (rank 0).
 
 Other workloads (``--workload``), one JSON line each, same keys:
 
@@ -35,8 +37,9 @@ Other workloads (``--workload``), one JSON line each, same keys:
                 inputs against the plain lexer, with hit rate and re-run
                 fraction; the output is compared token for token.
 
-``--impl reference`` times the CPU restatement alone (the reference's own
-Futhark/Haskell toolchain is not available) on the same workload shape.
+``--impl reference`` times the data-parallel CPU restatement alone (the
+reference's own Futhark/Haskell toolchain is not available) on the same
+single document.
 Under torchrun each rank runs its own inputs (weak scaling, replicas, no
 data-path collective); the step time is the max over ranks.
 """
@@ -177,63 +180,107 @@ def _host_threads() -> int:
     return max(1, min(n, 64))
 
 
-def _oracle_rate(o, d: bytes, threads: int, reps: int):
-    """Median seconds of `reps` steps; each step parses `d` once on each of
-    `threads` host threads at once (the C oracle releases the GIL and keeps no
-    state between calls, so the threads run in parallel)."""
-    from concurrent.futures import ThreadPoolExecutor
-    with ThreadPoolExecutor(threads) as ex:
-        assert all(r is not None for r in ex.map(lambda _: o.lex_parse(d), range(threads)))  # warm-up
-        ts = []
-        for _ in range(reps):
-            t0 = time.perf_counter()
-            res = list(ex.map(lambda _: o.lex_parse(d), range(threads)))
-            ts.append(time.perf_counter() - t0)
-            assert all(r is not None for r in res)
-    return statistics.median(ts)
+def _par_rate(P, d: bytes, reps: int):
+    """Median seconds of `reps` lex+parse runs of the data-parallel CPU
+    restatement over the whole document, after one warm-up run; the node
+    count of the last run."""
+    ok, nodes = P.lex_parse_count(d)  # warm-up
+    if not ok:
+        raise RuntimeError("CPU restatement rejected the benchmark document")
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        ok, nodes = P.lex_parse_count(d)
+        ts.append(time.perf_counter() - t0)
+        if not ok:
+            raise RuntimeError("CPU restatement rejected the benchmark document")
+    return statistics.median(ts), nodes
 
 
-def cpu_baseline(sample_bytes: int, reps: int):
-    """The oracle (lex_int then parse_int restated in C) on samples of the
-    workload, one per host thread, all threads at once."""
+def _config(size: int, sha: str):
+    """The workload as both arms name it (identical objects)."""
+    return {"workload": "json.alp full lex+parse, one %d MiB synthetic JSON document (depth <= %d), bytes -> "
+                        "preorder tree (i64 parent, u32 tag, u8 kind, i64 start, i64 end per node)"
+                        % (size >> 20, DEPTH),
+            "doc_bytes": size, "depth": DEPTH, "seed": SEED, "input_sha256": sha,
+            "l2": "inputs larger than L2 (no flush needed)"}
+
+
+def _par_sample(reps: int, size: int):
+    """The data-parallel CPU restatement of the templates (oracle/par.c,
+    OpenMP) on the benchmark document, on every host thread."""
     import oracle
     from alpacc_b200 import tables
-    tb = tables.load("json", "both")
-    o = oracle.Oracle(tb.blob())
-    threads = _host_threads()
-    per = max(1 << 20, sample_bytes // threads)
-    d = make_doc(SEED + 7, per).tobytes()
-    t = _oracle_rate(o, d, threads, reps)
-    return {"value": threads * per / t / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
-            "sample": "%d host threads at once, each lex+parse of its own %.1f MiB json.alp document (same "
-                      "generator, depth %d), median of %d" % (threads, per / 2**20, DEPTH, reps)}
+    P = oracle.Par(tables.load("json", "both").blob(), _host_threads())
+    doc = oracle.synth_json(size, DEPTH, SEED)
+    sha = _sha256(doc)
+    d = doc.tobytes()
+    t, nodes = _par_rate(P, d, reps)
+    return {"value": size / t / 1e9, "unit": "GB/s", "cores": P.threads, "kind": "port",
+            "sample": "the whole %d MiB document (%d nodes), lex+parse by the data-parallel restatement of "
+                      "futhark/lexer.fut + futhark/parser.fut (oracle/par.c, OpenMP, %d threads), median of %d "
+                      "after a warm-up" % (size >> 20, nodes, P.threads, reps),
+            "median_s": t}, sha
+
+
+def cpu_baseline(size: int, reps: int):
+    base, _ = _par_sample(reps, size)
+    return base
 
 
 def run_reference(args, rank: int, world: int):
+    """The reference arm: the reference's own CPU path for lex+parse is Futhark
+    multicore output of the Haskell generator, which cannot be built here (no
+    GHC, no futhark); its data-parallel algorithm restated in C with OpenMP
+    (oracle/par.c) runs in its place, on the same single document, every host
+    thread, input generated by the oracle library's copy of the generator."""
     if rank != 0:
         return
-    import oracle
-    from alpacc_b200 import tables
-    tb = tables.load("json", "both")
-    o = oracle.Oracle(tb.blob())
-    threads = _host_threads()
-    per = 8 << 20
-    d = make_doc(SEED + 7, per).tobytes()
-    step = _oracle_rate(o, d, threads, max(1, args.steps))
-    v = threads * per / step / 1e9
-    line = {"metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step * 1e3, "higher_is_better": True, "scaling": "weak",
+    size = args.doc_mib << 20
+    base, sha = _par_sample(max(5, args.steps), size)
+    v = base["value"]
+    line = {"metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": world, "steps": max(5, args.steps),
+            "warmup": 1, "ms_per_step": base["median_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic", "impl": "reference",
-            "config": {"workload": "json.alp lex+parse, 256 MiB-document generator (depth <= 16); the CPU "
-                                   "restatement parses an 8 MiB sample on each of %d host threads per step"
-                                   % threads,
-                       "doc_bytes": per * threads},
-            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port",
-                             "sample": "8 MiB json.alp document per host thread per step, %d threads at once (the "
-                                       "reference's Futhark multicore build needs GHC and futhark, absent "
-                                       "here; the restatement is sequential per document)" % threads},
+            "config": _config(size, sha), "cpu_baseline": base,
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def _sha_arrays(arrs, names, dtypes):
+    import hashlib
+    out = {}
+    for a, nm, dt in zip(arrs, names, dtypes):
+        out[nm] = hashlib.sha256(memoryview(np.ascontiguousarray(a).view(dt)).cast("B")).hexdigest()
+    return out
+
+
+def _parity_tree(doc: np.ndarray, got, N: int):
+    """SHA-256 of each output array of the GPU's tree against the oracle's
+    (oracle/oracle.c: the generated lex_int + parse_int restated
+    sequentially), at the benchmark's full size."""
+    import oracle
+    from alpacc_b200 import tables
+    o = oracle.Oracle(tables.load("json", "both").blob())
+    t0 = time.perf_counter()
+    want = o.lex_parse(doc.tobytes())
+    t = time.perf_counter() - t0
+    names = ["parent", "tag", "kind", "start", "end"]
+    dts = [np.int64, np.uint32, np.uint8, np.int64, np.int64]
+    res = {"config": "the benchmark document, whole tree", "arrays": names, "nodes": N,
+           "oracle": "oracle/oracle.c orc_lex_futhark + orc_parse_futhark (sequential restatement)",
+           "oracle_s": round(t, 2)}
+    if want is None:
+        res.update(sha256_equal=False, error="oracle rejected the document")
+        return res
+    sg = _sha_arrays([g[:N] for g in got], names, dts)
+    sw = _sha_arrays([w.astype(d) for w, d in zip(want, dts)], names, dts)
+    res["oracle_nodes"] = int(len(want[0]))
+    res["sha256_equal"] = bool(len(want[0]) == N and sg == sw)
+    res["sha256"] = sw
+    if not res["sha256_equal"]:
+        res["sha256_gpu"] = sg
+    return res
 
 
 def _traffic_table():
@@ -861,6 +908,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--doc-mib", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the full-size comparison with the oracle")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes (no autotuner run): for "
                     "launch lists whose first launches should be the measured ones")
     ap.add_argument("--workload", default="parse", choices=["parse", "lex", "batch", "spec", "graph", "shard"])
@@ -957,9 +1005,15 @@ def main():
     torch.cuda.synchronize()
     ms_e2e = _max_over_ranks(e0.elapsed_time(e1) / k_e2e, dist, local)
 
+    # full-size parity: the tree the e2e call brought back against the oracle
+    # (sequential restatement of the generated lex_int + parse_int)
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = _parity_tree(doc, [o.numpy() for o in outs], N)
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(64 << 20, 2)
+        base = cpu_baseline(size, 5)
 
     if dist:
         dist.barrier()
@@ -984,15 +1038,12 @@ def main():
         "vs_baseline": None,
         "dtype": "u8",
         "data": "synthetic",
-        "config": {"workload": "json.alp full lex+parse, one %d MiB synthetic JSON document per GPU "
-                               "(depth <= %d), bytes -> preorder tree" % (args.doc_mib, DEPTH),
-                   "doc_bytes": size, "nodes": N, "nodes_per_byte": N / size, "parallelism": "replicas",
-                   "tokens": counts["m"], "positions": counts["L"], "brackets": counts["B"],
-                   "brackets_searched": counts["K"],
-                   "l2": "inputs larger than L2 (no flush needed)", "seed": SEED,
-                   "input_sha256": _sha256(doc),
-                   "tuning": {"config": tuning["config"], "tile_shape": list(tuning["tile_shape"]),
-                              "candidates_ms": [[k, v, round(t, 4)] for k, v, t in tuning["timings"]]}},
+        "config": _config(size, _sha256(doc)),
+        "details": {"nodes": N, "nodes_per_byte": N / size, "parallelism": "replicas (one document per GPU)",
+                    "tokens": counts["m"], "positions": counts["L"], "brackets": counts["B"],
+                    "brackets_searched": counts["K"],
+                    "tuning": {"config": tuning["config"], "tile_shape": list(tuning["tile_shape"]),
+                               "candidates_ms": [[k, v, round(t, 4)] for k, v, t in tuning["timings"]]}},
         "roofline": roof,
         "path_roofline": path,
         "e2e": {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": size,
@@ -1002,6 +1053,8 @@ def main():
     }
     if base:
         line["cpu_baseline"] = base
+    if parity:
+        line["parity"] = parity
     print(json.dumps(line), flush=True)
 
 

@@ -63,7 +63,8 @@ int alp_set_stream(alp_ctx* ctx, void* stream);
  * admissible pair, [7] max brackets per pair; counts of the last call on this
  * context: [8] tokens, [9] parser positions (tokens + 2 per document),
  * [10] brackets, [11] brackets left for the bracket-matching search after
- * the pairs closed between adjacent positions are removed.  No reference
+ * the pairs closed between adjacent positions are removed; [12] device
+ * allocations (cudaMalloc calls) this context has made so far.  No reference
  * counterpart (measurement support). */
 int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out);
 
@@ -111,21 +112,25 @@ int alp_lex_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, uint32_t* h_term,
                  int64_t* h_end, int64_t cap, int64_t* n_tok, int* valid);
 
 /* lex_int without any device allocation (no counterpart in the reference).
- * For callers that cannot allocate device memory when they lex -- a caller
- * whose own pool owns all device memory, a latency-bound path where
- * cudaMalloc/cudaFree would synchronise the device, or a host callback that
- * must not enter the allocator.  Same results as alp_lex_into.
+ * For callers that cannot allocate device memory when they lex: a caller whose
+ * own pool reserved all device memory up front (a serving process that owns
+ * the GPU), or a path where cudaMalloc/cudaFree would synchronise the device
+ * and stall its other streams.  Same results as alp_lex_into.
  *   - Input is limited to 128 MiB (134217728 bytes); larger inputs fail with
  *     ALP_ERR_ARG and a message naming the limit.
  *   - Scratch is one fixed 393,472-byte array compiled into the library; every
  *     GPU that loads the library holds it until the process exits.  The
  *     outputs are the caller's buffers of `cap` tokens.
- *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress); make that first call before any stream capture.
- *   - All calls share the one array: calls that overlap on the GPU (other
- *     streams, other contexts on the same device) race and must not overlap.
- *   - The call makes no cudaMalloc/cudaFree and no allocating library call;
- *     only its error paths write the context's host-side message. */
+ *   - Every call looks up the array's device address (cudaGetSymbolAddress,
+ *     which allocates nothing); the first call on a device may load the
+ *     library's kernels there, so make it before any stream capture.
+ *   - All calls share the one array, which keeps the last call's contents (the
+ *     call clears the part it uses first): calls that overlap on the GPU
+ *     (other streams, other contexts on the same device) race and must not
+ *     overlap.
+ *   - The call blocks on the context stream until the token count is back.
+ *   - It makes no cudaMalloc/cudaFree and no allocating library call; only its
+ *     error paths write the context's host-side message. */
 int alp_lex_noalloc(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_term, int64_t* d_start,
                     int64_t* d_end, int64_t cap, int64_t* n_tok, int* valid);
 

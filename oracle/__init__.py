@@ -1,8 +1,16 @@
-"""ctypes front end of the CPU oracle (``oracle/oracle.c``).
+"""ctypes front end of the CPU oracle.
+
+* ``oracle.c`` -- the sequential restatement of the reference's lexer and
+  parser (the checker);
+* ``par.c``    -- the same results by the templates' data-parallel algorithm,
+  one document on all host cores with OpenMP (the timed CPU baseline);
+* the seeded workload generators, compiled from ``alpacc_b200/csrc/synth.c``
+  into this library as well, so that the CPU baseline generates its inputs
+  without loading the product's libraries.
 
 TEST INFRASTRUCTURE ONLY: the tests, ``__graft_entry__.smoke()`` and the CPU
-baseline leg of ``bench.py`` use it as the checker.  The product package
-``alpacc_b200`` never imports it.
+baseline legs of ``bench.py`` use it.  The product package ``alpacc_b200``
+never imports it.
 """
 
 from __future__ import annotations
@@ -17,13 +25,15 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 SRC = os.path.join(HERE, "oracle.c")
+SRCS = [SRC, os.path.join(HERE, "par.c"), os.path.join(HERE, "..", "alpacc_b200", "csrc", "synth.c")]
+DEPS = SRCS + [os.path.join(HERE, "oracle.h")]
 
 
 def build(force: bool = False) -> str:
-    """Compile the oracle with gcc (``-O2``, no GPU needed)."""
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+    """Compile the oracle with gcc (``-O2 -fopenmp``, no GPU needed)."""
+    if force or not os.path.exists(LIB) or any(os.path.getmtime(LIB) < os.path.getmtime(x) for x in DEPS):
         tmp = LIB + ".tmp%d" % os.getpid()
-        subprocess.check_call(["gcc", "-O2", "-shared", "-fPIC", "-o", tmp, SRC])
+        subprocess.check_call(["gcc", "-O2", "-fopenmp", "-shared", "-fPIC", "-o", tmp] + SRCS)
         os.replace(tmp, LIB)
     return LIB
 
@@ -48,6 +58,17 @@ def lib():
             getattr(L, name).argtypes = [vp, vp, vp, vp, i64, vp, vp, vp, vp, vp, i64, vp]
         L.orc_max_pair_prods.restype = i64
         L.orc_max_pair_prods.argtypes = [vp]
+        L.par_create.restype = vp
+        L.par_create.argtypes = [vp, ctypes.c_int]
+        L.par_free.argtypes = [vp]
+        L.par_threads.argtypes = [vp]
+        L.par_lex.argtypes = [vp, vp, i64, vp, vp, vp, vp]
+        L.par_parse.argtypes = [vp, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp]
+        L.par_lex_parse.argtypes = [vp, vp, i64, vp, vp, vp, vp, vp, vp]
+        for name in ("alp_synth_json", "alp_synth_arith", "alp_synth_sexp"):
+            f = getattr(L, name)
+            f.restype = i64
+            f.argtypes = [ctypes.c_uint64, i64, ctypes.c_int, vp]
         _lib = L
     return _lib
 
@@ -148,3 +169,88 @@ class Oracle:
         if toks is None:
             return None
         return self.parse_futhark(*toks)
+
+
+def _take(ptr: ctypes.c_void_p, n: int, dtype) -> np.ndarray:
+    """Copy n elements out of a context-owned par.c buffer."""
+    if n == 0 or not ptr.value:
+        return np.zeros(0, dtype)
+    return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(np.ctypeslib.as_ctypes_type(dtype))),
+                                 shape=(n,)).copy()
+
+
+class Par:
+    """The data-parallel restatement (``par.c``) over one grammar's table
+    blob: one document at a time on ``threads`` host threads (0: all).  Its
+    buffers live in the context; the methods copy results out."""
+
+    def __init__(self, blob: bytes, threads: int = 0):
+        self._o = Oracle(blob)
+        self.h = lib().par_create(self._o.h, threads)
+        if not self.h:
+            raise ValueError("par: key space too large for the direct index")
+        self.threads = int(lib().par_threads(self.h))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().par_free(self.h)
+            self.h = None
+
+    def lex(self, data):
+        """Tokens (term, start, end) or None when rejected."""
+        buf = np.frombuffer(data, dtype=np.uint8) if len(data) else np.zeros(1, np.uint8)
+        p = [ctypes.c_void_p() for _ in range(3)]
+        n = ctypes.c_int64(0)
+        ok = lib().par_lex(self.h, _p(buf), len(data), *[ctypes.byref(x) for x in p], ctypes.byref(n))
+        if ok < 0:
+            raise MemoryError("par.c: out of host memory")
+        out = (_take(p[0], n.value, np.uint32), _take(p[1], n.value, np.int64), _take(p[2], n.value, np.int64))
+        return out if ok else None
+
+    def parse(self, terms, starts, ends):
+        """Tree (parent, tag, kind, start, end) over a token array, or None."""
+        terms = np.ascontiguousarray(terms, dtype=np.uint32)
+        starts = np.ascontiguousarray(starts, dtype=np.int64)
+        ends = np.ascontiguousarray(ends, dtype=np.int64)
+        m = len(terms)
+        if m == 0:
+            terms, starts, ends = np.zeros(1, np.uint32), np.zeros(1, np.int64), np.zeros(1, np.int64)
+        p = [ctypes.c_void_p() for _ in range(5)]
+        n = ctypes.c_int64(0)
+        ok = lib().par_parse(self.h, _p(terms), _p(starts), _p(ends), m, *[ctypes.byref(x) for x in p],
+                             ctypes.byref(n))
+        return self._tree(ok, p, n.value)
+
+    def lex_parse(self, data):
+        """Bytes in, tree (parent, tag, kind, start, end) out, or None."""
+        buf = np.frombuffer(data, dtype=np.uint8) if len(data) else np.zeros(1, np.uint8)
+        p = [ctypes.c_void_p() for _ in range(5)]
+        n = ctypes.c_int64(0)
+        ok = lib().par_lex_parse(self.h, _p(buf), len(data), *[ctypes.byref(x) for x in p], ctypes.byref(n))
+        return self._tree(ok, p, n.value)
+
+    def lex_parse_count(self, data):
+        """(valid, nodes) of a lex+parse whose outputs stay in the context:
+        the timed form, without the copies into numpy arrays."""
+        buf = np.frombuffer(data, dtype=np.uint8) if len(data) else np.zeros(1, np.uint8)
+        p = [ctypes.c_void_p() for _ in range(5)]
+        n = ctypes.c_int64(0)
+        ok = lib().par_lex_parse(self.h, _p(buf), len(data), *[ctypes.byref(x) for x in p], ctypes.byref(n))
+        if ok < 0:
+            raise MemoryError("par.c: out of host memory")
+        return int(ok), n.value
+
+    @staticmethod
+    def _tree(ok, p, n):
+        if ok < 0:
+            raise MemoryError("par.c: out of host memory")
+        out = (_take(p[0], n, np.int64), _take(p[1], n, np.uint32), _take(p[2], n, np.uint8),
+               _take(p[3], n, np.int64), _take(p[4], n, np.int64))
+        return out if ok else None
+
+
+def synth_json(size: int, depth: int, seed: int) -> np.ndarray:
+    """The seeded JSON generator (same source as the product's generator)."""
+    out = np.empty(max(size, 2), dtype=np.uint8)
+    n = lib().alp_synth_json(seed, size, depth, _p(out))
+    return out[:n]

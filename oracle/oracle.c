@@ -16,39 +16,11 @@
  *
  * It reads the same table blob as the product library (layout documented
  * in alpacc_b200/tables.py), but only the plain forms: the 256-column DFA,
- * the token map and the admissible-pair list.  It never reads the GPU forms
- * (byte classes, endomorphism tables, key index).
+ * the token map and the admissible-pair list.  The sequential functions here
+ * never read the endomorphism forms; par.c (the data-parallel restatement)
+ * does.
  */
-#include <stdint.h>
-#include <stdlib.h>
-#include <string.h>
-
-#define ORC_MAGIC 0x42504C41u
-#define HIGHEST INT64_MAX
-
-typedef struct {
-    /* lexer */
-    int has_lexer;
-    uint32_t S, C, E, ignore_term, dead_term, n_terms;
-    const uint16_t *delta256; /* [S][256]: next | produce<<15 */
-    const uint32_t *token;    /* [S] */
-    const uint8_t *accept;    /* [S] */
-    /* parser */
-    int has_parser;
-    uint32_t q, k, n_term_syms, empty, start, end, n_prods;
-    const uint32_t *arity;
-    const int32_t *prod_term;
-    uint32_t n_pairs;
-    const uint32_t *pairs; /* [n_pairs][4] */
-    uint32_t n_stack;
-    const uint32_t *stack;
-    uint32_t n_pseq;
-    const uint32_t *pseq;
-    uint32_t n_keys;
-    const uint32_t *keys;     /* [n_keys][q+k], sorted */
-    const uint32_t *key_pair; /* [n_keys] */
-    uint8_t *copy;            /* private copy of the blob */
-} orc_tables;
+#include "oracle.h"
 
 static const uint8_t *rd32(const uint8_t *p, const uint8_t *e, uint32_t *v) {
     if (!p || p + 4 > e) return NULL;
@@ -85,14 +57,14 @@ orc_tables *orc_load(const void *blob, size_t len) {
         p = rd32(p, e, &t->ignore_term); p = rd32(p, e, &t->dead_term); p = rd32(p, e, &t->n_terms);
         if (!p) { orc_free(t); return NULL; }
         uint32_t S = t->S, C = t->C, E = t->E;
-        p = skip(p, e, 256);                                   /* byte classes */
+        t->cls = p; p = skip(p, e, 256);                       /* byte classes */
         t->delta256 = (const uint16_t *)p; p = skip(p, e, (size_t)S * 256 * 2);
         p = skip(p, e, (size_t)S * (C + 1) * 2);               /* class table */
         t->token = (const uint32_t *)p; p = skip(p, e, (size_t)S * 4);
         t->accept = p; p = skip(p, e, S);
-        p = skip(p, e, (size_t)E * (C + 1) * 2);
-        p = skip(p, e, (size_t)E * E * 2);
-        p = skip(p, e, (size_t)E * S * 2);
+        t->endo_step = (const uint16_t *)p; p = skip(p, e, (size_t)E * (C + 1) * 2);
+        t->endo_comp = (const uint16_t *)p; p = skip(p, e, (size_t)E * E * 2);
+        t->endo_app = (const uint16_t *)p; p = skip(p, e, (size_t)E * S * 2);
         if (!p) { orc_free(t); return NULL; }
     }
     if (hp) {
@@ -126,11 +98,9 @@ int orc_info(const orc_tables *t, uint32_t *out /* [8] */) {
 
 /* ---------------------------------------------------------------- lexer -- */
 
-#define INIT_STATE 1u
-
-static inline uint32_t nxt(const orc_tables *t, uint32_t s, uint8_t b) { return t->delta256[(size_t)s * 256 + b] & 0x7fffu; }
-static inline int prod(const orc_tables *t, uint32_t s, uint8_t b) { return (t->delta256[(size_t)s * 256 + b] >> 15) & 1; }
-static inline int is_ignore(const orc_tables *t, uint32_t term) { return t->ignore_term != 0xffffffffu && term == t->ignore_term; }
+#define nxt orc_nxt
+#define prod orc_prod
+#define is_ignore orc_is_ignore
 
 /* tokenize (src/Alpacc/Lexer/DFA.hs:415-447).  Returns 1 (valid), 0
  * (rejected: no tokens), -1 (capacity exceeded). */
