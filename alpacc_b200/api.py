@@ -402,15 +402,20 @@ class Grammar:
         return [(out[2 * i], out[2 * i + 1]) for i in range(k)]
 
     def get_tuning(self) -> List[int]:
-        """[tile shape, pair CTAs per SM, expand CTAs per SM, MLP kernel (0 tcgen05, 1 mma.sync)]."""
-        cfg = (ctypes.c_int32 * 4)()
-        native().alp_tune_get(self.h, cfg, 4)
+        """[tile shape, pair CTAs per SM, expand CTAs per SM, MLP kernel (0 tcgen05, 1 mma.sync),
+        lexer token pass (0 fused, 1 count pass + tile scan + token pass),
+        parser position pass (0 fused, 1 pair pass + tile-sum scan + expansion),
+        lexer state-scan chunks per lane (8, 16 or 32)]."""
+        cfg = (ctypes.c_int32 * 7)()
+        native().alp_tune_get(self.h, cfg, 7)
         return list(cfg)
 
     def set_tuning(self, cfg: Sequence[int]) -> None:
-        """Three values (launch shapes) or four (and the MLP inference kernel)."""
-        if len(cfg) not in (3, 4):
-            raise ValueError("tuning takes 3 or 4 values")
+        """Three values (launch shapes), four (and the MLP inference kernel),
+        five (and the lexer's token pass), six (and the parser's position
+        pass) or seven (and the lexer state scan's chunks per lane)."""
+        if len(cfg) not in (3, 4, 5, 6, 7):
+            raise ValueError("tuning takes 3 to 7 values")
         c = (ctypes.c_int32 * len(cfg))(*cfg)
         rc = native().alp_tune_set(self.h, c, len(cfg))
         if rc != ALP_OK:

@@ -39,6 +39,9 @@ struct Tuning {
     int pairs_ctas = 0;   // CTAs per SM of the persistent pair kernel (0: as many as fit)
     int expand_ctas = 0;  // same for the expand kernel
     int mlp = 0;          // boundary-MLP inference: 0 tcgen05 kernel, 1 mma.sync kernel
+    int lex_split = 1;    // lexer token pass: 0 fused (counts, look-back, tokens), 1 count pass + tile scan + token pass
+    int parse_split = 1;  // parser position pass: 0 fused (pairs, look-back, expand), 1 pair pass + scan + expand
+    int scan_g = 0;       // lexer state scan: chunks per lane, 8, 16 or 32 (0: LS_G)
 };
 
 struct alp_ctx {
@@ -75,6 +78,7 @@ struct alp_ctx {
     long long last_brackets = 0;
     long long last_kept = 0;              // brackets left for the search after closing adjacent pairs
     long long dev_allocs = 0;             // cudaMalloc calls made for this context's buffers
+    double est_nodes = 0, est_kept = 0;   // nodes and kept brackets per position of the last parse (sizes)
     DevBuf mlp[16];                       // MLP training activations
     DevBuf spec[16];                      // speculative lexer chunk arrays
     // host-input token streams (alp_lex_host_stream): copy streams, events,
@@ -467,6 +471,17 @@ struct Lex3Run {
     int sms;
 };
 
+int scan_g(const alp_ctx* ctx) { return ctx->tune.scan_g ? ctx->tune.scan_g : LS_G; }
+
+inline const void* scan_kernel_for(int g) {
+    if (g == 8) return (const void*)lex3_scan_kernel<8>;
+    if (g == 32) return (const void*)lex3_scan_kernel<32>;
+    return (const void*)lex3_scan_kernel<16>;
+}
+
+// the state scan over the chunk endomorphisms, chunks per lane as tuned
+int lex3_scan(alp_ctx* ctx, Lex3Run& r);
+
 int lex3_grid(alp_ctx* ctx, const Lex3Run& r, const void* k, int threads, size_t smem, long long work, unsigned* g) {
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem));
@@ -480,7 +495,7 @@ int lex3_prepare(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long
     r.tiles = (n + LX_TILE - 1) / LX_TILE;
     r.wide = (n + LX_WIDE - 1) / LX_WIDE;
     r.chunks = (n + LX_CHUNK - 1) / LX_CHUNK;
-    r.stiles = (r.chunks + LS_TILE - 1) / LS_TILE;
+    r.stiles = (r.chunks + ls_tile(scan_g(ctx)) - 1) / ls_tile(scan_g(ctx));
     r.nd = nd;
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t o_vec = 256, o_cs = o_vec + al(128 * (size_t)r.stiles), o_f = o_cs + al(8 * (size_t)r.tiles);
@@ -557,18 +572,13 @@ int lex3_fold(alp_ctx* ctx, Lex3Run& r) {
 
 // chunk endomorphisms -> chunk states -> chunk counts and tile counts
 int lex3_front(alp_ctx* ctx, Lex3Run& r, bool folded = false) {
-    unsigned g2, g3;
+    unsigned g3;
     int rc;
     if (!folded && (rc = lex3_fold(ctx, r))) return rc;
-    CK(cudaFuncSetAttribute(lex3_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_scan_smem));
     CK(cudaFuncSetAttribute(lex3_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_count_smem));
-    if ((rc = lex3_grid(ctx, r, (const void*)lex3_scan_kernel, LS_WARPS * 32, ctx->l3_scan_smem, r.stiles, &g2)) ||
-        (rc = lex3_grid(ctx, r, (const void*)lex3_count_kernel, LX_THREADS, ctx->l3_count_smem, r.wide, &g3)))
+    if ((rc = lex3_grid(ctx, r, (const void*)lex3_count_kernel, LX_THREADS, ctx->l3_count_smem, r.wide, &g3)))
         return rc;
-    mark(ctx, "start");
-    lex3_scan_kernel<<<g2, LS_WARPS * 32, ctx->l3_scan_smem, ctx->stream>>>(r.a);
-    CK(cudaGetLastError());
-    mark(ctx, "lex3_scan_kernel");
+    if ((rc = lex3_scan(ctx, r))) return rc;
     lex3_count_kernel<<<g3, LX_THREADS, ctx->l3_count_smem, ctx->stream>>>(r.a, r.sg);
     CK(cudaGetLastError());
     mark(ctx, "lex3_count_kernel");
@@ -618,15 +628,65 @@ int lex3_back(alp_ctx* ctx, Lex3Run& r, long long* total) {
     return ALP_OK;
 }
 
+// The fused token pass (counts, look-back over tiles, tokens) after the
+// state scan: one input pass fewer than lex3_front + lex3_back.
+template <typename TermT, typename PosT>
+int lex3_tok(alp_ctx* ctx, Lex3Run& r, long long* total) {
+    auto k = lex3_tok_kernel<TermT, PosT>;
+    unsigned g;
+    int rc;
+    const size_t sm = lex3_tok_smem(ctx->S);
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    if ((rc = lex3_grid(ctx, r, (const void*)k, LX_THREADS, sm, r.tiles, &g))) return rc;
+    CK(cudaMemsetAsync(r.a.tile_cs, 0, 8 * (size_t)r.tiles, ctx->stream));  // look-back words
+    mark(ctx, "start");
+    k<<<g, LX_THREADS, sm, ctx->stream>>>(r.a, r.sg);
+    CK(cudaGetLastError());
+    mark(ctx, "lex3_tok_kernel");
+    CK(cudaMemcpyAsync(ctx->h_res, r.a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
+    *total = ctx->h_res->count;
+    ctx->last_tokens = *total;
+    if (ctx->h_res->error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "token buffer too small");
+    return ALP_OK;
+}
+
+// chunk endomorphisms -> chunk states (no count pass)
+int lex3_states(alp_ctx* ctx, Lex3Run& r) {
+    int rc;
+    if ((rc = lex3_fold(ctx, r))) return rc;
+    return lex3_scan(ctx, r);
+}
+
+int lex3_scan(alp_ctx* ctx, Lex3Run& r) {
+    const void* k = scan_kernel_for(scan_g(ctx));
+    unsigned g2;
+    int rc;
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->l3_scan_smem));
+    if ((rc = lex3_grid(ctx, r, k, LS_WARPS * 32, ctx->l3_scan_smem, r.stiles, &g2))) return rc;
+    mark(ctx, "start");
+    {
+        void* args[] = {&r.a};
+        CK(cudaLaunchKernel(k, dim3(g2), dim3(LS_WARPS * 32), args, ctx->l3_scan_smem, ctx->stream));
+    }
+    mark(ctx, "lex3_scan_kernel");
+    return ALP_OK;
+}
+
 template <typename TermT, typename PosT>
 int lex3_run(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_off, long long nd, int sentinels,
              TermT* term, PosT* start, PosT* end, long long cap, uint8_t* valid, long long* total) {
     Lex3Run r;
     int rc;
-    if ((rc = lex3_prepare(ctx, d_in, n, d_off, nd, sentinels, term, start, end, cap, valid, r)) ||
-        (rc = lex3_front(ctx, r)))
-        return rc;
-    return lex3_back<TermT, PosT>(ctx, r, total);
+    if ((rc = lex3_prepare(ctx, d_in, n, d_off, nd, sentinels, term, start, end, cap, valid, r))) return rc;
+    if (ctx->tune.lex_split) {
+        if ((rc = lex3_front(ctx, r))) return rc;
+        return lex3_back<TermT, PosT>(ctx, r, total);
+    }
+    if ((rc = lex3_states(ctx, r))) return rc;
+    return lex3_tok<TermT, PosT>(ctx, r, total);
 }
 
 // Segmented lexer over documents at d_off[0..nd] (device).  sentinels: the
@@ -715,14 +775,76 @@ int put_doc_off(alp_ctx* ctx, long long n) {
 // tmp[T_TTERM..T_TEND] and per-document validity in `dvalid` -> tree.
 // `want_tree` 0 gives the production sequence only.  Node offsets of the
 // documents land in tmp[T_NODEOFF].
+// Output buffers for N nodes (context-owned when ctx_out) and the node and
+// bracket intermediates for N nodes and K kept brackets.
+int parse_buffers(alp_ctx* ctx, ParseOut* o, int ctx_out, long long N, long long K, ParseArgs& a) {
+    int rc;
+    if (ctx_out) {
+        if ((rc = grow(ctx, ctx->out[3], N * 8 + 8)) || (rc = grow(ctx, ctx->out[4], N * 4 + 8)) ||
+            (rc = grow(ctx, ctx->out[5], N + 8)) || (rc = grow(ctx, ctx->out[6], N * 8 + 8)) ||
+            (rc = grow(ctx, ctx->out[7], N * 8 + 8)))
+            return rc;
+        o->parent = (int64_t*)ctx->out[3].p;
+        o->tag = (uint32_t*)ctx->out[4].p;
+        o->kind = (uint8_t*)ctx->out[5].p;
+        o->start = (int64_t*)ctx->out[6].p;
+        o->end = (int64_t*)ctx->out[7].p;
+    }
+    if ((rc = grow(ctx, ctx->tmp[T_VBUF], N * 4 + 8)) || (rc = grow(ctx, ctx->tmp[T_BRBUF], K * 4 + 8)) ||
+        (rc = grow(ctx, ctx->tmp[T_DSBUF], K * 4 + 8)))
+        return rc;
+    a.tag = o->tag;
+    a.kind = o->kind;
+    a.nstart = o->start;
+    a.nend = o->end;
+    a.vbuf = (int32_t*)ctx->tmp[T_VBUF].p;
+    a.brbuf = (uint32_t*)ctx->tmp[T_BRBUF].p;
+    a.dsbuf = (int32_t*)ctx->tmp[T_DSBUF].p;
+    a.cap_nodes = N;
+    a.cap_brs = K;
+    return ALP_OK;
+}
+
+// The expand kernel with the pair lookup and a look-back over tiles in it,
+// for a grammar's (q, k) (see parse_pairs_kernel).
+inline const void* fused_expand_for(int q, int k) {
+    if (q == 1 && k == 1) return (const void*)parse_expand_kernel<1, 1, true>;
+    if (q == 1 && k == 2) return (const void*)parse_expand_kernel<1, 2, true>;
+    if (q == 1 && k == 3) return (const void*)parse_expand_kernel<1, 3, true>;
+    if (q == 2 && k == 1) return (const void*)parse_expand_kernel<2, 1, true>;
+    if (q == 2 && k == 2) return (const void*)parse_expand_kernel<2, 2, true>;
+    return (const void*)parse_expand_kernel<0, 0, true>;
+}
+
+int expand_grid(alp_ctx* ctx, const void* fn, size_t sm2, long long tiles, unsigned* g) {
+    int sms = 0, per2 = 0;
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, fn, PP_THREADS, sm2));
+    const long long x = (long long)persistent_ctas(per2, ctx->tune.expand_ctas) * sms;
+    *g = (unsigned)(x < tiles ? x : tiles);
+    return ALP_OK;
+}
+
+// Positions (⊢ tokens ⊣ per document, L of them) already in
+// tmp[T_TTERM..T_TEND] and per-document validity in `dvalid` -> tree.
+// `want_tree` 0 gives the production sequence only.  Node offsets of the
+// documents land in tmp[T_NODEOFF].
+//
+// Two forms of the position pass.  The fused one (one kernel: keys, pair
+// lookup, look-back over tiles, expansion) needs its output capacities before
+// it runs; they come from the nodes and kept brackets per position of the
+// last parse on this context, and when the document needs more, the pass runs
+// again at the exact sizes it reported.  The first parse on a context, and
+// grammars whose counts could pass 32 bits, take the two-pass form: the pair
+// kernel and a scan of its tile sums give the exact sizes first.
 int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, ParseOut* o, int64_t cap, int ctx_out,
                     int64_t* n_node, int want_tree) {
     *n_node = 0;
     if (L >= 0x7fffffffLL) return fail(ctx, ALP_ERR_ARG, "too many positions (%lld)", L);
     const long long tiles = (L + PP_TILE - 1) / PP_TILE;
     int rc;
-    if ((rc = grow(ctx, ctx->tmp[T_PID], (size_t)L * 2 + 64)) || (rc = grow(ctx, ctx->tmp[T_TSUMS], (tiles + tiles / ST_CHUNK + 2) * sizeof(PosSums))) ||
-        (rc = grow(ctx, ctx->tmp[T_NODEOFF], (size_t)(nd + 1) * 8)) || (rc = grow(ctx, ctx->tmp[T_BROFF], (size_t)(nd + 1) * 8)) ||
+    if ((rc = grow(ctx, ctx->tmp[T_NODEOFF], (size_t)(nd + 1) * 8)) || (rc = grow(ctx, ctx->tmp[T_BROFF], (size_t)(nd + 1) * 8)) ||
         (rc = grow(ctx, ctx->scratch, 256)))
         return rc;
     AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
@@ -735,88 +857,110 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     a.pend = (const uint32_t*)ctx->tmp[T_TEND].p;
     a.L = L;
     a.n_docs = nd;
-    a.pid = (uint16_t*)ctx->tmp[T_PID].p;
-    a.tile_sums = (PosSums*)ctx->tmp[T_TSUMS].p;
     a.res = d_res;
     a.node_off = (long long*)ctx->tmp[T_NODEOFF].p;
     a.br_off = (long long*)ctx->tmp[T_BROFF].p;
     a.doc_valid = dvalid;
-    const size_t sm1 = pairs_smem_bytes(ctx->pt.n_pairs, ctx->pt.q + ctx->pt.k);
-    CK(cudaFuncSetAttribute(pairs_kernel_for(ctx->pt.q, ctx->pt.k), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-    mark(ctx, "start");
-    unsigned g_pairs = 1, g_expand = 1;
-    {
-        int sms = 0, per1 = 0;
-        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, pairs_kernel_for(ctx->pt.q, ctx->pt.k), PP_THREADS, sm1));
-        const long long x = (long long)persistent_ctas(per1, ctx->tune.pairs_ctas) * sms;
-        g_pairs = (unsigned)(x < tiles ? x : tiles);
-        g_expand = (unsigned)(2LL * sms < tiles ? 2LL * sms : tiles);  // persistent; set below from occupancy
-    }
-    {
-        void* args[] = {&a};
-        CK(cudaLaunchKernel(pairs_kernel_for(ctx->pt.q, ctx->pt.k), dim3(g_pairs), dim3(PP_THREADS), args, sm1,
-                            ctx->stream));
-    }
-    mark(ctx, "parse_pairs_kernel");
-    {
-        const long long chunks = (tiles + ST_CHUNK - 1) / ST_CHUNK;
-        PosSums* csum = a.tile_sums + tiles;  // chunk sums after the tile sums
-        scan_tiles_reduce_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum, nullptr);
+    a.subst_terminals = want_tree;
+    const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
+    if (sm2 > 220 * 1024) return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
+    long long N = 0, B = 0, K = 0;
+    const bool fits32 = (unsigned long long)L * (unsigned long long)(ctx->ph.max_prods + 1) < (1ull << 32) &&
+                        (unsigned long long)L * (unsigned long long)(ctx->ph.max_brackets + 1) < (1ull << 32);
+    if (!ctx->tune.parse_split && fits32 && ctx->est_nodes > 0) {
+        // ---- fused: capacities from the last parse, exact sizes on a second run if short
+        const void* fn = fused_expand_for(ctx->pt.q, ctx->pt.k);
+        unsigned g = 1;
+        if ((rc = expand_grid(ctx, fn, sm2, tiles, &g))) return rc;
+        if ((rc = grow(ctx, ctx->tmp[T_TSUMS], (size_t)tiles * (4 + 2 * sizeof(PosSums)) + 256))) return rc;
+        uint8_t* lb = reinterpret_cast<uint8_t*>(ctx->tmp[T_TSUMS].p);
+        a.ticket = reinterpret_cast<unsigned int*>(lb);
+        a.lb_flag = reinterpret_cast<uint32_t*>(lb + 16);
+        const size_t o_agg = (16 + 4 * (size_t)tiles + 31) & ~(size_t)31;
+        a.lb_agg = reinterpret_cast<PosSums*>(lb + o_agg);
+        a.lb_inc = a.lb_agg + tiles;
+        long long capN = ctx_out ? (long long)(ctx->est_nodes * (double)L * 1.01) + 4096 : cap;
+        long long capK = (long long)(ctx->est_kept * (double)L * 1.01) + 4096;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            if ((rc = parse_buffers(ctx, o, ctx_out, capN, capK, a))) return rc;
+            CK(cudaMemsetAsync(lb, 0, 16 + 4 * (size_t)tiles, ctx->stream));  // ticket, look-back flags
+            mark(ctx, "start");
+            {
+                void* args[] = {&a};
+                CK(cudaLaunchKernel(fn, dim3(g), dim3(PP_THREADS), args, sm2, ctx->stream));
+            }
+            mark(ctx, "parse_expand_kernel(fused)");
+            if ((rc = read_result(ctx, d_res))) return rc;
+            N = ctx->h_res->aux[0];
+            B = ctx->h_res->aux[1];
+            K = ctx->h_res->aux[6];
+            if (N <= capN && K <= capK) break;
+            if (!ctx_out && N > cap) {
+                *n_node = N;
+                return fail(ctx, ALP_ERR_CAPACITY, "node buffer too small (%lld needed)", (long long)N);
+            }
+            if (attempt == 1) return fail(ctx, ALP_ERR_CUDA, "fused parse pass reported inconsistent sizes");
+            capN = ctx_out ? N : cap;  // run again at the exact sizes
+            capK = K;
+        }
+        a.cap_nodes = N;
+        a.cap_brs = K;
+    } else {
+        // ---- two passes: pair ids and tile sums, their scan, the sizes, then expand
+        if ((rc = grow(ctx, ctx->tmp[T_PID], (size_t)L * 2 + 64)) ||
+            (rc = grow(ctx, ctx->tmp[T_TSUMS], (tiles + tiles / ST_CHUNK + 2) * sizeof(PosSums))))
+            return rc;
+        a.pid = (uint16_t*)ctx->tmp[T_PID].p;
+        a.tile_sums = (PosSums*)ctx->tmp[T_TSUMS].p;
+        const size_t sm1 = pairs_smem_bytes(ctx->pt.n_pairs, ctx->pt.q + ctx->pt.k);
+        CK(cudaFuncSetAttribute(pairs_kernel_for(ctx->pt.q, ctx->pt.k), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+        mark(ctx, "start");
+        unsigned g_pairs = 1, g_expand = 1;
+        {
+            int sms = 0, per1 = 0;
+            CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, pairs_kernel_for(ctx->pt.q, ctx->pt.k), PP_THREADS, sm1));
+            const long long x = (long long)persistent_ctas(per1, ctx->tune.pairs_ctas) * sms;
+            g_pairs = (unsigned)(x < tiles ? x : tiles);
+        }
+        {
+            void* args[] = {&a};
+            CK(cudaLaunchKernel(pairs_kernel_for(ctx->pt.q, ctx->pt.k), dim3(g_pairs), dim3(PP_THREADS), args, sm1,
+                                ctx->stream));
+        }
+        mark(ctx, "parse_pairs_kernel");
+        {
+            const long long chunks = (tiles + ST_CHUNK - 1) / ST_CHUNK;
+            PosSums* csum = a.tile_sums + tiles;  // chunk sums after the tile sums
+            scan_tiles_reduce_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum, nullptr);
+            CK(cudaGetLastError());
+            scan_tiles_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum, d_res, a.node_off,
+                                                                             a.br_off, nd, nullptr);
+            CK(cudaGetLastError());
+        }
+        mark(ctx, "scan_tiles_reduce+scan_tiles");
+        if ((rc = read_result(ctx, d_res))) return rc;
+        // nodes, brackets, and brackets left after closing adjacent pairs
+        N = ctx->h_res->aux[0];
+        B = ctx->h_res->aux[1];
+        K = ctx->h_res->aux[6];
+        if (N > 0xffffffffLL || B > 0xffffffffLL) return fail(ctx, ALP_ERR_ARG, "tree too large");
+        if (!ctx_out && N > cap) {
+            *n_node = N;
+            return fail(ctx, ALP_ERR_CAPACITY, "node buffer too small (%lld needed)", (long long)N);
+        }
+        if ((rc = parse_buffers(ctx, o, ctx_out, N, K, a))) return rc;
+        if ((rc = expand_grid(ctx, (const void*)parse_expand_kernel<0, 0, false>, sm2, tiles, &g_expand))) return rc;
+        mark(ctx, "start");
+        parse_expand_kernel<0, 0, false><<<g_expand, PP_THREADS, sm2, ctx->stream>>>(a);
         CK(cudaGetLastError());
-        scan_tiles_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum, d_res, a.node_off,
-                                                                         a.br_off, nd, nullptr);
-        CK(cudaGetLastError());
+        mark(ctx, "parse_expand_kernel");
     }
-    mark(ctx, "scan_tiles_reduce+scan_tiles");
-    if ((rc = read_result(ctx, d_res))) return rc;
-    // nodes, brackets, and brackets left after closing adjacent pairs
-    const long long N = ctx->h_res->aux[0], B = ctx->h_res->aux[1], K = ctx->h_res->aux[6];
     ctx->last_positions = L;
     ctx->last_brackets = B;
     ctx->last_kept = K;
-    if (N > 0xffffffffLL || B > 0xffffffffLL) return fail(ctx, ALP_ERR_ARG, "tree too large");
-    if (ctx_out) {
-        if ((rc = grow(ctx, ctx->out[3], N * 8 + 8)) || (rc = grow(ctx, ctx->out[4], N * 4 + 8)) ||
-            (rc = grow(ctx, ctx->out[5], N + 8)) || (rc = grow(ctx, ctx->out[6], N * 8 + 8)) ||
-            (rc = grow(ctx, ctx->out[7], N * 8 + 8)))
-            return rc;
-        o->parent = (int64_t*)ctx->out[3].p;
-        o->tag = (uint32_t*)ctx->out[4].p;
-        o->kind = (uint8_t*)ctx->out[5].p;
-        o->start = (int64_t*)ctx->out[6].p;
-        o->end = (int64_t*)ctx->out[7].p;
-    } else if (N > cap) {
-        *n_node = N;
-        return fail(ctx, ALP_ERR_CAPACITY, "node buffer too small (%lld needed)", (long long)N);
-    }
-    if ((rc = grow(ctx, ctx->tmp[T_VBUF], N * 4 + 8)) || (rc = grow(ctx, ctx->tmp[T_BRBUF], K * 4 + 8)) ||
-        (rc = grow(ctx, ctx->tmp[T_DSBUF], K * 4 + 8)))
-        return rc;
-    a.tag = o->tag;
-    a.kind = o->kind;
-    a.subst_terminals = want_tree;
-    a.nstart = o->start;
-    a.nend = o->end;
-    a.vbuf = (int32_t*)ctx->tmp[T_VBUF].p;
-    a.brbuf = (uint32_t*)ctx->tmp[T_BRBUF].p;
-    a.dsbuf = (int32_t*)ctx->tmp[T_DSBUF].p;
-    a.cap_nodes = N;
-    a.cap_brs = K;
-    const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
-    if (sm2 > 220 * 1024) return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
-    CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-    mark(ctx, "start");
-    {
-        int sms = 0, per2 = 0;
-        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, parse_expand_kernel, PP_THREADS, sm2));
-        const long long x = (long long)persistent_ctas(per2, ctx->tune.expand_ctas) * sms;
-        g_expand = (unsigned)(x < tiles ? x : tiles);
-    }
-    parse_expand_kernel<<<g_expand, PP_THREADS, sm2, ctx->stream>>>(a);
-    CK(cudaGetLastError());
-    mark(ctx, "parse_expand_kernel");
+    ctx->est_nodes = (double)N / (double)L;
+    ctx->est_kept = (double)K / (double)L;
     if (want_tree) {
         if ((rc = run_ple(ctx, a.vbuf, N, nullptr, o->parent, T_N_TMIN, a.node_off, nd, dvalid, d_res))) return rc;
     }
@@ -1111,6 +1255,9 @@ int alp_tune_get(const alp_ctx* ctx, int32_t* cfg, int n) {
     cfg[1] = ctx->tune.pairs_ctas;
     cfg[2] = ctx->tune.expand_ctas;
     if (n > 3) cfg[3] = ctx->tune.mlp;
+    if (n > 4) cfg[4] = ctx->tune.lex_split;
+    if (n > 5) cfg[5] = ctx->tune.parse_split;
+    if (n > 6) cfg[6] = scan_g(ctx);
     return ALP_OK;
 }
 
@@ -1119,10 +1266,17 @@ int alp_tune_set(alp_ctx* ctx, const int32_t* cfg, int n) {
     if (cfg[0] < 0 || cfg[0] >= N_PLE_SHAPES || cfg[1] < 0 || cfg[1] > 32 || cfg[2] < 0 || cfg[2] > 32)
         return fail(ctx, ALP_ERR_ARG, "tuning values out of range");
     if (n > 3 && (cfg[3] < 0 || cfg[3] > 1)) return fail(ctx, ALP_ERR_ARG, "MLP kernel choice out of range");
-    if (n > 3) ctx->tune.mlp = cfg[3];
+    if (n > 4 && (cfg[4] < 0 || cfg[4] > 1)) return fail(ctx, ALP_ERR_ARG, "lexer token pass choice out of range");
+    if (n > 5 && (cfg[5] < 0 || cfg[5] > 1)) return fail(ctx, ALP_ERR_ARG, "parser position pass choice out of range");
+    if (n > 6 && cfg[6] != 0 && cfg[6] != 8 && cfg[6] != 16 && cfg[6] != 32)
+        return fail(ctx, ALP_ERR_ARG, "state-scan chunks per lane must be 8, 16 or 32");
     ctx->tune.ple = cfg[0];
     ctx->tune.pairs_ctas = cfg[1];
     ctx->tune.expand_ctas = cfg[2];
+    if (n > 3) ctx->tune.mlp = cfg[3];
+    if (n > 4) ctx->tune.lex_split = cfg[4];
+    if (n > 5) ctx->tune.parse_split = cfg[5];
+    if (n > 6) ctx->tune.scan_g = cfg[6];
     return ALP_OK;
 }
 
@@ -1190,17 +1344,42 @@ int alp_tune_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int reps, char*
         return r;
     };
     // one knob at a time, the others held at their best so far
+    double best = 1e30, ms = 0;
+    int arg = 0;
+    auto knob = [&](const char* what, int* field, const int* values, int count) -> int {
+        best = 1e30;
+        arg = values[0];
+        for (int i = 0; i < count; ++i) {
+            *field = values[i];
+            int r = measure(&ms);
+            if (r) return r;
+            line(what, values[i], ms);
+            if (ms < best) { best = ms; arg = values[i]; }
+        }
+        *field = arg;
+        return ALP_OK;
+    };
+    // lexer: the token pass's form, the state scan's chunks per lane
+    {
+        const int forms[] = {0, 1}, gs[] = {8, 16, 32};
+        if ((rc = knob("lex_token_pass_split", &ctx->tune.lex_split, forms, 2)) ||
+            (rc = knob("lex_scan_chunks_per_lane", &ctx->tune.scan_g, gs, 3)) ||
+            (rc = knob("parse_position_pass_split", &ctx->tune.parse_split, forms, 2)))
+            return done(rc);
+    }
     int fit_pairs = 1, fit_expand = 1;
     {
         const size_t sm1 = pairs_smem_bytes(ctx->pt.n_pairs, ctx->pt.q + ctx->pt.k);
         const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
+        const void* ex = ctx->tune.parse_split ? (const void*)parse_expand_kernel<0, 0, false>
+                                               : fused_expand_for(ctx->pt.q, ctx->pt.k);
         CK(cudaFuncSetAttribute(pairs_kernel_for(ctx->pt.q, ctx->pt.k), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-        CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+        CK(cudaFuncSetAttribute(ex, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit_pairs, pairs_kernel_for(ctx->pt.q, ctx->pt.k), PP_THREADS, sm1));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit_expand, parse_expand_kernel, PP_THREADS, sm2));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit_expand, ex, PP_THREADS, sm2));
     }
-    double best = 1e30, ms = 0;
-    int arg = 0;
+    best = 1e30;
+    arg = 0;
     for (int i = 0; i < N_PLE_SHAPES; ++i) {
         ctx->tune.ple = i;
         if ((rc = measure(&ms))) return done(rc);
@@ -1219,15 +1398,17 @@ int alp_tune_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int reps, char*
         if (ms < best) { best = ms; arg = c; }
     }
     ctx->tune.expand_ctas = arg;
-    best = 1e30;
-    arg = 0;
-    for (int c = 1; c <= fit_pairs; ++c) {
-        ctx->tune.pairs_ctas = c;
-        if ((rc = measure(&ms))) return done(rc);
-        line("pairs_ctas_per_sm", c, ms);
-        if (ms < best) { best = ms; arg = c; }
+    if (ctx->tune.parse_split) {  // the pair kernel runs only in the two-pass form
+        best = 1e30;
+        arg = 0;
+        for (int c = 1; c <= fit_pairs; ++c) {
+            ctx->tune.pairs_ctas = c;
+            if ((rc = measure(&ms))) return done(rc);
+            line("pairs_ctas_per_sm", c, ms);
+            if (ms < best) { best = ms; arg = c; }
+        }
+        ctx->tune.pairs_ctas = arg;
     }
-    ctx->tune.pairs_ctas = arg;
     line("best_ms", 0, best);
     return done(ALP_OK);
 }
@@ -2412,9 +2593,9 @@ int parse_positions_dev(alp_ctx* ctx, long long Lcap, const long long* dL, long 
     const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
     if (sm2 > 220 * 1024) return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
     CK(cudaFuncSetAttribute(pairs_kernel_for(ctx->pt.q, ctx->pt.k), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-    CK(cudaFuncSetAttribute(parse_expand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    CK(cudaFuncSetAttribute(parse_expand_kernel<0, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, pairs_kernel_for(ctx->pt.q, ctx->pt.k), PP_THREADS, sm1));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, parse_expand_kernel, PP_THREADS, sm2));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, parse_expand_kernel<0, 0, false>, PP_THREADS, sm2));
     const long long x1 = (long long)persistent_ctas(per1, ctx->tune.pairs_ctas) * sms,
                     x2 = (long long)persistent_ctas(per2, ctx->tune.expand_ctas) * sms;
     {
@@ -2431,7 +2612,7 @@ int parse_positions_dev(alp_ctx* ctx, long long Lcap, const long long* dL, long 
                                                                          a.br_off, nd, dL);
         CK(cudaGetLastError());
     }
-    parse_expand_kernel<<<(unsigned)(x2 < tiles ? x2 : tiles), PP_THREADS, sm2, ctx->stream>>>(a);
+    parse_expand_kernel<0, 0, false><<<(unsigned)(x2 < tiles ? x2 : tiles), PP_THREADS, sm2, ctx->stream>>>(a);
     CK(cudaGetLastError());
     if ((rc = run_ple(ctx, a.vbuf, cap_nodes, nullptr, o.parent, T_N_TMIN, a.node_off, nd, dvalid, d_res,
                       &d_res->aux[0])))

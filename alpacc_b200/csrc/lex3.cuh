@@ -38,8 +38,8 @@ constexpr int LX_TILE = LX_THREADS * LX_CHUNK;  // 8 KiB emit tile: one chunk pe
 constexpr int LX_WIDE = 2 * LX_TILE;            // 16 KiB fold / count tile: two chunks per thread
 constexpr int LX_STAGE = 2048;                  // tokens one emit tile stages in shared memory
 constexpr int LS_WARPS = 8;
-constexpr int LS_G = 16;                        // chunks per lane in the state scan
-constexpr int LS_TILE = LS_WARPS * 32 * LS_G;   // 4096 chunks per state-scan tile
+constexpr int LS_G = 16;                        // chunks per lane in the state scan (default; 8, 16 or 32)
+__host__ __device__ constexpr long long ls_tile(int g) { return (long long)LS_WARPS * 32 * g; }  // chunks per scan tile
 
 // ent entries: next state | flags.  Rows are LX_ROW entries apart so that
 // lanes reading the same byte in different states hit different banks.
@@ -94,7 +94,7 @@ struct Lex3Args {
     AlpResult* res;
     unsigned int num_tiles;        // 8 KiB tiles
     unsigned int num_wide;         // 16 KiB tiles
-    unsigned int num_scan_tiles;   // LS_TILE-chunk tiles
+    unsigned int num_scan_tiles;   // ls_tile(G)-chunk tiles of the state scan
     LexCarry* carry;               // stream piece: entry state and token start (null: plain input)
     long long pos_base;            // stream position of in[0] (added to output positions)
     int carry_tokens;              // outputs start at index carry->tokens - tok_first (else 0)
@@ -249,7 +249,10 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_fold_kernel(Lex3Args a, Le
 }
 
 // ---- kernel 2: states entering the chunks -----------------------------------
+// G chunks per lane (a tuned launch shape: 8, 16 or 32).
+template <int G>
 __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
+    static_assert(G == 8 || G == 16 || G == 32, "chunks per lane");
     extern __shared__ __align__(16) uint8_t smem[];
     const uint32_t rows = (uint32_t)(a.t.E + a.t.S);
     uint8_t* s_app = smem;
@@ -271,18 +274,20 @@ __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
         __syncthreads();
         const uint32_t tile = s_tile;
         if (tile >= a.num_scan_tiles) break;
-        const long long base = (long long)tile * LS_TILE + (long long)warp * (32 * LS_G) + (long long)lane * LS_G;
+        const long long base = (long long)tile * ls_tile(G) + (long long)warp * (32 * G) + (long long)lane * G;
 
-        // this lane's 16 chunk endomorphisms, two per word
-        uint32_t fr[LS_G / 2];
-        if (base + LS_G <= M) {
+        // this lane's G chunk endomorphisms, two per word
+        uint32_t fr[G / 2];
+        if (base + G <= M) {
             const uint4* p = reinterpret_cast<const uint4*>(a.chunk_f + base);
-            const uint4 v0 = p[0], v1 = p[1];
-            fr[0] = v0.x; fr[1] = v0.y; fr[2] = v0.z; fr[3] = v0.w;
-            fr[4] = v1.x; fr[5] = v1.y; fr[6] = v1.z; fr[7] = v1.w;
+#pragma unroll
+            for (int v = 0; v < G / 8; ++v) {
+                const uint4 x = p[v];
+                fr[4 * v] = x.x; fr[4 * v + 1] = x.y; fr[4 * v + 2] = x.z; fr[4 * v + 3] = x.w;
+            }
         } else {
 #pragma unroll
-            for (int q = 0; q < LS_G / 2; ++q) {
+            for (int q = 0; q < G / 2; ++q) {
                 const uint32_t lo = base + 2 * q < M ? a.chunk_f[base + 2 * q] : 0u;
                 const uint32_t hi = base + 2 * q + 1 < M ? a.chunk_f[base + 2 * q + 1] : 0u;
                 fr[q] = lo | (hi << 16);
@@ -294,7 +299,7 @@ __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
         for (int l2 = 0; l2 < 32; ++l2) {
             s_sv[warp][l2][lane] = (uint8_t)cur;
 #pragma unroll
-            for (int q = 0; q < LS_G / 2; ++q) {
+            for (int q = 0; q < G / 2; ++q) {
                 const uint32_t v = __shfl_sync(ALP_FULL_MASK, fr[q], l2);
                 cur = s_app[(v & 0xffffu) * 32 + cur];
                 cur = s_app[(v >> 16) * 32 + cur];
@@ -350,19 +355,28 @@ __global__ void __launch_bounds__(LS_WARPS * 32) lex3_scan_kernel(Lex3Args a) {
 
         const uint32_t win = s_wpre[warp][s_sin & 31u];
         uint32_t st = s_sv[warp][lane][win];
-        uint32_t ob[LS_G / 4] = {0, 0, 0, 0};
+        uint32_t ob[G / 4];
 #pragma unroll
-        for (int q = 0; q < LS_G / 2; ++q) {
+        for (int q = 0; q < G / 4; ++q) ob[q] = 0;
+#pragma unroll
+        for (int q = 0; q < G / 2; ++q) {
             ob[q >> 1] |= st << (16 * (q & 1));
             st = s_app[(fr[q] & 0xffffu) * 32 + st];
             ob[q >> 1] |= st << (16 * (q & 1) + 8);
             st = s_app[(fr[q] >> 16) * 32 + st];
         }
-        if (base + LS_G <= M) {
-            *reinterpret_cast<uint4*>(a.chunk_s + base) = make_uint4(ob[0], ob[1], ob[2], ob[3]);
+        if (base + G <= M) {
+            if constexpr (G == 8) {
+                *reinterpret_cast<uint2*>(a.chunk_s + base) = make_uint2(ob[0], ob[1]);
+            } else {
+#pragma unroll
+                for (int v = 0; v < G / 16; ++v)
+                    reinterpret_cast<uint4*>(a.chunk_s + base)[v] =
+                        make_uint4(ob[4 * v], ob[4 * v + 1], ob[4 * v + 2], ob[4 * v + 3]);
+            }
         } else {
 #pragma unroll
-            for (int g = 0; g < LS_G; ++g)
+            for (int g = 0; g < G; ++g)
                 if (base + g < M) a.chunk_s[base + g] = (uint8_t)(ob[g >> 2] >> (8 * (g & 3)));
         }
         __syncthreads();
@@ -793,6 +807,347 @@ __global__ void __launch_bounds__(LX_THREADS, 6) lex3_emit_kernel(Lex3Args a, Le
                     bk = base_of(d0, dmax, dk);
                 }
                 put((long long)(Xc + k) + sent * (2 * dk + 1), pk >> 16, spos(s_st[k], bk), en - bk + pb);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---- kernel 3+4+5 fused: counts, look-back over tiles, tokens ---------------
+// One pass over the input for what lex3_count_kernel, the tile scan and
+// lex3_emit_kernel do in three: each thread runs the DFA over its chunk once
+// from its known state, counting the tokens that end in it and keeping each
+// token's place and terminal as a record in shared memory; a block scan places
+// the threads in the tile; the tile publishes its (count, last start) and
+// finds its exclusive prefix by a decoupled look-back over earlier tiles
+// (futhark/lexer.fut:83-84,108-133: the take_right start scan and the
+// compaction offsets); the tokens go from the records into the stage and out
+// with coalesced stores.  Tiles come in ticket order, so every tile a
+// look-back waits for is running or done.  Tiles with document boundaries,
+// partial chunks or more tokens than the stage holds take their prefix first
+// and write through the compact loop of lex3_emit_kernel.
+//
+// Look-back word of a tile: [63:62] flag, [61:31] token count, [30:0] last
+// kept token start (LX_LB_NONE: none); the inclusive prefix once flagged P.
+// Inputs are below 2^31 bytes, so counts and positions fit 31 bits.
+constexpr uint32_t LX_LB_NONE = 0x7fffffffu;
+constexpr int LX_REC = 16;               // token records a thread keeps from its counting pass
+constexpr int LX_REC_ROW = LX_REC + 2;      // u16 per thread row: 9 words, an odd stride across lanes
+__host__ __device__ inline size_t lex3_tok_smem(int S) {
+    return lex3_stage_off(S) + (size_t)LX_STAGE * 8 + (size_t)LX_THREADS * LX_REC_ROW * 2;
+}
+
+__device__ __forceinline__ unsigned long long tk_pack(uint32_t flag, uint32_t c, uint32_t p) {
+    return ((unsigned long long)flag << 62) | ((unsigned long long)(c & 0x7fffffffu) << 31) |
+           (p == ALP_NONE32 ? LX_LB_NONE : (p & 0x7fffffffu));
+}
+__device__ __forceinline__ uint32_t tk_count(unsigned long long w) { return (uint32_t)(w >> 31) & 0x7fffffffu; }
+__device__ __forceinline__ uint32_t tk_pos(unsigned long long w) {
+    const uint32_t p = (uint32_t)w & 0x7fffffffu;
+    return p == LX_LB_NONE ? ALP_NONE32 : p;
+}
+
+// Warp 0: the (count, last start) of all tiles before `tile`, from the
+// look-back words; then publishes this tile's inclusive prefix.
+__device__ __forceinline__ void tk_lookback(unsigned long long* lb, unsigned tile, uint32_t Bc, uint32_t Bp,
+                                            unsigned int* err, uint32_t* s_xc, uint32_t* s_xp) {
+    const int lane = threadIdx.x & 31;
+    uint32_t Xc = 0, Xp = ALP_NONE32;
+    if (tile > 0) {
+        long long end = tile;
+        for (;;) {
+            const long long idx = end - 32 + lane;
+            const unsigned long long w2 = idx >= 0 ? wait64(&lb[idx], err) : tk_pack(ST_P, 0, ALP_NONE32);
+            const uint32_t pm = __ballot_sync(ALP_FULL_MASK, (uint32_t)(w2 >> 62) == ST_P);
+            const int p = pm ? 31 - __clz(pm) : -1;
+            uint32_t vc = lane >= p ? tk_count(w2) : 0u;
+            uint32_t vp = lane >= p ? tk_pos(w2) : ALP_NONE32;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {  // lanes in order: sum, take-right
+                const uint32_t oc = __shfl_down_sync(ALP_FULL_MASK, vc, d);
+                const uint32_t op = __shfl_down_sync(ALP_FULL_MASK, vp, d);
+                if (lane + d < 32) {
+                    vc += oc;
+                    if (op != ALP_NONE32) vp = op;
+                }
+            }
+            Xc += __shfl_sync(ALP_FULL_MASK, vc, 0);
+            vp = __shfl_sync(ALP_FULL_MASK, vp, 0);
+            if (Xp == ALP_NONE32) Xp = vp;
+            if (pm) break;
+            end -= 32;
+        }
+        if (lane == 0) st_volatile64(&lb[tile], tk_pack(ST_P, Xc + Bc, Bp != ALP_NONE32 ? Bp : Xp));
+    }
+    if (lane == 0) { *s_xc = Xc; *s_xp = Xp; }
+}
+
+template <typename TermT, typename PosT>
+__global__ void __launch_bounds__(LX_THREADS, 5) lex3_tok_kernel(Lex3Args a, LexSeg sg) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int S = a.t.S;
+    uint16_t* s_ent = reinterpret_cast<uint16_t*>(smem);
+    uint32_t* s_tok = reinterpret_cast<uint32_t*>(smem + lex3_tok_off(S));
+    uint32_t* s_pk = reinterpret_cast<uint32_t*>(smem + lex3_stage_off(S));  // end - t0 | term << 16
+    uint32_t* s_st = s_pk + LX_STAGE;                                        // start (absolute; NONE: before the tile)
+    uint16_t* s_rec = reinterpret_cast<uint16_t*>(s_st + LX_STAGE);          // [thread][LX_REC_ROW]: j | term << 5
+
+    __shared__ unsigned long long s_dmax;
+    __shared__ uint32_t s_head[LX_TILE / LX_CHUNK], s_last[LX_TILE / LX_CHUNK];
+    __shared__ uint32_t s_wc[LX_THREADS / 32], s_wp[LX_THREADS / 32];
+    __shared__ uint32_t s_doff[LX_DOCS];
+    __shared__ uint32_t s_tile, s_xc, s_xp;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(a.t.ent);
+        uint4* dst = reinterpret_cast<uint4*>(s_ent);
+        for (int i = tid; i < (S * LX_ROW * 2 + 15) / 16; i += LX_THREADS) dst[i] = src[i];
+    }
+    for (int i = tid; i < S; i += LX_THREADS) s_tok[i] = a.t.tokinfo[i];
+    const long long n = a.n;
+    const long long ND = sg.n_docs;
+    unsigned long long* lb = a.tile_cs;
+    auto doc_of = [&](long long d0, long long dmax, long long p) -> long long {
+        if (dmax == d0) return d0;
+        if (dmax - d0 < LX_DOCS) {
+            int lo = 0, hi = (int)(dmax - d0);
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if ((long long)s_doff[mid] <= p) lo = mid; else hi = mid - 1;
+            }
+            return d0 + lo;
+        }
+        return doc_upper(sg.doc_off, d0, dmax, p);
+    };
+    auto base_of = [&](long long d0, long long dmax, long long d) -> long long {
+        return (dmax - d0 < LX_DOCS) ? (long long)s_doff[d - d0] : sg.doc_off[d];
+    };
+    const uint32_t INIT = 1u;
+    TermT* o_term = reinterpret_cast<TermT*>(a.out_term);
+    PosT* o_start = reinterpret_cast<PosT*>(a.out_start);
+    PosT* o_end = reinterpret_cast<PosT*>(a.out_end);
+    const long long sent = sg.sentinels ? 1 : 0;
+    auto put = [&](long long idx, uint32_t term, long long st, long long en) {
+        if (idx < a.cap) {
+            o_term[idx] = (TermT)term;
+            o_start[idx] = (PosT)st;
+            o_end[idx] = (PosT)en;
+        } else {
+            atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
+        }
+    };
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(&a.tickets[1], 1u);
+        __syncthreads();
+        const unsigned tile = s_tile;
+        if (tile >= a.num_tiles) break;
+        const long long t0 = (long long)tile * LX_TILE;
+        const long long t1 = min(t0 + LX_TILE, n) - 1;
+        const long long d0 = ND > 1 ? a.tile_doc[tile] : 0;
+        if (tid == 0) s_dmax = (unsigned long long)d0;
+        s_head[tid] = 0;
+        s_last[tid] = 0;
+        __syncthreads();
+        lx_mark_docs(sg, n, d0, t0, t1, s_head, s_last, &s_dmax, s_doff);
+        __syncthreads();
+        const long long dmax = (long long)s_dmax;
+        const long long my = t0 + (long long)tid * LX_CHUNK;
+        const int lim = (int)max(0ll, min((long long)LX_CHUNK, n - my));
+        const uint32_t rel = (uint32_t)(my - t0);
+
+        uint4 w[2];
+        uint32_t s0 = INIT, head = 0, last = 0;
+        long long mydoc = d0;
+        if (lim > 0) {
+            lx_load<2>(a, my, lim, w);
+            s0 = a.chunk_s[my / LX_CHUNK];
+            head = s_head[tid];
+            last = s_last[tid];
+            mydoc = doc_of(d0, dmax, my);
+        } else {
+            w[0] = w[1] = make_uint4(0, 0, 0, 0);
+        }
+        const bool fast = lim == LX_CHUNK && (head | last) == 0;
+
+        // ---- counting pass: tokens ending in the chunk, its starts, records ----
+        uint32_t cnt = 0, lastp = ALP_NONE32, smask = 0;
+        if (fast) {
+            uint32_t st = s0;
+#pragma unroll
+            for (int j = 0; j < LX_CHUNK; ++j) {
+                const uint32_t e = s_ent[st * LX_ROW + byte_of(w, j)];
+                if (e & LX_EMIT) {
+                    if (cnt < (uint32_t)LX_REC) s_rec[tid * LX_REC_ROW + cnt] = (uint16_t)(j | ((e >> LX_TERM_SHIFT) << 5));
+                    ++cnt;
+                }
+                if (e & LX_START) smask |= 1u << j;
+                st = e & LX_NEXT;
+            }
+            if (smask) lastp = (uint32_t)(my + 31 - __clz(smask));
+        } else if (lim > 0) {
+            uint32_t lo;
+            cnt = lx_count_slow(a.in + my, lim, s0, head, last, s_ent, s_tok, &lo);
+            if (lo != LX_NOOFF) lastp = (uint32_t)(my + lo);
+        }
+
+        // ---- place in the tile: block scan of (count, last start) --------------
+        uint32_t ic = cnt, ip = lastp;
+        warp_scan_cs(ic, ip, lane);
+        uint32_t ec = __shfl_up_sync(ALP_FULL_MASK, ic, 1), ep = __shfl_up_sync(ALP_FULL_MASK, ip, 1);
+        if (lane == 0) { ec = 0; ep = ALP_NONE32; }
+        if (lane == 31) { s_wc[warp] = ic; s_wp[warp] = ip; }
+        const int slow_any = __syncthreads_or(lim > 0 && !fast);
+        uint32_t wc = 0, wp = ALP_NONE32, Bc = 0, Bp = ALP_NONE32;
+#pragma unroll
+        for (int w2 = 0; w2 < LX_THREADS / 32; ++w2) {
+            const uint32_t c2 = s_wc[w2], p2 = s_wp[w2];
+            if (w2 < warp) {
+                wc += c2;
+                if (p2 != ALP_NONE32) wp = p2;
+            }
+            Bc += c2;
+            if (p2 != ALP_NONE32) Bp = p2;
+        }
+        const bool staged = Bc <= (uint32_t)LX_STAGE;
+        const bool early = slow_any || !staged;  // the tile needs its prefix before it writes tokens
+        const uint32_t kx = wc + ec;              // the tile's tokens before this thread
+        const uint32_t curx = ep != ALP_NONE32 ? ep : wp;  // last start in the tile before this thread
+        if (tid == 0) {
+            if (tile == 0) st_volatile64(&lb[0], tk_pack(ST_P, Bc, Bp));
+            else st_volatile64(&lb[tile], tk_pack(ST_A, Bc, Bp));
+        }
+        if (early) {
+            if (warp == 0) tk_lookback(lb, tile, Bc, Bp, &a.res->error, &s_xc, &s_xp);
+            __syncthreads();
+        } else if (warp == 0) {
+            // the look-back first, while the other warps move their records to the stage
+            tk_lookback(lb, tile, Bc, Bp, &a.res->error, &s_xc, &s_xp);
+        }
+
+        // ---- tokens -----------------------------------------------------------------
+        if (fast && staged) {
+            uint32_t k = kx;
+            if (cnt <= (uint32_t)LX_REC) {
+                for (uint32_t r = 0; r < cnt; ++r) {
+                    const uint32_t rec = s_rec[tid * LX_REC_ROW + r];
+                    const uint32_t j = rec & 31u;
+                    const uint32_t m = smask & ((1u << j) - 1u);
+                    s_pk[k] = (rel + j) | ((rec >> 5) << 16);
+                    s_st[k] = m ? (uint32_t)(my + 31 - __clz(m)) : curx;
+                    ++k;
+                }
+            } else {
+                uint32_t st = s0, cur = curx;
+#pragma unroll
+                for (int j = 0; j < LX_CHUNK; ++j) {
+                    const uint32_t e = s_ent[st * LX_ROW + byte_of(w, j)];
+                    if (e & LX_EMIT) {
+                        s_pk[k] = (rel + j) | ((e >> LX_TERM_SHIFT) << 16);
+                        s_st[k] = cur;
+                        ++k;
+                    }
+                    if (e & LX_START) cur = (uint32_t)(my + j);
+                    st = e & LX_NEXT;
+                }
+            }
+        } else if (lim > 0) {
+            // an early tile: every thread's global place is known
+            uint32_t tcount = s_xc + kx;
+            uint32_t cur = curx != ALP_NONE32 ? curx : s_xp;
+            uint32_t st = s0;
+            long long doc = mydoc;
+            long long base = base_of(d0, dmax, doc);
+            auto tok = [&](uint32_t term, uint32_t st_abs, uint32_t en_abs) {
+                if (staged) {
+                    const uint32_t k = tcount - s_xc;
+                    s_pk[k] = (uint32_t)(en_abs - t0) | (term << 16);
+                    s_st[k] = st_abs;
+                } else {
+                    put((long long)tcount + sent * (2 * doc + 1), term, st_abs == ALP_NONE32 ? 0 : (long long)st_abs - base,
+                        (long long)en_abs - base);
+                }
+                ++tcount;
+            };
+#pragma unroll 1
+            for (int j = 0; j < lim; ++j) {
+                const long long pos = my + j;
+                if ((head >> j) & 1u) {
+                    // every document starting here (empty ones first, then the real one)
+                    doc = doc_of(d0, dmax, pos);
+                    long long dl = doc;
+                    while (dl > 0 && sg.doc_off[dl - 1] >= pos) --dl;
+                    base = pos;
+                    for (long long e2 = dl; e2 <= doc; ++e2) {
+                        sg.tok_off[e2] = tcount;
+                        if (sent) put((long long)tcount + 2 * e2, sg.sent_l, 0, 0);
+                        if (e2 < doc) {
+                            sg.valid[e2] = 0;
+                            if (sent) put((long long)tcount + 2 * e2 + 1, sg.sent_r, 0, 0);
+                        }
+                    }
+                    cur = (uint32_t)pos;
+                    st = INIT;
+                }
+                const uint32_t e = s_ent[st * LX_ROW + __ldg(a.in + pos)];
+                if (e & LX_EMIT) tok(e >> LX_TERM_SHIFT, cur, (uint32_t)pos);
+                if (e & LX_START) cur = (uint32_t)pos;
+                st = e & LX_NEXT;
+                if ((last >> j) & 1u) {
+                    const uint32_t ti = s_tok[st];
+                    if (!(ti & TOK_IGNORE)) tok(ti & TOK_TERM_MASK, cur, (uint32_t)(pos + 1));
+                    sg.valid[doc] = (ti & TOK_ACCEPT) ? 1 : 0;
+                    if (sent) put((long long)tcount + 2 * doc + 1, sg.sent_r, 0, 0);
+                }
+            }
+            mydoc = doc;
+            if (my <= n - 1 && n - 1 < my + LX_CHUNK) {
+                // documents that start at n (empty, at the end) and the closing offset
+                for (long long e2 = mydoc + 1; e2 < ND; ++e2) {
+                    sg.tok_off[e2] = tcount;
+                    sg.valid[e2] = 0;
+                    if (sent) {
+                        put((long long)tcount + 2 * e2, sg.sent_l, 0, 0);
+                        put((long long)tcount + 2 * e2 + 1, sg.sent_r, 0, 0);
+                    }
+                }
+                sg.tok_off[ND] = tcount;
+                a.res->count = tcount;
+                a.res->valid = 1;
+            }
+        }
+        __syncthreads();
+
+        // ---- coalesced copy of the staged tokens ---------------------------------
+        const uint32_t Xc = s_xc, Xp = s_xp;
+        auto sres = [&](uint32_t sv) -> uint32_t { return sv != ALP_NONE32 ? sv : Xp; };
+        if (staged && dmax == d0) {
+            // one document in the tile: every token's index and positions shift alike
+            const long long ib = (long long)Xc + sent * (2 * d0 + 1);
+            const long long off = -base_of(d0, dmax, d0);
+            for (uint32_t k = tid; k < Bc; k += LX_THREADS) {
+                const uint32_t pk = s_pk[k], sv = sres(s_st[k]);
+                const long long idx = ib + k;
+                if (idx < a.cap) {
+                    o_term[idx] = (TermT)(pk >> 16);
+                    o_start[idx] = (PosT)(sv == ALP_NONE32 ? 0 : (long long)sv + off);
+                    o_end[idx] = (PosT)(t0 + (pk & 0xffffu) + off);
+                } else {
+                    atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
+                }
+            }
+        } else if (staged) {
+            const long long b0 = base_of(d0, dmax, d0);
+            for (uint32_t k = tid; k < Bc; k += LX_THREADS) {
+                const uint32_t pk = s_pk[k], sv = sres(s_st[k]);
+                const long long en = t0 + (pk & 0xffffu);
+                long long dk = d0, bk = b0;
+                if (dmax > d0) {
+                    dk = doc_of(d0, dmax, en - 1);
+                    bk = base_of(d0, dmax, dk);
+                }
+                put((long long)(Xc + k) + sent * (2 * dk + 1), pk >> 16, sv == ALP_NONE32 ? 0 : (long long)sv - bk,
+                    en - bk);
             }
         }
         __syncthreads();

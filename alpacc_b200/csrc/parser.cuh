@@ -330,6 +330,11 @@ struct ParseArgs {
     long long cap_nodes;
     long long cap_brs;
     const long long* dL;        // when set: the position count, in device memory (L is then its capacity)
+    // the fused pair + expand pass: tile tickets and look-back over the position sums
+    unsigned int* ticket;       // [1], zero before the launch
+    uint32_t* lb_flag;          // [tiles] ST_X / ST_A / ST_P << 30, zero before the launch
+    PosSums* lb_agg;            // [tiles] the tile's own sums
+    PosSums* lb_inc;            // [tiles] the sums up to and including the tile
 };
 
 __device__ __forceinline__ uint32_t pos_term(const ParseArgs& a, long long i) {
@@ -652,6 +657,96 @@ __device__ __forceinline__ void ex_words(const ParseArgs& a, long long i0, uint2
     }
 }
 
+// The fused form's look-back over tiles: warp 0 publishes the tile's own
+// sums, combines the sums of earlier tiles (nearest first, 32 at a time) until
+// it meets an inclusive prefix, and publishes this tile's inclusive prefix.
+// Payloads are written before their flag with a fence in between; a reader
+// fences after it sees the flag.
+__device__ __forceinline__ PosSums ps_ld(const PosSums* p) {
+    const volatile uint4* v = reinterpret_cast<const volatile uint4*>(p);
+    const uint4 x = make_uint4(v[0].x, v[0].y, v[0].z, v[0].w), y = make_uint4(v[1].x, v[1].y, v[1].z, v[1].w);
+    PosSums r;
+    r.nodes = x.x; r.brs = x.y; r.depth = (int32_t)x.z; r.v = (int32_t)x.w;
+    r.terms = y.x; r.heads = y.y; r.hpos = (int32_t)y.z; r.cls = y.w;
+    return r;
+}
+__device__ __forceinline__ void ps_st(PosSums* p, const PosSums& r) {
+    volatile uint4* v = reinterpret_cast<volatile uint4*>(p);
+    v[0].x = r.nodes; v[0].y = r.brs; v[0].z = (uint32_t)r.depth; v[0].w = (uint32_t)r.v;
+    v[1].x = r.terms; v[1].y = r.heads; v[1].z = (uint32_t)r.hpos; v[1].w = r.cls;
+}
+__device__ __forceinline__ PosSums ps_shfl_down(const PosSums& x, int d) {
+    PosSums r;
+    r.nodes = __shfl_down_sync(ALP_FULL_MASK, x.nodes, d);
+    r.brs = __shfl_down_sync(ALP_FULL_MASK, x.brs, d);
+    r.depth = __shfl_down_sync(ALP_FULL_MASK, x.depth, d);
+    r.v = __shfl_down_sync(ALP_FULL_MASK, x.v, d);
+    r.terms = __shfl_down_sync(ALP_FULL_MASK, x.terms, d);
+    r.heads = __shfl_down_sync(ALP_FULL_MASK, x.heads, d);
+    r.hpos = __shfl_down_sync(ALP_FULL_MASK, x.hpos, d);
+    r.cls = __shfl_down_sync(ALP_FULL_MASK, x.cls, d);
+    return r;
+}
+__device__ __forceinline__ PosSums ps_lookback(const ParseArgs& a, long long tile, const PosSums& agg) {
+    const int lane = threadIdx.x & 31;
+    PosSums acc;
+    possums_zero(acc);
+    if (tile == 0) {
+        if (lane == 0) {
+            ps_st(&a.lb_inc[0], agg);
+            __threadfence();
+            st_volatile32(&a.lb_flag[0], ST_P << 30);
+        }
+        return acc;
+    }
+    if (lane == 0) {
+        ps_st(&a.lb_agg[tile], agg);
+        __threadfence();
+        st_volatile32(&a.lb_flag[tile], ST_A << 30);
+    }
+    long long end = tile;
+    for (;;) {
+        const long long idx = end - 32 + lane;
+        uint32_t f = ST_P;
+        if (idx >= 0) f = wait32(&a.lb_flag[idx], &a.res->error) >> 30;
+        const uint32_t pm = __ballot_sync(ALP_FULL_MASK, f == ST_P && idx >= 0);
+        const int p = pm ? 31 - __clz(pm) : -1;
+        __threadfence();
+        PosSums x;
+        possums_zero(x);
+        if (idx >= 0 && lane >= p) x = lane == p ? ps_ld(&a.lb_inc[idx]) : ps_ld(&a.lb_agg[idx]);
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {  // lanes in order
+            const PosSums o = ps_shfl_down(x, d);
+            if (lane + d < 32) x = ps_combine(x, o);
+        }
+        PosSums win;
+        win.nodes = __shfl_sync(ALP_FULL_MASK, x.nodes, 0);
+        win.brs = __shfl_sync(ALP_FULL_MASK, x.brs, 0);
+        win.depth = __shfl_sync(ALP_FULL_MASK, x.depth, 0);
+        win.v = __shfl_sync(ALP_FULL_MASK, x.v, 0);
+        win.terms = __shfl_sync(ALP_FULL_MASK, x.terms, 0);
+        win.heads = __shfl_sync(ALP_FULL_MASK, x.heads, 0);
+        win.hpos = __shfl_sync(ALP_FULL_MASK, x.hpos, 0);
+        win.cls = __shfl_sync(ALP_FULL_MASK, x.cls, 0);
+        acc = ps_combine(win, acc);
+        if (pm) break;
+        end -= 32;
+    }
+    if (lane == 0) {
+        ps_st(&a.lb_inc[tile], ps_combine(acc, agg));
+        __threadfence();
+        st_volatile32(&a.lb_flag[tile], ST_P << 30);
+    }
+    return acc;
+}
+
+// FUSED (QT, KT as in parse_pairs_kernel): the pair ids come from the key
+// windows of a shared-memory copy of the tile's terminals, and the tile's
+// exclusive position sums from a look-back over earlier tiles (tiles taken in
+// ticket order, so every tile a look-back waits for is running or done).  The
+// pair kernel, the tile-sum scans and the pair-id array are then not needed.
+template <int QT, int KT, bool FUSED>
 __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     PairInfo* s_pi = reinterpret_cast<PairInfo*>(smem);
@@ -663,27 +758,89 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     // the node windows; a record stays one 16-byte store)
     int4* s_pos = reinterpret_cast<int4*>(smem + expand_tables_bytes(a.t.n_pairs, a.t.n_pseq, a.t.n_stack));
     uint16_t* s_own = reinterpret_cast<uint16_t*>(s_pos + PP_TILE * 5 / 4);  // [EX_WIN] owner of each node
+    // FUSED: the tile's terminals [base - q - 1, base + PP_TILE + k), before s_own is used
+    uint32_t* s_term = reinterpret_cast<uint32_t*>(s_own);
+    static_assert((PP_TILE + 17 + 1) * 4 <= 2 * EX_WIN, "the key window fits the owner array");
     __shared__ PosSums s_w[PP_THREADS / 32];
-    __shared__ uint32_t s_tn;
+    __shared__ PosSums s_tp;
+    __shared__ uint32_t s_tn, s_tile;
+    __shared__ uint32_t s_pow[17];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int q = QT > 0 ? QT : a.t.q, k = KT > 0 ? KT : a.t.k, W = q + k;
     if (a.dL) a.L = *a.dL;
     for (int i = tid; i < a.t.n_pairs * (int)(sizeof(PairInfo) / 4); i += PP_THREADS)
         reinterpret_cast<uint32_t*>(s_pi)[i] = reinterpret_cast<const uint32_t*>(a.t.pairs)[i];
     for (int i = tid; i < a.t.n_pseq; i += PP_THREADS) s_prec[i] = a.t.pseq_rec[i];
     for (int i = tid; i < a.t.n_stack; i += PP_THREADS) s_srec[i] = a.t.stack_rec[i];
-    const uint32_t SL = a.t.start, SR = a.t.end;
+    if (FUSED && tid == 0) {
+        uint32_t pw = 1;
+        for (int j = 0; j < W; ++j) { s_pow[W - 1 - j] = pw; pw *= (uint32_t)a.t.T; }
+    }
+    const uint32_t SL = a.t.start, SR = a.t.end, EMPTY = a.t.empty;
     const long long n_tiles = (a.L + PP_TILE - 1) / PP_TILE;
-    // this thread's pair ids and terminals, one tile ahead (loads in flight
-    // while the block works on the current tile)
-    uint2 nw, nt;
-    ex_words(a, (long long)blockIdx.x * PP_TILE + tid * PP_ITEMS, nw, nt);
-    for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    // (not fused) this thread's pair ids and terminals, one tile ahead (loads in
+    // flight while the block works on the current tile)
+    uint2 nw = make_uint2(0, 0), nt = make_uint2(0, 0);
+    if (!FUSED) ex_words(a, (long long)blockIdx.x * PP_TILE + tid * PP_ITEMS, nw, nt);
+    for (long long it = blockIdx.x;; it += gridDim.x) {
         __syncthreads();  // the previous tile is done with the shared arrays
+        long long tile = it;
+        if (FUSED) {
+            if (tid == 0) s_tile = atomicAdd(a.ticket, 1u);
+            __syncthreads();
+            tile = s_tile;
+        }
+        if (tile >= n_tiles) break;
         const long long i0 = tile * PP_TILE + tid * PP_ITEMS;
-        const PosSums tp = a.tile_sums[tile];
+        PosSums tp;
         uint16_t ids[PP_ITEMS];
         uint32_t hm = 0, em = 0;  // head / end bits of this thread's positions
-        {
+        uint32_t prev_id = NO_PAIR, next_id = NO_PAIR;
+        bool next_head = false;
+        if (FUSED) {
+            const long long base = tile * PP_TILE;
+            for (int i = tid; i < PP_TILE + W + 1; i += PP_THREADS) s_term[i] = pos_term(a, base - q - 1 + i);
+            __syncthreads();
+            // the pair id at tile-local position pl; s_term[pl + 1 + jj] is position base + pl - q + jj
+            auto pair_at = [&](int pl) -> uint16_t {
+                const int o = pl + 1;
+                const uint32_t c = s_term[o + q];
+                uint32_t x = c * s_pow[q];
+                bool ok = c != SL;  // a window never reaches past its document's ⊢ (left) or ⊣ (right)
+#pragma unroll
+                for (int jj = q - 1; jj >= 0; --jj) {
+                    const uint32_t t = s_term[o + jj];
+                    x += (ok ? t : EMPTY) * s_pow[jj];
+                    ok = ok && t != SL;
+                }
+                ok = c != SR;
+#pragma unroll
+                for (int jj = q + 1; jj < W; ++jj) {
+                    const uint32_t t = s_term[o + jj];
+                    x += (ok ? t : EMPTY) * s_pow[jj];
+                    ok = ok && t != SR;
+                }
+                return __ldg(&a.t.key_index[x]);
+            };
+            const int pl0 = tid * PP_ITEMS;
+            if (lane == 0 && i0 > 0 && i0 - 1 < a.L) prev_id = pair_at(pl0 - 1);
+            if (lane == 31 && i0 + PP_ITEMS < a.L) {
+                next_id = pair_at(pl0 + PP_ITEMS);
+                next_head = s_term[pl0 + PP_ITEMS + 1 + q] == SL;
+            }
+#pragma unroll
+            for (int j = 0; j < PP_ITEMS; ++j) {
+                ids[j] = NO_PAIR;
+                if (i0 + j < a.L) {
+                    ids[j] = pair_at(pl0 + j);
+                    const uint32_t c = s_term[pl0 + j + 1 + q];
+                    if (c == SL) hm |= 1u << j;
+                    if (c == SR) em |= 1u << j;
+                }
+            }
+            possums_zero(tp);
+        } else {
+            tp = a.tile_sums[tile];
             const uint32_t c[PP_ITEMS] = {nt.x & 0xffffu, nt.x >> 16, nt.y & 0xffffu, nt.y >> 16};
             ids[0] = (uint16_t)nw.x; ids[1] = (uint16_t)(nw.x >> 16); ids[2] = (uint16_t)nw.y; ids[3] = (uint16_t)(nw.y >> 16);
 #pragma unroll
@@ -693,12 +850,19 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                     if (c[j] == SR) em |= 1u << j;
                 }
             }
+            if (tile + gridDim.x < n_tiles) ex_words(a, i0 + (long long)gridDim.x * PP_TILE, nw, nt);
+            if (lane == 0 && i0 > 0 && i0 - 1 < a.L) prev_id = a.pid[i0 - 1];
+            if (lane == 31 && i0 + PP_ITEMS < a.L) {
+                next_id = a.pid[i0 + PP_ITEMS];
+                next_head = (uint32_t)a.P[i0 + PP_ITEMS] == SL;
+            }
         }
-        if (tile + gridDim.x < n_tiles) ex_words(a, i0 + (long long)gridDim.x * PP_TILE, nw, nt);
         // ---- pairs closed between each position and the one before it (adj_closed),
         // with the previous lefts carried along; cl[PP_ITEMS] is the next thread's cl[0]
-        const uint32_t up = __shfl_up_sync(ALP_FULL_MASK, (uint32_t)ids[PP_ITEMS - 1], 1);
-        const uint32_t prev_id = lane > 0 ? up : (i0 > 0 && i0 - 1 < a.L ? (uint32_t)a.pid[i0 - 1] : NO_PAIR);
+        {
+            const uint32_t up = __shfl_up_sync(ALP_FULL_MASK, (uint32_t)ids[PP_ITEMS - 1], 1);
+            if (lane > 0) prev_id = up;
+        }
         uint32_t cl[PP_ITEMS + 1];
         PosSums mine;
         possums_zero(mine);
@@ -729,8 +893,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             const uint32_t dn = __shfl_down_sync(ALP_FULL_MASK, cl[0], 1);
             cl[PP_ITEMS] = dn;
             if (lane == 31) {  // the next warp's first position
-                const long long n0 = i0 + PP_ITEMS;
-                cl[PP_ITEMS] = n0 < a.L ? adj_closed(s_pi, ids[PP_ITEMS - 1], a.pid[n0], (uint32_t)a.P[n0] == SL) : 0u;
+                cl[PP_ITEMS] = i0 + PP_ITEMS < a.L ? adj_closed(s_pi, ids[PP_ITEMS - 1], next_id, next_head) : 0u;
             }
         }
         const PosSums inc = ps_warp_scan(mine, lane);
@@ -746,8 +909,40 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             if (lane == 0) possums_zero(we);
             if (lane < PP_THREADS / 32) s_w[lane] = we;
             if (lane == PP_THREADS / 32 - 1) s_tn = wi.nodes;
+            if (FUSED) {
+                // the tile's own sums: the last warp's inclusive value
+                constexpr int LW = PP_THREADS / 32 - 1;
+                PosSums agg;
+                agg.nodes = __shfl_sync(ALP_FULL_MASK, wi.nodes, LW);
+                agg.brs = __shfl_sync(ALP_FULL_MASK, wi.brs, LW);
+                agg.depth = __shfl_sync(ALP_FULL_MASK, wi.depth, LW);
+                agg.v = __shfl_sync(ALP_FULL_MASK, wi.v, LW);
+                agg.terms = __shfl_sync(ALP_FULL_MASK, wi.terms, LW);
+                agg.heads = __shfl_sync(ALP_FULL_MASK, wi.heads, LW);
+                agg.hpos = __shfl_sync(ALP_FULL_MASK, wi.hpos, LW);
+                agg.cls = __shfl_sync(ALP_FULL_MASK, wi.cls, LW);
+                const PosSums pre = ps_lookback(a, tile, agg);
+                if (lane == 0) {
+                    s_tp = pre;
+                    if (tile == n_tiles - 1) {
+                        // totals (the host checks beforehand that they fit 32 bits)
+                        const PosSums tot = ps_combine(pre, agg);
+                        a.res->aux[0] = (long long)tot.nodes;
+                        a.res->aux[1] = (long long)tot.brs;
+                        a.res->aux[2] = tot.depth;
+                        a.res->aux[3] = tot.v;
+                        a.res->aux[4] = (long long)tot.terms;
+                        a.res->aux[5] = (long long)tot.heads;
+                        a.res->aux[7] = (long long)tot.cls;
+                        a.res->aux[6] = (long long)tot.brs - 2 * (long long)tot.cls;
+                        a.node_off[a.n_docs] = a.res->aux[0];
+                        a.br_off[a.n_docs] = a.res->aux[6];
+                    }
+                }
+            }
         }
         __syncthreads();
+        if (FUSED) tp = s_tp;
         // ---- per position: records and the one-position document rules --------
         uint32_t nof[PP_ITEMS], cnt[PP_ITEMS];  // first node (tile-local), n_prod
         // brackets: the depth before each position and where its kept brackets go

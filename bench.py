@@ -247,6 +247,31 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def _pcie(local: int, h2d_bytes: int, d2h_bytes: int):
+    """Plain pinned-memory copy bandwidth of this GPU's host link, each
+    direction alone (CUDA events, best of 3 copies of 512 MiB), and the time
+    the step's own copies would take at those rates: the floor of e2e."""
+    import torch
+    nb = 512 << 20
+    dev = torch.empty(nb, dtype=torch.uint8, device=f"cuda:{local}")
+    host = torch.empty(nb, dtype=torch.uint8, pin_memory=True)
+    out = {}
+    for name, dst, src in (("h2d", dev, host), ("d2h", host, dev)):
+        best = None
+        for _ in range(4):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            dst.copy_(src, non_blocking=True)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        out[name + "_gbs"] = nb / (best * 1e-3) / 1e9
+    out["copy_floor_ms"] = (h2d_bytes / out["h2d_gbs"] + d2h_bytes / out["d2h_gbs"]) / 1e6
+    del dev, host
+    return out
+
+
 def _sha_arrays(arrs, names, dtypes):
     import hashlib
     out = {}
@@ -309,6 +334,8 @@ def _kernel_alg_bytes(name, units, parse_layout=True):
     tok = 10 if parse_layout else 20
     table = {
         "parse_expand_kernel": 4 * L + 8 * m + 25 * N + 8 * K,   # ids in, spans in, node fields + kept brackets out
+        "parse_expand_kernel(fused)": 2 * L + 8 * m + 25 * N + 8 * K,  # terminals in (keys), spans in, same out
+        "lex3_tok_kernel": n + c + tok * m,                    # bytes and chunk states in, tokens out
         "ple_tile_kernel(nodes)": 12 * N,                      # values in, parents out
         "ple_tile_kernel(brackets)": 8 * K,                    # kept brackets' depth values and symbols in
         "lex3_emit_kernel": n + 3 * c + tok * m,               # bytes, chunk states and counts in, tokens out
@@ -595,6 +622,44 @@ def run_batch(args, rank: int, world: int, local: int):
 
     e2e_step()
     ms_e2e, _ = _timed(e2e_step, max(1, min(args.steps, 3)), local, dist)
+
+    # the same batches captured once each as a CUDA graph (alp_parse_graph_*),
+    # replayed; outputs compared with alp_parse_batch's on the device
+    graph = {}
+    if not args.no_graph:
+        for st in sets:
+            for k2 in ("h_x", "h_o", "d_x", "d_o", "h_out", "h_noff", "h_valid"):
+                st.pop(k2, None)
+        torch.cuda.empty_cache()
+        pgs = []
+        exact = True
+        for st in sets:
+            want = st["g"].parse_batch_int(st["x"], st["o"])
+            pg = st["g"].parse_batch_graph(st["x"], st["o"], cap_nodes=st["N"].value + 64,
+                                           cap_brackets=st["counts"]["B"] + 64)
+            pg.launch()
+            got = pg.result()
+            exact = exact and len(got[0]) == len(want[0]) and torch.equal(got[1], want[1]) and \
+                torch.equal(got[2], want[2]) and all(torch.equal(getattr(got[0], f), getattr(want[0], f))
+                                                     for f in ("parent", "tag", "kind", "start", "end"))
+            del want, got
+            pgs.append(pg)
+        if not exact:
+            raise RuntimeError("graph replay differs from alp_parse_batch")
+
+        def gstep():
+            for pg in pgs:
+                pg.launch()
+
+        for _ in range(max(3, args.warmup)):
+            gstep()
+        ms_graph, _ = _timed(gstep, args.steps, local, dist)
+        for pg in pgs:
+            pg.result()
+            pg.close()
+        graph = {"api": "alp_parse_graph_create once per grammar, then alp_parse_graph_launch per step",
+                 "ms_per_step": ms_graph, "value": _gbs(world, sum(len(st["data"]) for st in sets), ms_graph),
+                 "unit": "GB/s", "vs_alp_parse_batch": ms / ms_graph, "bit_exact": True}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -618,6 +683,8 @@ def run_batch(args, rank: int, world: int, local: int):
                   "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}, clocks, units=units)
     line["path_roofline"]["scope"] = ("both alp_parse_batch calls: input bytes + 29 B per node + 17 B per "
                                       "document (offsets in, node offsets and validity out), over the step time")
+    if graph:
+        line["graph"] = graph
     print(json.dumps(line), flush=True)
 
 
@@ -909,6 +976,7 @@ def main():
     ap.add_argument("--doc-mib", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the full-size comparison with the oracle")
+    ap.add_argument("--no-graph", action="store_true", help="batch workload: skip the CUDA-graph replay")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes (no autotuner run): for "
                     "launch lists whose first launches should be the measured ones")
     ap.add_argument("--workload", default="parse", choices=["parse", "lex", "batch", "spec", "graph", "shard"])
@@ -1004,6 +1072,7 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = _max_over_ranks(e0.elapsed_time(e1) / k_e2e, dist, local)
+    pcie = _pcie(local, size, NODE_BYTES * N)
 
     # full-size parity: the tree the e2e call brought back against the oracle
     # (sequential restatement of the generated lex_int + parse_int)
@@ -1047,7 +1116,7 @@ def main():
         "roofline": roof,
         "path_roofline": path,
         "e2e": {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": size,
-                "d2h_bytes_per_step": NODE_BYTES * N, "ms_per_step": ms_e2e},
+                "d2h_bytes_per_step": NODE_BYTES * N, "ms_per_step": ms_e2e, "pcie": pcie},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
     }

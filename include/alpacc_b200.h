@@ -87,7 +87,15 @@ int alp_check_bounded_wait(alp_ctx* ctx);
  * cfg[1] and cfg[2] the CTAs per SM of the persistent pair and expand kernels
  * (0: as many as fit); with n >= 4, cfg[3] the boundary-MLP inference kernel
  * (0: tcgen05 tensor-memory kernel, the default; 1: mma.sync kernel, whose
- * predictions may differ where two logits are within rounding).
+ * predictions may differ where two logits are within rounding); with n >= 5,
+ * cfg[4] the lexer's token pass (0: one fused pass that counts, looks back
+ * over tiles and writes tokens; 1: a count pass, a tile scan and a token
+ * pass, the default); with n >= 6, cfg[5] the parser's position pass (0: one
+ * fused pass that looks up the pairs, looks back over tiles and expands, sized
+ * from the previous parse on the context; 1: a pair pass and a scan of its
+ * tile sums before the expansion, the default); with n >= 7, cfg[6] the lexer state
+ * scan's chunks per lane (8, 16 or 32; 0 or 16 the default).  The tuner tries
+ * the lexer's knobs first, then the parser's.
  * alp_tune_parse times alp_parse on a sample (the median
  * of `reps` calls per candidate, CUDA events), one knob at a time, keeps the
  * fastest setting in the context and writes "knob value ms" lines to

@@ -52,11 +52,19 @@ def _check(g, o, data: bytes):
 
 @pytest.mark.parametrize("name", GRAMMARS)
 @pytest.mark.parametrize("mode", ["lexer", "both"])
-def test_generated_sizes(has_gpu, name, mode):
+@pytest.mark.parametrize("split", [1, 0])
+def test_generated_sizes(has_gpu, name, mode, split):
+    """split: the token pass as count pass + tile scan + token pass (1) or as
+    one fused pass with a look-back over tiles (0)."""
     g, o = _ctx(name, mode)
     sizes = [1, 2, 3, 15, 16, 17, 255, 4095, 4096, 4097, 8191, 65536 + 7, 131072 * 8 + 3, 1 << 22]
-    for i, size in enumerate(sizes):
-        _check(g, o, _gen(name, size, 100 + i).tobytes())
+    saved = g.get_tuning()
+    try:
+        g.set_tuning(saved[:4] + [split])
+        for i, size in enumerate(sizes):
+            _check(g, o, _gen(name, size, 100 + i).tobytes())
+    finally:
+        g.set_tuning(saved)
 
 
 @pytest.mark.parametrize("name", GRAMMARS)
@@ -120,3 +128,40 @@ def test_dense_tokens_and_unaligned_input(has_gpu):
         want = o.lex_futhark(bytes(b"   "[off:]) + doc)
         for a, b in zip(got, want):
             np.testing.assert_array_equal(a.cpu().numpy().astype(b.dtype), b)
+
+
+@pytest.mark.parametrize("mode", ["lexer", "both"])
+def test_token_pass_fallbacks(has_gpu, mode):
+    """The fused token pass keeps up to 16 token records per 32-byte chunk and
+    stages up to 2048 tokens per 8 KiB tile: chunks with more tokens re-run
+    the DFA, tiles with more take their prefix first and write directly.
+    Both against the oracle, and the split passes (count pass, tile scan,
+    token pass) against the fused one."""
+    g, o = _ctx("json", mode)
+    ga, oa = _ctx("arithmetic", mode)
+    unit = b"[" * 20 + b"]" * 20 + b',"' + b"x" * 200 + b'",'   # dense chunks in staged tiles
+    doc = b"[" + unit * 3000 + b"1]"
+    saved = [x.get_tuning() for x in (g, ga)]
+    try:
+        for x, c in zip((g, ga), saved):
+            x.set_tuning(c[:4] + [0])
+        _check(ga, oa, b"1+" * 100000 + b"1")                     # every byte a token
+        _check(ga, oa, b"(" * 70000 + b"1" + b")" * 70000)
+        _check(g, o, doc)
+        _check(g, o, b"[" + b"1," * 8 + b"1" * 9 + b"," + (b"[1]," * 10000) + b"1]")
+    finally:
+        for x, c in zip((g, ga), saved):
+            x.set_tuning(c)
+    d = _gen("json", 3_000_000, 41).tobytes()
+    cfg = g.get_tuning()
+    try:
+        g.set_tuning(cfg[:4] + [0])
+        fused = [x.cpu().numpy() for x in g.lex_int(d)]
+        _check(g, o, doc)
+        g.set_tuning(cfg[:4] + [1])
+        split = [x.cpu().numpy() for x in g.lex_int(d)]
+        _check(g, o, doc)
+    finally:
+        g.set_tuning(cfg)
+    for a, b in zip(fused, split):
+        np.testing.assert_array_equal(a, b)

@@ -174,3 +174,85 @@ def test_adjacent_bracket_pairs_counted(has_gpu, name):
         assert info[10] == brackets
         assert info[11] == brackets - 2 * closed
         assert 0 < info[11] < brackets or brackets == 0
+
+
+@pytest.mark.parametrize("name", ["json", "arithmetic", "sexp"])
+def test_fused_and_two_pass_position_forms(has_gpu, name):
+    """The position pass has two forms: one fused kernel (pair lookup, look-back
+    over tiles, expansion) sized from the previous parse on the context, and
+    the pair pass + tile-sum scan + expansion that sizes exactly first.  A
+    fresh context's first parse takes the second form, later ones the first;
+    both against the oracle, and a document much denser in nodes and brackets
+    than the one before it (the fused form's estimate is short, so it runs
+    again at the exact sizes)."""
+    from alpacc_b200.api import Grammar
+    tb = tables.load(name, "both")
+    o = oracle.Oracle(tb.blob())
+    g = Grammar(tb)
+    sparse = {"json": b'["' + b"x" * 300000 + b'"]', "arithmetic": b"1" * 300000,
+              "sexp": b"(" + b"a" * 300000 + b")"}[name]
+    dense = {"json": b"[" + b"[1]," * 100000 + b"1]", "arithmetic": b"(" * 50000 + b"1" + b")" * 50000,
+             "sexp": b"(" + b"()" * 150000 + b")"}[name]
+    docs = [_gen(name, 2_000_003, 501).tobytes(), _gen(name, 777_777, 502).tobytes(), sparse, dense,
+            _gen(name, 3_000_000, 503).tobytes()]
+    cfg = g.get_tuning()
+    try:
+        g.set_tuning(cfg[:5] + [0])
+        for d in docs:  # first call: two-pass form; then fused, estimates from the previous document
+            _check(g, o, d)
+        # a batch in the fused form: documents restart the sums inside tiles
+        sizes = synth.lognormal_sizes(500, median=700, sigma=1.5, cap=30000, seed=504)
+        data, off = synth.batch(name if name != "arithmetic" else "json", sizes, 8, 504) if name != "arithmetic" \
+            else (None, None)
+        if data is not None:
+            tree, node_off, valid = g.parse_batch_int(data, off)
+            par, tag, kind, st, en = (x.cpu().numpy() for x in (tree.parent, tree.tag, tree.kind, tree.start,
+                                                                 tree.end))
+            node_off, valid = node_off.cpu().numpy(), valid.cpu().numpy()
+            for i in range(len(sizes)):
+                want = o.lex_parse(data[off[i]:off[i + 1]].tobytes())
+                assert bool(valid[i]) == (want is not None)
+                if want is not None:
+                    a, b = node_off[i], node_off[i + 1]
+                    for got, w in zip((par[a:b], tag[a:b], kind[a:b], st[a:b], en[a:b]), want):
+                        np.testing.assert_array_equal(got.astype(w.dtype), w)
+        g.set_tuning(cfg[:5] + [1])
+        for d in docs[:2]:
+            _check(g, o, d)
+    finally:
+        g.set_tuning(cfg)
+
+
+def test_fused_caller_buffer_too_small(has_gpu):
+    """alp_parse_into with a node capacity below the tree's size reports the
+    size needed, in either form of the position pass."""
+    import ctypes
+    import torch
+    from alpacc_b200 import api
+    g, o, tb = _ctx("json")
+    d = torch.from_numpy(_gen("json", 400_000, 601)).cuda()
+    want = o.lex_parse(d.cpu().numpy().tobytes())
+    N = len(want[0])
+    L = api.native()
+    for split in (0, 1):
+        cfg = g.get_tuning()
+        g.set_tuning(cfg[:5] + [split])
+        try:
+            assert g.parse_int(d) is not None  # a parse on the context first: estimates exist
+            outs = [torch.empty(N // 2, dtype=dt, device="cuda") for dt in
+                    (torch.int64, torch.int32, torch.uint8, torch.int64, torch.int64)]
+            n, v = ctypes.c_int64(0), ctypes.c_int(0)
+            rc = L.alp_parse_into(g.h, ctypes.c_void_p(d.data_ptr()), d.numel(),
+                                  *[ctypes.c_void_p(x.data_ptr()) for x in outs], N // 2, ctypes.byref(n),
+                                  ctypes.byref(v))
+            assert rc == api.ALP_ERR_CAPACITY and n.value == N
+            outs = [torch.empty(N, dtype=dt, device="cuda") for dt in
+                    (torch.int64, torch.int32, torch.uint8, torch.int64, torch.int64)]
+            rc = L.alp_parse_into(g.h, ctypes.c_void_p(d.data_ptr()), d.numel(),
+                                  *[ctypes.c_void_p(x.data_ptr()) for x in outs], N, ctypes.byref(n),
+                                  ctypes.byref(v))
+            assert rc == 0 and v.value == 1 and n.value == N
+            for a, w in zip(outs, want):
+                np.testing.assert_array_equal(a.cpu().numpy().astype(w.dtype), w)
+        finally:
+            g.set_tuning(cfg)

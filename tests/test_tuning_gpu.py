@@ -82,14 +82,38 @@ def test_tuner_keeps_a_valid_exact_setting(has_gpu):
     try:
         res = g.tune(sample, reps=2)
         cfg = res["config"]
-        assert 0 <= cfg[0] < len(Grammar.tile_shapes()) and cfg[1] >= 1 and cfg[2] >= 1
+        assert 0 <= cfg[0] < len(Grammar.tile_shapes()) and cfg[2] >= 1
+        assert cfg[4] in (0, 1) and cfg[5] in (0, 1) and cfg[6] in (8, 16, 32)
         names = {k for k, _, _ in res["timings"]}
-        assert {"expand_ctas_per_sm", "pairs_ctas_per_sm", "best_ms"} <= names
+        assert {"expand_ctas_per_sm", "best_ms", "lex_token_pass_split", "lex_scan_chunks_per_lane",
+                "parse_position_pass_split"} <= names
+        assert ("pairs_ctas_per_sm" in names) == (cfg[5] == 1)
         assert sum(1 for k, _, _ in res["timings"] if k.startswith("ple_shape_")) == len(Grammar.tile_shapes())
         _same(_tree(g, sample), want)
         small = _gen("json", 20000, 3, 8)
         _same(_tree(g, small), _oracle(o, small))
         with pytest.raises(AlpError):
             g.set_tuning([len(Grammar.tile_shapes()), 0, 0])
+    finally:
+        g.set_tuning(saved)
+
+
+@pytest.mark.parametrize("name", ["json", "sexp"])
+def test_every_lexer_knob_against_oracle(has_gpu, name):
+    """Every lexer setting the tuner may pick (state-scan chunks per lane 8,
+    16, 32; fused or split token pass) and both forms of the parser's position
+    pass give the oracle's tree."""
+    g, o = _ctx(name)
+    docs = [_gen(name, 3_000_001, 88, 16 if name == "json" else 20), b"", b"x"]
+    docs.append(_gen(name, 200_000, 89, 16 if name == "json" else 20))
+    wants = [_oracle(o, d) for d in docs]
+    saved = g.get_tuning()
+    try:
+        for gs in (8, 16, 32):
+            for lex_split in (0, 1):
+                for parse_split in (0, 1):
+                    g.set_tuning(saved[:4] + [lex_split, parse_split, gs])
+                    for d, w in zip(docs, wants):
+                        _same(_tree(g, d), w)
     finally:
         g.set_tuning(saved)
