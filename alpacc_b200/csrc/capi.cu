@@ -389,9 +389,12 @@ int persistent_ctas(int fit, int tuned) {
 
 // With dn, n is a capacity and the element count is read from device memory
 // (no host round trip; grids cover the capacity).
+// A shard of a document (xq set): elements with no answer inside the shard are
+// appended to xq for the shards before it, and parents are shifted by out_off.
 int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, int64_t* parent, int first,
             const long long* seg_off, long long n_seg, uint8_t* seg_valid, AlpResult* d_res,
-            const long long* dn = nullptr) {
+            const long long* dn = nullptr, long long out_off = 0, unsigned long long* xq = nullptr,
+            unsigned int* xq_count = nullptr, long long xq_cap = 0) {
     if (n == 0) return ALP_OK;
     const PleShape& sh = ple_shapes[ctx->tune.ple];
     const int tile = sh.threads * sh.items;
@@ -425,6 +428,10 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     a.esc_cap = n;
     a.res = d_res;
     a.dn = dn;
+    a.out_off = out_off;
+    a.xq = xq;
+    a.xq_count = xq_count;
+    a.xq_cap = xq_cap;
     CK(cudaFuncSetAttribute(sh.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
     mark(ctx, "start");
     {
@@ -452,6 +459,10 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     e.seg_valid = seg_valid;
     e.res = d_res;
     e.tile = tile;
+    e.out_off = out_off;
+    e.xq = xq;
+    e.xq_count = xq_count;
+    e.xq_cap = xq_cap;
     ple_escape_kernel<<<148 * 4, 256, 0, ctx->stream>>>(e);
     CK(cudaGetLastError());
     mark(ctx, sym ? "tile_min+ple_escape(brackets)" : "tile_min+ple_escape(nodes)");
@@ -1966,6 +1977,396 @@ void alp_lex_shard_free(alp_lex_shard* s) {
     if (s->d_carry) cudaFree(s->d_carry);
     if (s->d_fn) cudaFree(s->d_fn);
     if (s->h) cudaFreeHost(s->h);
+    delete s;
+}
+
+}  // extern "C"
+
+// ---- shards of one document's parse ---------------------------------------
+// Rank r holds a contiguous slice of the document's tokens.  Three small
+// all-gathers join the ranks: (1) the terminals at each slice's edges, from
+// which every rank has the key windows across its edges (futhark/parser.fut:
+// 117-122) and the pair ids just outside it; (2) each slice's position sums
+// (nodes, brackets, depth, exscan(arity - 1), terminal productions, pairs
+// closed at its first position), from which every rank has the sums of the
+// slices before it (futhark/parser.fut:153-166, 286-290); (3) each slice's
+// staircases of node values and bracket depth values, which answer the
+// previous-smaller-or-equal searches that leave a slice (futhark/parser.fut:
+// 72-108, 174-184, 291-298).
+struct alp_parse_shard {
+    alp_ctx* ctx = nullptr;
+    long long m = 0, L = 0;
+    int first = 0, last = 0;
+    uint32_t halo_l[PS_HALO], halo_r[PS_HALO];
+    uint32_t prev_pair = NO_PAIR, next_pair = NO_PAIR;
+    long long sums[10] = {};
+    long long N = 0, K = 0, node_base = 0, br_base = 0, pos_base = 0;
+    long long n_stair_n = 0, n_stair_b = 0;
+    DevBuf xq_n, xq_b, st_n_val, st_n_idx, st_b_val, st_b_sym, st_scratch, counts, prev_n, prev_b, seg;
+    int expanded = 0;
+};
+
+namespace {
+
+// The pair at position p of a window of terminals `at` (parse_pairs_kernel's
+// pair_at on the host).
+template <typename At>
+uint32_t host_pair(const ParseHost& ph, At at, long long p) {
+    const int q = ph.q, W = ph.q + ph.k;
+    uint32_t pw[17];
+    uint32_t x = 1;
+    for (int j = 0; j < W; ++j) { pw[W - 1 - j] = x; x *= ph.T; }
+    const uint32_t c = at(p);
+    uint32_t key = c * pw[q];
+    bool ok = c != ph.start;
+    for (int jj = q - 1; jj >= 0; --jj) {
+        const uint32_t t = at(p - q + jj);
+        key += (ok ? t : ph.empty) * pw[jj];
+        ok = ok && t != ph.start;
+    }
+    ok = c != ph.end;
+    for (int jj = q + 1; jj < W; ++jj) {
+        const uint32_t t = at(p - q + jj);
+        key += (ok ? t : ph.empty) * pw[jj];
+        ok = ok && t != ph.end;
+    }
+    return key < ph.key_index.size() ? ph.key_index[key] : NO_PAIR;
+}
+
+uint32_t host_closed(const ParseHost& ph, uint32_t prev, uint32_t cur) {
+    if (prev == NO_PAIR || cur == NO_PAIR) return 0;
+    const PairInfo& a = ph.pairs[prev];
+    const PairInfo& b = ph.pairs[cur];
+    const uint32_t la = (uint32_t)(((int32_t)a.n_br + (int32_t)a.d_depth) >> 1);
+    const uint32_t lb = (uint32_t)(((int32_t)b.n_br + (int32_t)b.d_depth) >> 1);
+    return std::min(la, (uint32_t)b.n_br - lb);
+}
+
+void shard_args(alp_parse_shard* s, ParseArgs& a, AlpResult* d_res) {
+    alp_ctx* ctx = s->ctx;
+    memset(&a, 0, sizeof a);
+    a.t = ctx->pt;
+    a.P = (const uint16_t*)ctx->tmp[T_TTERM].p;
+    a.pstart = (const uint32_t*)ctx->tmp[T_TSTART].p;
+    a.pend = (const uint32_t*)ctx->tmp[T_TEND].p;
+    a.L = s->L;
+    a.n_docs = 1;
+    a.pid = (uint16_t*)ctx->tmp[T_PID].p;
+    a.tile_sums = (PosSums*)ctx->tmp[T_TSUMS].p;
+    a.res = d_res;
+    a.node_off = (long long*)ctx->tmp[T_NODEOFF].p;
+    a.br_off = (long long*)ctx->tmp[T_BROFF].p;
+    a.doc_valid = (uint8_t*)ctx->tmp[T_DVALID].p;
+    a.subst_terminals = 1;
+    a.shard = 1;
+    memcpy(a.halo_l, s->halo_l, sizeof a.halo_l);
+    memcpy(a.halo_r, s->halo_r, sizeof a.halo_r);
+    a.prev_pair = s->prev_pair;
+    a.next_pair = s->next_pair;
+}
+
+}  // namespace
+
+extern "C" {
+
+int alp_parse_shard_begin(alp_ctx* ctx, const uint32_t* d_term, const int64_t* d_start, const int64_t* d_end,
+                          int64_t m, int is_first, int is_last, uint32_t* h_edge, int64_t* n_pos,
+                          alp_parse_shard** out) {
+    if (!ctx || !out || !h_edge || !n_pos || m < 0 || (m > 0 && (!d_term || !d_start || !d_end)))
+        return fail(ctx, ALP_ERR_ARG, "alp_parse_shard_begin: bad arguments");
+    if (!ctx->has_parser || !ctx->has_lexer) return fail(ctx, ALP_ERR_MODE, "these tables are not lexer+parser tables");
+    if (ctx->ph.q + ctx->ph.k > PS_HALO) return fail(ctx, ALP_ERR_ARG, "lookback + lookahead above %d", PS_HALO);
+    CK(cudaSetDevice(ctx->device));
+    *out = nullptr;
+    alp_parse_shard* s = new alp_parse_shard();
+    s->ctx = ctx;
+    s->m = m;
+    s->first = is_first ? 1 : 0;
+    s->last = is_last ? 1 : 0;
+    s->L = m + s->first + s->last;
+    const long long L = s->L;
+    int rc;
+    if (L >= 0x7fffffffLL) { delete s; return fail(ctx, ALP_ERR_ARG, "too many positions (%lld)", L); }
+    if ((rc = grow(ctx, ctx->tmp[T_TTERM], (size_t)L * 2 + 16)) || (rc = grow(ctx, ctx->tmp[T_TSTART], (size_t)L * 4 + 16)) ||
+        (rc = grow(ctx, ctx->tmp[T_TEND], (size_t)L * 4 + 16)) || (rc = grow(ctx, ctx->scratch, 256)) ||
+        (rc = grow(ctx, ctx->tmp[T_DVALID], 16))) {
+        delete s;
+        return rc;
+    }
+    AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
+    if ((rc = set_result(ctx, d_res, 1))) { delete s; return rc; }
+    if (L > 0) {
+        shard_positions_kernel<<<grid_for(L), 256, 0, ctx->stream>>>(d_term, d_start, d_end, m, s->first, s->last,
+                                                                    (uint16_t*)ctx->tmp[T_TTERM].p,
+                                                                    (uint32_t*)ctx->tmp[T_TSTART].p,
+                                                                    (uint32_t*)ctx->tmp[T_TEND].p, ctx->pt.start,
+                                                                    ctx->pt.end, d_res);
+        CK(cudaGetLastError());
+    }
+    if ((rc = read_result(ctx, d_res))) { delete s; return rc; }
+    if (!ctx->h_res->valid) { delete s; return fail(ctx, ALP_ERR_ARG, "terminal id out of range"); }
+    CK(cudaMemsetAsync(ctx->tmp[T_DVALID].p, 1, 1, ctx->stream));
+    // the terminals of the first and last PS_HALO positions, empty where the slice is shorter
+    uint16_t hh[2 * PS_HALO];
+    const long long e = L < PS_HALO ? L : PS_HALO;
+    for (int i = 0; i < 2 * PS_HALO; ++i) h_edge[i] = ctx->pt.empty;
+    if (e > 0) {
+        CK(cudaMemcpy(hh, ctx->tmp[T_TTERM].p, (size_t)e * 2, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hh + PS_HALO, (uint16_t*)ctx->tmp[T_TTERM].p + (L - e), (size_t)e * 2, cudaMemcpyDeviceToHost));
+        for (long long i = 0; i < e; ++i) {
+            h_edge[i] = hh[i];
+            h_edge[2 * PS_HALO - e + i] = hh[PS_HALO + i];
+        }
+    }
+    *n_pos = L;
+    *out = s;
+    return ALP_OK;
+}
+
+int alp_parse_shard_sums(alp_parse_shard* s, const uint32_t* halo_l, const uint32_t* halo_r, int64_t* sums) {
+    if (!s || !halo_l || !halo_r || !sums) return ALP_ERR_ARG;
+    alp_ctx* ctx = s->ctx;
+    CK(cudaSetDevice(ctx->device));
+    memcpy(s->halo_l, halo_l, sizeof s->halo_l);
+    memcpy(s->halo_r, halo_r, sizeof s->halo_r);
+    const long long L = s->L;
+    // the slice's own terminals at its edges, then the pair ids just outside it
+    std::vector<uint16_t> head((size_t)std::min<long long>(L, PS_HALO)), tail(head.size());
+    if (!head.empty()) {
+        CK(cudaMemcpy(head.data(), ctx->tmp[T_TTERM].p, head.size() * 2, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(tail.data(), (uint16_t*)ctx->tmp[T_TTERM].p + (L - (long long)tail.size()), tail.size() * 2,
+                      cudaMemcpyDeviceToHost));
+    }
+    auto at = [&](long long p) -> uint32_t {
+        if (p < 0) return p >= -PS_HALO ? s->halo_l[PS_HALO + p] : ctx->pt.empty;
+        if (p >= L) return p - L < PS_HALO ? s->halo_r[p - L] : ctx->pt.empty;
+        if (p < (long long)head.size()) return head[(size_t)p];
+        if (p >= L - (long long)tail.size()) return tail[(size_t)(p - (L - (long long)tail.size()))];
+        return ctx->pt.empty;  // not reached: windows stay within PS_HALO of an edge
+    };
+    s->prev_pair = s->first ? NO_PAIR : host_pair(ctx->ph, at, -1);
+    s->next_pair = s->last ? NO_PAIR : host_pair(ctx->ph, at, L);
+    const long long tiles = (L + PP_TILE - 1) / PP_TILE;
+    int rc;
+    if ((rc = grow(ctx, ctx->tmp[T_PID], (size_t)L * 2 + 64)) ||
+        (rc = grow(ctx, ctx->tmp[T_TSUMS], (tiles + tiles / ST_CHUNK + 2) * sizeof(PosSums))) ||
+        (rc = grow(ctx, ctx->tmp[T_NODEOFF], 16)) || (rc = grow(ctx, ctx->tmp[T_BROFF], 16)))
+        return rc;
+    AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
+    if ((rc = set_result(ctx, d_res, 1))) return rc;
+    ParseArgs a;
+    shard_args(s, a, d_res);
+    long long first_pair = NO_PAIR;
+    if (L > 0) {
+        const size_t sm1 = pairs_smem_bytes(ctx->pt.n_pairs, ctx->pt.q + ctx->pt.k);
+        const void* fn = pairs_kernel_for(ctx->pt.q, ctx->pt.k);
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+        int sms = 0, per1 = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, fn, PP_THREADS, sm1));
+        const long long x = (long long)persistent_ctas(per1, ctx->tune.pairs_ctas) * sms;
+        {
+            void* args[] = {&a};
+            CK(cudaLaunchKernel(fn, dim3((unsigned)(x < tiles ? x : tiles)), dim3(PP_THREADS), args, sm1, ctx->stream));
+        }
+        const long long chunks = (tiles + ST_CHUNK - 1) / ST_CHUNK;
+        PosSums* csum = a.tile_sums + tiles;
+        scan_tiles_reduce_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum, nullptr);
+        CK(cudaGetLastError());
+        scan_tiles_kernel<<<(unsigned)chunks, ST_CHUNK, 0, ctx->stream>>>(a.tile_sums, tiles, csum, d_res, a.node_off,
+                                                                         a.br_off, 1, nullptr);
+        CK(cudaGetLastError());
+        uint16_t p0 = NO_PAIR;
+        CK(cudaMemcpyAsync(ctx->h_stage, a.pid, 2, cudaMemcpyDeviceToHost, ctx->stream));
+        if ((rc = read_result(ctx, d_res))) return rc;
+        memcpy(&p0, ctx->h_stage, 2);
+        first_pair = p0;
+    }
+    const AlpResult& r = *ctx->h_res;
+    // nodes, brackets, depth, v, terminal productions, heads, last head (global) or -1, closed pairs
+    // (with those at the first position), the pairs closed at the first position, first pair id
+    s->sums[0] = L > 0 ? r.aux[0] : 0;
+    s->sums[1] = L > 0 ? r.aux[1] : 0;
+    s->sums[2] = L > 0 ? r.aux[2] : 0;
+    s->sums[3] = L > 0 ? r.aux[3] : 0;
+    s->sums[4] = L > 0 ? r.aux[4] : 0;
+    s->sums[5] = L > 0 ? r.aux[5] : 0;
+    s->sums[6] = s->first ? 0 : -1;
+    s->sums[7] = L > 0 ? r.aux[7] : 0;
+    s->sums[8] = s->first ? 0 : host_closed(ctx->ph, s->prev_pair, (uint32_t)first_pair);
+    s->sums[9] = first_pair;
+    if (s->sums[0] > 0xffffffffLL || s->sums[1] > 0xffffffffLL) return fail(ctx, ALP_ERR_ARG, "tree too large");
+    memcpy(sums, s->sums, sizeof s->sums);
+    return ALP_OK;
+}
+
+int alp_parse_shard_expand(alp_parse_shard* s, const int64_t* pre, int64_t pos_base, int64_t closed_next,
+                           int64_t* n_node, int64_t* n_stair_nodes, int64_t* n_stair_brackets) {
+    if (!s || !pre || !n_node || !n_stair_nodes || !n_stair_brackets) return ALP_ERR_ARG;
+    alp_ctx* ctx = s->ctx;
+    CK(cudaSetDevice(ctx->device));
+    PosSums p;
+    p.nodes = (uint32_t)pre[0]; p.brs = (uint32_t)pre[1]; p.depth = (int32_t)pre[2]; p.v = (int32_t)pre[3];
+    p.terms = (uint32_t)pre[4]; p.heads = (uint32_t)pre[5]; p.hpos = (int32_t)pre[6]; p.cls = (uint32_t)pre[7];
+    s->pos_base = pos_base;
+    s->node_base = pre[0];
+    s->br_base = pre[1] - 2 * pre[7] - s->sums[8];
+    s->N = s->sums[0];
+    s->K = s->sums[1] - 2 * s->sums[7] + s->sums[8] - closed_next;
+    if (s->K < 0) return fail(ctx, ALP_ERR_ARG, "inconsistent closed-pair counts between shards");
+    const long long L = s->L, N = s->N, K = s->K;
+    int rc;
+    AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
+    if ((rc = set_result(ctx, d_res, 1))) return rc;
+    ParseArgs a;
+    shard_args(s, a, d_res);
+    a.pre = p;
+    a.node_base = s->node_base;
+    a.br_base = s->br_base;
+    a.pos_base = pos_base;
+    ParseOut o{};
+    if ((rc = parse_buffers(ctx, &o, 1, N, K, a))) return rc;
+    const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
+    if (L > 0) {
+        const long long tiles = (L + PP_TILE - 1) / PP_TILE;
+        unsigned g = 1;
+        if ((rc = expand_grid(ctx, (const void*)parse_expand_kernel<0, 0, false>, sm2, tiles, &g))) return rc;
+        parse_expand_kernel<0, 0, false><<<g, PP_THREADS, sm2, ctx->stream>>>(a);
+        CK(cudaGetLastError());
+    }
+    // one document: its first element is here only on the first shard (-1: it started before)
+    long long seg[4] = {s->first ? 0 : -1, N, s->first ? 0 : -1, K};
+    if ((rc = grow(ctx, s->seg, sizeof seg)) || (rc = grow(ctx, s->xq_n, (size_t)N * 8 + 16)) ||
+        (rc = grow(ctx, s->xq_b, (size_t)K * 8 + 16)) || (rc = grow(ctx, s->counts, 64)))
+        return rc;
+    CK(cudaMemcpyAsync(s->seg.p, seg, sizeof seg, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(s->counts.p, 0, 64, ctx->stream));
+    const long long* d_seg = (const long long*)s->seg.p;
+    unsigned int* cnt = (unsigned int*)s->counts.p;  // [0] node queries, [1] bracket queries
+    long long* lens = (long long*)((uint8_t*)s->counts.p + 16);  // [0] node staircase, [1] bracket staircase
+    uint8_t* dvalid = a.doc_valid;
+    if ((rc = run_ple(ctx, a.vbuf, N, nullptr, o.parent, T_N_TMIN, d_seg, 1, dvalid, d_res, nullptr,
+                      s->first ? 0 : s->node_base - 1, (unsigned long long*)s->xq_n.p, cnt, N)) ||
+        (rc = run_ple(ctx, a.dsbuf, K, a.brbuf, nullptr, T_B_TMIN, d_seg + 2, 1, dvalid, d_res, nullptr, 0,
+                      (unsigned long long*)s->xq_b.p, cnt + 1, K)))
+        return rc;
+    // the shard's staircases from its tiles'
+    const PleShape& sh = ple_shapes[ctx->tune.ple];
+    const int tile = sh.threads * sh.items;
+    if ((rc = grow(ctx, s->st_n_val, (size_t)N * 4 + 16)) || (rc = grow(ctx, s->st_n_idx, (size_t)N * 8 + 16)) ||
+        (rc = grow(ctx, s->st_b_val, (size_t)K * 4 + 16)) || (rc = grow(ctx, s->st_b_sym, (size_t)K * 4 + 16)) ||
+        (rc = grow(ctx, s->st_scratch, (size_t)((std::max(N, K) + tile - 1) / tile) * 4 + 16)))
+        return rc;
+    if (N > 0)
+        shard_stair_kernel<<<1, 1024, 0, ctx->stream>>>(
+            (const int32_t*)ctx->tmp[T_N_TMIN].p, (const int32_t*)ctx->tmp[T_N_SVAL].p,
+            (const uint32_t*)ctx->tmp[T_N_SIDX].p, (const int32_t*)ctx->tmp[T_N_SLEN].p, (N + tile - 1) / tile, tile,
+            nullptr, s->node_base, (int32_t*)s->st_scratch.p, (int32_t*)s->st_n_val.p, (long long*)s->st_n_idx.p,
+            nullptr, lens);
+    if (K > 0)
+        shard_stair_kernel<<<1, 1024, 0, ctx->stream>>>(
+            (const int32_t*)ctx->tmp[T_B_TMIN].p, (const int32_t*)ctx->tmp[T_B_SVAL].p,
+            (const uint32_t*)ctx->tmp[T_B_SIDX].p, (const int32_t*)ctx->tmp[T_B_SLEN].p, (K + tile - 1) / tile, tile,
+            a.brbuf, 0, (int32_t*)s->st_scratch.p, (int32_t*)s->st_b_val.p, nullptr, (uint32_t*)s->st_b_sym.p,
+            lens + 1);
+    CK(cudaGetLastError());
+    long long h_lens[2] = {0, 0};
+    CK(cudaMemcpyAsync(ctx->h_stage, lens, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    if ((rc = read_result(ctx, d_res))) return rc;
+    memcpy(h_lens, ctx->h_stage, 16);
+    s->n_stair_n = N > 0 ? h_lens[0] : 0;
+    s->n_stair_b = K > 0 ? h_lens[1] : 0;
+    s->expanded = 1;
+    *n_node = N;
+    *n_stair_nodes = s->n_stair_n;
+    *n_stair_brackets = s->n_stair_b;
+    return ALP_OK;
+}
+
+int alp_parse_shard_stairs(alp_parse_shard* s, int32_t* h_nval, int64_t* h_nidx, int32_t* h_bval, uint32_t* h_bsym) {
+    if (!s || !s->expanded) return ALP_ERR_ARG;
+    alp_ctx* ctx = s->ctx;
+    CK(cudaSetDevice(ctx->device));
+    if (s->n_stair_n) {
+        if (!h_nval || !h_nidx) return fail(ctx, ALP_ERR_ARG, "null staircase buffer");
+        CK(cudaMemcpy(h_nval, s->st_n_val.p, (size_t)s->n_stair_n * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(h_nidx, s->st_n_idx.p, (size_t)s->n_stair_n * 8, cudaMemcpyDeviceToHost));
+    }
+    if (s->n_stair_b) {
+        if (!h_bval || !h_bsym) return fail(ctx, ALP_ERR_ARG, "null staircase buffer");
+        CK(cudaMemcpy(h_bval, s->st_b_val.p, (size_t)s->n_stair_b * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(h_bsym, s->st_b_sym.p, (size_t)s->n_stair_b * 4, cudaMemcpyDeviceToHost));
+    }
+    return ALP_OK;
+}
+
+int alp_parse_shard_resolve(alp_parse_shard* s, int n_prev, const int64_t* n_off, const int32_t* nval,
+                            const int64_t* nidx, const int64_t* b_off, const int32_t* bval, const uint32_t* bsym,
+                            int* valid) {
+    if (!s || !s->expanded || !valid || n_prev < 0 || (n_prev > 0 && (!n_off || !b_off))) return ALP_ERR_ARG;
+    alp_ctx* ctx = s->ctx;
+    CK(cudaSetDevice(ctx->device));
+    int rc;
+    const long long nn = n_prev > 0 ? n_off[n_prev] : 0, nb = n_prev > 0 ? b_off[n_prev] : 0;
+    const size_t offb = 8 * ((size_t)n_prev + 1);
+    if ((rc = grow(ctx, s->prev_n, 2 * offb + (size_t)nn * 12 + 64)) ||
+        (rc = grow(ctx, s->prev_b, (size_t)nb * 8 + 64)))
+        return rc;
+    uint8_t* pn = (uint8_t*)s->prev_n.p;
+    long long* d_noff = (long long*)pn;
+    long long* d_boff = (long long*)(pn + offb);
+    long long* d_nidx = (long long*)(pn + 2 * offb);
+    int32_t* d_nval = (int32_t*)(pn + 2 * offb + (size_t)nn * 8);
+    int32_t* d_bval = (int32_t*)s->prev_b.p;
+    uint32_t* d_bsym = (uint32_t*)((uint8_t*)s->prev_b.p + (size_t)nb * 4);
+    if (n_prev > 0) {
+        CK(cudaMemcpy(d_noff, n_off, offb, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_boff, b_off, offb, cudaMemcpyHostToDevice));
+        if (nn) {
+            CK(cudaMemcpy(d_nidx, nidx, (size_t)nn * 8, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(d_nval, nval, (size_t)nn * 4, cudaMemcpyHostToDevice));
+        }
+        if (nb) {
+            CK(cudaMemcpy(d_bval, bval, (size_t)nb * 4, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(d_bsym, bsym, (size_t)nb * 4, cudaMemcpyHostToDevice));
+        }
+    }
+    AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
+    unsigned int* cnt = (unsigned int*)s->counts.p;
+    uint8_t* dvalid = (uint8_t*)ctx->tmp[T_DVALID].p;
+    shard_resolve_kernel<<<148 * 4, 256, 0, ctx->stream>>>((const unsigned long long*)s->xq_n.p, cnt, s->N, n_prev,
+                                                          d_noff, d_nval, d_nidx, nullptr, (long long*)ctx->out[3].p,
+                                                          nullptr, dvalid);
+    CK(cudaGetLastError());
+    shard_resolve_kernel<<<148 * 4, 256, 0, ctx->stream>>>((const unsigned long long*)s->xq_b.p, cnt + 1, s->K, n_prev,
+                                                          d_boff, d_bval, nullptr, d_bsym, nullptr,
+                                                          (const uint32_t*)ctx->tmp[T_BRBUF].p, dvalid);
+    CK(cudaGetLastError());
+    if ((rc = read_result(ctx, d_res))) return rc;
+    return read_valid0(ctx, dvalid, valid);
+}
+
+int alp_parse_shard_tree(alp_parse_shard* s, int64_t** d_parent, uint32_t** d_tag, uint8_t** d_kind,
+                         int64_t** d_start, int64_t** d_end, int64_t* n_node, int64_t* first_node) {
+    if (!s || !s->expanded || !d_parent || !d_tag || !d_kind || !d_start || !d_end || !n_node || !first_node)
+        return ALP_ERR_ARG;
+    alp_ctx* ctx = s->ctx;
+    *d_parent = (int64_t*)ctx->out[3].p;
+    *d_tag = (uint32_t*)ctx->out[4].p;
+    *d_kind = (uint8_t*)ctx->out[5].p;
+    *d_start = (int64_t*)ctx->out[6].p;
+    *d_end = (int64_t*)ctx->out[7].p;
+    *n_node = s->N;
+    *first_node = s->node_base;
+    return ALP_OK;
+}
+
+void alp_parse_shard_free(alp_parse_shard* s) {
+    if (!s) return;
+    if (s->ctx) cudaSetDevice(s->ctx->device);
+    for (DevBuf* b : {&s->xq_n, &s->xq_b, &s->st_n_val, &s->st_n_idx, &s->st_b_val, &s->st_b_sym, &s->st_scratch,
+                      &s->counts, &s->prev_n, &s->prev_b, &s->seg})
+        if (b->p) cudaFree(b->p);
     delete s;
 }
 

@@ -56,6 +56,10 @@ struct ParseTables {
 struct ParseHost {
     int q = 0, k = 0, n_terms = 0, n_prods = 0, n_pairs = 0, max_prods = 0, max_brackets = 0;
     long long key_space = 0;
+    // host copies for the pairs at shard boundaries (alp_parse_shard_*)
+    std::vector<uint16_t> key_index;
+    std::vector<PairInfo> pairs;
+    uint32_t T = 0, empty = 0, start = 0, end = 0;
 };
 
 inline int load_parser(ParseTables& pt, ParseHost& ph, const uint8_t* p, const uint8_t* e,
@@ -197,6 +201,9 @@ inline int load_parser(ParseTables& pt, ParseHost& ph, const uint8_t* p, const u
     pt.empty = empty; pt.start = start; pt.end = end;
     ph.q = (int)q; ph.k = (int)k; ph.n_terms = (int)n_terms; ph.n_prods = (int)n_prods; ph.n_pairs = (int)n_pairs;
     ph.max_prods = maxp; ph.max_brackets = maxb; ph.key_space = space;
+    ph.key_index = std::move(index);
+    ph.pairs = info;
+    ph.T = T; ph.empty = empty; ph.start = start; ph.end = end;
     return 0;
 }
 
@@ -213,6 +220,7 @@ constexpr int PLE_THREADS = 256;
 constexpr int PLE_ITEMS = 16;
 constexpr int PLE_TILE = PLE_THREADS * PLE_ITEMS;  // elements per tile
 constexpr uint16_t NO_PAIR = 0xffff;
+constexpr int PS_HALO = 16;                        // halo terminals a shard keeps on each side (q + k <= 16)
 
 // Running sums over positions.  Positions are the documents' ⊢ tokens ⊣
 // sequences back to back; nodes, brackets and heads (⊢ count) run over all
@@ -335,10 +343,23 @@ struct ParseArgs {
     uint32_t* lb_flag;          // [tiles] ST_X / ST_A / ST_P << 30, zero before the launch
     PosSums* lb_agg;            // [tiles] the tile's own sums
     PosSums* lb_inc;            // [tiles] the sums up to and including the tile
+    // one shard of a document's positions (alp_parse_shard_*, two-pass form):
+    // the terminals around it, the pair ids of the positions just outside it,
+    // the sums of the shards before it and where its outputs start
+    int shard;
+    uint32_t halo_l[PS_HALO];   // terminals of positions -PS_HALO .. -1 (empty past the document)
+    uint32_t halo_r[PS_HALO];   // terminals of positions L .. L + PS_HALO - 1
+    uint32_t prev_pair, next_pair;  // NO_PAIR: no position there
+    PosSums pre;
+    long long node_base;        // global index of the shard's first node
+    long long br_base;          // global index of its first kept bracket
+    long long pos_base;         // global position of its position 0
 };
 
 __device__ __forceinline__ uint32_t pos_term(const ParseArgs& a, long long i) {
-    return (i < 0 || i >= a.L) ? a.t.empty : (uint32_t)a.P[i];
+    if (i < 0) return (a.shard && i >= -PS_HALO) ? a.halo_l[PS_HALO + i] : a.t.empty;
+    if (i >= a.L) return (a.shard && i - a.L < PS_HALO) ? a.halo_r[i - a.L] : a.t.empty;
+    return (uint32_t)a.P[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -407,6 +428,7 @@ __global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
         const long long ip = base + (long long)tid * PP_ITEMS - 1;
         bool h;
         if (ip >= 0 && ip < a.L) before = pair_at(tid * PP_ITEMS - 1, h);
+        else if (ip == -1 && a.shard) before = a.prev_pair;  // the last position of the shard before
     }
     uint16_t ids[PP_ITEMS];
     uint32_t hb = 0;
@@ -840,7 +862,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             }
             possums_zero(tp);
         } else {
-            tp = a.tile_sums[tile];
+            tp = a.shard ? ps_combine(a.pre, a.tile_sums[tile]) : a.tile_sums[tile];
             const uint32_t c[PP_ITEMS] = {nt.x & 0xffffu, nt.x >> 16, nt.y & 0xffffu, nt.y >> 16};
             ids[0] = (uint16_t)nw.x; ids[1] = (uint16_t)(nw.x >> 16); ids[2] = (uint16_t)nw.y; ids[3] = (uint16_t)(nw.y >> 16);
 #pragma unroll
@@ -852,9 +874,12 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             }
             if (tile + gridDim.x < n_tiles) ex_words(a, i0 + (long long)gridDim.x * PP_TILE, nw, nt);
             if (lane == 0 && i0 > 0 && i0 - 1 < a.L) prev_id = a.pid[i0 - 1];
+            else if (lane == 0 && i0 == 0 && a.shard) prev_id = a.prev_pair;
             if (lane == 31 && i0 + PP_ITEMS < a.L) {
                 next_id = a.pid[i0 + PP_ITEMS];
                 next_head = (uint32_t)a.P[i0 + PP_ITEMS] == SL;
+            } else if (lane == 31 && i0 + PP_ITEMS == a.L && a.shard) {
+                next_id = a.next_pair;  // the next shard's first position (never a document head)
             }
         }
         // ---- pairs closed between each position and the one before it (adj_closed),
@@ -888,12 +913,17 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                     mine = ps_combine(mine, e);
                     lprev = nl;
                     pv = ids[j] != NO_PAIR;
+                } else if (a.shard && i0 + j == a.L && pv && a.next_pair != NO_PAIR) {
+                    // the next shard's first position closes this shard's last lefts
+                    const PairInfo& pn = s_pi[a.next_pair];
+                    cl[j] = min(lprev, (uint32_t)pn.n_br - pair_lefts(pn));
                 }
             }
             const uint32_t dn = __shfl_down_sync(ALP_FULL_MASK, cl[0], 1);
             cl[PP_ITEMS] = dn;
             if (lane == 31) {  // the next warp's first position
-                cl[PP_ITEMS] = i0 + PP_ITEMS < a.L ? adj_closed(s_pi, ids[PP_ITEMS - 1], next_id, next_head) : 0u;
+                cl[PP_ITEMS] = (i0 + PP_ITEMS < a.L || (a.shard && i0 + PP_ITEMS == a.L))
+                                   ? adj_closed(s_pi, ids[PP_ITEMS - 1], next_id, next_head) : 0u;
             }
         }
         const PosSums inc = ps_warp_scan(mine, lane);
@@ -1012,8 +1042,8 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                 for (uint32_t r = cl[j]; r < hi; ++r) {
                     const uint2 rec = s_srec[pi.stack_begin + r];
                     const int32_t before = depj[j] + (int32_t)(int16_t)(rec.y & 0xffffu);
-                    const unsigned long long g = (unsigned long long)kof[j] + (r - cl[j]);
-                    if (g < (unsigned long long)a.cap_brs) {
+                    const long long g = (long long)kof[j] + (r - cl[j]) - (a.shard ? a.br_base : 0);
+                    if (g >= 0 && g < a.cap_brs) {
                         a.brbuf[g] = rec.x;
                         a.dsbuf[g] = (rec.x >> 31) ? before : before - 1;  // after a right bracket, before a left
                     }
@@ -1032,13 +1062,14 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             }
             __syncthreads();
             for (uint32_t e0 = tid; e0 < wn; e0 += EX_U * PP_THREADS) {
-                uint32_t tg[EX_U], kd[EX_U], gi[EX_U];
+                uint32_t tg[EX_U], kd[EX_U];
+                long long gi[EX_U];
                 int32_t vv[EX_U];
                 int64_t st[EX_U], en[EX_U];
 #pragma unroll
                 for (int u = 0; u < EX_U; ++u) {
                     const uint32_t e = e0 + u * PP_THREADS;
-                    tg[u] = 0; kd[u] = 0; vv[u] = 0; st[u] = 0; en[u] = 0; gi[u] = 0xffffffffu;
+                    tg[u] = 0; kd[u] = 0; vv[u] = 0; st[u] = 0; en[u] = 0; gi[u] = -1;
                     if (e < wn) {
                         const uint32_t g = w0 + e;
                         const int4 ps = s_pos[ex_slot(s_own[e])];
@@ -1046,19 +1077,19 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                         const uint32_t tm1 = rec.x >> 16;  // terminal + 1, 0: not a terminal production
                         vv[u] = ps.y + (int32_t)(int16_t)(rec.y & 0xffffu);
                         tg[u] = rec.x & 0xffffu;
-                        gi[u] = tp.nodes + g;
+                        gi[u] = (long long)tp.nodes + g - (a.shard ? a.node_base : 0);
                         if (tm1 && a.subst_terminals) {
                             // the k-th terminal production of a document takes its k-th token's span
                             tg[u] = tm1 - 1;
                             kd[u] = 1;
-                            const uint32_t ti = (uint32_t)ps.z + (rec.y >> 16);
-                            if (ti < a.L) { st[u] = __ldg(&a.pstart[ti]); en[u] = __ldg(&a.pend[ti]); }
+                            const long long ti = (long long)((uint32_t)ps.z + (rec.y >> 16)) - (a.shard ? a.pos_base : 0);
+                            if (ti >= 0 && ti < a.L) { st[u] = __ldg(&a.pstart[ti]); en[u] = __ldg(&a.pend[ti]); }
                         }
                     }
                 }
 #pragma unroll
                 for (int u = 0; u < EX_U; ++u) {
-                    if (gi[u] != 0xffffffffu && (long long)gi[u] < a.cap_nodes) {
+                    if (gi[u] >= 0 && gi[u] < a.cap_nodes) {
                         const size_t g = gi[u];
                         a.vbuf[g] = vv[u];
                         a.tag[g] = tg[u];
@@ -1093,6 +1124,10 @@ struct PleArgs {
     long long esc_cap;
     AlpResult* res;
     const long long* dn;         // when set: the element count, in device memory (n is then its capacity)
+    long long out_off;           // nodes: added to every parent written (a shard's global node numbering)
+    unsigned long long* xq;      // when set (a shard): elements with no answer in the shard, index << 32 | value,
+    unsigned int* xq_count;      //   for the shards before it to answer
+    long long xq_cap;
 };
 
 // Shared memory: the tile's values and a second array (bracket symbols, or
@@ -1319,7 +1354,7 @@ __global__ void __launch_bounds__(PT, 1024 / PT) ple_tile_kernel(PleArgs a) {
     if (!brackets) {
         for (int e = tid; e < (PT * PI); e += PT) {
             const long long g = base + e;
-            if (g < a.n) a.out_parent[g] = s_aux[ple_pad<PI>(e)];
+            if (g < a.n) a.out_parent[g] = (long long)s_aux[ple_pad<PI>(e)] + a.out_off;
         }
     }
 
@@ -1440,6 +1475,10 @@ struct EscArgs {
     uint8_t* seg_valid;
     AlpResult* res;
     int tile;                    // elements per tile
+    long long out_off;           // as PleArgs
+    unsigned long long* xq;
+    unsigned int* xq_count;
+    long long xq_cap;
 };
 
 __global__ void ple_escape_kernel(EscArgs a) {
@@ -1462,7 +1501,13 @@ __global__ void ple_escape_kernel(EscArgs a) {
         }
         const long long doc = seg_upper(a.seg_off, 0, a.n_seg - 1, g);
         const long long dbase = a.seg_off[doc];
-        if (a.sym) {
+        if (ans < 0 && a.xq) {
+            // a shard: the answer lies in a shard before this one
+            const unsigned int slot = atomicAdd(a.xq_count, 1u);
+            if ((long long)slot < a.xq_cap) a.xq[slot] = r;
+            else atomicOr(&a.res->error, ALP_DEV_ERR_CAPACITY);
+            if (!a.sym) a.out_parent[g] = -1;
+        } else if (a.sym) {
             if (ans < dbase) {
                 a.seg_valid[doc] = 0;
             }
@@ -1471,8 +1516,145 @@ __global__ void ple_escape_kernel(EscArgs a) {
                 if (!(l >> 31) || (l & 0x7fffffffu) != (rr & 0x7fffffffu)) a.seg_valid[doc] = 0;
             }
         } else {
-            a.out_parent[g] = ans < 0 ? -1 : ans - dbase;
+            a.out_parent[g] = ans < 0 ? -1 : ans - dbase + a.out_off;
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Shards of one document (alp_parse_shard_*): cross-shard previous-smaller-or-equal
+// ---------------------------------------------------------------------------
+// A shard's staircase: the elements strictly smaller than every element after
+// them in the shard, left to right (so ascending values).  Built from the
+// tiles' staircases: tile t contributes the first of its entries that lie
+// below the minimum of every later tile.  One CTA; `scratch` holds a count per
+// tile.  Nodes take a global index (local + idx_off), brackets their symbol.
+__global__ void __launch_bounds__(1024) shard_stair_kernel(const int32_t* tile_min, const int32_t* stair_val,
+                                                           const uint32_t* stair_idx, const int32_t* stair_len,
+                                                           long long tiles, int tile, const uint32_t* sym,
+                                                           long long idx_off, int32_t* scratch, int32_t* out_val,
+                                                           long long* out_idx, uint32_t* out_sym, long long* out_len) {
+    __shared__ int32_t s_w[32];
+    __shared__ long long s_base;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int32_t carry = INT32_MAX;  // minimum of the tiles after the current chunk
+    for (long long c0 = ((tiles - 1) / 1024) * 1024; c0 >= 0; c0 -= 1024) {
+        const long long t = c0 + tid;
+        int32_t x = t < tiles ? tile_min[t] : INT32_MAX;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {  // x = minimum over this lane and the lanes after it
+            const int32_t o = __shfl_down_sync(ALP_FULL_MASK, x, d);
+            if (lane + d < 32) x = min(x, o);
+        }
+        if (lane == 0) s_w[warp] = x;
+        __syncthreads();
+        int32_t after = carry, chunk = INT32_MAX;
+        for (int w2 = 0; w2 < 32; ++w2) {
+            if (w2 > warp) after = min(after, s_w[w2]);
+            chunk = min(chunk, s_w[w2]);
+        }
+        int32_t ex = __shfl_down_sync(ALP_FULL_MASK, x, 1);
+        if (lane == 31) ex = INT32_MAX;
+        const int32_t below = min(ex, after);  // minimum of every tile after t
+        if (t < tiles) {
+            const int32_t* sv = stair_val + t * (long long)tile;
+            int lo = 0, hi = stair_len[t];  // first entry not below `below` (entries ascend)
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (sv[mid] < below) lo = mid + 1; else hi = mid;
+            }
+            scratch[t] = lo;
+        }
+        carry = min(carry, chunk);
+        __syncthreads();
+    }
+    if (tid == 0) s_base = 0;
+    __syncthreads();
+    for (long long c0 = 0; c0 < tiles; c0 += 1024) {
+        const long long t = c0 + tid;
+        const uint32_t cnt = t < tiles ? (uint32_t)scratch[t] : 0u;
+        const uint32_t incl = warp_scan_add(cnt, lane);
+        if (lane == 31) s_w[warp] = (int32_t)incl;
+        __syncthreads();
+        uint32_t wpre = 0, total = 0;
+        for (int w2 = 0; w2 < 32; ++w2) {
+            if (w2 < warp) wpre += (uint32_t)s_w[w2];
+            total += (uint32_t)s_w[w2];
+        }
+        const long long o = s_base + wpre + incl - cnt;
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const long long src = t * (long long)tile + k;
+            const uint32_t ix = stair_idx[src];
+            out_val[o + k] = stair_val[src];
+            if (out_idx) out_idx[o + k] = (long long)ix + idx_off;
+            if (out_sym) out_sym[o + k] = sym[ix];
+        }
+        __syncthreads();
+        if (tid == 0) s_base += total;
+        __syncthreads();
+    }
+    if (tid == 0) *out_len = s_base;
+}
+
+// Answers from the shards before this one for the elements that found none
+// inside it (xq: index << 32 | value): the nearest earlier shard whose
+// staircase starts at or below the value, and in it the last entry at or
+// below the value (futhark/parser.fut:72-108 over the whole document).
+// Nodes get that entry's global index as parent; a right bracket's entry must
+// be a left of its symbol (futhark/parser.fut:168-184), else the document is
+// rejected.
+__global__ void shard_resolve_kernel(const unsigned long long* xq, const unsigned int* xq_count, long long xq_cap,
+                                     int n_prev, const long long* prev_off, const int32_t* pval,
+                                     const long long* pidx, const uint32_t* psym, long long* out_parent,
+                                     const uint32_t* sym, uint8_t* valid) {
+    const long long cnt = min((long long)*xq_count, xq_cap);
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cnt;
+         e += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long r = xq[e];
+        const long long g = (long long)(r >> 32);
+        const int32_t x = (int32_t)(uint32_t)r;
+        long long ans = -1;
+        for (int rk = n_prev - 1; rk >= 0 && ans < 0; --rk) {
+            long long lo = prev_off[rk], hi = prev_off[rk + 1] - 1;
+            if (hi < lo || pval[lo] > x) continue;
+            while (lo < hi) {  // last entry at or below x
+                const long long mid = (lo + hi + 1) >> 1;
+                if (pval[mid] <= x) lo = mid; else hi = mid - 1;
+            }
+            ans = lo;
+        }
+        if (sym) {
+            if (ans < 0) {
+                valid[0] = 0;
+            } else {
+                const uint32_t l = psym[ans], rr = sym[g];
+                if (!(l >> 31) || (l & 0x7fffffffu) != (rr & 0x7fffffffu)) valid[0] = 0;
+            }
+        } else {
+            out_parent[g] = ans < 0 ? -1 : pidx[ans];
+        }
+    }
+}
+
+// A shard's positions: its tokens, with ⊢ before them on the document's first
+// shard and ⊣ after them on its last (spans stay the document's).
+__global__ void shard_positions_kernel(const uint32_t* term, const int64_t* ts, const int64_t* te, long long m,
+                                       int first, int last, uint16_t* P, uint32_t* s32, uint32_t* e32, uint32_t sl,
+                                       uint32_t sr, AlpResult* res) {
+    const long long L = m + first + last;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L; i += (long long)gridDim.x * blockDim.x) {
+        if ((first && i == 0) || (last && i == L - 1)) {
+            P[i] = (uint16_t)(first && i == 0 ? sl : sr);
+            s32[i] = 0;
+            e32[i] = 0;
+            continue;
+        }
+        const long long k = i - first;
+        const uint32_t t = term[k];
+        if (t > 0xffffu || t == sl || t == sr) res->valid = 0;
+        P[i] = (uint16_t)t;
+        s32[i] = (uint32_t)ts[k];
+        e32[i] = (uint32_t)te[k];
     }
 }
 

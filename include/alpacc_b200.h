@@ -198,6 +198,54 @@ int alp_lex_shard_emit(alp_lex_shard* s, int64_t carried_start, uint32_t* d_term
                        int64_t* d_end, int64_t cap, int64_t* n_tok, int* valid);
 void alp_lex_shard_free(alp_lex_shard* s);
 
+/* One document parsed by several GPUs (no counterpart in the reference, whose
+ * API parses one document per call; it splits the scans of
+ * futhark/parser.fut:110-332 at slice edges).  Rank r holds a contiguous slice
+ * of the document's tokens (as alp_lex_shard gives them, spans in document
+ * positions); the first slice's positions start with ⊢ and the last's end
+ * with ⊣.  Three small all-gathers join the ranks:
+ *   - begin: the slice's positions; h_edge[0..15] the terminals of its first
+ *     16 positions and h_edge[16..31] of its last 16 (the parser's empty
+ *     terminal where the slice is shorter), *n_pos its position count.
+ *     Gather (h_edge, n_pos) from every rank.
+ *   - sums: halo_l[16] / halo_r[16] the terminals of the 16 positions before
+ *     and after the slice (empty past the document), from the gathered edges.
+ *     sums[10]: nodes, brackets, depth, sum of (arity - 1), terminal
+ *     productions, document heads, the last head's position (-1: none),
+ *     bracket pairs closed between adjacent positions, those closed at the
+ *     slice's first position with the slice before, the first position's
+ *     pair id.  Gather sums from every rank.
+ *   - expand: pre[8] the first eight sums combined over the slices before
+ *     (depth, v and terminal counts restart after a head), pos_base the
+ *     positions before the slice, closed_next the next slice's sums[8] (0 on
+ *     the last).  Writes the slice's nodes (parents within the slice, spans
+ *     and tags final) and matches its brackets; gives the sizes of its two
+ *     staircases (node values and bracket depths strictly below everything
+ *     after them in the slice).
+ *   - stairs: copies the staircases out (values; global node index or bracket
+ *     symbol).  Gather them from every rank.
+ *   - resolve: the staircases of the slices before, concatenated in rank
+ *     order with offsets n_off / b_off [n_prev + 1]; answers what had no
+ *     answer in the slice; *valid this slice's verdict (the document is
+ *     accepted iff every slice's is 1).
+ *   - tree: the slice's nodes (context-owned, until the next call on the
+ *     context) and the global index of its first node.
+ * One shard per context at a time. */
+typedef struct alp_parse_shard alp_parse_shard;
+int alp_parse_shard_begin(alp_ctx* ctx, const uint32_t* d_term, const int64_t* d_start, const int64_t* d_end,
+                          int64_t m, int is_first, int is_last, uint32_t* h_edge, int64_t* n_pos,
+                          alp_parse_shard** out);
+int alp_parse_shard_sums(alp_parse_shard* s, const uint32_t* halo_l, const uint32_t* halo_r, int64_t* sums);
+int alp_parse_shard_expand(alp_parse_shard* s, const int64_t* pre, int64_t pos_base, int64_t closed_next,
+                           int64_t* n_node, int64_t* n_stair_nodes, int64_t* n_stair_brackets);
+int alp_parse_shard_stairs(alp_parse_shard* s, int32_t* h_nval, int64_t* h_nidx, int32_t* h_bval, uint32_t* h_bsym);
+int alp_parse_shard_resolve(alp_parse_shard* s, int n_prev, const int64_t* n_off, const int32_t* nval,
+                            const int64_t* nidx, const int64_t* b_off, const int32_t* bval, const uint32_t* bsym,
+                            int* valid);
+int alp_parse_shard_tree(alp_parse_shard* s, int64_t** d_parent, uint32_t** d_tag, uint8_t** d_kind,
+                         int64_t** d_start, int64_t** d_end, int64_t* n_node, int64_t* first_node);
+void alp_parse_shard_free(alp_parse_shard* s);
+
 /* alp_lex_host over a stream of `piece`-byte pieces (0: 16 MiB): the copy of
  * one piece in, the lexing of the one before and the copy of the tokens of the
  * one before that out overlap on three CUDA streams.  Same results as
