@@ -1102,9 +1102,11 @@ __global__ void positions_kernel(long long* pos, long long count, long long C) {
 
 int gemm(alp_ctx* ctx, const __nv_bfloat16* A, long long sa_m, long long sa_k, const __nv_bfloat16* B, long long sb_k,
          long long sb_n, float* C, long long ldc, int M, int N, int K) {
-    GemmArgs g{A, sa_m, sa_k, B, sb_k, sb_n, C, ldc, M, N, K, 0};
-    dim3 grid((N + 63) / 64, (M + 63) / 64);
-    gemm_bf16_kernel<<<grid, 128, 0, ctx->stream>>>(g);
+    AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
+    GemmArgs g{A, sa_m, sa_k, B, sb_k, sb_n, C, ldc, M, N, K, 0, &d_res->error};
+    dim3 grid((N + UG_BN - 1) / UG_BN, (M + UG_BM - 1) / UG_BM);
+    CK(cudaFuncSetAttribute(umma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UG_SMEM));
+    umma_gemm_kernel<<<grid, 128, UG_SMEM, ctx->stream>>>(g);
     CK(cudaGetLastError());
     return ALP_OK;
 }
@@ -2002,7 +2004,7 @@ struct alp_parse_shard {
     long long sums[10] = {};
     long long N = 0, K = 0, node_base = 0, br_base = 0, pos_base = 0;
     long long n_stair_n = 0, n_stair_b = 0;
-    DevBuf xq_n, xq_b, st_n_val, st_n_idx, st_b_val, st_b_sym, st_scratch, counts, prev_n, prev_b, seg;
+    DevBuf xq_n, xq_b, st_n_val, st_n_idx, st_b_val, st_b_sym, st_scratch, counts, prev_n, prev_b, seg, halo;
     int expanded = 0;
 };
 
@@ -2059,8 +2061,7 @@ void shard_args(alp_parse_shard* s, ParseArgs& a, AlpResult* d_res) {
     a.doc_valid = (uint8_t*)ctx->tmp[T_DVALID].p;
     a.subst_terminals = 1;
     a.shard = 1;
-    memcpy(a.halo_l, s->halo_l, sizeof a.halo_l);
-    memcpy(a.halo_r, s->halo_r, sizeof a.halo_r);
+    a.halo = (const uint32_t*)s->halo.p;
     a.prev_pair = s->prev_pair;
     a.next_pair = s->next_pair;
 }
@@ -2129,6 +2130,10 @@ int alp_parse_shard_sums(alp_parse_shard* s, const uint32_t* halo_l, const uint3
     CK(cudaSetDevice(ctx->device));
     memcpy(s->halo_l, halo_l, sizeof s->halo_l);
     memcpy(s->halo_r, halo_r, sizeof s->halo_r);
+    int rc0;
+    if ((rc0 = grow(ctx, s->halo, 2 * PS_HALO * sizeof(uint32_t)))) return rc0;
+    CK(cudaMemcpy(s->halo.p, s->halo_l, PS_HALO * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((uint32_t*)s->halo.p + PS_HALO, s->halo_r, PS_HALO * sizeof(uint32_t), cudaMemcpyHostToDevice));
     const long long L = s->L;
     // the slice's own terminals at its edges, then the pair ids just outside it
     std::vector<uint16_t> head((size_t)std::min<long long>(L, PS_HALO)), tail(head.size());
@@ -2234,8 +2239,10 @@ int alp_parse_shard_expand(alp_parse_shard* s, const int64_t* pre, int64_t pos_b
         parse_expand_kernel<0, 0, false><<<g, PP_THREADS, sm2, ctx->stream>>>(a);
         CK(cudaGetLastError());
     }
-    // one document: its first element is here only on the first shard (-1: it started before)
-    long long seg[4] = {s->first ? 0 : -1, N, s->first ? 0 : -1, K};
+    // one document: its first node is here only when no node comes before the shard (the
+    // root, parent 0; -1: the document started before), likewise its first kept bracket
+    const bool root_here = s->node_base == 0;
+    long long seg[4] = {root_here ? 0 : -1, N, s->br_base == 0 ? 0 : -1, K};
     if ((rc = grow(ctx, s->seg, sizeof seg)) || (rc = grow(ctx, s->xq_n, (size_t)N * 8 + 16)) ||
         (rc = grow(ctx, s->xq_b, (size_t)K * 8 + 16)) || (rc = grow(ctx, s->counts, 64)))
         return rc;
@@ -2246,7 +2253,7 @@ int alp_parse_shard_expand(alp_parse_shard* s, const int64_t* pre, int64_t pos_b
     long long* lens = (long long*)((uint8_t*)s->counts.p + 16);  // [0] node staircase, [1] bracket staircase
     uint8_t* dvalid = a.doc_valid;
     if ((rc = run_ple(ctx, a.vbuf, N, nullptr, o.parent, T_N_TMIN, d_seg, 1, dvalid, d_res, nullptr,
-                      s->first ? 0 : s->node_base - 1, (unsigned long long*)s->xq_n.p, cnt, N)) ||
+                      root_here ? 0 : s->node_base - 1, (unsigned long long*)s->xq_n.p, cnt, N)) ||
         (rc = run_ple(ctx, a.dsbuf, K, a.brbuf, nullptr, T_B_TMIN, d_seg + 2, 1, dvalid, d_res, nullptr, 0,
                       (unsigned long long*)s->xq_b.p, cnt + 1, K)))
         return rc;
@@ -2365,7 +2372,7 @@ void alp_parse_shard_free(alp_parse_shard* s) {
     if (!s) return;
     if (s->ctx) cudaSetDevice(s->ctx->device);
     for (DevBuf* b : {&s->xq_n, &s->xq_b, &s->st_n_val, &s->st_n_idx, &s->st_b_val, &s->st_b_sym, &s->st_scratch,
-                      &s->counts, &s->prev_n, &s->prev_b, &s->seg})
+                      &s->counts, &s->prev_n, &s->prev_b, &s->seg, &s->halo})
         if (b->p) cudaFree(b->p);
     delete s;
 }
@@ -2504,8 +2511,11 @@ int alp_mlp_train_step(alp_ctx* ctx, float* params, uint16_t* wbf, float* grads,
         (rc = grow(ctx, sb[M_DZ3], M * MLP_OUT * 4)) || (rc = grow(ctx, sb[M_DZ3B], M * MLP_OUT * 2)) ||
         (rc = grow(ctx, sb[M_DH], M * MLP_H * 4)) || (rc = grow(ctx, sb[M_DZ], M * MLP_H * 4)) ||
         (rc = grow(ctx, sb[M_DZB], M * MLP_H * 2)) || (rc = grow(ctx, sb[M_DX], M * MLP_IN * 4)) ||
-        (rc = grow(ctx, sb[M_SCAL], 64)))
+        (rc = grow(ctx, sb[M_SCAL], 64)) || (rc = grow(ctx, ctx->scratch, 256)))
         return rc;
+    // the GEMMs' bounded MMA waits report through the result block's error word
+    AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
+    CK(cudaMemsetAsync(&d_res->error, 0, sizeof(unsigned int), ctx->stream));
     __nv_bfloat16* emb_b = reinterpret_cast<__nv_bfloat16*>(wbf);
     __nv_bfloat16* w1_b = emb_b + 256 * MLP_EMB;
     __nv_bfloat16* w2_b = w1_b + MLP_IN * MLP_H;
@@ -2549,8 +2559,11 @@ int alp_mlp_train_step(alp_ctx* ctx, float* params, uint16_t* wbf, float* grads,
     }
     if (h_loss || h_acc) {
         float hs[2];
+        unsigned int err = 0;
         CK(cudaMemcpyAsync(hs, scal, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(&err, &d_res->error, sizeof err, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        if (err & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "tensor-core GEMM wait timed out");
         unsigned int corr;
         memcpy(&corr, &hs[1], 4);
         if (h_loss) *h_loss = hs[0] / (float)batch;

@@ -3,8 +3,9 @@
 // The network predicts the DFA state at a chunk boundary from the 64 bytes
 // before it: byte -> 16-d embedding (64 x 16 = 1024 inputs) -> 128 -> 128 ->
 // logits over the lexer's states (padded to 32).  Weights and activations
-// enter the tensor cores as BF16, every product accumulates in FP32
-// (mma.sync m16n8k16).  There is no reference counterpart: alpacc has no
+// enter the tensor cores as BF16, every product accumulates in FP32: training
+// GEMMs and the default inference kernel on tcgen05, the earlier inference
+// kernel on mma.sync m16n8k16.  There is no reference counterpart: alpacc has no
 // learned component; the speculative lexer that uses these predictions is
 // verified against the exact composition scan, so its output is bit-exact
 // whatever the network predicts.
@@ -57,9 +58,16 @@ __device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
 }
 
 // ---------------------------------------------------------------------------
-// Generic GEMM for training: C[M][N] (FP32) = A[M][K] . B[K][N], A and B BF16
-// addressed by strides (so transposes are free).  M, N, K multiples of 16.
-// 64 x 64 tile per block, 4 warps of 32 x 32.
+// Generic GEMM for training on the fifth-generation tensor cores:
+// C[M][N] (FP32) (+)= A[M][K] . B[K][N], A and B BF16 addressed by strides (so
+// transposes are free), M, N, K multiples of 16.  One CTA of 128 threads per
+// 128 x UG_BN tile of C (N <= UG_BN: one tile of N columns).  Each K step of 64:
+// the threads stage A (128 rows) and B^T (tile columns as rows) as K-major
+// 128-byte-swizzled tiles, one thread issues four K = 16 MMAs into the tensor
+// memory accumulator and commits them to an mbarrier (waits bounded), which
+// hands the tiles back for the next step; the four warps then read their 32
+// accumulator rows with tcgen05.ld.  Training moves about 0.3 MFLOP per
+// window, so the kernel keeps one stage and no warp roles.
 // ---------------------------------------------------------------------------
 struct GemmArgs {
     const __nv_bfloat16* A;
@@ -70,60 +78,106 @@ struct GemmArgs {
     long long ldc;
     int M, N, K;
     int accumulate;             // C += instead of C =
+    unsigned int* err;          // ALP_DEV_ERR_TIMEOUT when an MMA wait gives up
 };
 
-__global__ void __launch_bounds__(128) gemm_bf16_kernel(GemmArgs g) {
-    __shared__ __align__(16) __nv_bfloat16 sA[64][16 + 8];
-    __shared__ __align__(16) __nv_bfloat16 sB[64][16 + 8];  // transposed: [n][k]
+constexpr int UG_BM = 128;
+constexpr int UG_BN = 128;
+constexpr int UG_BK = 64;
+constexpr size_t UG_SMEM = (size_t)UG_BM * 128 + (size_t)UG_BN * 128 + 1024;  // A and B tiles, 1 KiB alignment slack
+
+__global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_abort;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int gid = lane >> 2, tig = lane & 3;
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
-    for (int k0 = 0; k0 < g.K; k0 += 16) {
-        for (int e = tid; e < 64 * 16; e += 128) {
-            const int r = e >> 4, c = e & 15;
-            const int m = m0 + r, n = n0 + r, k = k0 + c;
-            sA[r][c] = (m < g.M) ? g.A[m * g.sa_m + (long long)k * g.sa_k] : __float2bfloat16(0.f);
-            sB[r][c] = (n < g.N) ? g.B[(long long)k * g.sb_k + n * g.sb_n] : __float2bfloat16(0.f);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const int r = wm + i * 16 + gid;
-            const uint32_t a0 = *reinterpret_cast<const uint32_t*>(&sA[r][tig * 2]);
-            const uint32_t a1 = *reinterpret_cast<const uint32_t*>(&sA[r + 8][tig * 2]);
-            const uint32_t a2 = *reinterpret_cast<const uint32_t*>(&sA[r][tig * 2 + 8]);
-            const uint32_t a3 = *reinterpret_cast<const uint32_t*>(&sA[r + 8][tig * 2 + 8]);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int n = wn + j * 8 + gid;
-                const uint32_t b0 = *reinterpret_cast<const uint32_t*>(&sB[n][tig * 2]);
-                const uint32_t b1 = *reinterpret_cast<const uint32_t*>(&sB[n][tig * 2 + 8]);
-                mma_bf16(acc[i][j], a0, a1, a2, a3, b0, b1);
-            }
-        }
-        __syncthreads();
+    const uint32_t base = ((uint32_t)__cvta_generic_to_shared(smem_raw) + 1023u) & ~1023u;
+    uint8_t* sp = smem_raw + (base - (uint32_t)__cvta_generic_to_shared(smem_raw));
+    const uint32_t sa = base, sb = base + UG_BM * 128;
+    const int m0 = blockIdx.y * UG_BM, n0 = blockIdx.x * UG_BN;
+    const int bn = min(UG_BN, g.N - n0);               // columns of this tile: a multiple of 16
+    const uint32_t ncols = bn <= 32 ? 32u : (bn <= 64 ? 64u : 128u);
+    if (warp == 0) tmem_alloc(&s_tmem, ncols);
+    if (tid == 0) {
+        mbar_init(&s_bar, 1);
+        mbar_fence_init();
+        s_abort = 0;
     }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = umma_idesc_bf16_f32(UG_BM, bn);
+    uint32_t phase = 0;
+    for (int k0 = 0; k0 < g.K; k0 += UG_BK) {
+        // stage A rows m0.. and B columns n0.. (as rows), K-major, 16-byte chunks
+        for (int e = tid; e < (UG_BM + bn) * 8; e += 128) {
+            const int r = e >> 3, c = e & 7;
+            const bool is_a = r < UG_BM;
+            const int row = is_a ? r : r - UG_BM;
+            uint32_t w[4];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+            for (int h = 0; h < 4; ++h) {
+                uint32_t v = 0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+                for (int q = 0; q < 2; ++q) {
+                    const int k = k0 + c * 8 + 2 * h + q;
+                    __nv_bfloat16 x = __float2bfloat16(0.f);
+                    if (k < g.K) {
+                        if (is_a) {
+                            const int m = m0 + row;
+                            if (m < g.M) x = g.A[(long long)m * g.sa_m + (long long)k * g.sa_k];
+                        } else {
+                            x = g.B[(long long)k * g.sb_k + (long long)(n0 + row) * g.sb_n];
+                        }
+                    }
+                    v |= (uint32_t)__bfloat16_as_ushort(x) << (16 * q);
+                }
+                w[h] = v;
+            }
+            *reinterpret_cast<uint4*>(sp + (is_a ? 0 : UG_BM * 128) + sw128_offset((uint32_t)row, (uint32_t)c)) =
+                make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const int m = m0 + wm + i * 16 + gid + (r >= 2 ? 8 : 0);
-                const int n = n0 + wn + j * 8 + tig * 2 + (r & 1);
-                if (m < g.M && n < g.N) {
-                    float* c = &g.C[(long long)m * g.ldc + n];
-                    *c = g.accumulate ? *c + acc[i][j][r] : acc[i][j][r];
+            for (int kk = 0; kk < UG_BK / 16; ++kk)
+                if (k0 + kk * 16 < g.K)
+                    umma_bf16(tmem, umma_desc_sw128(sa) + 2 * kk, umma_desc_sw128(sb) + 2 * kk, idesc,
+                              (k0 > 0 || kk > 0) ? 1u : 0u);
+            umma_commit(&s_bar);
+        }
+        // the tiles are free again once the MMAs that read them are done
+        if (!mbar_wait(&s_bar, phase, g.err)) s_abort = 1;
+        phase ^= 1u;
+        tc_fence_after();
+        __syncthreads();
+        if (s_abort) break;
+    }
+    // epilogue: warp w holds accumulator rows 32w .. 32w + 31
+    if (!s_abort) {
+        const int m = m0 + warp * 32 + lane;
+        for (int c0 = 0; c0 < bn; c0 += 32) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (m < g.M) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int n = n0 + c0 + j;
+                    if (c0 + j < bn) {
+                        float* c = &g.C[(long long)m * g.ldc + n];
+                        *c = g.accumulate ? *c + v[j] : v[j];
+                    }
                 }
             }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_free(tmem, ncols);
 }
 
 // ---------------------------------------------------------------------------

@@ -347,8 +347,9 @@ struct ParseArgs {
     // the terminals around it, the pair ids of the positions just outside it,
     // the sums of the shards before it and where its outputs start
     int shard;
-    uint32_t halo_l[PS_HALO];   // terminals of positions -PS_HALO .. -1 (empty past the document)
-    uint32_t halo_r[PS_HALO];   // terminals of positions L .. L + PS_HALO - 1
+    // [2 * PS_HALO] in device memory: terminals of positions -PS_HALO .. -1, then of
+    // positions L .. L + PS_HALO - 1 (empty past the document)
+    const uint32_t* halo;
     uint32_t prev_pair, next_pair;  // NO_PAIR: no position there
     PosSums pre;
     long long node_base;        // global index of the shard's first node
@@ -357,8 +358,8 @@ struct ParseArgs {
 };
 
 __device__ __forceinline__ uint32_t pos_term(const ParseArgs& a, long long i) {
-    if (i < 0) return (a.shard && i >= -PS_HALO) ? a.halo_l[PS_HALO + i] : a.t.empty;
-    if (i >= a.L) return (a.shard && i - a.L < PS_HALO) ? a.halo_r[i - a.L] : a.t.empty;
+    if (i < 0) return (a.shard && i >= -PS_HALO) ? __ldg(&a.halo[PS_HALO + i]) : a.t.empty;
+    if (i >= a.L) return (a.shard && i - a.L < PS_HALO) ? __ldg(&a.halo[PS_HALO + (i - a.L)]) : a.t.empty;
     return (uint32_t)a.P[i];
 }
 
@@ -373,7 +374,7 @@ __host__ __device__ inline size_t pairs_smem_bytes(int n_pairs, int window) {
 // QT, KT > 0: the lookback and lookahead fixed at compile time (window loops
 // unrolled); 0: read from the tables.
 template <int QT, int KT>
-__global__ void __launch_bounds__(PP_THREADS) parse_pairs_kernel(ParseArgs a) {
+__global__ void __launch_bounds__(PP_THREADS, 3) parse_pairs_kernel(ParseArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     PairInfo* s_pi = reinterpret_cast<PairInfo*>(smem);
     uint32_t* s_term = reinterpret_cast<uint32_t*>(smem + sizeof(PairInfo) * a.t.n_pairs);

@@ -846,84 +846,113 @@ def _wrap_valid(st):
     return api._wrap(st["g"].h, st["ptrs"][6].value or 0, st["n_docs"], torch.uint8, st["g"].device)
 
 
-def run_spec(args, rank: int, world: int, local: int):
-    """Learned boundary-state speculation against the plain lexer."""
+def _spec_eval(name, depth, eval_seed, size, args, local, dist, chunks):
+    """Train the boundary MLP on the GPU (pairs labelled by the exact lexer on
+    documents from other seeds), then time alp_lex_speculative at each chunk
+    size against alp_lex on one document, tokens compared on the device.
+    Returns (summary, grammar, model, device input, best (C, ms, tokens), clocks)."""
     import ctypes
     import torch
     from alpacc_b200 import api, spec, synth, tables
+    dev = f"cuda:{local}"
+    L = api.native()
+    g = api.Grammar(tables.load(name, "lexer"), device=local)
+    g._stream()
+    t0 = time.perf_counter()
+    docs = [synth.json_doc(16 << 20, depth, SEED_TRAIN + k) if name == "json"
+            else synth.sexp_doc(16 << 20, depth, SEED_TRAIN + k) for k in range(10)]
+    win, lab = spec.dataset(g, docs, 1000000, SEED_TRAIN)
+    model = spec.BoundaryModel(g, seed=1)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    hist = model.train(win, lab, epochs=1, batch=4096, lr=2e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t1
+    del win, lab, docs
+    doc = synth.json_doc(size, depth, eval_seed) if name == "json" else synth.sexp_doc(size, depth, eval_seed)
+    x = torch.from_numpy(doc).to(dev)
+    ptrs = [ctypes.c_void_p() for _ in range(3)]
+    n_tok, valid = ctypes.c_int64(0), ctypes.c_int(0)
+
+    def plain():
+        rc = L.alp_lex(g.h, ctypes.c_void_p(x.data_ptr()), size, *[ctypes.byref(p) for p in ptrs],
+                       ctypes.byref(n_tok), ctypes.byref(valid))
+        if rc != 0 or not valid.value:
+            raise RuntimeError("alp_lex failed")
+
+    for _ in range(max(3, args.warmup)):
+        plain()
+    ms_plain, clk = _timed(plain, args.steps, local, dist)
+    M = n_tok.value
+    ref = [api._wrap(g.h, p.value or 0, M, dt, g.device).clone()
+           for p, dt in zip(ptrs, (torch.int32, torch.int64, torch.int64))]
+    res = {"train_pairs": int(hist["steps"]) * 4096, "train_s": t_train, "train_acc": hist["last_acc"],
+           "prep_s": t1 - t0, "plain_gbs": size / (ms_plain * 1e-3) / 1e9, "plain_ms": ms_plain, "tokens": M,
+           "chunks": {}}
+    Ls = spec._L()
+    sptr = [ctypes.c_void_p() for _ in range(3)]
+    sn, sv = ctypes.c_int64(0), ctypes.c_int(0)
+    stats = (ctypes.c_int64 * 4)()
+    best = None
+    for C in chunks:
+
+        def sp():
+            rc = Ls.alp_lex_speculative(g.h, ctypes.c_void_p(model.wbf.data_ptr()),
+                                        ctypes.c_void_p(model.params.data_ptr()), model.n_states,
+                                        ctypes.c_void_p(x.data_ptr()), size, C, *[ctypes.byref(p) for p in sptr],
+                                        ctypes.byref(sn), ctypes.byref(sv), stats)
+            if rc != 0:
+                raise RuntimeError("alp_lex_speculative failed: %s" % L.alp_last_error(g.h).decode())
+
+        for _ in range(max(3, args.warmup)):
+            sp()
+        ms_sp, _ = _timed(sp, args.steps, local, dist)
+        st = list(stats)
+        exact = bool(sv.value) and sn.value == M and all(
+            torch.equal(api._wrap(g.h, p.value or 0, M, r.dtype, g.device), r) for p, r in zip(sptr, ref))
+        res["chunks"][str(C)] = {"gbs": size / (ms_sp * 1e-3) / 1e9, "ms": ms_sp,
+                                 "hit_rate": 1.0 - st[1] / max(1, st[0]), "rerun_fraction": st[2] / max(1, st[0]),
+                                 "rounds": st[3], "bit_exact": bool(exact), "vs_plain": ms_plain / ms_sp}
+        if not exact:
+            raise RuntimeError("speculative tokens differ from the plain lexer (%s, C=%d)" % (name, C))
+        if best is None or ms_sp < best[1]:
+            best = (C, ms_sp, M)
+    return res, g, model, x, best, clk
+
+
+def spec_summary(args, local):
+    """The default line's `spec` object: json.alp lexer, one 512 MiB document,
+    learned speculation at its better chunk size against the plain lexer."""
+    size = 512 << 20
+    res, g, model, x, best, _ = _spec_eval("json", 8, SEED_LEX, size, args, local, None, (1024, 4096))
+    C = best[0]
+    c = res["chunks"][str(C)]
+    out = {"workload": "json.alp lexer, one %d MiB document (depth <= 8), MLP trained on %d boundary pairs from "
+                       "other seeds" % (size >> 20, res["train_pairs"]),
+           "chunk": C, "gbs": c["gbs"], "plain_gbs": res["plain_gbs"], "vs_plain": c["vs_plain"],
+           "hit_rate": c["hit_rate"], "rerun_fraction": c["rerun_fraction"], "bit_exact": c["bit_exact"],
+           "train_s": res["train_s"], "chunks": res["chunks"]}
+    del x, model, g
+    return out
+
+
+def run_spec(args, rank: int, world: int, local: int):
+    """Learned boundary-state speculation against the plain lexer."""
+    import torch
     torch.cuda.set_device(local)
     dist = _dist_init(world)
     dev = f"cuda:{local}"
     size = (args.doc_mib << 20) if args.doc_mib_given else 512 << 20
-    L = api.native()
     results = {}
     kern_all = []
     best = None
     mlp_line = None
     clocks = None
     for name, depth, eval_seed in (("json", 8, SEED_LEX), ("sexp", 20, SEED_BATCH + 1)):
-        g = api.Grammar(tables.load(name, "lexer"), device=local)
-        g._stream()
-        # training pairs: documents from other seeds, about 10^7 boundaries
-        t0 = time.perf_counter()
-        docs = [synth.json_doc(16 << 20, depth, SEED_TRAIN + k) if name == "json"
-                else synth.sexp_doc(16 << 20, depth, SEED_TRAIN + k) for k in range(10)]
-        win, lab = spec.dataset(g, docs, 1000000, SEED_TRAIN)
-        model = spec.BoundaryModel(g, seed=1)
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        hist = model.train(win, lab, epochs=1, batch=4096, lr=2e-3)
-        torch.cuda.synchronize()
-        t_train = time.perf_counter() - t1
-        del win, lab
-        doc = synth.json_doc(size, depth, eval_seed) if name == "json" else synth.sexp_doc(size, depth, eval_seed)
-        x = torch.from_numpy(doc).to(dev)
-        ptrs = [ctypes.c_void_p() for _ in range(3)]
-        n_tok, valid = ctypes.c_int64(0), ctypes.c_int(0)
-
-        def plain():
-            rc = L.alp_lex(g.h, ctypes.c_void_p(x.data_ptr()), size, *[ctypes.byref(p) for p in ptrs],
-                           ctypes.byref(n_tok), ctypes.byref(valid))
-            if rc != 0 or not valid.value:
-                raise RuntimeError("alp_lex failed")
-
-        for _ in range(max(3, args.warmup)):
-            plain()
-        ms_plain, clk = _timed(plain, args.steps, local, dist)
+        res, g, model, x, b, clk = _spec_eval(name, depth, eval_seed, size, args, local, dist, (256, 1024, 4096))
         clocks = clocks or clk
-        M = n_tok.value
-        ref = [api._wrap(g.h, p.value or 0, M, dt, g.device).clone()
-               for p, dt in zip(ptrs, (torch.int32, torch.int64, torch.int64))]
-        res = {"train_pairs": int(hist["steps"]) * 4096, "train_s": t_train, "train_acc": hist["last_acc"],
-               "plain_gbs": size / (ms_plain * 1e-3) / 1e9, "tokens": M, "chunks": {}}
-        Ls = spec._L()
-        sptr = [ctypes.c_void_p() for _ in range(3)]
-        sn, sv = ctypes.c_int64(0), ctypes.c_int(0)
-        stats = (ctypes.c_int64 * 4)()
-        for C in (256, 1024, 4096):
-
-            def sp():
-                rc = Ls.alp_lex_speculative(g.h, ctypes.c_void_p(model.wbf.data_ptr()),
-                                            ctypes.c_void_p(model.params.data_ptr()), model.n_states,
-                                            ctypes.c_void_p(x.data_ptr()), size, C, *[ctypes.byref(p) for p in sptr],
-                                            ctypes.byref(sn), ctypes.byref(sv), stats)
-                if rc != 0:
-                    raise RuntimeError("alp_lex_speculative failed: %s" % L.alp_last_error(g.h).decode())
-
-            for _ in range(max(3, args.warmup)):
-                sp()
-            ms_sp, _ = _timed(sp, args.steps, local, dist)
-            st = list(stats)
-            exact = bool(sv.value) and sn.value == M and all(
-                torch.equal(api._wrap(g.h, p.value or 0, M, r.dtype, g.device), r) for p, r in zip(sptr, ref))
-            res["chunks"][str(C)] = {"gbs": size / (ms_sp * 1e-3) / 1e9, "ms": ms_sp,
-                                     "hit_rate": 1.0 - st[1] / max(1, st[0]), "rerun_fraction": st[2] / max(1, st[0]),
-                                     "rounds": st[3], "bit_exact": bool(exact),
-                                     "vs_plain": ms_plain / ms_sp}
-            if not exact:
-                raise RuntimeError("speculative tokens differ from the plain lexer (%s, C=%d)" % (name, C))
-            if name == "json" and (best is None or ms_sp < best[1]):
-                best = (C, ms_sp, M)
+        if name == "json":
+            best = b
         g.profile(True)
         model.lex(x, best[0] if name == "json" else 1024)
         kern_all += [("%s:%s" % (name, k), t) for k, t in g.timings()]
@@ -977,8 +1006,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the full-size comparison with the oracle")
     ap.add_argument("--no-graph", action="store_true", help="batch workload: skip the CUDA-graph replay")
+    ap.add_argument("--no-spec", action="store_true", help="default workload: skip the learned-speculation object")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes (no autotuner run): for "
                     "launch lists whose first launches should be the measured ones")
+    ap.add_argument("--tuning", default=None, help="comma-separated tuning values (alp_tune_set) instead of the "
+                    "autotuner: to repeat a tuned run's configuration, e.g. under a profiler")
     ap.add_argument("--workload", default="parse", choices=["parse", "lex", "batch", "spec", "graph", "shard"])
     ap.add_argument("--batch-docs", type=int, default=100000, help="JSON documents of the batch workload "
                     "(half as many sexp documents); smaller values are for profiling")
@@ -1020,7 +1052,10 @@ def main():
                                                                        L.alp_last_error(g.h).decode()))
 
     # launch shapes from the autotuner, timed on this document (outside the timed region)
-    if args.no_tune:
+    if args.tuning:
+        g.set_tuning([int(x) for x in args.tuning.split(",")])
+        tuning = {"config": g.get_tuning(), "tile_shape": g.tile_shapes()[g.get_tuning()[0]], "timings": []}
+    elif args.no_tune:
         tuning = {"config": g.get_tuning(), "tile_shape": g.tile_shapes()[g.get_tuning()[0]], "timings": []}
     else:
         tuning = g.tune(d_in, reps=3)
@@ -1084,6 +1119,12 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(size, 5)
 
+    # learned speculation on the json.alp lexer, timed apart from the plain scan above
+    spec_res = None
+    if rank == 0 and world == 1 and not args.no_spec:
+        del h_in, outs
+        spec_res = spec_summary(args, local)
+
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -1124,6 +1165,8 @@ def main():
         line["cpu_baseline"] = base
     if parity:
         line["parity"] = parity
+    if spec_res:
+        line["spec"] = spec_res
     print(json.dumps(line), flush=True)
 
 
