@@ -84,6 +84,9 @@ struct alp_ctx {
     // host-input token streams (alp_lex_host_stream): copy streams, events,
     // two slots of piece and token buffers, the carry and its pinned mirrors
     cudaStream_t cp_in = nullptr, cp_out = nullptr;
+    // the bracket search runs beside the node search on this stream (fork / join events)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_in[2] = {}, ev_done[2] = {}, ev_out[2] = {};
     DevBuf pipe;
     DevBuf carry;
@@ -394,8 +397,9 @@ int persistent_ctas(int fit, int tuned) {
 int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, int64_t* parent, int first,
             const long long* seg_off, long long n_seg, uint8_t* seg_valid, AlpResult* d_res,
             const long long* dn = nullptr, long long out_off = 0, unsigned long long* xq = nullptr,
-            unsigned int* xq_count = nullptr, long long xq_cap = 0) {
+            unsigned int* xq_count = nullptr, long long xq_cap = 0, cudaStream_t stream = nullptr) {
     if (n == 0) return ALP_OK;
+    cudaStream_t st = stream ? stream : ctx->stream;
     const PleShape& sh = ple_shapes[ctx->tune.ple];
     const int tile = sh.threads * sh.items;
     const long long tiles = (n + tile - 1) / tile;
@@ -410,7 +414,7 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
         return rc;
     unsigned int* esc_count = reinterpret_cast<unsigned int*>(reinterpret_cast<uint8_t*>(ctx->tmp[first + 6].p) +
                                                               (size_t)n * 8);
-    CK(cudaMemsetAsync(esc_count, 0, 16, ctx->stream));
+    CK(cudaMemsetAsync(esc_count, 0, 16, st));
     PleArgs a;
     a.val = val;
     a.n = n;
@@ -436,10 +440,10 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     mark(ctx, "start");
     {
         void* args[] = {&a};
-        CK(cudaLaunchKernel(sh.fn, dim3((unsigned)tiles), dim3(sh.threads), args, sh.smem, ctx->stream));
+        CK(cudaLaunchKernel(sh.fn, dim3((unsigned)tiles), dim3(sh.threads), args, sh.smem, st));
     }
     mark(ctx, sym ? "ple_tile_kernel(brackets)" : "ple_tile_kernel(nodes)");
-    tile_min_levels_kernel<<<(unsigned)((n32 + 255) / 256), 256, 0, ctx->stream>>>(
+    tile_min_levels_kernel<<<(unsigned)((n32 + 255) / 256), 256, 0, st>>>(
         a.tile_min, tiles, (int32_t*)ctx->tmp[first + 1].p, (int32_t*)ctx->tmp[first + 2].p, dn, tile);
     CK(cudaGetLastError());
     EscArgs e;
@@ -463,7 +467,7 @@ int run_ple(alp_ctx* ctx, const int32_t* val, long long n, const uint32_t* sym, 
     e.xq = xq;
     e.xq_count = xq_count;
     e.xq_cap = xq_cap;
-    ple_escape_kernel<<<148 * 4, 256, 0, ctx->stream>>>(e);
+    ple_escape_kernel<<<148 * 4, 256, 0, st>>>(e);
     CK(cudaGetLastError());
     mark(ctx, sym ? "tile_min+ple_escape(brackets)" : "tile_min+ple_escape(nodes)");
     return ALP_OK;
@@ -972,10 +976,30 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     ctx->last_kept = K;
     ctx->est_nodes = (double)N / (double)L;
     ctx->est_kept = (double)K / (double)L;
-    if (want_tree) {
+    if (want_tree && !ctx->prof) {
+        // the node and bracket searches share nothing but the result block (atomic
+        // error bits) and document validity (cleared only): the bracket search runs on a
+        // second stream beside the node search, each half-filling the SMs alone
+        if (!ctx->aux) {
+            CK(cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+        }
+        CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
+        CK(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
+        if ((rc = run_ple(ctx, a.dsbuf, K, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res, nullptr, 0,
+                          nullptr, nullptr, 0, ctx->aux)))
+            return rc;
         if ((rc = run_ple(ctx, a.vbuf, N, nullptr, o->parent, T_N_TMIN, a.node_off, nd, dvalid, d_res))) return rc;
+        CK(cudaEventRecord(ctx->ev_join, ctx->aux));
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+    } else {
+        // profiled calls keep one stream, so that every kernel's time is its own
+        if (want_tree) {
+            if ((rc = run_ple(ctx, a.vbuf, N, nullptr, o->parent, T_N_TMIN, a.node_off, nd, dvalid, d_res))) return rc;
+        }
+        if ((rc = run_ple(ctx, a.dsbuf, K, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res))) return rc;
     }
-    if ((rc = run_ple(ctx, a.dsbuf, K, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res))) return rc;
     if ((rc = read_result(ctx, d_res))) return rc;
     *n_node = N;
     return ALP_OK;
@@ -1187,6 +1211,9 @@ void alp_ctx_destroy(alp_ctx* ctx) {
     }
     if (ctx->cp_in) cudaStreamDestroy(ctx->cp_in);
     if (ctx->cp_out) cudaStreamDestroy(ctx->cp_out);
+    if (ctx->aux) cudaStreamDestroy(ctx->aux);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     delete ctx;
 }
 
@@ -2217,7 +2244,7 @@ int alp_parse_shard_expand(alp_parse_shard* s, const int64_t* pre, int64_t pos_b
     s->node_base = pre[0];
     s->br_base = pre[1] - 2 * pre[7] - s->sums[8];
     s->N = s->sums[0];
-    s->K = s->sums[1] - 2 * s->sums[7] + s->sums[8] - closed_next;
+    s->K = s->L > 0 ? s->sums[1] - 2 * s->sums[7] + s->sums[8] - closed_next : 0;
     if (s->K < 0) return fail(ctx, ALP_ERR_ARG, "inconsistent closed-pair counts between shards");
     const long long L = s->L, N = s->N, K = s->K;
     int rc;

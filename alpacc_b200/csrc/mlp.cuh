@@ -111,11 +111,16 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
     const uint32_t idesc = umma_idesc_bf16_f32(UG_BM, bn);
     uint32_t phase = 0;
     for (int k0 = 0; k0 < g.K; k0 += UG_BK) {
-        // stage A rows m0.. and B columns n0.. (as rows), K-major, 16-byte chunks
+        // stage A rows m0.. and B columns n0.. (as rows), K-major, 16-byte chunks; an
+        // operand whose rows are contiguous in memory (K strided: a transpose) is read with
+        // consecutive threads on consecutive rows, so that every load is coalesced
+        const bool a_rows = g.sa_m == 1 && g.sa_k != 1, b_rows = g.sb_n == 1 && g.sb_k != 1;
         for (int e = tid; e < (UG_BM + bn) * 8; e += 128) {
-            const int r = e >> 3, c = e & 7;
-            const bool is_a = r < UG_BM;
-            const int row = is_a ? r : r - UG_BM;
+            const bool is_a = e < UG_BM * 8;
+            const int ee = is_a ? e : e - UG_BM * 8, rows = is_a ? UG_BM : bn;
+            const bool by_rows = is_a ? a_rows : b_rows;
+            const int row = by_rows ? ee % rows : ee >> 3;
+            const int c = by_rows ? ee / rows : ee & 7;
             uint32_t w[4];
 #pragma unroll
             for (int h = 0; h < 4; ++h) {

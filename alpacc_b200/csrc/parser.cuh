@@ -481,8 +481,21 @@ __global__ void __launch_bounds__(PP_THREADS, 3) parse_pairs_kernel(ParseArgs a)
         for (int j = 0; j < PP_ITEMS; ++j)
             if (i0 + j < a.L) a.pid[i0 + j] = ids[j];
     }
-    // ordered block reduce: the warps' totals, then warp 0 over them
-    PosSums inc = ps_warp_scan(acc, lane);
+    // ordered block reduce: the warps' totals, then warp 0 over them; a warp without a
+    // document head adds its fields with one warp reduction each
+    PosSums inc;
+    if (!__any_sync(ALP_FULL_MASK, acc.heads != 0)) {
+        inc.nodes = __reduce_add_sync(ALP_FULL_MASK, acc.nodes);
+        inc.brs = __reduce_add_sync(ALP_FULL_MASK, acc.brs);
+        inc.depth = __reduce_add_sync(ALP_FULL_MASK, acc.depth);
+        inc.v = __reduce_add_sync(ALP_FULL_MASK, acc.v);
+        inc.terms = __reduce_add_sync(ALP_FULL_MASK, acc.terms);
+        inc.cls = __reduce_add_sync(ALP_FULL_MASK, acc.cls);
+        inc.heads = 0;
+        inc.hpos = -1;
+    } else {
+        inc = ps_warp_scan(acc, lane);
+    }
     if (lane == 31) s_w[warp] = inc;
     __syncthreads();
     if (warp == 0) {

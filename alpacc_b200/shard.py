@@ -321,7 +321,9 @@ def prefix(sums: Sequence[np.ndarray], rank: int):
 
 def closed_next(sums: Sequence[np.ndarray], edges: Sequence[Tuple[np.ndarray, int]], rank: int) -> int:
     """Bracket pairs the next slice with positions closes at its first
-    position (the slices between, if any, are empty)."""
+    position (the slices between, if any, are empty); none for an empty slice."""
+    if int(edges[rank][1]) == 0:
+        return 0
     for r in range(rank + 1, len(sums)):
         if int(edges[r][1]) > 0:
             return int(sums[r][8])

@@ -53,3 +53,5 @@ def test_closed_next_skips_empty_slices():
     edges[1] = (None, 3)
     assert shard.closed_next(sums, edges, 0) == 4
     assert shard.closed_next(sums, edges, 3) == 0
+    edges[1] = (None, 0)
+    assert shard.closed_next(sums, edges, 1) == 0  # an empty slice closes nothing
