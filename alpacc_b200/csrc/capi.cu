@@ -1117,21 +1117,42 @@ int tokens_in(alp_ctx* ctx, const uint32_t* term, const int64_t* ts, const int64
 
 
 // ---- learned speculation: MLP training and inference, speculative lexer ----
-enum { M_X = 0, M_Z1, M_H1, M_H1B, M_Z2, M_H2, M_H2B, M_Z3, M_DZ3, M_DZ3B, M_DH, M_DZ, M_DZB, M_DX, M_SCAL, M_CNT };
+enum { M_X = 0, M_Z1, M_H1, M_H1B, M_Z2, M_H2, M_H2B, M_Z3, M_DZ3, M_DZ3B, M_DH, M_DZ, M_DZB, M_DX, M_SCAL, M_PART,
+       M_CNT };
 
 __global__ void positions_kernel(long long* pos, long long count, long long C) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x)
         pos[i] = (i + 1) * C;
 }
 
+inline unsigned grid_for(long long n);
+
 int gemm(alp_ctx* ctx, const __nv_bfloat16* A, long long sa_m, long long sa_k, const __nv_bfloat16* B, long long sb_k,
          long long sb_n, float* C, long long ldc, int M, int N, int K) {
     AlpResult* d_res = reinterpret_cast<AlpResult*>(ctx->scratch.p);
-    GemmArgs g{A, sa_m, sa_k, B, sb_k, sb_n, C, ldc, M, N, K, 0, &d_res->error};
-    dim3 grid((N + UG_BN - 1) / UG_BN, (M + UG_BM - 1) / UG_BM);
+    const long long tiles = (long long)((N + UG_BN - 1) / UG_BN) * ((M + UG_BM - 1) / UG_BM);
+    // split K while the tiles alone leave most SMs idle and each split keeps >= 4 K steps
+    int splits = 1;
+    while (tiles * splits < 128 && K / (splits * 2) >= 4 * UG_BK) splits *= 2;
+    const int kper = ((K + splits * UG_BK - 1) / (splits * UG_BK)) * UG_BK;
+    splits = (K + kper - 1) / kper;
+    GemmArgs g{A, sa_m, sa_k, B, sb_k, sb_n, C, ldc, M, N, K, 0, &d_res->error, kper, 0};
+    const long long stride = (long long)M * N;
+    if (splits > 1) {
+        int rc;
+        if ((rc = grow(ctx, ctx->mlp[M_PART], (size_t)splits * stride * 4))) return rc;
+        g.C = reinterpret_cast<float*>(ctx->mlp[M_PART].p);
+        g.ldc = N;
+        g.part_stride = stride;
+    }
+    dim3 grid((N + UG_BN - 1) / UG_BN, (M + UG_BM - 1) / UG_BM, splits);
     CK(cudaFuncSetAttribute(umma_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UG_SMEM));
     umma_gemm_kernel<<<grid, 128, UG_SMEM, ctx->stream>>>(g);
     CK(cudaGetLastError());
+    if (splits > 1) {
+        gemm_splits_kernel<<<grid_for(stride), 256, 0, ctx->stream>>>(g.C, stride, splits, C, ldc, M, N, 0);
+        CK(cudaGetLastError());
+    }
     return ALP_OK;
 }
 

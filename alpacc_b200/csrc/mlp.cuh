@@ -79,6 +79,8 @@ struct GemmArgs {
     int M, N, K;
     int accumulate;             // C += instead of C =
     unsigned int* err;          // ALP_DEV_ERR_TIMEOUT when an MMA wait gives up
+    int kper;                   // K per split (blockIdx.z); each split writes its own partial C
+    long long part_stride;      // floats between splits' partials (0: one split, C itself)
 };
 
 constexpr int UG_BM = 128;
@@ -110,7 +112,12 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
     const uint32_t tmem = s_tmem;
     const uint32_t idesc = umma_idesc_bf16_f32(UG_BM, bn);
     uint32_t phase = 0;
-    for (int k0 = 0; k0 < g.K; k0 += UG_BK) {
+    const int kb = blockIdx.z * g.kper, ke = min(g.K, kb + g.kper);
+    float* C = g.C + blockIdx.z * g.part_stride;
+    // 16-byte loads where an operand's K run is contiguous and aligned
+    const bool a_vec = g.sa_k == 1 && (g.sa_m & 7) == 0 && (reinterpret_cast<uintptr_t>(g.A) & 15) == 0;
+    const bool b_vec = g.sb_k == 1 && (g.sb_n & 7) == 0 && (reinterpret_cast<uintptr_t>(g.B) & 15) == 0;
+    for (int k0 = kb; k0 < ke; k0 += UG_BK) {
         // stage A rows m0.. and B columns n0.. (as rows), K-major, 16-byte chunks; an
         // operand whose rows are contiguous in memory (K strided: a transpose) is read with
         // consecutive threads on consecutive rows, so that every load is coalesced
@@ -121,25 +128,38 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
             const bool by_rows = is_a ? a_rows : b_rows;
             const int row = by_rows ? ee % rows : ee >> 3;
             const int c = by_rows ? ee / rows : ee & 7;
-            uint32_t w[4];
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                uint32_t v = 0;
-#pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    const int k = k0 + c * 8 + 2 * h + q;
-                    __nv_bfloat16 x = __float2bfloat16(0.f);
-                    if (k < g.K) {
-                        if (is_a) {
-                            const int m = m0 + row;
-                            if (m < g.M) x = g.A[(long long)m * g.sa_m + (long long)k * g.sa_k];
-                        } else {
-                            x = g.B[(long long)k * g.sb_k + (long long)(n0 + row) * g.sb_n];
-                        }
-                    }
-                    v |= (uint32_t)__bfloat16_as_ushort(x) << (16 * q);
+            uint32_t w[4] = {0, 0, 0, 0};
+            const int kc = k0 + c * 8;
+            const bool vec = (is_a ? a_vec : b_vec) && kc + 8 <= ke;
+            if (vec) {
+                uint4 x = make_uint4(0, 0, 0, 0);
+                if (is_a) {
+                    const int m = m0 + row;
+                    if (m < g.M) x = __ldg(reinterpret_cast<const uint4*>(g.A + (long long)m * g.sa_m + kc));
+                } else {
+                    x = __ldg(reinterpret_cast<const uint4*>(g.B + (long long)(n0 + row) * g.sb_n + kc));
                 }
-                w[h] = v;
+                w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
+            } else {
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    uint32_t v = 0;
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const int k = kc + 2 * h + q;
+                        __nv_bfloat16 x = __float2bfloat16(0.f);
+                        if (k < ke) {
+                            if (is_a) {
+                                const int m = m0 + row;
+                                if (m < g.M) x = g.A[(long long)m * g.sa_m + (long long)k * g.sa_k];
+                            } else {
+                                x = g.B[(long long)k * g.sb_k + (long long)(n0 + row) * g.sb_n];
+                            }
+                        }
+                        v |= (uint32_t)__bfloat16_as_ushort(x) << (16 * q);
+                    }
+                    w[h] = v;
+                }
             }
             *reinterpret_cast<uint4*>(sp + (is_a ? 0 : UG_BM * 128) + sw128_offset((uint32_t)row, (uint32_t)c)) =
                 make_uint4(w[0], w[1], w[2], w[3]);
@@ -150,9 +170,9 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
             tc_fence_after();
 #pragma unroll
             for (int kk = 0; kk < UG_BK / 16; ++kk)
-                if (k0 + kk * 16 < g.K)
+                if (k0 + kk * 16 < ke)
                     umma_bf16(tmem, umma_desc_sw128(sa) + 2 * kk, umma_desc_sw128(sb) + 2 * kk, idesc,
-                              (k0 > 0 || kk > 0) ? 1u : 0u);
+                              (k0 > kb || kk > 0) ? 1u : 0u);
             umma_commit(&s_bar);
         }
         // the tiles are free again once the MMAs that read them are done
@@ -173,8 +193,8 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
                 for (int j = 0; j < 32; ++j) {
                     const int n = n0 + c0 + j;
                     if (c0 + j < bn) {
-                        float* c = &g.C[(long long)m * g.ldc + n];
-                        *c = g.accumulate ? *c + v[j] : v[j];
+                        float* c = &C[(long long)m * g.ldc + n];
+                        *c = (g.accumulate && !g.part_stride) ? *c + v[j] : v[j];
                     }
                 }
             }
@@ -183,6 +203,20 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
     tc_fence_before();
     __syncthreads();
     if (warp == 0) tmem_free(tmem, ncols);
+}
+
+// The split-K partials of umma_gemm_kernel summed in split order (the same
+// order every run, so the gradients are deterministic).
+__global__ void gemm_splits_kernel(const float* part, long long stride, int splits, float* C, long long ldc, int M,
+                                   int N, int accumulate) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (long long)M * N;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long m = e / N, n = e % N;
+        float x = 0.f;
+        for (int z = 0; z < splits; ++z) x += part[z * stride + m * N + n];
+        float* c = &C[m * ldc + n];
+        *c = accumulate ? *c + x : x;
+    }
 }
 
 // ---------------------------------------------------------------------------

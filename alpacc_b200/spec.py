@@ -207,15 +207,35 @@ def main(argv=None) -> None:
     predictions (random-init weights, json lexer) at evenly spaced positions
     of a synthetic 64 MiB json document, three calls, and the inference time
     of the last one (CUDA events).  Kernel 0 is the tcgen05 kernel, 1 the
-    mma.sync kernel; a small fixed workload for profiling either."""
+    mma.sync kernel; a small fixed workload for profiling either.
+    ``--train S``: S training steps of 4096 windows from a 4 MiB document
+    (labels from the exact lexer), and the time of the last one; a small
+    fixed workload for profiling the training kernels."""
     import argparse
     import torch
     from . import synth, tables
     ap = argparse.ArgumentParser(prog="python -m alpacc_b200.spec")
-    ap.add_argument("--predict", type=int, required=True)
+    ap.add_argument("--predict", type=int, default=0)
+    ap.add_argument("--train", type=int, default=0)
     ap.add_argument("--kernel", type=int, default=0, choices=[0, 1])
     args = ap.parse_args(argv)
     g = api.Grammar(tables.load("json", "lexer"))
+    if args.train:
+        m = BoundaryModel(g, seed=5)
+        win, lab = dataset(g, [synth.json_doc(4 << 20, 8, 3)], 4096 * args.train, 7)
+        b = 4096
+        for i in range(args.train - 1):
+            m.train_step(win[i * b:(i + 1) * b], lab[i * b:(i + 1) * b])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        loss, acc = m.train_step(win[-b:], lab[-b:])
+        e1.record()
+        torch.cuda.synchronize()
+        print("train steps %d  batch %d  last step %.4f ms  loss %.4f  acc %.4f" % (
+            args.train, b, e0.elapsed_time(e1), loss, acc))
+        return
+    if not args.predict:
+        ap.error("one of --predict or --train")
     g.set_tuning(g.get_tuning()[:3] + [args.kernel])
     m = BoundaryModel(g, seed=5)
     size = 64 << 20
