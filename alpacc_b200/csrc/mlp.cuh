@@ -67,7 +67,8 @@ __device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
 // memory accumulator and commits them to an mbarrier (waits bounded), which
 // hands the tiles back for the next step; the four warps then read their 32
 // accumulator rows with tcgen05.ld.  Training moves about 0.3 MFLOP per
-// window, so the kernel keeps one stage and no warp roles.
+// window, so the kernel keeps one shared-memory stage and no warp roles; the
+// next K step waits in registers (loads issued before the MMA wait).
 // ---------------------------------------------------------------------------
 struct GemmArgs {
     const __nv_bfloat16* A;
@@ -117,52 +118,76 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
     // 16-byte loads where an operand's K run is contiguous and aligned
     const bool a_vec = g.sa_k == 1 && (g.sa_m & 7) == 0 && (reinterpret_cast<uintptr_t>(g.A) & 15) == 0;
     const bool b_vec = g.sb_k == 1 && (g.sb_n & 7) == 0 && (reinterpret_cast<uintptr_t>(g.B) & 15) == 0;
-    for (int k0 = kb; k0 < ke; k0 += UG_BK) {
-        // stage A rows m0.. and B columns n0.. (as rows), K-major, 16-byte chunks; an
-        // operand whose rows are contiguous in memory (K strided: a transpose) is read with
-        // consecutive threads on consecutive rows, so that every load is coalesced
-        const bool a_rows = g.sa_m == 1 && g.sa_k != 1, b_rows = g.sb_n == 1 && g.sb_k != 1;
-        for (int e = tid; e < (UG_BM + bn) * 8; e += 128) {
-            const bool is_a = e < UG_BM * 8;
-            const int ee = is_a ? e : e - UG_BM * 8, rows = is_a ? UG_BM : bn;
-            const bool by_rows = is_a ? a_rows : b_rows;
-            const int row = by_rows ? ee % rows : ee >> 3;
-            const int c = by_rows ? ee / rows : ee & 7;
-            uint32_t w[4] = {0, 0, 0, 0};
+    // an operand whose rows are contiguous in memory (K strided: a transpose) is read with
+    // consecutive threads on consecutive rows, so that every load is coalesced
+    const bool a_rows = g.sa_m == 1 && g.sa_k != 1, b_rows = g.sb_n == 1 && g.sb_k != 1;
+    // Each thread stages UG_CHUNKS 16-byte chunks of a K step: chunks 0 .. UG_BM/16 - 1
+    // of A's rows m0.., the rest of B's columns n0.. (as rows), K-major.  All of a
+    // step's loads are issued into registers before any is stored, and the next step's
+    // loads are issued while the tensor cores work on this one, so a step costs about
+    // one memory latency instead of one per chunk.
+    constexpr int UG_CHUNKS = (UG_BM + UG_BN) * 8 / 128;
+    constexpr int UG_ACH = UG_BM * 8 / 128;
+    auto chunk_at = [&](int i, int& row, int& c) {
+        const bool is_a = i < UG_ACH;
+        const int ee = tid + (is_a ? i : i - UG_ACH) * 128, rows = is_a ? UG_BM : bn;
+        const bool by_rows = is_a ? a_rows : b_rows;
+        row = by_rows ? ee % rows : ee >> 3;
+        c = by_rows ? ee / rows : ee & 7;
+        return (is_a ? UG_BM : bn) * 8 > ee;  // B's chunks past bn columns stay unused
+    };
+    auto load_step = [&](int k0, uint4 (&r)[UG_CHUNKS]) {
+#pragma unroll
+        for (int i = 0; i < UG_CHUNKS; ++i) {
+            const bool is_a = i < UG_ACH;
+            int row, c;
+            r[i] = make_uint4(0, 0, 0, 0);
+            if (!chunk_at(i, row, c)) continue;
             const int kc = k0 + c * 8;
-            const bool vec = (is_a ? a_vec : b_vec) && kc + 8 <= ke;
-            if (vec) {
-                uint4 x = make_uint4(0, 0, 0, 0);
+            if ((is_a ? a_vec : b_vec) && kc + 8 <= ke) {
                 if (is_a) {
                     const int m = m0 + row;
-                    if (m < g.M) x = __ldg(reinterpret_cast<const uint4*>(g.A + (long long)m * g.sa_m + kc));
+                    if (m < g.M) r[i] = __ldg(reinterpret_cast<const uint4*>(g.A + (long long)m * g.sa_m + kc));
                 } else {
-                    x = __ldg(reinterpret_cast<const uint4*>(g.B + (long long)(n0 + row) * g.sb_n + kc));
+                    r[i] = __ldg(reinterpret_cast<const uint4*>(g.B + (long long)(n0 + row) * g.sb_n + kc));
                 }
-                w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
             } else {
+                uint32_t w[4];
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
                     uint32_t v = 0;
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
                         const int k = kc + 2 * h + q;
-                        __nv_bfloat16 x = __float2bfloat16(0.f);
+                        unsigned short x = 0;
                         if (k < ke) {
                             if (is_a) {
                                 const int m = m0 + row;
-                                if (m < g.M) x = g.A[(long long)m * g.sa_m + (long long)k * g.sa_k];
+                                if (m < g.M)
+                                    x = __ldg(reinterpret_cast<const unsigned short*>(g.A) + (long long)m * g.sa_m +
+                                              (long long)k * g.sa_k);
                             } else {
-                                x = g.B[(long long)k * g.sb_k + (long long)(n0 + row) * g.sb_n];
+                                x = __ldg(reinterpret_cast<const unsigned short*>(g.B) + (long long)k * g.sb_k +
+                                          (long long)(n0 + row) * g.sb_n);
                             }
                         }
-                        v |= (uint32_t)__bfloat16_as_ushort(x) << (16 * q);
+                        v |= (uint32_t)x << (16 * q);
                     }
                     w[h] = v;
                 }
+                r[i] = make_uint4(w[0], w[1], w[2], w[3]);
             }
-            *reinterpret_cast<uint4*>(sp + (is_a ? 0 : UG_BM * 128) + sw128_offset((uint32_t)row, (uint32_t)c)) =
-                make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    };
+    uint4 regs[UG_CHUNKS];
+    if (kb < ke) load_step(kb, regs);
+    for (int k0 = kb; k0 < ke; k0 += UG_BK) {
+#pragma unroll
+        for (int i = 0; i < UG_CHUNKS; ++i) {
+            int row, c;
+            if (chunk_at(i, row, c))
+                *reinterpret_cast<uint4*>(sp + (i < UG_ACH ? 0 : UG_BM * 128) + sw128_offset((uint32_t)row, (uint32_t)c)) =
+                    regs[i];
         }
         fence_async_smem();
         __syncthreads();
@@ -175,6 +200,7 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
                               (k0 > kb || kk > 0) ? 1u : 0u);
             umma_commit(&s_bar);
         }
+        if (k0 + UG_BK < ke) load_step(k0 + UG_BK, regs);  // in flight while the MMAs run
         // the tiles are free again once the MMAs that read them are done
         if (!mbar_wait(&s_bar, phase, g.err)) s_abort = 1;
         phase ^= 1u;
@@ -185,10 +211,18 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(GemmArgs g) {
     // epilogue: warp w holds accumulator rows 32w .. 32w + 31
     if (!s_abort) {
         const int m = m0 + warp * 32 + lane;
+        // 16-byte stores when the rows of C allow them (columns come in multiples of 16)
+        const bool c_vec = !(g.accumulate && !g.part_stride) && (g.ldc & 3) == 0 &&
+                           (reinterpret_cast<uintptr_t>(C) & 15) == 0 && (n0 & 3) == 0;
         for (int c0 = 0; c0 < bn; c0 += 32) {
             float v[32];
             tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (m < g.M) {
+            if (m < g.M && c_vec) {
+                float4* row = reinterpret_cast<float4*>(&C[(long long)m * g.ldc + n0 + c0]);
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (c0 + 4 * j < bn) row[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+            } else if (m < g.M) {
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int n = n0 + c0 + j;
