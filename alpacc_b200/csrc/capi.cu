@@ -831,6 +831,35 @@ inline const void* fused_expand_for(int q, int k) {
     return (const void*)parse_expand_kernel<0, 0, true>;
 }
 
+// Dynamic shared memory of an expand launch (*sm): its tables, position records and
+// node owners, and past them up to EX_SPAN_BYTES more for the tile's token spans, as
+// many as leave room for the CTAs per SM that run without them (or the tuned count).
+int expand_smem(alp_ctx* ctx, const void* fn, ParseArgs& a, size_t* sm) {
+    const size_t base = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
+    *sm = base;
+    a.span_cap = 0;
+    int fit = 0, per_sm = 0, reserved = 0, optin = 0;
+    cudaFuncAttributes fa;
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)base));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, fn, PP_THREADS, base));
+    CK(cudaFuncGetAttributes(&fa, fn));
+    CK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
+    CK(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, ctx->device));
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    const int ctas = persistent_ctas(fit, ctx->tune.expand_ctas);
+    long long room = (long long)per_sm / ctas - reserved - (long long)fa.sharedSizeBytes - (long long)base;
+    room = std::min(room, (long long)optin - (long long)fa.sharedSizeBytes - (long long)base);
+    room = std::min(room, (long long)EX_SPAN_BYTES) & ~31LL;
+    if (room < 1024) return ALP_OK;
+    int fit2 = 0;
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(base + room)));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit2, fn, PP_THREADS, base + room));
+    if (fit2 < ctas) return ALP_OK;  // token spans through L1, as without the stage
+    a.span_cap = (int)(room / 8);     // a multiple of 4
+    *sm = base + (size_t)room;
+    return ALP_OK;
+}
+
 int expand_grid(alp_ctx* ctx, const void* fn, size_t sm2, long long tiles, unsigned* g) {
     int sms = 0, per2 = 0;
     CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
@@ -877,8 +906,9 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     a.br_off = (long long*)ctx->tmp[T_BROFF].p;
     a.doc_valid = dvalid;
     a.subst_terminals = want_tree;
-    const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
-    if (sm2 > 220 * 1024) return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
+    if (expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack) > 220 * 1024)
+        return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
+    size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
     long long N = 0, B = 0, K = 0;
     const bool fits32 = (unsigned long long)L * (unsigned long long)(ctx->ph.max_prods + 1) < (1ull << 32) &&
                         (unsigned long long)L * (unsigned long long)(ctx->ph.max_brackets + 1) < (1ull << 32);
@@ -965,7 +995,9 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
             return fail(ctx, ALP_ERR_CAPACITY, "node buffer too small (%lld needed)", (long long)N);
         }
         if ((rc = parse_buffers(ctx, o, ctx_out, N, K, a))) return rc;
-        if ((rc = expand_grid(ctx, (const void*)parse_expand_kernel<0, 0, false>, sm2, tiles, &g_expand))) return rc;
+        if ((rc = expand_smem(ctx, (const void*)parse_expand_kernel<0, 0, false>, a, &sm2)) ||
+            (rc = expand_grid(ctx, (const void*)parse_expand_kernel<0, 0, false>, sm2, tiles, &g_expand)))
+            return rc;
         mark(ctx, "start");
         parse_expand_kernel<0, 0, false><<<g_expand, PP_THREADS, sm2, ctx->stream>>>(a);
         CK(cudaGetLastError());
@@ -3052,10 +3084,11 @@ int parse_positions_dev(alp_ctx* ctx, long long Lcap, const long long* dL, long 
     int sms = 0, per1 = 0, per2 = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
     const size_t sm1 = pairs_smem_bytes(ctx->pt.n_pairs, ctx->pt.q + ctx->pt.k);
-    const size_t sm2 = expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack);
-    if (sm2 > 220 * 1024) return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
+    if (expand_smem_bytes(ctx->pt.n_pairs, ctx->pt.n_pseq, ctx->pt.n_stack) > 220 * 1024)
+        return fail(ctx, ALP_ERR_TABLE, "parser tables too large for shared memory");
+    size_t sm2 = 0;
+    if ((rc = expand_smem(ctx, (const void*)parse_expand_kernel<0, 0, false>, a, &sm2))) return rc;
     CK(cudaFuncSetAttribute(pairs_kernel_for(ctx->pt.q, ctx->pt.k), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-    CK(cudaFuncSetAttribute(parse_expand_kernel<0, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per1, pairs_kernel_for(ctx->pt.q, ctx->pt.k), PP_THREADS, sm1));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, parse_expand_kernel<0, 0, false>, PP_THREADS, sm2));
     const long long x1 = (long long)persistent_ctas(per1, ctx->tune.pairs_ctas) * sms,

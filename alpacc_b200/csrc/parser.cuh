@@ -355,6 +355,9 @@ struct ParseArgs {
     long long node_base;        // global index of the shard's first node
     long long br_base;          // global index of its first kept bracket
     long long pos_base;         // global position of its position 0
+    // token spans the expand kernel's span stage holds per array (0: none): the shared
+    // memory past the node-owner array, 8 bytes per span
+    int span_cap;
 };
 
 __device__ __forceinline__ uint32_t pos_term(const ParseArgs& a, long long i) {
@@ -654,6 +657,7 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
 // search that follows.
 // ---------------------------------------------------------------------------
 constexpr int EX_WIN = 8192;                     // nodes per window
+constexpr int EX_SPAN_BYTES = 18432;             // shared bytes for the tile's token spans, where they fit
 constexpr int EX_U = 2;                          // nodes a thread emits at once (token span loads in flight)
 constexpr uint32_t EX_NO_TOKEN = 0xffffffffu;
 // per position: a node record, one unused slot after every thread's four
@@ -661,6 +665,15 @@ constexpr uint32_t EX_NO_TOKEN = 0xffffffffu;
 // (64 bytes apart without the pad) hit distinct banks
 constexpr size_t EX_POS_BYTES = (size_t)PP_TILE * 5 / 4 * 16;
 __device__ __forceinline__ int ex_slot(int pl) { return pl + (pl >> 2); }
+
+// 16 bytes from global to shared memory without registers (cp.async; `bytes` < 16
+// reads that many and zero-fills the rest)
+__device__ __forceinline__ void ex_cp16(void* dst, const void* src, uint32_t bytes) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void ex_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void ex_cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // pair infos (20 bytes each), then the 8-byte records from a 16-byte boundary
 __host__ __device__ inline size_t expand_rec_off(int n_pairs) {
@@ -799,7 +812,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     static_assert((PP_TILE + 17 + 1) * 4 <= 2 * EX_WIN, "the key window fits the owner array");
     __shared__ PosSums s_w[PP_THREADS / 32];
     __shared__ PosSums s_tp;
-    __shared__ uint32_t s_tn, s_tile;
+    __shared__ uint32_t s_tn, s_tile, s_slo, s_shi;
     __shared__ uint32_t s_pow[17];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int q = QT > 0 ? QT : a.t.q, k = KT > 0 ? KT : a.t.k, W = q + k;
@@ -952,7 +965,16 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             PosSums we = ps_shfl_up(wi, 1);
             if (lane == 0) possums_zero(we);
             if (lane < PP_THREADS / 32) s_w[lane] = we;
-            if (lane == PP_THREADS / 32 - 1) s_tn = wi.nodes;
+            if (lane == PP_THREADS / 32 - 1) {
+                s_tn = wi.nodes;
+                if (!FUSED) {
+                    // the tile's terminal nodes take the spans of positions [s_slo, s_shi): the
+                    // first terminal index after the last head before the tile, and after the tile
+                    const PosSums tot = ps_combine(tp, wi);
+                    s_slo = (uint32_t)tp.hpos + 1u + tp.terms;
+                    s_shi = (uint32_t)tot.hpos + 1u + tot.terms;
+                }
+            }
             if (FUSED) {
                 // the tile's own sums: the last warp's inclusive value
                 constexpr int LW = PP_THREADS / 32 - 1;
@@ -987,6 +1009,28 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
         }
         __syncthreads();
         if (FUSED) tp = s_tp;
+        // ---- the tile's token spans, copied into shared memory (past the node owners)
+        // while the positions and brackets are processed; the node windows read them there
+        uint32_t* s_span = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(s_own) + 2 * EX_WIN);
+        long long sp_lo = 0;
+        uint32_t sp_n = 0;
+        if (!FUSED && a.span_cap > 0 && !a.shard &&
+            ((reinterpret_cast<uintptr_t>(a.pstart) | reinterpret_cast<uintptr_t>(a.pend)) & 15) == 0) {
+            const long long lo = (long long)(s_slo & ~3u), hi = min((long long)s_shi, a.L);
+            if (hi > lo && ((hi - lo + 3) & ~3ll) <= (long long)a.span_cap) {  // the same in every thread
+                sp_lo = lo;
+                sp_n = (uint32_t)(hi - lo);
+                const uint32_t chunks = (sp_n + 3) / 4;
+                for (uint32_t c = tid; c < 2 * chunks; c += PP_THREADS) {
+                    const bool e = c >= chunks;
+                    const uint32_t cc = e ? c - chunks : c;
+                    const long long idx = lo + 4 * (long long)cc;
+                    ex_cp16(s_span + (e ? a.span_cap : 0) + 4 * cc, (e ? a.pend : a.pstart) + idx,
+                            (uint32_t)min(16ll, 4 * (a.L - idx)));
+                }
+                ex_cp_commit();
+            }
+        }
         // ---- per position: records and the one-position document rules --------
         uint32_t nof[PP_ITEMS], cnt[PP_ITEMS];  // first node (tile-local), n_prod
         // brackets: the depth before each position and where its kept brackets go
@@ -1065,6 +1109,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             }
         }
         const uint32_t tn = s_tn;
+        if (sp_n) ex_cp_wait_all();  // this thread's span copies; the window barrier publishes them
         // ---- nodes, one window at a time ---------------------------------------------
         for (uint32_t w0 = 0; w0 < tn; w0 += EX_WIN) {
             const uint32_t wn = min(tn - w0, (uint32_t)EX_WIN);
@@ -1097,7 +1142,14 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                             tg[u] = tm1 - 1;
                             kd[u] = 1;
                             const long long ti = (long long)((uint32_t)ps.z + (rec.y >> 16)) - (a.shard ? a.pos_base : 0);
-                            if (ti >= 0 && ti < a.L) { st[u] = __ldg(&a.pstart[ti]); en[u] = __ldg(&a.pend[ti]); }
+                            const long long d = ti - sp_lo;
+                            if (d >= 0 && d < (long long)sp_n) {
+                                st[u] = s_span[d];
+                                en[u] = s_span[a.span_cap + d];
+                            } else if (ti >= 0 && ti < a.L) {
+                                st[u] = __ldg(&a.pstart[ti]);
+                                en[u] = __ldg(&a.pend[ti]);
+                            }
                         }
                     }
                 }
