@@ -1506,6 +1506,62 @@ int alp_tune_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int reps, char*
     return done(ALP_OK);
 }
 
+int alp_write_reference_format(int mode, int64_t n_docs, const uint8_t* valid, const int64_t* off,
+                               const uint32_t* id, const int64_t* parent, const uint8_t* kind,
+                               const int64_t* start, const int64_t* end, uint8_t* out, size_t cap,
+                               size_t* len) {
+    if (!len || n_docs < 0 || (n_docs > 0 && (!valid || !off))) return ALP_ERR_ARG;
+    *len = 0;
+    size_t rec;
+    switch (mode) {
+        case ALP_WIRE_LEXER: rec = 24; if (!id || !start || !end) return ALP_ERR_ARG; break;
+        case ALP_WIRE_LEXPARSE: rec = 33; if (!id || !parent || !kind || !start || !end) return ALP_ERR_ARG; break;
+        case ALP_WIRE_PARSER: rec = 8; if (!id) return ALP_ERR_ARG; break;
+        default: return ALP_ERR_ARG;
+    }
+    // the size first: a boolean per input, a count and the records per accepted one
+    size_t total = 8;
+    for (int64_t d = 0; d < n_docs; ++d) {
+        if (off[d] < 0 || off[d + 1] < off[d]) return ALP_ERR_ARG;
+        total += 1;
+        if (valid[d]) total += 8 + rec * (size_t)(off[d + 1] - off[d]);
+    }
+    *len = total;
+    if (!out) return ALP_OK;
+    if (cap < total) return ALP_ERR_CAPACITY;
+    if (mode == ALP_WIRE_LEXPARSE)
+        for (int64_t d = 0; d < n_docs; ++d)
+            if (valid[d])
+                for (int64_t e = off[d]; e < off[d + 1]; ++e)
+                    if (kind[e] > 1) return ALP_ERR_ARG;
+    uint8_t* p = out;
+    auto u64 = [&p](uint64_t v) {
+        for (int b = 7; b >= 0; --b) *p++ = (uint8_t)(v >> (8 * b));
+    };
+    u64((uint64_t)n_docs);
+    for (int64_t d = 0; d < n_docs; ++d) {
+        *p++ = valid[d] ? 1 : 0;
+        if (!valid[d]) continue;
+        u64((uint64_t)(off[d + 1] - off[d]));
+        for (int64_t e = off[d]; e < off[d + 1]; ++e) {
+            if (mode == ALP_WIRE_LEXER) {
+                u64(id[e]);
+                u64((uint64_t)start[e]);
+                u64((uint64_t)end[e]);
+            } else if (mode == ALP_WIRE_LEXPARSE) {
+                *p++ = kind[e];
+                u64((uint64_t)parent[e]);
+                u64(id[e]);
+                u64(kind[e] ? (uint64_t)start[e] : 0);
+                u64(kind[e] ? (uint64_t)end[e] : 0);
+            } else {
+                u64(id[e]);
+            }
+        }
+    }
+    return ALP_OK;
+}
+
 int alp_memcpy(alp_ctx* ctx, void* dst, const void* src, size_t bytes) {
     if (!ctx || (bytes && (!dst || !src))) return ALP_ERR_ARG;
     CK(cudaSetDevice(ctx->device));

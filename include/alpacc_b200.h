@@ -316,6 +316,32 @@ int alp_parse_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int
                     int64_t** d_parent, uint32_t** d_tag, uint8_t** d_kind, int64_t** d_start,
                     int64_t** d_end, int64_t** d_node_off, uint8_t** d_valid, int64_t* n_node_total);
 
+/* The reference's test wire format, written from batch results in host memory
+ * (host code only, no GPU work): the `.outputs` files that `alpacc test`
+ * generates and compares, big-endian u64 counts and fields, one boolean byte
+ * per input (src/Alpacc/Test/Lexer.hs:59-85, src/Alpacc/Test/LexerParser.hs:54-99,
+ * src/Alpacc/Test/Parser.hs:41-56).  A C, cgo or JNI caller that holds
+ * alp_lex_batch / alp_parse_batch / alp_pre_productions results can write the
+ * file these tools diff without a second serialiser.
+ *   ALP_WIRE_LEXER     per accepted input: u64 n, then n x (u64 term, u64 start,
+ *                      u64 end) from id / start / end;
+ *   ALP_WIRE_LEXPARSE  n x (u8 kind, u64 parent, u64 id, u64 start, u64 end) from
+ *                      kind / parent / id / start / end (spans written as 0 for
+ *                      production nodes, kind 0);
+ *   ALP_WIRE_PARSER    n x u64 production from id.
+ * Input i's elements are [off[i], off[i+1]); valid[i] = 0 writes only its
+ * boolean.  Arrays a mode does not read may be NULL.  *len receives the size of
+ * the file; with out == NULL that is all (a size query, ALP_OK), with cap < *len
+ * nothing is written and ALP_ERR_CAPACITY is returned.  ALP_ERR_ARG for an unknown
+ * mode, a missing array, offsets that decrease, or a kind other than 0 or 1. */
+#define ALP_WIRE_LEXER 0
+#define ALP_WIRE_LEXPARSE 1
+#define ALP_WIRE_PARSER 2
+int alp_write_reference_format(int mode, int64_t n_docs, const uint8_t* valid, const int64_t* off,
+                               const uint32_t* id, const int64_t* parent, const uint8_t* kind,
+                               const int64_t* start, const int64_t* end, uint8_t* out, size_t cap,
+                               size_t* len);
+
 /* The batched parse as a CUDA graph (no reference counterpart).  alp_parse_batch
  * waits on the host three times (input size, token total, node and bracket
  * totals) to size its outputs; for a fixed batch shape this set-up captures the

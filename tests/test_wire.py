@@ -94,3 +94,86 @@ def test_malformed_files_are_rejected():
         wire.read_lexparse_outputs(u64(1) + b"\x01" + u64(1) + b"\x05" + u64(0) * 4)
     with pytest.raises(ValueError):
         wire.read_inputs(wire.write_inputs([b"x"]) + b"\x00")
+
+
+def _c_writer():
+    import ctypes
+    from alpacc_b200 import build
+    lib = ctypes.CDLL(build.build_cuda())
+    f = lib.alp_write_reference_format
+    vp = ctypes.c_void_p
+    f.argtypes = [ctypes.c_int, ctypes.c_int64, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_size_t,
+                  ctypes.POINTER(ctypes.c_size_t)]
+    return f
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def _c_write(f, mode, valid, off, id_=None, parent=None, kind=None, start=None, end=None, cap=None):
+    import ctypes
+    n = ctypes.c_size_t(0)
+    rc = f(mode, len(valid), _ptr(valid), _ptr(off), _ptr(id_), _ptr(parent), _ptr(kind), _ptr(start), _ptr(end),
+           None, 0, ctypes.byref(n))
+    assert rc == 0
+    buf = np.zeros(max(n.value if cap is None else cap, 1), np.uint8)
+    rc = f(mode, len(valid), _ptr(valid), _ptr(off), _ptr(id_), _ptr(parent), _ptr(kind), _ptr(start), _ptr(end),
+           _ptr(buf), len(buf) if cap is None else cap, ctypes.byref(n))
+    return rc, bytes(buf[:n.value]), n.value
+
+
+def test_c_abi_writer_matches_wire_module():
+    """alp_write_reference_format (host code in the C library, no GPU) writes the
+    same bytes as this module for every output kind, rejected inputs and empty
+    ones included."""
+    f = _c_writer()
+    rng = np.random.default_rng(3)
+    counts = [0, 5, 1, 0, 17, 3]
+    valid = np.array([1, 1, 0, 1, 1, 0], np.uint8)
+    off = np.zeros(len(counts) + 1, np.int64)
+    off[1:] = np.cumsum(counts)
+    m = int(off[-1])
+    term = rng.integers(0, 40, m).astype(np.uint32)
+    start = rng.integers(0, 1 << 40, m).astype(np.int64)
+    end = start + rng.integers(1, 9, m)
+    parent = rng.integers(0, 1 << 33, m).astype(np.int64)
+    kind = rng.integers(0, 2, m).astype(np.uint8)
+    sl = [slice(off[i], off[i + 1]) for i in range(len(counts))]
+
+    rc, got, _ = _c_write(f, 0, valid, off, id_=term, start=start, end=end)
+    assert rc == 0
+    assert got == wire.write_lexer_outputs([(term[s], start[s], end[s]) if v else None for s, v in zip(sl, valid)])
+
+    rc, got, _ = _c_write(f, 1, valid, off, id_=term, parent=parent, kind=kind, start=start, end=end)
+    assert rc == 0
+    want = wire.write_lexparse_outputs([(parent[s], term[s], kind[s], start[s], end[s]) if v else None
+                                        for s, v in zip(sl, valid)])
+    assert got == want
+
+    rc, got, _ = _c_write(f, 2, valid, off, id_=term)
+    assert rc == 0
+    assert got == wire.write_parser_outputs([term[s] if v else None for s, v in zip(sl, valid)])
+
+    empty = np.zeros(0, np.uint8)
+    rc, got, _ = _c_write(f, 2, empty, np.zeros(1, np.int64), id_=term)
+    assert rc == 0 and got == u64(0)
+
+
+def test_c_abi_writer_errors():
+    import ctypes
+    f = _c_writer()
+    valid = np.array([1], np.uint8)
+    off = np.array([0, 2], np.int64)
+    ids = np.array([3, 4], np.uint32)
+    kind = np.array([1, 2], np.uint8)
+    z = np.zeros(2, np.int64)
+    rc, _, need = _c_write(f, 2, valid, off, id_=ids, cap=4)
+    assert rc == 5 and need == 8 + 1 + 8 + 16  # ALP_ERR_CAPACITY, with the size needed
+    rc, _, _ = _c_write(f, 1, valid, off, id_=ids, parent=z, kind=kind, start=z, end=z)
+    assert rc == 1  # kind 2
+    n = ctypes.c_size_t(0)
+    assert f(7, 1, _ptr(valid), _ptr(off), _ptr(ids), None, None, None, None, None, 0, ctypes.byref(n)) == 1
+    assert f(0, 1, _ptr(valid), _ptr(off), _ptr(ids), None, None, None, None, None, 0, ctypes.byref(n)) == 1
+    bad = np.array([2, 1], np.int64)
+    assert f(2, 1, _ptr(valid), _ptr(bad), _ptr(ids), None, None, None, None, None, 0, ctypes.byref(n)) == 1
