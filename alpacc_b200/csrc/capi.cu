@@ -1019,12 +1019,14 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
         }
         CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
         CK(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
-        if ((rc = run_ple(ctx, a.dsbuf, K, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res, nullptr, 0,
-                          nullptr, nullptr, 0, ctx->aux)))
-            return rc;
-        if ((rc = run_ple(ctx, a.vbuf, N, nullptr, o->parent, T_N_TMIN, a.node_off, nd, dvalid, d_res))) return rc;
+        rc = run_ple(ctx, a.dsbuf, K, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res, nullptr, 0, nullptr,
+                     nullptr, 0, ctx->aux);
+        if (!rc) rc = run_ple(ctx, a.vbuf, N, nullptr, o->parent, T_N_TMIN, a.node_off, nd, dvalid, d_res);
+        // joined on an error too: no later call on this context may reuse buffers that
+        // the bracket search could still be reading
         CK(cudaEventRecord(ctx->ev_join, ctx->aux));
         CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+        if (rc) return rc;
     } else {
         // profiled calls keep one stream, so that every kernel's time is its own
         if (want_tree) {

@@ -393,11 +393,35 @@ __global__ void __launch_bounds__(PP_THREADS, 3) parse_pairs_kernel(ParseArgs a)
         for (int j = 0; j < W; ++j) { s_pow[W - 1 - j] = pw; pw *= (uint32_t)a.t.T; }
     }
     const long long n_tiles = (a.L + PP_TILE - 1) / PP_TILE;
+    // The window of a tile, one tile ahead in registers (its loads in flight while the
+    // block works on the tile before): this thread's four terminals, and for the first
+    // W + 1 threads one of the window's edge terminals (q + 1 before the tile, k after).
+    // Terminal ids fit 16 bits: the four are kept as two words.
+    auto window_loads = [&](long long b, uint2& t4, uint32_t& te) {
+        const long long i0 = b + (long long)tid * PP_ITEMS;
+        if (i0 >= 0 && i0 + PP_ITEMS <= a.L && (reinterpret_cast<uintptr_t>(a.P) & 7) == 0) {
+            t4 = __ldg(reinterpret_cast<const uint2*>(a.P + i0));
+        } else {
+            t4 = make_uint2(pos_term(a, i0) | (pos_term(a, i0 + 1) << 16), pos_term(a, i0 + 2) | (pos_term(a, i0 + 3) << 16));
+        }
+        te = 0;
+        if (tid <= q) te = pos_term(a, b - q - 1 + tid);
+        else if (tid <= W) te = pos_term(a, b + PP_TILE + (tid - q - 1));
+    };
+    uint2 nt4 = make_uint2(0, 0);
+    uint32_t nte = 0;
+    if ((long long)blockIdx.x < n_tiles) window_loads((long long)blockIdx.x * PP_TILE, nt4, nte);
     for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const long long base = tile * PP_TILE;
-    const int span = PP_TILE + W + 1;  // window [base - q - 1, base + PP_TILE + k)
     __syncthreads();  // the previous tile is done with s_term and s_w
-    for (int i = tid; i < span; i += PP_THREADS) s_term[i] = pos_term(a, base - q - 1 + i);
+    // window [base - q - 1, base + PP_TILE + k): s_term[q + 1 + pl] is position base + pl
+    {
+        uint32_t* d = s_term + q + 1 + tid * PP_ITEMS;
+        d[0] = nt4.x & 0xffffu; d[1] = nt4.x >> 16; d[2] = nt4.y & 0xffffu; d[3] = nt4.y >> 16;
+        if (tid <= q) s_term[tid] = nte;
+        else if (tid <= W) s_term[PP_TILE + tid] = nte;
+    }
+    if (tile + gridDim.x < n_tiles) window_loads(base + (long long)gridDim.x * PP_TILE, nt4, nte);
     __syncthreads();
     const uint32_t SL = a.t.start, SR = a.t.end, EMPTY = a.t.empty;
     // the pair id at tile-local position pl (-1: the position before the tile);
