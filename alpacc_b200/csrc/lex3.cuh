@@ -214,9 +214,20 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_fold_kernel(Lex3Args a, Le
     for (int i = tid; i < S * C1; i += LX_THREADS) s_cd[i] = a.t.cdelta[i];
     for (int i = tid; i < (int)E * C1; i += LX_THREADS) s_step[i] = a.t.step[i];
     const long long n = a.n;
+    // this thread's 64 bytes of a tile, one tile ahead (in flight while the block folds
+    // the tile before)
+    uint4 nw[4];
+    auto tile_bytes = [&](unsigned ft, uint4 (&w)[4]) {
+        const long long my = (long long)ft * LX_WIDE + (long long)tid * (2 * LX_CHUNK);
+        const int lim = (int)max(0ll, min((long long)(2 * LX_CHUNK), n - my));
+        if (lim > 0) lx_load<4>(a, my, lim, w);
+    };
+    if (blockIdx.x < a.num_wide) tile_bytes(blockIdx.x, nw);
     for (unsigned ft = blockIdx.x; ft < a.num_wide; ft += gridDim.x) {
         const long long t0 = (long long)ft * LX_WIDE;
         const long long t1 = min(t0 + LX_WIDE, n) - 1;
+        uint4 w[4] = {nw[0], nw[1], nw[2], nw[3]};
+        if (ft + gridDim.x < a.num_wide) tile_bytes(ft + gridDim.x, nw);
         s_head[tid] = 0;
         s_head[tid + LX_THREADS] = 0;
         __syncthreads();
@@ -225,8 +236,6 @@ __global__ void __launch_bounds__(LX_THREADS, 4) lex3_fold_kernel(Lex3Args a, Le
         const long long my = t0 + (long long)tid * (2 * LX_CHUNK);
         const int lim = (int)max(0ll, min((long long)(2 * LX_CHUNK), n - my));
         if (lim > 0) {
-            uint4 w[4];
-            lx_load<4>(a, my, lim, w);
             const uint32_t ha = s_head[2 * tid], hb = s_head[2 * tid + 1];
             const long long c = my / LX_CHUNK;
             if (lim == 2 * LX_CHUNK && (ha | hb) == 0) {
