@@ -995,12 +995,15 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
             return fail(ctx, ALP_ERR_CAPACITY, "node buffer too small (%lld needed)", (long long)N);
         }
         if ((rc = parse_buffers(ctx, o, ctx_out, N, K, a))) return rc;
-        if ((rc = expand_smem(ctx, (const void*)parse_expand_kernel<0, 0, false>, a, &sm2)) ||
-            (rc = expand_grid(ctx, (const void*)parse_expand_kernel<0, 0, false>, sm2, tiles, &g_expand)))
-            return rc;
+        // one document: the expansion's thread-level sums need no restarts
+        const void* ex = nd == 1 ? (const void*)parse_expand_kernel<0, 0, false, true>
+                                 : (const void*)parse_expand_kernel<0, 0, false, false>;
+        if ((rc = expand_smem(ctx, ex, a, &sm2)) || (rc = expand_grid(ctx, ex, sm2, tiles, &g_expand))) return rc;
         mark(ctx, "start");
-        parse_expand_kernel<0, 0, false><<<g_expand, PP_THREADS, sm2, ctx->stream>>>(a);
-        CK(cudaGetLastError());
+        {
+            void* args[] = {&a};
+            CK(cudaLaunchKernel(ex, dim3(g_expand), dim3(PP_THREADS), args, sm2, ctx->stream));
+        }
         mark(ctx, "parse_expand_kernel");
     }
     ctx->last_positions = L;

@@ -254,6 +254,23 @@ __device__ __forceinline__ PosSums ps_combine(const PosSums& a, const PosSums& b
     r.cls = a.cls + b.cls;
     return r;
 }
+// ps_combine where all positions belong to one document: its only ⊢ is position 0,
+// before which every sum is zero, so that restarting there is the same as adding; the
+// position of the last ⊢ is kept as before.
+template <bool ONE>
+__device__ __forceinline__ PosSums ps_join(const PosSums& a, const PosSums& b) {
+    if (!ONE) return ps_combine(a, b);
+    PosSums r;
+    r.nodes = a.nodes + b.nodes;
+    r.brs = a.brs + b.brs;
+    r.heads = a.heads + b.heads;
+    r.depth = a.depth + b.depth;
+    r.v = a.v + b.v;
+    r.terms = a.terms + b.terms;
+    r.hpos = b.heads ? b.hpos : a.hpos;
+    r.cls = a.cls + b.cls;
+    return r;
+}
 __device__ __forceinline__ PosSums ps_shfl_up(const PosSums& x, int d) {
     PosSums r;
     r.nodes = __shfl_up_sync(ALP_FULL_MASK, x.nodes, d);
@@ -819,7 +836,9 @@ __device__ __forceinline__ PosSums ps_lookback(const ParseArgs& a, long long til
 // exclusive position sums from a look-back over earlier tiles (tiles taken in
 // ticket order, so every tile a look-back waits for is running or done).  The
 // pair kernel, the tile-sum scans and the pair-id array are then not needed.
-template <int QT, int KT, bool FUSED>
+// ONE: the positions are one document (not a shard of one): the thread-level
+// sums are plain sums and every position's document is document 0.
+template <int QT, int KT, bool FUSED, bool ONE = false>
 __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     PairInfo* s_pi = reinterpret_cast<PairInfo*>(smem);
@@ -961,7 +980,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                     }
                     if (head) { e.heads = 1; e.hpos = (int32_t)(i0 + j); }
                     cl[j] = e.cls;
-                    mine = ps_combine(mine, e);
+                    mine = ps_join<ONE>(mine, e);
                     lprev = nl;
                     pv = ids[j] != NO_PAIR;
                 } else if (a.shard && i0 + j == a.L && pv && a.next_pair != NO_PAIR) {
@@ -994,7 +1013,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                 if (!FUSED) {
                     // the tile's terminal nodes take the spans of positions [s_slo, s_shi): the
                     // first terminal index after the last head before the tile, and after the tile
-                    const PosSums tot = ps_combine(tp, wi);
+                    const PosSums tot = ps_join<ONE>(tp, wi);
                     s_slo = (uint32_t)tp.hpos + 1u + tp.terms;
                     s_shi = (uint32_t)tot.hpos + 1u + tot.terms;
                 }
@@ -1061,7 +1080,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
         uint32_t kof[PP_ITEMS];
         int32_t depj[PP_ITEMS];
         {
-            PosSums run = ps_combine(ps_combine(tp, s_w[warp]), ex);  // before this thread's first position
+            PosSums run = ps_join<ONE>(ps_join<ONE>(tp, s_w[warp]), ex);  // before this thread's first position
 #pragma unroll
             for (int j = 0; j < PP_ITEMS; ++j) {
                 const long long i = i0 + j;
@@ -1073,8 +1092,8 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                 if (i < a.L) {
                     const bool head = (hm >> j) & 1u;
                     const int32_t dep = head ? 0 : run.depth;
-                    const long long doc = (long long)run.heads + (head ? 1 : 0) - 1;
-                    const bool dok = doc >= 0 && doc < a.n_docs;
+                    const long long doc = ONE ? 0 : (long long)run.heads + (head ? 1 : 0) - 1;
+                    const bool dok = ONE || (doc >= 0 && doc < a.n_docs);
                     depj[j] = dep;
                     // the previous position's top lefts against this position's first rights
                     const uint32_t pid_prev = j == 0 ? prev_id : (uint32_t)ids[j - 1];
@@ -1110,7 +1129,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                     if (((em >> j) & 1u) && (dep + e.depth != 0) && dok) a.doc_valid[doc] = 0;  // unbalanced at the end
                     if (head) { e.heads = 1; e.hpos = (int32_t)i; }
                     e.cls = m;
-                    run = ps_combine(run, e);
+                    run = ps_join<ONE>(run, e);
                 }
             }
         }
