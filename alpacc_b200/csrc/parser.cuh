@@ -699,7 +699,8 @@ __global__ void __launch_bounds__(ST_CHUNK) scan_tiles_kernel(PosSums* s, long l
 // ---------------------------------------------------------------------------
 constexpr int EX_WIN = 8192;                     // nodes per window
 constexpr int EX_SPAN_BYTES = 18432;             // shared bytes for the tile's token spans, where they fit
-constexpr int EX_U = 2;                          // nodes a thread emits at once (token span loads in flight)
+constexpr int EX_U = 1;                          // nodes a thread emits at once (2 and 4 measured slower
+                                                 // once the token spans come from shared memory)
 constexpr uint32_t EX_NO_TOKEN = 0xffffffffu;
 // per position: a node record, one unused slot after every thread's four
 // positions, so that the 32 lanes of a warp writing their first position
