@@ -728,20 +728,21 @@ __host__ __device__ inline size_t expand_smem_bytes(int n_pairs, int n_pseq, int
     return expand_tables_bytes(n_pairs, n_pseq, n_stack) + EX_POS_BYTES + 2 * (size_t)EX_WIN;
 }
 
-// Pair ids and terminals of the PP_ITEMS positions from i0 as two 8-byte
-// words (one vector load each when all are in range; ids past the end read
-// as no pair).
+// Pair ids and (TERMS) terminals of the PP_ITEMS positions from i0 as two
+// 8-byte words (one vector load each when all are in range; ids past the end
+// read as no pair).
+template <bool TERMS>
 __device__ __forceinline__ void ex_words(const ParseArgs& a, long long i0, uint2& w, uint2& t) {
     static_assert(PP_ITEMS == 4, "a thread's positions are one 8-byte word");
     if (i0 + PP_ITEMS <= a.L) {
         w = __ldg(reinterpret_cast<const uint2*>(a.pid + i0));
-        t = __ldg(reinterpret_cast<const uint2*>(a.P + i0));
+        if (TERMS) t = __ldg(reinterpret_cast<const uint2*>(a.P + i0));
     } else {
         uint32_t x[PP_ITEMS], y[PP_ITEMS];
 #pragma unroll
         for (int j = 0; j < PP_ITEMS; ++j) {
             x[j] = i0 + j < a.L ? a.pid[i0 + j] : NO_PAIR;
-            y[j] = i0 + j < a.L ? a.P[i0 + j] : 0xffffu;
+            y[j] = (TERMS && i0 + j < a.L) ? a.P[i0 + j] : 0xffffu;
         }
         w = make_uint2(x[0] | (x[1] << 16), x[2] | (x[3] << 16));
         t = make_uint2(y[0] | (y[1] << 16), y[2] | (y[3] << 16));
@@ -874,7 +875,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
     // (not fused) this thread's pair ids and terminals, one tile ahead (loads in
     // flight while the block works on the current tile)
     uint2 nw = make_uint2(0, 0), nt = make_uint2(0, 0);
-    if (!FUSED) ex_words(a, (long long)blockIdx.x * PP_TILE + tid * PP_ITEMS, nw, nt);
+    if (!FUSED) ex_words<!ONE>(a, (long long)blockIdx.x * PP_TILE + tid * PP_ITEMS, nw, nt);
     for (long long it = blockIdx.x;; it += gridDim.x) {
         __syncthreads();  // the previous tile is done with the shared arrays
         long long tile = it;
@@ -934,21 +935,27 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
             possums_zero(tp);
         } else {
             tp = a.shard ? ps_combine(a.pre, a.tile_sums[tile]) : a.tile_sums[tile];
-            const uint32_t c[PP_ITEMS] = {nt.x & 0xffffu, nt.x >> 16, nt.y & 0xffffu, nt.y >> 16};
             ids[0] = (uint16_t)nw.x; ids[1] = (uint16_t)(nw.x >> 16); ids[2] = (uint16_t)nw.y; ids[3] = (uint16_t)(nw.y >> 16);
+            if (ONE) {
+                // one document: its ⊢ is position 0 and its ⊣ position L - 1
+                if (i0 == 0) hm = 1u;
+                if (a.L - 1 >= i0 && a.L - 1 < i0 + PP_ITEMS) em = 1u << (uint32_t)(a.L - 1 - i0);
+            } else {
+                const uint32_t c[PP_ITEMS] = {nt.x & 0xffffu, nt.x >> 16, nt.y & 0xffffu, nt.y >> 16};
 #pragma unroll
-            for (int j = 0; j < PP_ITEMS; ++j) {
-                if (i0 + j < a.L) {
-                    if (c[j] == SL) hm |= 1u << j;
-                    if (c[j] == SR) em |= 1u << j;
+                for (int j = 0; j < PP_ITEMS; ++j) {
+                    if (i0 + j < a.L) {
+                        if (c[j] == SL) hm |= 1u << j;
+                        if (c[j] == SR) em |= 1u << j;
+                    }
                 }
             }
-            if (tile + gridDim.x < n_tiles) ex_words(a, i0 + (long long)gridDim.x * PP_TILE, nw, nt);
+            if (tile + gridDim.x < n_tiles) ex_words<!ONE>(a, i0 + (long long)gridDim.x * PP_TILE, nw, nt);
             if (lane == 0 && i0 > 0 && i0 - 1 < a.L) prev_id = a.pid[i0 - 1];
             else if (lane == 0 && i0 == 0 && a.shard) prev_id = a.prev_pair;
             if (lane == 31 && i0 + PP_ITEMS < a.L) {
                 next_id = a.pid[i0 + PP_ITEMS];
-                next_head = (uint32_t)a.P[i0 + PP_ITEMS] == SL;
+                next_head = !ONE && (uint32_t)a.P[i0 + PP_ITEMS] == SL;  // one document: no ⊢ after position 0
             } else if (lane == 31 && i0 + PP_ITEMS == a.L && a.shard) {
                 next_id = a.next_pair;  // the next shard's first position (never a document head)
             }
