@@ -255,19 +255,19 @@ __device__ __forceinline__ PosSums ps_combine(const PosSums& a, const PosSums& b
     return r;
 }
 // ps_combine where all positions belong to one document: its only ⊢ is position 0,
-// before which every sum is zero, so that restarting there is the same as adding; the
-// position of the last ⊢ is kept as before.
+// before which every sum is zero, so that restarting there is the same as adding.
+// The ⊢ count and position are then not needed (left 0).
 template <bool ONE>
 __device__ __forceinline__ PosSums ps_join(const PosSums& a, const PosSums& b) {
     if (!ONE) return ps_combine(a, b);
     PosSums r;
     r.nodes = a.nodes + b.nodes;
     r.brs = a.brs + b.brs;
-    r.heads = a.heads + b.heads;
+    r.heads = 0;
     r.depth = a.depth + b.depth;
     r.v = a.v + b.v;
     r.terms = a.terms + b.terms;
-    r.hpos = b.heads ? b.hpos : a.hpos;
+    r.hpos = 0;
     r.cls = a.cls + b.cls;
     return r;
 }
@@ -986,7 +986,7 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                         nl = pair_lefts(pi);
                         if (!head && pv) e.cls = min(lprev, (uint32_t)pi.n_br - nl);
                     }
-                    if (head) { e.heads = 1; e.hpos = (int32_t)(i0 + j); }
+                    if (head && !ONE) { e.heads = 1; e.hpos = (int32_t)(i0 + j); }
                     cl[j] = e.cls;
                     mine = ps_join<ONE>(mine, e);
                     lprev = nl;
@@ -1022,8 +1022,9 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                     // the tile's terminal nodes take the spans of positions [s_slo, s_shi): the
                     // first terminal index after the last head before the tile, and after the tile
                     const PosSums tot = ps_join<ONE>(tp, wi);
-                    s_slo = (uint32_t)tp.hpos + 1u + tp.terms;
-                    s_shi = (uint32_t)tot.hpos + 1u + tot.terms;
+                    // (one document: the last ⊢ is position 0)
+                    s_slo = (ONE ? 0u : (uint32_t)tp.hpos) + 1u + tp.terms;
+                    s_shi = (ONE ? 0u : (uint32_t)tot.hpos) + 1u + tot.terms;
                 }
             }
             if (FUSED) {
@@ -1099,7 +1100,8 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                 depj[j] = 0;
                 if (i < a.L) {
                     const bool head = (hm >> j) & 1u;
-                    const int32_t dep = head ? 0 : run.depth;
+                    // (one document: every sum before position 0 is zero, the last ⊢ is position 0)
+                    const int32_t dep = (head && !ONE) ? 0 : run.depth;
                     const long long doc = ONE ? 0 : (long long)run.heads + (head ? 1 : 0) - 1;
                     const bool dok = ONE || (doc >= 0 && doc < a.n_docs);
                     depj[j] = dep;
@@ -1127,15 +1129,17 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                         if (dok) a.doc_valid[doc] = 0;  // no admissible pair
                     } else {
                         const PairInfo pi = s_pi[ids[j]];
-                        s_pos[ex_slot(pl)] = make_int4((int32_t)pi.prod_begin - (int32_t)nof[j], head ? 0 : run.v,
-                                              (int32_t)((uint32_t)(head ? i : run.hpos) + 1u + (head ? 0u : run.terms)),
-                                              dep);
+                        s_pos[ex_slot(pl)] =
+                            ONE ? make_int4((int32_t)pi.prod_begin - (int32_t)nof[j], run.v, (int32_t)(1u + run.terms), dep)
+                                : make_int4((int32_t)pi.prod_begin - (int32_t)nof[j], head ? 0 : run.v,
+                                            (int32_t)((uint32_t)(head ? i : run.hpos) + 1u + (head ? 0u : run.terms)),
+                                            dep);
                         if (dep + (int32_t)pi.min_ds < 0 && dok) a.doc_valid[doc] = 0;  // depth below zero
                         e.nodes = pi.n_prod; e.brs = pi.n_br; e.depth = pi.d_depth; e.v = pi.d_v; e.terms = pi.n_term;
                         cnt[j] = (uint32_t)pi.n_prod | ((uint32_t)pi.n_br << 16);
                     }
                     if (((em >> j) & 1u) && (dep + e.depth != 0) && dok) a.doc_valid[doc] = 0;  // unbalanced at the end
-                    if (head) { e.heads = 1; e.hpos = (int32_t)i; }
+                    if (head && !ONE) { e.heads = 1; e.hpos = (int32_t)i; }
                     e.cls = m;
                     run = ps_join<ONE>(run, e);
                 }
