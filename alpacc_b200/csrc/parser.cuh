@@ -271,6 +271,36 @@ __device__ __forceinline__ PosSums ps_join(const PosSums& a, const PosSums& b) {
     r.cls = a.cls + b.cls;
     return r;
 }
+// The one-document forms of the warp scan and shift: no ⊢ anywhere but position 0
+// (whose sums before it are zero), so the six counted fields are plain prefix sums
+// and the ⊢ fields stay 0.
+__device__ __forceinline__ PosSums ps_warp_scan_one(PosSums x, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t on = __shfl_up_sync(ALP_FULL_MASK, x.nodes, d);
+        const uint32_t ob = __shfl_up_sync(ALP_FULL_MASK, x.brs, d);
+        const int32_t od = __shfl_up_sync(ALP_FULL_MASK, x.depth, d);
+        const int32_t ov = __shfl_up_sync(ALP_FULL_MASK, x.v, d);
+        const uint32_t ot = __shfl_up_sync(ALP_FULL_MASK, x.terms, d);
+        const uint32_t oc = __shfl_up_sync(ALP_FULL_MASK, x.cls, d);
+        if (lane >= d) { x.nodes += on; x.brs += ob; x.depth += od; x.v += ov; x.terms += ot; x.cls += oc; }
+    }
+    x.heads = 0;
+    x.hpos = 0;
+    return x;
+}
+__device__ __forceinline__ PosSums ps_shfl_up_one(const PosSums& x, int d) {
+    PosSums r;
+    r.nodes = __shfl_up_sync(ALP_FULL_MASK, x.nodes, d);
+    r.brs = __shfl_up_sync(ALP_FULL_MASK, x.brs, d);
+    r.depth = __shfl_up_sync(ALP_FULL_MASK, x.depth, d);
+    r.v = __shfl_up_sync(ALP_FULL_MASK, x.v, d);
+    r.terms = __shfl_up_sync(ALP_FULL_MASK, x.terms, d);
+    r.cls = __shfl_up_sync(ALP_FULL_MASK, x.cls, d);
+    r.heads = 0;
+    r.hpos = 0;
+    return r;
+}
 __device__ __forceinline__ PosSums ps_shfl_up(const PosSums& x, int d) {
     PosSums r;
     r.nodes = __shfl_up_sync(ALP_FULL_MASK, x.nodes, d);
@@ -1004,16 +1034,16 @@ __global__ void __launch_bounds__(PP_THREADS, 2) parse_expand_kernel(ParseArgs a
                                    ? adj_closed(s_pi, ids[PP_ITEMS - 1], next_id, next_head) : 0u;
             }
         }
-        const PosSums inc = ps_warp_scan(mine, lane);
-        PosSums ex = ps_shfl_up(inc, 1);
+        const PosSums inc = ONE ? ps_warp_scan_one(mine, lane) : ps_warp_scan(mine, lane);
+        PosSums ex = ONE ? ps_shfl_up_one(inc, 1) : ps_shfl_up(inc, 1);
         if (lane == 0) possums_zero(ex);
         if (lane == 31) s_w[warp] = inc;
         __syncthreads();
         if (warp == 0) {
             PosSums w;
             if (lane < PP_THREADS / 32) w = s_w[lane]; else possums_zero(w);
-            const PosSums wi = ps_warp_scan(w, lane);
-            PosSums we = ps_shfl_up(wi, 1);
+            const PosSums wi = ONE ? ps_warp_scan_one(w, lane) : ps_warp_scan(w, lane);
+            PosSums we = ONE ? ps_shfl_up_one(wi, 1) : ps_shfl_up(wi, 1);
             if (lane == 0) possums_zero(we);
             if (lane < PP_THREADS / 32) s_w[lane] = we;
             if (lane == PP_THREADS / 32 - 1) {
