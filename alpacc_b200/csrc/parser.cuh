@@ -1406,7 +1406,7 @@ __global__ void __launch_bounds__(PT, 1024 / PT) ple_tile_kernel(PleArgs a) {
     for (int j = 0; j < PI; ++j) {
         if (j < lim) {
             const long long g = gfirst + j;
-            while (g >= dnext && doc + 1 < a.n_seg) {
+            while (sd0 != sd1 && g >= dnext && doc + 1 < a.n_seg) {  // (a tile in one document: never)
                 ++doc;
                 dbase = a.seg_off[doc];
                 dnext = a.seg_off[doc + 1];
