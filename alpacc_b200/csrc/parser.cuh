@@ -1456,10 +1456,14 @@ __global__ void __launch_bounds__(PT, 1024 / PT) ple_tile_kernel(PleArgs a) {
                 // the nearest earlier chunk with minimum <= x: the few chunks just
                 // before the element's first (most answers are near), then the tree
                 const int ce = e / PI;
+                // the four chunk minima read at once (clamped indices), the nearest fitting one kept
+                int32_t near[4];
+#pragma unroll
+                for (int back = 1; back <= 4; ++back) near[back - 1] = tree[PT + max(ce - back, 0)];
                 int c = -1;
 #pragma unroll
-                for (int back = 1; back <= 4; ++back)
-                    if (c < 0 && ce - back >= 0 && tree[PT + ce - back] <= x) c = ce - back;
+                for (int back = 4; back >= 1; --back)
+                    if (ce - back >= 0 && near[back - 1] <= x) c = ce - back;
                 bool found = c >= 0;
                 if (!found && ce > 4) {
                     int node = PT + ce - 4;  // chunks left of those
