@@ -68,6 +68,9 @@ struct alp_ctx {
     DevBuf out[8];                        // context-owned outputs
     DevBuf tmp[32];                       // intermediates
     long long* h_stage = nullptr;         // pinned staging for small host->device values
+    // when set (pinned, in h_stage): the lexer copies the validity of document 0
+    // here in the same wait as its token count, which saves the caller a wait of its own
+    uint8_t* lex_valid0 = nullptr;
     AlpResult* h_res = nullptr;           // pinned
     // optional per-kernel timing (alp_ctx_profile)
     int prof = 0;
@@ -635,6 +638,7 @@ int lex3_back(alp_ctx* ctx, Lex3Run& r, long long* total) {
     int rc;
     if ((rc = lex3_emit<TermT, PosT>(ctx, r))) return rc;
     CK(cudaMemcpyAsync(ctx->h_res, r.a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
+    if (ctx->lex_valid0) CK(cudaMemcpyAsync(ctx->lex_valid0, r.sg.valid, 1, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
     *total = ctx->h_res->count;
@@ -660,6 +664,7 @@ int lex3_tok(alp_ctx* ctx, Lex3Run& r, long long* total) {
     CK(cudaGetLastError());
     mark(ctx, "lex3_tok_kernel");
     CK(cudaMemcpyAsync(ctx->h_res, r.a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
+    if (ctx->lex_valid0) CK(cudaMemcpyAsync(ctx->lex_valid0, r.sg.valid, 1, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
     *total = ctx->h_res->count;
@@ -769,6 +774,7 @@ int lex_seg(alp_ctx* ctx, const uint8_t* d_in, long long n, const long long* d_o
     CK(cudaGetLastError());
     mark(ctx, "lex_seg_kernel");
     CK(cudaMemcpyAsync(ctx->h_res, a.res, sizeof(AlpResult), cudaMemcpyDeviceToHost, ctx->stream));
+    if (ctx->lex_valid0) CK(cudaMemcpyAsync(ctx->lex_valid0, valid, 1, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (ctx->h_res->error & ALP_DEV_ERR_TIMEOUT) return fail(ctx, ALP_ERR_TIMEOUT, "lexer look-back timed out");
     *total = ctx->h_res->count;
@@ -882,8 +888,9 @@ int expand_grid(alp_ctx* ctx, const void* fn, size_t sm2, long long tiles, unsig
 // again at the exact sizes it reported.  The first parse on a context, and
 // grammars whose counts could pass 32 bits, take the two-pass form: the pair
 // kernel and a scan of its tile sums give the exact sizes first.
+// h_valid0 (pinned, optional): document 0's validity, read in the same final wait.
 int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, ParseOut* o, int64_t cap, int ctx_out,
-                    int64_t* n_node, int want_tree) {
+                    int64_t* n_node, int want_tree, uint8_t* h_valid0 = nullptr) {
     *n_node = 0;
     if (L >= 0x7fffffffLL) return fail(ctx, ALP_ERR_ARG, "too many positions (%lld)", L);
     const long long tiles = (L + PP_TILE - 1) / PP_TILE;
@@ -1037,6 +1044,7 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
         }
         if ((rc = run_ple(ctx, a.dsbuf, K, a.brbuf, nullptr, T_B_TMIN, a.br_off, nd, dvalid, d_res))) return rc;
     }
+    if (h_valid0) CK(cudaMemcpyAsync(h_valid0, dvalid, 1, cudaMemcpyDeviceToHost, ctx->stream));
     if ((rc = read_result(ctx, d_res))) return rc;
     *n_node = N;
     return ALP_OK;
@@ -1101,17 +1109,22 @@ int parse_core(alp_ctx* ctx, const uint8_t* d_in, int64_t n, ParseOut* o, int64_
         return rc;
     uint8_t* dvalid = (uint8_t*)ctx->tmp[T_DVALID].p;
     long long m = 0;
+    // the document's validity comes back with the lexer's token count and with the
+    // parser's final counts (pinned bytes in h_stage), not in waits of their own
+    uint8_t* hv = reinterpret_cast<uint8_t*>(ctx->h_stage) + 200;
+    hv[0] = 0;  // stays 0 for an empty input (the lexer then launches nothing)
+    hv[1] = 0;
+    ctx->lex_valid0 = hv;
     rc = lex_seg<uint16_t, uint32_t>(ctx, d_in, n, (const long long*)ctx->tmp[T_DOCOFF].p, 1, 1,
                                      (uint16_t*)ctx->tmp[T_TTERM].p, (uint32_t*)ctx->tmp[T_TSTART].p,
                                      (uint32_t*)ctx->tmp[T_TEND].p, (long long)tcap, dvalid, &m);
+    ctx->lex_valid0 = nullptr;
     if (rc) return rc;
-    int lv = 0;
-    if ((rc = read_valid0(ctx, dvalid, &lv))) return rc;
-    if (!lv) return ALP_OK;
+    if (!hv[0]) return ALP_OK;
     int64_t N = 0;
-    rc = parse_positions(ctx, m + 2, 1, dvalid, o, cap, ctx_out, &N, 1);
+    rc = parse_positions(ctx, m + 2, 1, dvalid, o, cap, ctx_out, &N, 1, hv + 1);
     if (rc) { *n_node = N; return rc; }
-    if ((rc = read_valid0(ctx, dvalid, valid))) return rc;
+    *valid = hv[1] ? 1 : 0;
     *n_node = *valid ? N : 0;
     return ALP_OK;
 }
