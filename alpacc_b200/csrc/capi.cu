@@ -68,6 +68,17 @@ struct alp_ctx {
     DevBuf out[8];                        // context-owned outputs
     DevBuf tmp[32];                       // intermediates
     long long* h_stage = nullptr;         // pinned staging for small host->device values
+    // alp_parse_host's host buffers: the node fields the searches leave alone start to
+    // the host as soon as the expansion has written them
+    struct HostTree {
+        uint32_t* tag;
+        uint8_t* kind;
+        int64_t* start;
+        int64_t* end;
+        long long cap;
+        bool started;
+    }* host_tree = nullptr;
+    cudaEvent_t ev_nodes = nullptr;
     // when set (pinned, in h_stage): the lexer copies the validity of document 0
     // here in the same wait as its token count, which saves the caller a wait of its own
     uint8_t* lex_valid0 = nullptr;
@@ -1018,6 +1029,19 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
     ctx->last_kept = K;
     ctx->est_nodes = (double)N / (double)L;
     ctx->est_kept = (double)K / (double)L;
+    if (ctx->host_tree && want_tree && N > 0 && N <= ctx->host_tree->cap) {
+        // tags, kinds and spans are final: their copy to the host overlaps the searches
+        alp_ctx::HostTree& h = *ctx->host_tree;
+        if (!ctx->cp_out) CK(cudaStreamCreateWithFlags(&ctx->cp_out, cudaStreamNonBlocking));
+        if (!ctx->ev_nodes) CK(cudaEventCreateWithFlags(&ctx->ev_nodes, cudaEventDisableTiming));
+        CK(cudaEventRecord(ctx->ev_nodes, ctx->stream));
+        CK(cudaStreamWaitEvent(ctx->cp_out, ctx->ev_nodes, 0));
+        h.started = true;
+        CK(cudaMemcpyAsync(h.tag, o->tag, (size_t)N * 4, cudaMemcpyDeviceToHost, ctx->cp_out));
+        CK(cudaMemcpyAsync(h.kind, o->kind, (size_t)N, cudaMemcpyDeviceToHost, ctx->cp_out));
+        CK(cudaMemcpyAsync(h.start, o->start, (size_t)N * 8, cudaMemcpyDeviceToHost, ctx->cp_out));
+        CK(cudaMemcpyAsync(h.end, o->end, (size_t)N * 8, cudaMemcpyDeviceToHost, ctx->cp_out));
+    }
     if (want_tree && !ctx->prof) {
         // the node and bracket searches share nothing but the result block (atomic
         // error bits) and document validity (cleared only): the bracket search runs on a
@@ -1285,6 +1309,7 @@ void alp_ctx_destroy(alp_ctx* ctx) {
     if (ctx->aux) cudaStreamDestroy(ctx->aux);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->ev_nodes) cudaEventDestroy(ctx->ev_nodes);
     delete ctx;
 }
 
@@ -2569,19 +2594,36 @@ int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_pare
     if ((rc = grow(ctx, ctx->tmp[T_HIN], (size_t)n + 16))) return rc;
     if (n) CK(cudaMemcpyAsync(ctx->tmp[T_HIN].p, h_in, (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
     ParseOut o{};
+    // tags, kinds and spans may start to the host during the searches (on cp_out); every
+    // return below waits for them, so that no copy outlives the call
+    alp_ctx::HostTree ht{h_tag, h_kind, h_start, h_end, (long long)cap, false};
+    ctx->host_tree = (cap > 0 && h_tag && h_kind && h_start && h_end) ? &ht : nullptr;
     rc = parse_core(ctx, (const uint8_t*)ctx->tmp[T_HIN].p, n, &o, 0, 1, n_node, valid);
-    if (rc) return rc;
-    if (*n_node > cap) return fail(ctx, ALP_ERR_CAPACITY, "host node buffer too small");
+    ctx->host_tree = nullptr;
+    auto join = [&]() -> int {
+        if (ht.started) CK(cudaStreamSynchronize(ctx->cp_out));
+        return ALP_OK;
+    };
+    if (rc) {
+        join();
+        return rc;
+    }
+    if (*n_node > cap) {
+        join();
+        return fail(ctx, ALP_ERR_CAPACITY, "host node buffer too small");
+    }
     const size_t N = (size_t)*n_node;
     if (N) {
         CK(cudaMemcpyAsync(h_parent, o.parent, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(h_tag, o.tag, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(h_kind, o.kind, N, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(h_start, o.start, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(h_end, o.end, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        if (!ht.started) {
+            CK(cudaMemcpyAsync(h_tag, o.tag, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaMemcpyAsync(h_kind, o.kind, N, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaMemcpyAsync(h_start, o.start, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaMemcpyAsync(h_end, o.end, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        }
         CK(cudaStreamSynchronize(ctx->stream));
     }
-    return ALP_OK;
+    return join();
 }
 
 int alp_parse_tokens(alp_ctx* ctx, const uint32_t* d_term, const int64_t* d_tstart, const int64_t* d_tend, int64_t m,
