@@ -139,6 +139,51 @@ def test_host_buffers(has_gpu):
         np.testing.assert_array_equal(a, b)
 
 
+def test_host_buffers_json_and_rejections(has_gpu):
+    """alp_parse_host on json (tags, kinds and spans start back to the host while the
+    searches run): the tree of a 3 MiB document, a document the parser rejects after the
+    lexer accepted it, and one the lexer rejects."""
+    g, o, _ = _ctx("json")
+    d = _gen("json", (3 << 20) + 11, 21)
+    got = g.parse_host(d)
+    want = o.lex_parse(d.tobytes())
+    for a, b in zip(got, want):
+        np.testing.assert_array_equal(a, b)
+    bad_parse = b'{"a": [1, 2}, "b": 3}'   # every token fine, the brackets do not match
+    assert o.lex_parse(bad_parse) is None and o.tokenize(bad_parse) is not None
+    assert g.parse_host(np.frombuffer(bad_parse, np.uint8)) is None
+    bad_lex = b'{"a": @}'
+    assert o.tokenize(bad_lex) is None
+    assert g.parse_host(np.frombuffer(bad_lex, np.uint8)) is None
+    # the context is fine afterwards
+    got = g.parse_host(d)
+    for a, b in zip(got, want):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_host_buffers_too_small(has_gpu):
+    """A host capacity below the node count: ALP_ERR_CAPACITY with the count needed, and
+    nothing written past the capacity (no copy was started early)."""
+    import ctypes
+    from alpacc_b200 import api
+    g, o, _ = _ctx("json")
+    d = _gen("json", 200_000, 22)
+    n_want = len(o.lex_parse(d.tobytes())[0])
+    cap = n_want // 2
+    canary = 0x5a
+    bufs = [np.full(cap + 64, canary, dt) for dt in (np.int64, np.uint32, np.uint8, np.int64, np.int64)]
+    n, valid = ctypes.c_int64(0), ctypes.c_int(0)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = api.native().alp_parse_host(g.h, vp(d), len(d), *[vp(b) for b in bufs], cap, ctypes.byref(n),
+                                     ctypes.byref(valid))
+    assert rc == 5 and n.value == n_want
+    for b in bufs:
+        assert (b[cap:] == canary).all()
+    got = g.parse_host(d)  # and a call with room works
+    for a, w in zip(got, o.lex_parse(d.tobytes())):
+        np.testing.assert_array_equal(a, w)
+
+
 def _bracket_counts(tb, data: bytes):
     """Brackets of the LLP pair sequence and the pairs closed between adjacent
     positions (a position's first rights against the previous position's top
