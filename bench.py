@@ -332,8 +332,10 @@ def _kernel_alg_bytes(name, units, parse_layout=True):
     K = units.get("K", B)
     c = (n + 31) // 32
     tok = 10 if parse_layout else 20
+    # one document: the expansion takes its ⊢ / ⊣ from the position, so it reads no terminal ids
+    ids_in = 2 * L if units.get("one_doc") else 4 * L
     table = {
-        "parse_expand_kernel": 4 * L + 8 * m + 25 * N + 8 * K,   # ids in, spans in, node fields + kept brackets out
+        "parse_expand_kernel": ids_in + 8 * m + 25 * N + 8 * K,  # ids in, spans in, node fields + kept brackets out
         "parse_expand_kernel(fused)": 2 * L + 8 * m + 25 * N + 8 * K,  # terminals in (keys), spans in, same out
         "lex3_tok_kernel": n + c + tok * m,                    # bytes and chunk states in, tokens out
         "ple_tile_kernel(nodes)": 12 * N,                      # values in, parents out
@@ -1133,7 +1135,7 @@ def main():
     alg_bytes = size + NODE_BYTES * N
     # one mark per kernel, except "a+b" marks that cover two launches
     launches_per_step = sum(1 + k.count("+") for k, _ in kern)
-    roof, path = _roofline(kern, dict(counts, n=size, N=N), ms, alg_bytes)
+    roof, path = _roofline(kern, dict(counts, n=size, N=N, one_doc=True), ms, alg_bytes)
     path["scope"] = "whole alp_parse call: %d input bytes + %d B per node, over the step time" % (size, NODE_BYTES)
     line = {
         "metric": METRIC,
