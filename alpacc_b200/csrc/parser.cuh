@@ -1566,22 +1566,24 @@ __global__ void __launch_bounds__(PT, 1024 / PT) ple_tile_kernel(PleArgs a) {
 }
 
 // Level-1/2 minima over groups of 32 / 1024 tiles.
+// Thread g: the minimum of tiles [32g, 32g + 32); lane 0 of each warp: the minimum of
+// its 32 lanes' groups, tiles [1024w, 1024w + 1024) (warps hold 32 consecutive groups).
 __global__ void tile_min_levels_kernel(const int32_t* tmin, long long tiles, int32_t* m32, int32_t* m1024,
                                        const long long* dn, int tile) {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (dn) tiles = min(tiles, (*dn + tile - 1) / tile);  // tiles is then the capacity
     const long long n32 = (tiles + 31) / 32;
+    int32_t m = INT32_MAX;
     if (g < n32) {
-        int32_t m = INT32_MAX;
-        for (long long t = g * 32; t < tiles && t < g * 32 + 32; ++t) m = min(m, tmin[t]);
+#pragma unroll 8
+        for (int k = 0; k < 32; ++k) {
+            const long long t = g * 32 + k;
+            if (t < tiles) m = min(m, __ldg(&tmin[t]));
+        }
         m32[g] = m;
     }
-    const long long n1024 = (tiles + 1023) / 1024;
-    if (g < n1024) {
-        int32_t m = INT32_MAX;
-        for (long long t = g * 1024; t < tiles && t < g * 1024 + 1024; ++t) m = min(m, tmin[t]);
-        m1024[g] = m;
-    }
+    m = __reduce_min_sync(ALP_FULL_MASK, m);
+    if ((threadIdx.x & 31) == 0 && g / 32 < (tiles + 1023) / 1024) m1024[g / 32] = m;
 }
 
 // Nearest tile before `t` whose minimum is <= x, or -1.
