@@ -1,12 +1,19 @@
 // C ABI of alpacc_b200 (include/alpacc_b200.h): context, table upload, and
 // the host side of every entry point.  Kernels live in the .cuh files.
 #include <cuda_runtime.h>
+#include <immintrin.h>
+#include <sched.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/alpacc_b200.h"
@@ -29,6 +36,124 @@ constexpr int LEX_TILE = LEX_THREADS * LEX_ITEMS;
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Host widening.  alp_parse_host brings node fields whose values all lie in
+// [-1, 2^31) across PCIe as 32-bit values and sign-extends them into the
+// caller's 64-bit arrays on the host, chunk by chunk while later chunks are
+// still in flight: 17 bytes a node cross the bus instead of 29.  The widening
+// runs on a pool of host threads (the calling thread joins in) in slices of
+// WIDEN_SLICE elements, with streaming stores (no read of the destination).
+// ---------------------------------------------------------------------------
+constexpr size_t WIDEN_SLICE = (size_t)1 << 18;
+constexpr long long WIDEN_CHUNK = 1LL << 22;  // elements per device->host copy and event
+
+__attribute__((target("avx2"))) void widen_avx2(const int32_t* s, int64_t* d, size_t n) {
+    size_t i = 0;
+    for (; i < n && ((uintptr_t)(d + i) & 31); ++i) d[i] = s[i];
+    for (; i + 4 <= n; i += 4) {
+        const __m128i x = _mm_loadu_si128(reinterpret_cast<const __m128i*>(s + i));
+        _mm256_stream_si256(reinterpret_cast<__m256i*>(d + i), _mm256_cvtepi32_epi64(x));
+    }
+    for (; i < n; ++i) d[i] = s[i];
+    _mm_sfence();
+}
+
+void widen(const int32_t* s, int64_t* d, size_t n) {
+    static const bool avx2 = __builtin_cpu_supports("avx2");
+    if (avx2 && ((uintptr_t)d & 7) == 0) {
+        widen_avx2(s, d, n);
+        return;
+    }
+    for (size_t i = 0; i < n; ++i) d[i] = s[i];
+}
+
+// Worker threads for widen(): the host's CPUs this process may run on, less the
+// calling thread (ALP_HOST_THREADS sets the count).
+int host_workers() {
+    if (const char* e = getenv("ALP_HOST_THREADS")) {
+        const int v = atoi(e);
+        if (v >= 1) return std::min(v, 256);
+    }
+    cpu_set_t set;
+    int n = 1;
+    if (sched_getaffinity(0, sizeof set, &set) == 0) n = CPU_COUNT(&set);
+    return std::max(1, std::min(n - 1, 255));
+}
+
+class HostPool {
+  public:
+    explicit HostPool(int workers) {
+        for (int i = 0; i < workers; ++i) th_.emplace_back([this] { run(); });
+    }
+    ~HostPool() {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : th_) t.join();
+    }
+    void push(const int32_t* s, int64_t* d, size_t n) {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            for (size_t o = 0; o < n; o += WIDEN_SLICE) q_.push_back({s + o, d + o, std::min(WIDEN_SLICE, n - o)});
+        }
+        cv_.notify_all();
+    }
+    // Widen one queued slice on the calling thread; false when none is queued.
+    bool help() {
+        Slice x;
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            if (q_.empty()) return false;
+            x = q_.front();
+            q_.pop_front();
+            ++busy_;
+        }
+        finish(x);
+        return true;
+    }
+    // Every pushed slice written.
+    void wait() {
+        while (help()) {
+        }
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [&] { return q_.empty() && busy_ == 0; });
+    }
+
+  private:
+    struct Slice {
+        const int32_t* s;
+        int64_t* d;
+        size_t n;
+    };
+    void finish(const Slice& x) {
+        widen(x.s, x.d, x.n);
+        std::lock_guard<std::mutex> lk(m_);
+        if (--busy_ == 0 && q_.empty()) done_.notify_all();
+    }
+    void run() {
+        for (;;) {
+            Slice x;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return stop_ || !q_.empty(); });
+                if (q_.empty()) return;  // stopping
+                x = q_.front();
+                q_.pop_front();
+                ++busy_;
+            }
+            finish(x);
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex m_;
+    std::condition_variable cv_, done_;
+    std::deque<Slice> q_;
+    size_t busy_ = 0;
+    bool stop_ = false;
 };
 
 }  // namespace
@@ -77,8 +202,23 @@ struct alp_ctx {
         int64_t* end;
         long long cap;
         bool started;
+        bool wide;   // spans sent as 32-bit values, widened on the host
     }* host_tree = nullptr;
     cudaEvent_t ev_nodes = nullptr;
+    // 32-bit node fields on their way to the host: pinned landing buffer, the copies
+    // in issue order (each with the event recorded after it), and the widening threads
+    int32_t* h_narrow = nullptr;
+    size_t h_narrow_bytes = 0;
+    struct Landing {
+        cudaEvent_t ev;
+        const int32_t* src;
+        int64_t* dst;
+        size_t n;
+    };
+    std::vector<Landing> landing;
+    std::vector<cudaEvent_t> ev_chunks;
+    HostPool* pool = nullptr;
+    long long last_h2d = 0, last_d2h = 0;  // data bytes the last host-buffer call moved
     // when set (pinned, in h_stage): the lexer copies the validity of document 0
     // here in the same wait as its token count, which saves the caller a wait of its own
     uint8_t* lex_valid0 = nullptr;
@@ -148,6 +288,78 @@ int fail(alp_ctx* c, int code, const char* fmt, ...) {
         cudaError_t e_ = (call);                                                                  \
         if (e_ != cudaSuccess) return fail(ctx, ALP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
+
+// 64-bit node fields as 32-bit values (each in [-1, 2^31)) for the copy to the
+// host; b and ob may be null.  Grid-stride, four elements per thread per step.
+constexpr int NARROW_GRID = 148 * 8;
+__global__ void narrow_i64_kernel(const int64_t* __restrict__ a, const int64_t* __restrict__ b, long long n,
+                                  int32_t* __restrict__ oa, int32_t* __restrict__ ob) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const long long i = i0 + u * stride;
+            if (i < n) {
+                oa[i] = (int32_t)__ldg(a + i);
+                if (b) ob[i] = (int32_t)__ldg(b + i);
+            }
+        }
+    }
+}
+
+// The pinned landing buffer of alp_parse_host's 32-bit node fields.  Every earlier
+// call has waited for its copies, so the old buffer is free when it is replaced.
+int grow_landing(alp_ctx* ctx, size_t bytes) {
+    if (ctx->h_narrow_bytes >= bytes && ctx->h_narrow) return ALP_OK;
+    if (ctx->h_narrow) cudaFreeHost(ctx->h_narrow);
+    ctx->h_narrow = nullptr;
+    ctx->h_narrow_bytes = 0;
+    CK(cudaHostAlloc((void**)&ctx->h_narrow, bytes, cudaHostAllocDefault));
+    ctx->h_narrow_bytes = bytes;
+    return ALP_OK;
+}
+
+// n 32-bit values at d to the host landing buffer h on stream s, in chunks, each
+// followed by an event; the host widens a chunk into dst once its event has passed.
+int land(alp_ctx* ctx, const int32_t* d, int32_t* h, int64_t* dst, long long n, cudaStream_t s) {
+    for (long long c = 0; c < n; c += WIDEN_CHUNK) {
+        const long long len = std::min(WIDEN_CHUNK, n - c);
+        CK(cudaMemcpyAsync(h + c, d + c, (size_t)len * 4, cudaMemcpyDeviceToHost, s));
+        const size_t k = ctx->landing.size();
+        while (ctx->ev_chunks.size() <= k) {
+            cudaEvent_t e;
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            ctx->ev_chunks.push_back(e);
+        }
+        CK(cudaEventRecord(ctx->ev_chunks[k], s));
+        ctx->landing.push_back({ctx->ev_chunks[k], h + c, dst + c, (size_t)len});
+    }
+    return ALP_OK;
+}
+
+// Widen every landed chunk, in the order the copies were issued: the calling
+// thread polls the next chunk's event and widens queued slices meanwhile.
+int drain_landing(alp_ctx* ctx) {
+    if (!ctx->pool) ctx->pool = new HostPool(host_workers());
+    int rc = ALP_OK;
+    size_t next = 0;
+    while (next < ctx->landing.size()) {
+        const alp_ctx::Landing& l = ctx->landing[next];
+        const cudaError_t e = cudaEventQuery(l.ev);
+        if (e == cudaSuccess) {
+            ctx->pool->push(l.src, l.dst, l.n);
+            ++next;
+        } else if (e == cudaErrorNotReady) {
+            if (!ctx->pool->help()) std::this_thread::yield();
+        } else {
+            rc = fail(ctx, ALP_ERR_CUDA, "copy to the host: %s", cudaGetErrorString(e));
+            break;
+        }
+    }
+    ctx->pool->wait();
+    ctx->landing.clear();
+    return rc;
+}
 
 int grow(alp_ctx* ctx, DevBuf& b, size_t bytes) {
     if (b.bytes >= bytes && b.p) return ALP_OK;
@@ -355,7 +567,7 @@ enum {
     T_HIN = 0, T_TTERM, T_TSTART, T_TEND, T_PID, T_TSUMS, T_VBUF, T_BRBUF, T_DSBUF,
     T_N_TMIN, T_N_M32, T_N_M1024, T_N_SVAL, T_N_SIDX, T_N_SLEN, T_N_ESC,
     T_B_TMIN, T_B_M32, T_B_M1024, T_B_SVAL, T_B_SIDX, T_B_SLEN, T_B_ESC,
-    T_DOCOFF, T_TOKOFF, T_NODEOFF, T_BROFF, T_DVALID, T_CNT
+    T_DOCOFF, T_TOKOFF, T_NODEOFF, T_BROFF, T_DVALID, T_NARROW, T_CNT
 };
 
 struct ParseOut {
@@ -1037,10 +1249,24 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
         CK(cudaEventRecord(ctx->ev_nodes, ctx->stream));
         CK(cudaStreamWaitEvent(ctx->cp_out, ctx->ev_nodes, 0));
         h.started = true;
-        CK(cudaMemcpyAsync(h.tag, o->tag, (size_t)N * 4, cudaMemcpyDeviceToHost, ctx->cp_out));
-        CK(cudaMemcpyAsync(h.kind, o->kind, (size_t)N, cudaMemcpyDeviceToHost, ctx->cp_out));
-        CK(cudaMemcpyAsync(h.start, o->start, (size_t)N * 8, cudaMemcpyDeviceToHost, ctx->cp_out));
-        CK(cudaMemcpyAsync(h.end, o->end, (size_t)N * 8, cudaMemcpyDeviceToHost, ctx->cp_out));
+        if (N <= 0x7fffffffLL) {
+            // spans (in [0, 2^31): inputs are shorter) cross as 32-bit values and are widened
+            // on the host as they land; tags and kinds follow the parents (alp_parse_host)
+            if ((rc = grow(ctx, ctx->tmp[T_NARROW], (size_t)N * 12)) || (rc = grow_landing(ctx, (size_t)N * 12)))
+                return rc;
+            int32_t* d32 = (int32_t*)ctx->tmp[T_NARROW].p;
+            narrow_i64_kernel<<<NARROW_GRID, 256, 0, ctx->cp_out>>>(o->start, o->end, N, d32, d32 + N);
+            CK(cudaGetLastError());
+            h.wide = true;
+            if ((rc = land(ctx, d32, ctx->h_narrow, h.start, N, ctx->cp_out)) ||
+                (rc = land(ctx, d32 + N, ctx->h_narrow + N, h.end, N, ctx->cp_out)))
+                return rc;
+        } else {
+            CK(cudaMemcpyAsync(h.tag, o->tag, (size_t)N * 4, cudaMemcpyDeviceToHost, ctx->cp_out));
+            CK(cudaMemcpyAsync(h.kind, o->kind, (size_t)N, cudaMemcpyDeviceToHost, ctx->cp_out));
+            CK(cudaMemcpyAsync(h.start, o->start, (size_t)N * 8, cudaMemcpyDeviceToHost, ctx->cp_out));
+            CK(cudaMemcpyAsync(h.end, o->end, (size_t)N * 8, cudaMemcpyDeviceToHost, ctx->cp_out));
+        }
     }
     if (want_tree && !ctx->prof) {
         // the node and bracket searches share nothing but the result block (atomic
@@ -1310,6 +1536,9 @@ void alp_ctx_destroy(alp_ctx* ctx) {
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     if (ctx->ev_nodes) cudaEventDestroy(ctx->ev_nodes);
+    for (cudaEvent_t e : ctx->ev_chunks) cudaEventDestroy(e);
+    if (ctx->h_narrow) cudaFreeHost(ctx->h_narrow);
+    delete ctx->pool;
     delete ctx;
 }
 
@@ -1323,10 +1552,11 @@ int alp_set_stream(alp_ctx* ctx, void* stream) {
 
 int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out) {
     if (!ctx || !out) return ALP_ERR_ARG;
-    int64_t v[13] = {ctx->has_lexer, ctx->has_parser, ctx->has_parser ? ctx->ph.n_terms : ctx->n_terms,
+    int64_t v[15] = {ctx->has_lexer, ctx->has_parser, ctx->has_parser ? ctx->ph.n_terms : ctx->n_terms,
                      ctx->ph.n_prods, ctx->ph.q, ctx->ph.k, ctx->ph.max_prods, ctx->ph.max_brackets,
-                     ctx->last_tokens, ctx->last_positions, ctx->last_brackets, ctx->last_kept, ctx->dev_allocs};
-    for (int i = 0; i < n_out && i < 13; ++i) out[i] = v[i];
+                     ctx->last_tokens, ctx->last_positions, ctx->last_brackets, ctx->last_kept, ctx->dev_allocs,
+                     ctx->last_h2d, ctx->last_d2h};
+    for (int i = 0; i < n_out && i < 15; ++i) out[i] = v[i];
     return ALP_OK;
 }
 
@@ -2596,12 +2826,17 @@ int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_pare
     ParseOut o{};
     // tags, kinds and spans may start to the host during the searches (on cp_out); every
     // return below waits for them, so that no copy outlives the call
-    alp_ctx::HostTree ht{h_tag, h_kind, h_start, h_end, (long long)cap, false};
+    alp_ctx::HostTree ht{h_tag, h_kind, h_start, h_end, (long long)cap, false, false};
     ctx->host_tree = (cap > 0 && h_tag && h_kind && h_start && h_end) ? &ht : nullptr;
+    ctx->landing.clear();
+    ctx->last_h2d = n;
+    ctx->last_d2h = 0;
     rc = parse_core(ctx, (const uint8_t*)ctx->tmp[T_HIN].p, n, &o, 0, 1, n_node, valid);
     ctx->host_tree = nullptr;
+    // no copy outlives the call, nor a landed chunk its widening
     auto join = [&]() -> int {
         if (ht.started) CK(cudaStreamSynchronize(ctx->cp_out));
+        ctx->landing.clear();
         return ALP_OK;
     };
     if (rc) {
@@ -2613,7 +2848,27 @@ int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_pare
         return fail(ctx, ALP_ERR_CAPACITY, "host node buffer too small");
     }
     const size_t N = (size_t)*n_node;
-    if (N) {
+    if (N && ht.wide) {
+        // parents (in [0, N)) narrowed after the searches and sent behind the spans; tags
+        // and kinds last, so that the widening of the parents overlaps their copy
+        int32_t* d32 = (int32_t*)ctx->tmp[T_NARROW].p + 2 * N;
+        narrow_i64_kernel<<<NARROW_GRID, 256, 0, ctx->stream>>>(o.parent, nullptr, (long long)N, d32, nullptr);
+        auto issue = [&]() -> int {
+            CK(cudaGetLastError());
+            CK(cudaEventRecord(ctx->ev_nodes, ctx->stream));
+            CK(cudaStreamWaitEvent(ctx->cp_out, ctx->ev_nodes, 0));
+            int r2 = land(ctx, d32, ctx->h_narrow + 2 * N, h_parent, (long long)N, ctx->cp_out);
+            if (r2) return r2;
+            CK(cudaMemcpyAsync(h_tag, o.tag, N * 4, cudaMemcpyDeviceToHost, ctx->cp_out));
+            CK(cudaMemcpyAsync(h_kind, o.kind, N, cudaMemcpyDeviceToHost, ctx->cp_out));
+            return ALP_OK;
+        };
+        if ((rc = issue()) || (rc = drain_landing(ctx))) {
+            join();
+            return rc;
+        }
+        ctx->last_d2h = (long long)N * 17;
+    } else if (N) {
         CK(cudaMemcpyAsync(h_parent, o.parent, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
         if (!ht.started) {
             CK(cudaMemcpyAsync(h_tag, o.tag, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
@@ -2622,6 +2877,7 @@ int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_pare
             CK(cudaMemcpyAsync(h_end, o.end, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
         }
         CK(cudaStreamSynchronize(ctx->stream));
+        ctx->last_d2h = (long long)N * 29;
     }
     return join();
 }

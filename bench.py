@@ -397,10 +397,11 @@ def _ctx_counts(g):
     import ctypes
     from alpacc_b200 import api
     L = api.native()
-    out = (ctypes.c_int64 * 12)()
+    out = (ctypes.c_int64 * 15)()
     L.alp_ctx_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
-    L.alp_ctx_info(g.h, out, 12)
-    return {"m": int(out[8]), "L": int(out[9]), "B": int(out[10]), "K": int(out[11])}
+    L.alp_ctx_info(g.h, out, 15)
+    return {"m": int(out[8]), "L": int(out[9]), "B": int(out[10]), "K": int(out[11]),
+            "h2d": int(out[13]), "d2h": int(out[14])}
 
 
 SEED_LEX = 0xA1FACC00 + 1
@@ -1109,7 +1110,9 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = _max_over_ranks(e0.elapsed_time(e1) / k_e2e, dist, local)
-    pcie = _pcie(local, size, NODE_BYTES * N)
+    # the bytes the call moved: parents and spans cross as 32-bit values
+    moved = _ctx_counts(g)
+    pcie = _pcie(local, moved["h2d"], moved["d2h"])
 
     # full-size parity: the tree the e2e call brought back against the oracle
     # (sequential restatement of the generated lex_int + parse_int)
@@ -1158,8 +1161,10 @@ def main():
                                "candidates_ms": [[k, v, round(t, 4)] for k, v, t in tuning["timings"]]}},
         "roofline": roof,
         "path_roofline": path,
-        "e2e": {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": size,
-                "d2h_bytes_per_step": NODE_BYTES * N, "ms_per_step": ms_e2e, "pcie": pcie},
+        "e2e": {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": moved["h2d"],
+                "d2h_bytes_per_step": moved["d2h"], "ms_per_step": ms_e2e, "pcie": pcie,
+                "d2h_form": "i32 parents and spans (sign-extended into the caller's i64 arrays on the host "
+                            "while later chunks are in flight), u32 tags, u8 kinds"},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
     }

@@ -64,8 +64,9 @@ int alp_set_stream(alp_ctx* ctx, void* stream);
  * context: [8] tokens, [9] parser positions (tokens + 2 per document),
  * [10] brackets, [11] brackets left for the bracket-matching search after
  * the pairs closed between adjacent positions are removed; [12] device
- * allocations (cudaMalloc calls) this context has made so far.  No reference
- * counterpart (measurement support). */
+ * allocations (cudaMalloc calls) this context has made so far; [13], [14]
+ * data bytes the last alp_parse_host call moved to the device (input) and to
+ * the host (tree).  No reference counterpart (measurement support). */
 int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out);
 
 /* Per-kernel timing (no reference counterpart; measurement support): when on,
@@ -261,6 +262,12 @@ int alp_parse(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t** d_parent, 
 int alp_parse_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t* d_parent, uint32_t* d_tag,
                    uint8_t* d_kind, int64_t* d_start, int64_t* d_end, int64_t cap, int64_t* n_node,
                    int* valid);
+/* The same from and into host memory.  Parents and spans cross PCIe as 32-bit
+ * values (17 bytes a node instead of 29) and host threads sign-extend them into
+ * the caller's arrays as each 4 Mi-node chunk lands, while later chunks are
+ * still in flight; the call returns when every output is written.  The threads
+ * are the CPUs the process may run on, less the calling thread, or
+ * ALP_HOST_THREADS when that is set (read once per context). */
 int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_parent, uint32_t* h_tag,
                    uint8_t* h_kind, int64_t* h_start, int64_t* h_end, int64_t cap, int64_t* n_node,
                    int* valid);

@@ -161,6 +161,50 @@ def test_host_buffers_json_and_rejections(has_gpu):
         np.testing.assert_array_equal(a, b)
 
 
+def test_host_widening_chunks(has_gpu):
+    """alp_parse_host sends parents and spans as 32-bit values and widens them on the
+    host chunk by chunk (4 Mi nodes per copy, 256 Ki values per slice): a 32 MiB json
+    document (several chunks of each field, a partial last one) into pageable arrays,
+    into pinned arrays, and into arrays one element off a 32-byte boundary, with the
+    default threads and with one; the bytes it reports moving match 17 per node."""
+    import ctypes
+    import torch
+    from alpacc_b200 import api
+    g, o, tb = _ctx("json")
+    d = _gen("json", (32 << 20) + 5, 23)
+    want = o.lex_parse(d.tobytes())
+    N = len(want[0])
+    assert N > 2 * (1 << 22) and N % (1 << 18) != 0
+    got = g.parse_host(d)
+    for a, b in zip(got, want):
+        np.testing.assert_array_equal(a, b)
+    info = (ctypes.c_int64 * 15)()
+    assert api.native().alp_ctx_info(g.h, info, 15) == 0
+    assert info[13] == len(d) and info[14] == 17 * N
+    vp = lambda a: ctypes.c_void_p(a.data_ptr())
+    n, valid = ctypes.c_int64(0), ctypes.c_int(0)
+    h_in = torch.from_numpy(d).pin_memory()
+    dts = (torch.int64, torch.int32, torch.uint8, torch.int64, torch.int64)
+    for shift in (0, 1):
+        bufs = [torch.full((N + 8,), 90, dtype=dt, pin_memory=True) for dt in dts]
+        outs = [b[shift:shift + N] for b in bufs]
+        rc = api.native().alp_parse_host(g.h, vp(h_in), len(d), *[vp(x) for x in outs], N, ctypes.byref(n),
+                                         ctypes.byref(valid))
+        assert rc == 0 and valid.value == 1 and n.value == N
+        for x, w in zip(outs, want):
+            np.testing.assert_array_equal(x.numpy().astype(w.dtype), w)
+        for b in bufs:  # nothing written outside the N elements
+            assert (b[:shift] == 90).all() and (b[shift + N:] == 90).all()
+    os.environ["ALP_HOST_THREADS"] = "1"
+    try:
+        g1 = api.Grammar(tb)
+        got = g1.parse_host(d)
+    finally:
+        del os.environ["ALP_HOST_THREADS"]
+    for a, b in zip(got, want):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_host_buffers_too_small(has_gpu):
     """A host capacity below the node count: ALP_ERR_CAPACITY with the count needed, and
     nothing written past the capacity (no copy was started early)."""
