@@ -5,6 +5,7 @@
 #include <sched.h>
 
 #include <algorithm>
+#include <atomic>
 #include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
@@ -41,13 +42,20 @@ struct DevBuf {
 // ---------------------------------------------------------------------------
 // Host widening.  alp_parse_host brings node fields whose values all lie in
 // [-1, 2^31) across PCIe as 32-bit values and sign-extends them into the
-// caller's 64-bit arrays on the host, chunk by chunk while later chunks are
-// still in flight: 17 bytes a node cross the bus instead of 29.  The widening
-// runs on a pool of host threads (the calling thread joins in) in slices of
-// WIDEN_SLICE elements, with streaming stores (no read of the destination).
+// caller's 64-bit arrays on the host while later chunks are still in flight:
+// 17 bytes a node cross the bus instead of 29.  The chunks land in a ring of
+// RING_SLOTS pinned slots of RING_CHUNK values (64 MiB in all: the copies and
+// the widening's reads stay within a small working set instead of streaming a
+// landing buffer the size of the tree through DRAM); a slot takes the next
+// chunk once its widening is done.  The widening runs on a pool of at most
+// HOST_WORKERS threads (the calling thread joins in; more threads than that
+// took memory bandwidth from the copies) in slices of WIDEN_SLICE values, with
+// streaming stores (no read of the destination).
 // ---------------------------------------------------------------------------
 constexpr size_t WIDEN_SLICE = (size_t)1 << 18;
-constexpr long long WIDEN_CHUNK = 1LL << 22;  // elements per device->host copy and event
+constexpr int RING_SLOTS = 16;
+constexpr int HOST_WORKERS = 6;
+constexpr long long RING_CHUNK = 1LL << 20;
 
 __attribute__((target("avx2"))) void widen_avx2(const int32_t* s, int64_t* d, size_t n) {
     size_t i = 0;
@@ -70,7 +78,7 @@ void widen(const int32_t* s, int64_t* d, size_t n) {
 }
 
 // Worker threads for widen(): the host's CPUs this process may run on, less the
-// calling thread (ALP_HOST_THREADS sets the count).
+// calling thread, at most HOST_WORKERS (ALP_HOST_THREADS sets the count).
 int host_workers() {
     if (const char* e = getenv("ALP_HOST_THREADS")) {
         const int v = atoi(e);
@@ -79,7 +87,7 @@ int host_workers() {
     cpu_set_t set;
     int n = 1;
     if (sched_getaffinity(0, sizeof set, &set) == 0) n = CPU_COUNT(&set);
-    return std::max(1, std::min(n - 1, 255));
+    return std::max(1, std::min(n - 1, HOST_WORKERS));
 }
 
 class HostPool {
@@ -95,10 +103,14 @@ class HostPool {
         cv_.notify_all();
         for (auto& t : th_) t.join();
     }
-    void push(const int32_t* s, int64_t* d, size_t n) {
+    static int slices(size_t n) { return (int)((n + WIDEN_SLICE - 1) / WIDEN_SLICE); }
+    // Queue the widening of n values; *left (set to slices(n) by the caller) counts
+    // the slices not yet written.
+    void push(const int32_t* s, int64_t* d, size_t n, std::atomic<int>* left) {
         {
             std::lock_guard<std::mutex> lk(m_);
-            for (size_t o = 0; o < n; o += WIDEN_SLICE) q_.push_back({s + o, d + o, std::min(WIDEN_SLICE, n - o)});
+            for (size_t o = 0; o < n; o += WIDEN_SLICE)
+                q_.push_back({s + o, d + o, std::min(WIDEN_SLICE, n - o), left});
         }
         cv_.notify_all();
     }
@@ -128,9 +140,11 @@ class HostPool {
         const int32_t* s;
         int64_t* d;
         size_t n;
+        std::atomic<int>* left;
     };
     void finish(const Slice& x) {
         widen(x.s, x.d, x.n);
+        x.left->fetch_sub(1, std::memory_order_release);
         std::lock_guard<std::mutex> lk(m_);
         if (--busy_ == 0 && q_.empty()) done_.notify_all();
     }
@@ -205,18 +219,17 @@ struct alp_ctx {
         bool wide;   // spans sent as 32-bit values, widened on the host
     }* host_tree = nullptr;
     cudaEvent_t ev_nodes = nullptr;
-    // 32-bit node fields on their way to the host: pinned landing buffer, the copies
-    // in issue order (each with the event recorded after it), and the widening threads
-    int32_t* h_narrow = nullptr;
-    size_t h_narrow_bytes = 0;
-    struct Landing {
-        cudaEvent_t ev;
-        const int32_t* src;
-        int64_t* dst;
-        size_t n;
+    // node fields on their way to the host (alp_parse_host): the copies in the order to
+    // issue them, the pinned ring their 32-bit values land in, and the widening threads
+    struct HostCopy {
+        const void* src;  // device
+        void* dst;        // host: the caller's 64-bit array (widened) or its array (direct)
+        size_t n;         // widened: 32-bit values; direct: bytes
+        bool widen;
     };
-    std::vector<Landing> landing;
-    std::vector<cudaEvent_t> ev_chunks;
+    std::vector<HostCopy> copies;
+    int32_t* h_ring = nullptr;
+    cudaEvent_t ev_ring[RING_SLOTS] = {};
     HostPool* pool = nullptr;
     long long last_h2d = 0, last_d2h = 0;  // data bytes the last host-buffer call moved
     // when set (pinned, in h_stage): the lexer copies the validity of document 0
@@ -289,11 +302,14 @@ int fail(alp_ctx* c, int code, const char* fmt, ...) {
         if (e_ != cudaSuccess) return fail(ctx, ALP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
-// 64-bit node fields as 32-bit values (each in [-1, 2^31)) for the copy to the
-// host; b and ob may be null.  Grid-stride, four elements per thread per step.
+// 64-bit fields as 32-bit values (each in [-1, 2^31)) for the copy to the host;
+// b and ob may be null; when dn is set, the count is min(n, *dn).  Grid-stride,
+// four elements per thread per step.
 constexpr int NARROW_GRID = 148 * 8;
 __global__ void narrow_i64_kernel(const int64_t* __restrict__ a, const int64_t* __restrict__ b, long long n,
-                                  int32_t* __restrict__ oa, int32_t* __restrict__ ob) {
+                                  int32_t* __restrict__ oa, int32_t* __restrict__ ob,
+                                  const long long* dn = nullptr) {
+    if (dn) n = min(n, *dn);
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
 #pragma unroll
@@ -307,57 +323,76 @@ __global__ void narrow_i64_kernel(const int64_t* __restrict__ a, const int64_t* 
     }
 }
 
-// The pinned landing buffer of alp_parse_host's 32-bit node fields.  Every earlier
-// call has waited for its copies, so the old buffer is free when it is replaced.
-int grow_landing(alp_ctx* ctx, size_t bytes) {
-    if (ctx->h_narrow_bytes >= bytes && ctx->h_narrow) return ALP_OK;
-    if (ctx->h_narrow) cudaFreeHost(ctx->h_narrow);
-    ctx->h_narrow = nullptr;
-    ctx->h_narrow_bytes = 0;
-    CK(cudaHostAlloc((void**)&ctx->h_narrow, bytes, cudaHostAllocDefault));
-    ctx->h_narrow_bytes = bytes;
-    return ALP_OK;
-}
-
-// n 32-bit values at d to the host landing buffer h on stream s, in chunks, each
-// followed by an event; the host widens a chunk into dst once its event has passed.
-int land(alp_ctx* ctx, const int32_t* d, int32_t* h, int64_t* dst, long long n, cudaStream_t s) {
-    for (long long c = 0; c < n; c += WIDEN_CHUNK) {
-        const long long len = std::min(WIDEN_CHUNK, n - c);
-        CK(cudaMemcpyAsync(h + c, d + c, (size_t)len * 4, cudaMemcpyDeviceToHost, s));
-        const size_t k = ctx->landing.size();
-        while (ctx->ev_chunks.size() <= k) {
-            cudaEvent_t e;
-            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-            ctx->ev_chunks.push_back(e);
-        }
-        CK(cudaEventRecord(ctx->ev_chunks[k], s));
-        ctx->landing.push_back({ctx->ev_chunks[k], h + c, dst + c, (size_t)len});
-    }
-    return ALP_OK;
-}
-
-// Widen every landed chunk, in the order the copies were issued: the calling
-// thread polls the next chunk's event and widens queued slices meanwhile.
-int drain_landing(alp_ctx* ctx) {
+// Issue ctx->copies on stream s in order: a direct copy at once, a widened one
+// when a ring slot is free.  The calling thread hands each landed slot (its
+// event passed, in issue order) to the widening threads and widens slices
+// itself meanwhile.  Returns when every copy has landed and been widened.
+int send_to_host(alp_ctx* ctx, cudaStream_t s) {
     if (!ctx->pool) ctx->pool = new HostPool(host_workers());
-    int rc = ALP_OK;
+    if (!ctx->h_ring) {
+        CK(cudaHostAlloc((void**)&ctx->h_ring, (size_t)RING_SLOTS * RING_CHUNK * 4, cudaHostAllocDefault));
+        for (auto& e : ctx->ev_ring) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    HostPool& pool = *ctx->pool;
+    int state[RING_SLOTS] = {};  // 0 free, 1 copy in flight, 2 widening
+    std::atomic<int> left[RING_SLOTS];
+    const alp_ctx::HostCopy* job[RING_SLOTS] = {};
+    for (auto& l : left) l.store(0);
+    std::deque<int> flying;  // slots with a copy in flight, in issue order
     size_t next = 0;
-    while (next < ctx->landing.size()) {
-        const alp_ctx::Landing& l = ctx->landing[next];
-        const cudaError_t e = cudaEventQuery(l.ev);
-        if (e == cudaSuccess) {
-            ctx->pool->push(l.src, l.dst, l.n);
-            ++next;
-        } else if (e == cudaErrorNotReady) {
-            if (!ctx->pool->help()) std::this_thread::yield();
-        } else {
-            rc = fail(ctx, ALP_ERR_CUDA, "copy to the host: %s", cudaGetErrorString(e));
+    int rc = ALP_OK;
+    auto free_slot = [&]() -> int {
+        for (int k = 0; k < RING_SLOTS; ++k) {
+            if (state[k] == 2 && left[k].load(std::memory_order_acquire) == 0) state[k] = 0;
+            if (state[k] == 0) return k;
+        }
+        return -1;
+    };
+    while (!rc) {
+        for (; next < ctx->copies.size(); ++next) {
+            const alp_ctx::HostCopy& c = ctx->copies[next];
+            cudaError_t e;
+            if (!c.widen) {
+                e = cudaMemcpyAsync(c.dst, c.src, c.n, cudaMemcpyDeviceToHost, s);
+            } else {
+                const int k = free_slot();
+                if (k < 0) break;
+                e = cudaMemcpyAsync(ctx->h_ring + (size_t)k * RING_CHUNK, c.src, c.n * 4, cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_ring[k], s);
+                state[k] = 1;
+                job[k] = &c;
+                flying.push_back(k);
+            }
+            if (e != cudaSuccess) {
+                rc = fail(ctx, ALP_ERR_CUDA, "copy to the host: %s", cudaGetErrorString(e));
+                break;
+            }
+        }
+        if (rc) break;
+        if (!flying.empty()) {
+            const int k = flying.front();
+            const cudaError_t e = cudaEventQuery(ctx->ev_ring[k]);
+            if (e == cudaSuccess) {
+                flying.pop_front();
+                state[k] = 2;
+                left[k].store(HostPool::slices(job[k]->n), std::memory_order_relaxed);
+                pool.push(ctx->h_ring + (size_t)k * RING_CHUNK, (int64_t*)job[k]->dst, job[k]->n, &left[k]);
+                continue;
+            }
+            if (e != cudaErrorNotReady) {
+                rc = fail(ctx, ALP_ERR_CUDA, "copy to the host: %s", cudaGetErrorString(e));
+                break;
+            }
+        } else if (next == ctx->copies.size()) {
             break;
         }
+        if (!pool.help()) std::this_thread::yield();
     }
-    ctx->pool->wait();
-    ctx->landing.clear();
+    // on an error too: no slice may outlive the call, nor a copy into the ring
+    pool.wait();
+    ctx->copies.clear();
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (!rc && e != cudaSuccess) rc = fail(ctx, ALP_ERR_CUDA, "copy to the host: %s", cudaGetErrorString(e));
     return rc;
 }
 
@@ -1250,17 +1285,13 @@ int parse_positions(alp_ctx* ctx, long long L, long long nd, uint8_t* dvalid, Pa
         CK(cudaStreamWaitEvent(ctx->cp_out, ctx->ev_nodes, 0));
         h.started = true;
         if (N <= 0x7fffffffLL) {
-            // spans (in [0, 2^31): inputs are shorter) cross as 32-bit values and are widened
-            // on the host as they land; tags and kinds follow the parents (alp_parse_host)
-            if ((rc = grow(ctx, ctx->tmp[T_NARROW], (size_t)N * 12)) || (rc = grow_landing(ctx, (size_t)N * 12)))
-                return rc;
+            // spans (in [0, 2^31): inputs are shorter) to 32-bit values during the searches;
+            // alp_parse_host sends them with the parents, tags and kinds
+            if ((rc = grow(ctx, ctx->tmp[T_NARROW], (size_t)N * 12))) return rc;
             int32_t* d32 = (int32_t*)ctx->tmp[T_NARROW].p;
             narrow_i64_kernel<<<NARROW_GRID, 256, 0, ctx->cp_out>>>(o->start, o->end, N, d32, d32 + N);
             CK(cudaGetLastError());
             h.wide = true;
-            if ((rc = land(ctx, d32, ctx->h_narrow, h.start, N, ctx->cp_out)) ||
-                (rc = land(ctx, d32 + N, ctx->h_narrow + N, h.end, N, ctx->cp_out)))
-                return rc;
         } else {
             CK(cudaMemcpyAsync(h.tag, o->tag, (size_t)N * 4, cudaMemcpyDeviceToHost, ctx->cp_out));
             CK(cudaMemcpyAsync(h.kind, o->kind, (size_t)N, cudaMemcpyDeviceToHost, ctx->cp_out));
@@ -1536,8 +1567,9 @@ void alp_ctx_destroy(alp_ctx* ctx) {
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     if (ctx->ev_nodes) cudaEventDestroy(ctx->ev_nodes);
-    for (cudaEvent_t e : ctx->ev_chunks) cudaEventDestroy(e);
-    if (ctx->h_narrow) cudaFreeHost(ctx->h_narrow);
+    for (cudaEvent_t e : ctx->ev_ring)
+        if (e) cudaEventDestroy(e);
+    if (ctx->h_ring) cudaFreeHost(ctx->h_ring);
     delete ctx->pool;
     delete ctx;
 }
@@ -1981,14 +2013,33 @@ int alp_lex_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, uint32_t* h_term,
     if (n) CK(cudaMemcpyAsync(ctx->tmp[0].p, h_in, (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
     uint32_t* dt;
     int64_t *ds, *de;
+    ctx->last_h2d = n;
+    ctx->last_d2h = 0;
     rc = alp_lex(ctx, (const uint8_t*)ctx->tmp[0].p, n, &dt, &ds, &de, n_tok, valid);
     if (rc) return rc;
     if (*n_tok > cap) return fail(ctx, ALP_ERR_CAPACITY, "host token buffer too small");
-    if (*n_tok) {
-        CK(cudaMemcpyAsync(h_term, dt, (size_t)*n_tok * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(h_start, ds, (size_t)*n_tok * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(h_end, de, (size_t)*n_tok * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    const size_t M = (size_t)*n_tok;
+    if (M && M <= 0x7fffffffu) {
+        // spans (positions below 2^31) cross as 32-bit values, widened on the host
+        if ((rc = grow(ctx, ctx->tmp[T_NARROW], M * 8))) return rc;
+        int32_t* d32 = (int32_t*)ctx->tmp[T_NARROW].p;
+        narrow_i64_kernel<<<NARROW_GRID, 256, 0, ctx->stream>>>(ds, de, (long long)M, d32, d32 + M);
+        CK(cudaGetLastError());
+        ctx->copies.clear();
+        for (size_t c = 0; c < M; c += (size_t)RING_CHUNK) {
+            const size_t len = std::min((size_t)RING_CHUNK, M - c);
+            ctx->copies.push_back({d32 + c, h_start + c, len, true});
+            ctx->copies.push_back({d32 + M + c, h_end + c, len, true});
+            ctx->copies.push_back({dt + c, h_term + c, len * 4, false});
+        }
+        if ((rc = send_to_host(ctx, ctx->stream))) return rc;
+        ctx->last_d2h = (long long)M * 12;
+    } else if (M) {
+        CK(cudaMemcpyAsync(h_term, dt, M * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(h_start, ds, M * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(h_end, de, M * 8, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        ctx->last_d2h = (long long)M * 20;
     }
     return ALP_OK;
 }
@@ -2166,9 +2217,11 @@ int alp_lex_host_stream(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t pi
     CK(cudaSetDevice(ctx->device));
     const long long P = piece < n ? piece : ((n + 255) & ~255ll);
     const long long tcap = P + 1;  // tokens of one piece: one per byte at most, plus the last token
+    // positions below 2^31: spans cross as 32-bit values, widened on the host
+    const bool narrow = n <= 0x7fffffffLL;
     const size_t b_in = (size_t)P + 256, b_term = ((size_t)tcap * 4 + 255) & ~(size_t)255,
                  b_pos = ((size_t)tcap * 8 + 255) & ~(size_t)255;
-    const size_t b_slot = b_in + b_term + 2 * b_pos;
+    const size_t b_slot = b_in + b_term + 2 * b_pos + (narrow ? 2 * b_term : 0);
     if ((rc = grow(ctx, ctx->pipe, 2 * b_slot)) || (rc = grow(ctx, ctx->carry, sizeof(LexCarry)))) return rc;
     if (!ctx->cp_in) {
         CK(cudaStreamCreateWithFlags(&ctx->cp_in, cudaStreamNonBlocking));
@@ -2192,6 +2245,12 @@ int alp_lex_host_stream(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t pi
     auto term_of = [&](int k) { return reinterpret_cast<uint32_t*>(slots + k * b_slot + b_in); };
     auto start_of = [&](int k) { return reinterpret_cast<int64_t*>(slots + k * b_slot + b_in + b_term); };
     auto end_of = [&](int k) { return reinterpret_cast<int64_t*>(slots + k * b_slot + b_in + b_term + b_pos); };
+    auto s32_of = [&](int k) { return reinterpret_cast<int32_t*>(slots + k * b_slot + b_in + b_term + 2 * b_pos); };
+    auto e32_of = [&](int k) {
+        return reinterpret_cast<int32_t*>(slots + k * b_slot + b_in + 2 * b_term + 2 * b_pos);
+    };
+    ctx->last_h2d = n;
+    ctx->last_d2h = 0;
     const long long np = (n + P - 1) / P;
     long long copied = 0;  // tokens handed to the host so far
     bool overflow = false;
@@ -2204,10 +2263,23 @@ int alp_lex_host_stream(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t pi
         if (c.error & ALP_DEV_ERR_CAPACITY) return fail(ctx, ALP_ERR_CAPACITY, "piece token buffer too small");
         const long long m = c.piece;
         if (copied + m > cap) overflow = true;
-        if (!overflow && m > 0) {
+        if (!overflow && m > 0 && narrow) {
+            // the piece's tokens out through the ring, widened before the next piece's
+            ctx->copies.clear();
+            for (long long o = 0; o < m; o += RING_CHUNK) {
+                const size_t len = (size_t)std::min(RING_CHUNK, m - o);
+                ctx->copies.push_back({s32_of(k) + o, h_start + copied + o, len, true});
+                ctx->copies.push_back({e32_of(k) + o, h_end + copied + o, len, true});
+                ctx->copies.push_back({term_of(k) + o, h_term + copied + o, len * 4, false});
+            }
+            int r2 = send_to_host(ctx, ctx->cp_out);
+            if (r2) return r2;
+            ctx->last_d2h += m * 12;
+        } else if (!overflow && m > 0) {
             CK(cudaMemcpyAsync(h_term + copied, term_of(k), (size_t)m * 4, cudaMemcpyDeviceToHost, ctx->cp_out));
             CK(cudaMemcpyAsync(h_start + copied, start_of(k), (size_t)m * 8, cudaMemcpyDeviceToHost, ctx->cp_out));
             CK(cudaMemcpyAsync(h_end + copied, end_of(k), (size_t)m * 8, cudaMemcpyDeviceToHost, ctx->cp_out));
+            ctx->last_d2h += m * 20;
         }
         CK(cudaEventRecord(ctx->ev_out[k], ctx->cp_out));
         copied += m;
@@ -2226,6 +2298,11 @@ int alp_lex_host_stream(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t pi
             return rc;
         if (i == np - 1 && (rc = stream_end(ctx, d_carry, n, 0, 0, term_of(k), start_of(k), end_of(k), tcap)))
             return rc;
+        if (narrow) {
+            narrow_i64_kernel<<<NARROW_GRID, 256, 0, ctx->stream>>>(start_of(k), end_of(k), tcap, s32_of(k), e32_of(k),
+                                                                     &d_carry->piece);
+            CK(cudaGetLastError());
+        }
         CK(cudaMemcpyAsync(&ctx->h_carry[k], d_carry, sizeof(LexCarry), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaEventRecord(ctx->ev_done[k], ctx->stream));
         if (i >= 1 && (rc = retire(i - 1))) return rc;
@@ -2828,15 +2905,15 @@ int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_pare
     // return below waits for them, so that no copy outlives the call
     alp_ctx::HostTree ht{h_tag, h_kind, h_start, h_end, (long long)cap, false, false};
     ctx->host_tree = (cap > 0 && h_tag && h_kind && h_start && h_end) ? &ht : nullptr;
-    ctx->landing.clear();
+    ctx->copies.clear();
     ctx->last_h2d = n;
     ctx->last_d2h = 0;
     rc = parse_core(ctx, (const uint8_t*)ctx->tmp[T_HIN].p, n, &o, 0, 1, n_node, valid);
     ctx->host_tree = nullptr;
-    // no copy outlives the call, nor a landed chunk its widening
+    // no copy outlives the call
     auto join = [&]() -> int {
         if (ht.started) CK(cudaStreamSynchronize(ctx->cp_out));
-        ctx->landing.clear();
+        ctx->copies.clear();
         return ALP_OK;
     };
     if (rc) {
@@ -2849,21 +2926,27 @@ int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_pare
     }
     const size_t N = (size_t)*n_node;
     if (N && ht.wide) {
-        // parents (in [0, N)) narrowed after the searches and sent behind the spans; tags
-        // and kinds last, so that the widening of the parents overlaps their copy
-        int32_t* d32 = (int32_t*)ctx->tmp[T_NARROW].p + 2 * N;
-        narrow_i64_kernel<<<NARROW_GRID, 256, 0, ctx->stream>>>(o.parent, nullptr, (long long)N, d32, nullptr);
+        // parents (in [0, N)) to 32-bit values after the searches; then every field goes
+        // out chunk by chunk, the widened ones interleaved with the direct copies of tags
+        // and kinds so that the widening has the whole transfer to keep up
+        int32_t* d32 = (int32_t*)ctx->tmp[T_NARROW].p;
+        narrow_i64_kernel<<<NARROW_GRID, 256, 0, ctx->stream>>>(o.parent, nullptr, (long long)N, d32 + 2 * N,
+                                                                 nullptr);
         auto issue = [&]() -> int {
             CK(cudaGetLastError());
             CK(cudaEventRecord(ctx->ev_nodes, ctx->stream));
             CK(cudaStreamWaitEvent(ctx->cp_out, ctx->ev_nodes, 0));
-            int r2 = land(ctx, d32, ctx->h_narrow + 2 * N, h_parent, (long long)N, ctx->cp_out);
-            if (r2) return r2;
-            CK(cudaMemcpyAsync(h_tag, o.tag, N * 4, cudaMemcpyDeviceToHost, ctx->cp_out));
-            CK(cudaMemcpyAsync(h_kind, o.kind, N, cudaMemcpyDeviceToHost, ctx->cp_out));
-            return ALP_OK;
+            for (size_t c = 0; c < N; c += (size_t)RING_CHUNK) {
+                const size_t len = std::min((size_t)RING_CHUNK, N - c);
+                ctx->copies.push_back({d32 + c, h_start + c, len, true});
+                ctx->copies.push_back({d32 + N + c, h_end + c, len, true});
+                ctx->copies.push_back({d32 + 2 * N + c, h_parent + c, len, true});
+                ctx->copies.push_back({o.tag + c, h_tag + c, len * 4, false});
+                ctx->copies.push_back({o.kind + c, h_kind + c, len, false});
+            }
+            return send_to_host(ctx, ctx->cp_out);
         };
-        if ((rc = issue()) || (rc = drain_landing(ctx))) {
+        if ((rc = issue())) {
             join();
             return rc;
         }

@@ -532,6 +532,7 @@ def run_lex(args, rank: int, world: int, local: int):
     if n2.value != whole[0] or not all(torch.equal(o[:M], w) for o, w in zip(outs, whole[1])):
         raise RuntimeError("alp_lex_host_stream tokens differ from alp_lex_host")
     ms_e2e, _ = _timed(e2e_stream, max(1, min(args.steps, 5)), local, dist)
+    moved = _ctx_counts(g)  # the spans cross as 32-bit values
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -545,9 +546,11 @@ def run_lex(args, rank: int, world: int, local: int):
                   "l2": "inputs larger than L2 (no flush needed)", "seed": SEED_LEX,
                   "input_sha256": _sha256(doc)},
                  size + 20 * M, kern,
-                 {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": size,
-                  "d2h_bytes_per_step": 20 * M, "ms_per_step": ms_e2e,
+                 {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": moved["h2d"],
+                  "d2h_bytes_per_step": moved["d2h"], "ms_per_step": ms_e2e,
                   "api": "alp_lex_host_stream, 32 MiB pieces, pinned host buffers",
+                  "d2h_form": "i32 spans (sign-extended into the caller's i64 arrays on the host while later "
+                              "chunks are in flight), u32 ids",
                   "whole_input": {"api": "alp_lex_host", "value": _gbs(world, size, ms_whole),
                                   "ms_per_step": ms_whole}}, clocks,
                  units={"n": size, "m": M}, parse_layout=False)

@@ -65,8 +65,9 @@ int alp_set_stream(alp_ctx* ctx, void* stream);
  * [10] brackets, [11] brackets left for the bracket-matching search after
  * the pairs closed between adjacent positions are removed; [12] device
  * allocations (cudaMalloc calls) this context has made so far; [13], [14]
- * data bytes the last alp_parse_host call moved to the device (input) and to
- * the host (tree).  No reference counterpart (measurement support). */
+ * data bytes the last host-buffer call (alp_parse_host, alp_lex_host,
+ * alp_lex_host_stream) moved to the device (input) and to the host (tree or
+ * tokens).  No reference counterpart (measurement support). */
 int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out);
 
 /* Per-kernel timing (no reference counterpart; measurement support): when on,
@@ -116,7 +117,10 @@ int alp_lex(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t** d_term, int
             int64_t** d_end, int64_t* n_tok, int* valid);
 int alp_lex_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, uint32_t* d_term, int64_t* d_start,
                  int64_t* d_end, int64_t cap, int64_t* n_tok, int* valid);
-/* Same as alp_lex_into with host buffers: copies in, lexes, copies out. */
+/* Same as alp_lex_into with host buffers: copies in, lexes, copies out.  The
+ * spans of an input shorter than 2^31 bytes cross PCIe as 32-bit values and
+ * are widened on the host as they land (12 bytes a token instead of 20), as in
+ * alp_parse_host. */
 int alp_lex_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, uint32_t* h_term, int64_t* h_start,
                  int64_t* h_end, int64_t cap, int64_t* n_tok, int* valid);
 
@@ -251,7 +255,8 @@ void alp_parse_shard_free(alp_parse_shard* s);
  * one piece in, the lexing of the one before and the copy of the tokens of the
  * one before that out overlap on three CUDA streams.  Same results as
  * alp_lex_host, for inputs of any size; host buffers should be pinned
- * (cudaHostAlloc) for the copies to overlap. */
+ * (cudaHostAlloc) for the copies to overlap.  Below 2^31 bytes the spans cross
+ * as 32-bit values, widened on the host as they land. */
 int alp_lex_host_stream(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t piece, uint32_t* h_term,
                         int64_t* h_start, int64_t* h_end, int64_t cap, int64_t* n_tok, int* valid);
 
@@ -263,11 +268,12 @@ int alp_parse_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t* d_pare
                    uint8_t* d_kind, int64_t* d_start, int64_t* d_end, int64_t cap, int64_t* n_node,
                    int* valid);
 /* The same from and into host memory.  Parents and spans cross PCIe as 32-bit
- * values (17 bytes a node instead of 29) and host threads sign-extend them into
- * the caller's arrays as each 4 Mi-node chunk lands, while later chunks are
- * still in flight; the call returns when every output is written.  The threads
- * are the CPUs the process may run on, less the calling thread, or
- * ALP_HOST_THREADS when that is set (read once per context). */
+ * values (17 bytes a node instead of 29) into a 64 MiB ring of pinned slots,
+ * and host threads sign-extend each landed 1 Mi-value chunk into the caller's
+ * arrays while later chunks are still in flight; the call returns when every
+ * output is written.  The threads: the CPUs the process may run on, less the
+ * calling thread, at most six; or ALP_HOST_THREADS when that is set (read once
+ * per context). */
 int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_parent, uint32_t* h_tag,
                    uint8_t* h_kind, int64_t* h_start, int64_t* h_end, int64_t cap, int64_t* n_node,
                    int* valid);

@@ -163,8 +163,9 @@ def test_host_buffers_json_and_rejections(has_gpu):
 
 def test_host_widening_chunks(has_gpu):
     """alp_parse_host sends parents and spans as 32-bit values and widens them on the
-    host chunk by chunk (4 Mi nodes per copy, 256 Ki values per slice): a 32 MiB json
-    document (several chunks of each field, a partial last one) into pageable arrays,
+    host chunk by chunk (1 Mi values per copy through a ring of sixteen slots, 256 Ki
+    values per slice): a 32 MiB json document (nine chunks of each field, 45 copies in
+    all, so the ring wraps, and a partial last chunk and slice) into pageable arrays,
     into pinned arrays, and into arrays one element off a 32-byte boundary, with the
     default threads and with one; the bytes it reports moving match 17 per node."""
     import ctypes

@@ -152,10 +152,16 @@ def test_host_stream_vs_oracle(has_gpu, name):
 
 
 def test_host_stream_large_pinned(has_gpu):
+    """40 MiB through 8 MiB pieces into pinned buffers, against alp_lex_host and against
+    the device tokens of alp_lex (both host calls send the spans as 32-bit values and
+    widen them on the host; alp_lex's are the 64-bit device arrays)."""
     import torch
     g, _ = _ctx("json")
     data = _gen("json", (40 << 20) + 999, 91)
     want = g.lex_host(data)
+    dev = tuple(x.cpu().numpy() for x in g.lex_int(data))
+    assert len(want[0]) > 4 * (1 << 20)  # several 1 Mi-value chunks of each field
+    _same(want, dev)
     cap = len(data) + 1
     out = (torch.empty(cap, dtype=torch.int32).pin_memory(), torch.empty(cap, dtype=torch.int64).pin_memory(),
            torch.empty(cap, dtype=torch.int64).pin_memory())
