@@ -67,6 +67,7 @@ def native() -> ctypes.CDLL:
         L.alp_pre_productions.argtypes = [vp, vp, i64, P(vp), P(i64), P(i32)]
         L.alp_lex_batch.argtypes = [vp, vp, vp, i64, P(vp), P(vp), P(vp), P(vp), P(vp), P(i64)]
         L.alp_parse_batch.argtypes = [vp, vp, vp, i64, P(vp), P(vp), P(vp), P(vp), P(vp), P(vp), P(vp), P(i64)]
+        L.alp_parse_batch_host.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp, vp, vp, vp, i64, P(i64)]
         L.alp_lex_stream_begin.argtypes = [vp, vp, vp, vp, i64, P(vp)]
         L.alp_lex_stream_push.argtypes = [vp, vp, i64]
         L.alp_lex_stream_tokens.argtypes = [vp, P(i64)]
@@ -469,6 +470,33 @@ class Grammar:
         tree = self._tree(*ptrs[:5], k)
         return (tree, _wrap(self.h, ptrs[5].value or 0, nd + 1, torch.int64, self.device),
                 _wrap(self.h, ptrs[6].value or 0, nd, torch.uint8, self.device))
+
+
+    def parse_batch_host(self, data, offsets, cap: Optional[int] = None):
+        """alp_parse_batch_host: documents back to back in host memory ->
+        (parent, tag, kind, start, end, node_off, valid) numpy arrays; parents and
+        spans are relative to each document."""
+        arr = np.ascontiguousarray(data, dtype=np.uint8)
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        nd = len(off) - 1
+        # without a capacity: a guess of one node per byte, and the exact count on a retry
+        caps = [cap] if cap is not None else [len(arr) + 2 * nd + 1024, None]
+        node_off = np.empty(nd + 1, np.int64)
+        valid = np.empty(nd, np.uint8)
+        total = ctypes.c_int64(0)
+        self._stream()
+        vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        for c in caps:
+            c = total.value if c is None else c
+            outs = [np.empty(max(c, 1), dt) for dt in (np.int64, np.uint32, np.uint8, np.int64, np.int64)]
+            rc = native().alp_parse_batch_host(self.h, vp(arr), vp(off), nd, *[vp(o) for o in outs], vp(node_off),
+                                               vp(valid), c, ctypes.byref(total))
+            if rc != ALP_ERR_CAPACITY:
+                break
+        if rc != ALP_OK:
+            self._err(rc)
+        k = total.value
+        return tuple(o[:k] for o in outs) + (node_off, valid)
 
 
 class TokenStream:

@@ -602,7 +602,7 @@ enum {
     T_HIN = 0, T_TTERM, T_TSTART, T_TEND, T_PID, T_TSUMS, T_VBUF, T_BRBUF, T_DSBUF,
     T_N_TMIN, T_N_M32, T_N_M1024, T_N_SVAL, T_N_SIDX, T_N_SLEN, T_N_ESC,
     T_B_TMIN, T_B_M32, T_B_M1024, T_B_SVAL, T_B_SIDX, T_B_SLEN, T_B_ESC,
-    T_DOCOFF, T_TOKOFF, T_NODEOFF, T_BROFF, T_DVALID, T_NARROW, T_CNT
+    T_DOCOFF, T_TOKOFF, T_NODEOFF, T_BROFF, T_DVALID, T_NARROW, T_HOFF, T_CNT
 };
 
 struct ParseOut {
@@ -1491,6 +1491,84 @@ inline unsigned grid_for(long long n) {
     long long g = (n + 255) / 256;
     if (g > 148 * 16) g = 148 * 16;
     return (unsigned)(g < 1 ? 1 : g);
+}
+
+// The tail of alp_parse_host and alp_parse_batch_host: after the parse (rc) the
+// tree's N nodes to the caller's host arrays (capacity cap), with parents and
+// spans as 32-bit values widened on the host when parse_positions narrowed the
+// spans (ht.wide), else as plain copies.  Waits for every copy in either case.
+int tree_to_host(alp_ctx* ctx, int rc, const ParseOut& o, int64_t n_node, int64_t cap, alp_ctx::HostTree& ht,
+                 int64_t* h_parent) {
+    auto join = [&]() -> int {
+        if (ht.started) CK(cudaStreamSynchronize(ctx->cp_out));
+        ctx->copies.clear();
+        return ALP_OK;
+    };
+    if (rc) {
+        join();
+        return rc;
+    }
+    if (n_node > cap) {
+        join();
+        return fail(ctx, ALP_ERR_CAPACITY, "host node buffer too small");
+    }
+    const size_t N = (size_t)n_node;
+    if (N && ht.wide) {
+        // parents (in [0, N)) to 32-bit values after the searches; then every field goes
+        // out chunk by chunk, the widened ones interleaved with the direct copies of tags
+        // and kinds so that the widening has the whole transfer to keep up
+        int32_t* d32 = (int32_t*)ctx->tmp[T_NARROW].p;
+        narrow_i64_kernel<<<NARROW_GRID, 256, 0, ctx->stream>>>(o.parent, nullptr, (long long)N, d32 + 2 * N,
+                                                                 nullptr);
+        auto issue = [&]() -> int {
+            CK(cudaGetLastError());
+            CK(cudaEventRecord(ctx->ev_nodes, ctx->stream));
+            CK(cudaStreamWaitEvent(ctx->cp_out, ctx->ev_nodes, 0));
+            for (size_t c = 0; c < N; c += (size_t)RING_CHUNK) {
+                const size_t len = std::min((size_t)RING_CHUNK, N - c);
+                ctx->copies.push_back({d32 + c, ht.start + c, len, true});
+                ctx->copies.push_back({d32 + N + c, ht.end + c, len, true});
+                ctx->copies.push_back({d32 + 2 * N + c, h_parent + c, len, true});
+                ctx->copies.push_back({o.tag + c, ht.tag + c, len * 4, false});
+                ctx->copies.push_back({o.kind + c, ht.kind + c, len, false});
+            }
+            return send_to_host(ctx, ctx->cp_out);
+        };
+        if ((rc = issue())) {
+            join();
+            return rc;
+        }
+        ctx->last_d2h += (long long)N * 17;
+    } else if (N) {
+        CK(cudaMemcpyAsync(h_parent, o.parent, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        if (!ht.started) {
+            CK(cudaMemcpyAsync(ht.tag, o.tag, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaMemcpyAsync(ht.kind, o.kind, N, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaMemcpyAsync(ht.start, o.start, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaMemcpyAsync(ht.end, o.end, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        CK(cudaStreamSynchronize(ctx->stream));
+        ctx->last_d2h += (long long)N * 29;
+    }
+    return join();
+}
+
+// alp_parse_batch after its argument checks: n bytes of documents at d_in with
+// offsets d_off[0..n_docs] (both on the device); the tree in o, N nodes.
+int parse_batch_core(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int64_t n_docs, int64_t n, ParseOut* o,
+                     int64_t* N) {
+    int rc;
+    const size_t tcap = (size_t)n + 2 * (size_t)n_docs + 16;
+    if ((rc = grow(ctx, ctx->tmp[T_TTERM], tcap * 2)) || (rc = grow(ctx, ctx->tmp[T_TSTART], tcap * 4)) ||
+        (rc = grow(ctx, ctx->tmp[T_TEND], tcap * 4)) || (rc = grow(ctx, ctx->tmp[T_DVALID], (size_t)n_docs + 16)))
+        return rc;
+    uint8_t* dvalid = (uint8_t*)ctx->tmp[T_DVALID].p;
+    long long m = 0;
+    rc = lex_seg<uint16_t, uint32_t>(ctx, d_in, n, (const long long*)d_off, n_docs, 1, (uint16_t*)ctx->tmp[T_TTERM].p,
+                                     (uint32_t*)ctx->tmp[T_TSTART].p, (uint32_t*)ctx->tmp[T_TEND].p, (long long)tcap,
+                                     dvalid, &m);
+    if (rc) return rc;
+    return parse_positions(ctx, m + 2 * n_docs, n_docs, dvalid, o, 0, 1, N, 1);
 }
 
 }  // namespace
@@ -2901,8 +2979,8 @@ int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_pare
     if ((rc = grow(ctx, ctx->tmp[T_HIN], (size_t)n + 16))) return rc;
     if (n) CK(cudaMemcpyAsync(ctx->tmp[T_HIN].p, h_in, (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
     ParseOut o{};
-    // tags, kinds and spans may start to the host during the searches (on cp_out); every
-    // return below waits for them, so that no copy outlives the call
+    // spans may be narrowed for the host during the searches (on cp_out); every return
+    // below waits for that stream, so that no copy outlives the call
     alp_ctx::HostTree ht{h_tag, h_kind, h_start, h_end, (long long)cap, false, false};
     ctx->host_tree = (cap > 0 && h_tag && h_kind && h_start && h_end) ? &ht : nullptr;
     ctx->copies.clear();
@@ -2910,59 +2988,7 @@ int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_pare
     ctx->last_d2h = 0;
     rc = parse_core(ctx, (const uint8_t*)ctx->tmp[T_HIN].p, n, &o, 0, 1, n_node, valid);
     ctx->host_tree = nullptr;
-    // no copy outlives the call
-    auto join = [&]() -> int {
-        if (ht.started) CK(cudaStreamSynchronize(ctx->cp_out));
-        ctx->copies.clear();
-        return ALP_OK;
-    };
-    if (rc) {
-        join();
-        return rc;
-    }
-    if (*n_node > cap) {
-        join();
-        return fail(ctx, ALP_ERR_CAPACITY, "host node buffer too small");
-    }
-    const size_t N = (size_t)*n_node;
-    if (N && ht.wide) {
-        // parents (in [0, N)) to 32-bit values after the searches; then every field goes
-        // out chunk by chunk, the widened ones interleaved with the direct copies of tags
-        // and kinds so that the widening has the whole transfer to keep up
-        int32_t* d32 = (int32_t*)ctx->tmp[T_NARROW].p;
-        narrow_i64_kernel<<<NARROW_GRID, 256, 0, ctx->stream>>>(o.parent, nullptr, (long long)N, d32 + 2 * N,
-                                                                 nullptr);
-        auto issue = [&]() -> int {
-            CK(cudaGetLastError());
-            CK(cudaEventRecord(ctx->ev_nodes, ctx->stream));
-            CK(cudaStreamWaitEvent(ctx->cp_out, ctx->ev_nodes, 0));
-            for (size_t c = 0; c < N; c += (size_t)RING_CHUNK) {
-                const size_t len = std::min((size_t)RING_CHUNK, N - c);
-                ctx->copies.push_back({d32 + c, h_start + c, len, true});
-                ctx->copies.push_back({d32 + N + c, h_end + c, len, true});
-                ctx->copies.push_back({d32 + 2 * N + c, h_parent + c, len, true});
-                ctx->copies.push_back({o.tag + c, h_tag + c, len * 4, false});
-                ctx->copies.push_back({o.kind + c, h_kind + c, len, false});
-            }
-            return send_to_host(ctx, ctx->cp_out);
-        };
-        if ((rc = issue())) {
-            join();
-            return rc;
-        }
-        ctx->last_d2h = (long long)N * 17;
-    } else if (N) {
-        CK(cudaMemcpyAsync(h_parent, o.parent, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        if (!ht.started) {
-            CK(cudaMemcpyAsync(h_tag, o.tag, N * 4, cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaMemcpyAsync(h_kind, o.kind, N, cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaMemcpyAsync(h_start, o.start, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaMemcpyAsync(h_end, o.end, N * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        }
-        CK(cudaStreamSynchronize(ctx->stream));
-        ctx->last_d2h = (long long)N * 29;
-    }
-    return join();
+    return tree_to_host(ctx, rc, o, *n_node, cap, ht, h_parent);
 }
 
 int alp_parse_tokens(alp_ctx* ctx, const uint32_t* d_term, const int64_t* d_tstart, const int64_t* d_tend, int64_t m,
@@ -3439,20 +3465,10 @@ int alp_parse_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int
     const int64_t n = ctx->h_stage[0];
     int rc = check_in(ctx, d_in, n, true);
     if (rc) return rc;
-    const size_t tcap = (size_t)n + 2 * (size_t)n_docs + 16;
-    if ((rc = grow(ctx, ctx->tmp[T_TTERM], tcap * 2)) || (rc = grow(ctx, ctx->tmp[T_TSTART], tcap * 4)) ||
-        (rc = grow(ctx, ctx->tmp[T_TEND], tcap * 4)) || (rc = grow(ctx, ctx->tmp[T_DVALID], (size_t)n_docs + 16)))
-        return rc;
-    uint8_t* dvalid = (uint8_t*)ctx->tmp[T_DVALID].p;
-    long long m = 0;
-    rc = lex_seg<uint16_t, uint32_t>(ctx, d_in, n, (const long long*)d_off, n_docs, 1, (uint16_t*)ctx->tmp[T_TTERM].p,
-                                     (uint32_t*)ctx->tmp[T_TSTART].p, (uint32_t*)ctx->tmp[T_TEND].p, (long long)tcap,
-                                     dvalid, &m);
-    if (rc) return rc;
     ParseOut o{};
     int64_t N = 0;
-    rc = parse_positions(ctx, m + 2 * n_docs, n_docs, dvalid, &o, 0, 1, &N, 1);
-    if (rc) return rc;
+    if ((rc = parse_batch_core(ctx, d_in, d_off, n_docs, n, &o, &N))) return rc;
+    uint8_t* dvalid = (uint8_t*)ctx->tmp[T_DVALID].p;
     *d_parent = o.parent;
     *d_tag = o.tag;
     *d_kind = o.kind;
@@ -3461,6 +3477,46 @@ int alp_parse_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int
     *d_node_off = (int64_t*)ctx->tmp[T_NODEOFF].p;
     *d_valid = dvalid;
     *n_node_total = N;
+    return ALP_OK;
+}
+
+int alp_parse_batch_host(alp_ctx* ctx, const uint8_t* h_in, const int64_t* h_off, int64_t n_docs, int64_t* h_parent,
+                         uint32_t* h_tag, uint8_t* h_kind, int64_t* h_start, int64_t* h_end, int64_t* h_node_off,
+                         uint8_t* h_valid, int64_t cap, int64_t* n_node_total) {
+    if (!ctx) return ALP_ERR_ARG;
+    if (n_docs < 1 || !h_off || !h_node_off || !h_valid || !n_node_total || cap < 0 ||
+        (cap > 0 && (!h_parent || !h_tag || !h_kind || !h_start || !h_end)))
+        return fail(ctx, ALP_ERR_ARG, "bad batch arguments");
+    if (!ctx->has_lexer || !ctx->has_parser) return fail(ctx, ALP_ERR_MODE, "these tables are not lexer+parser tables");
+    *n_node_total = 0;
+    if (h_off[0] != 0) return fail(ctx, ALP_ERR_ARG, "offsets must start at 0");
+    for (int64_t i = 0; i < n_docs; ++i)
+        if (h_off[i + 1] < h_off[i]) return fail(ctx, ALP_ERR_ARG, "offsets must not decrease");
+    const int64_t n = h_off[n_docs];
+    int rc = check_in(ctx, h_in, n, true);
+    if (rc) return rc;
+    CK(cudaSetDevice(ctx->device));
+    const size_t b_off = (size_t)(n_docs + 1) * 8;
+    if ((rc = grow(ctx, ctx->tmp[T_HIN], (size_t)n + 16)) || (rc = grow(ctx, ctx->tmp[T_HOFF], b_off))) return rc;
+    if (n) CK(cudaMemcpyAsync(ctx->tmp[T_HIN].p, h_in, (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->tmp[T_HOFF].p, h_off, b_off, cudaMemcpyHostToDevice, ctx->stream));
+    ParseOut o{};
+    alp_ctx::HostTree ht{h_tag, h_kind, h_start, h_end, (long long)cap, false, false};
+    ctx->host_tree = cap > 0 ? &ht : nullptr;
+    ctx->copies.clear();
+    ctx->last_h2d = n + (long long)b_off;
+    ctx->last_d2h = 0;
+    int64_t N = 0;
+    rc = parse_batch_core(ctx, (const uint8_t*)ctx->tmp[T_HIN].p, (const int64_t*)ctx->tmp[T_HOFF].p, n_docs, n, &o,
+                          &N);
+    ctx->host_tree = nullptr;
+    *n_node_total = N;
+    if ((rc = tree_to_host(ctx, rc, o, N, cap, ht, h_parent))) return rc;
+    // the per-document node offsets and validity
+    CK(cudaMemcpyAsync(h_node_off, ctx->tmp[T_NODEOFF].p, b_off, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(h_valid, ctx->tmp[T_DVALID].p, (size_t)n_docs, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->last_d2h += (long long)b_off + n_docs;
     return ALP_OK;
 }
 

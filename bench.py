@@ -601,33 +601,44 @@ def run_batch(args, rank: int, world: int, local: int):
         st["counts"] = _ctx_counts(st["g"])
         valid = _wrap_valid(st)
         st["accepted"] = int(valid.sum())
-    # end to end: inputs and offsets from pinned host memory, the trees, node
+    # end to end through alp_parse_batch_host: documents and offsets from pinned host
+    # memory, the trees (parents and spans as 32-bit values widened on the host), node
     # offsets and validity back to pinned host memory, all inside the timed region
-    h2d = d2h = 0
     for st in sets:
         N, D = st["N"].value, st["n_docs"]
         st["h_x"] = torch.from_numpy(st["data"]).pin_memory()
         st["h_o"] = torch.from_numpy(st["off"]).pin_memory()
-        st["d_x"] = torch.empty_like(st["x"])
-        st["d_o"] = torch.empty_like(st["o"])
         st["h_out"] = [torch.empty(N * w, dtype=torch.uint8, pin_memory=True) for w in (8, 4, 1, 8, 8)]
         st["h_noff"] = torch.empty((D + 1) * 8, dtype=torch.uint8, pin_memory=True)
         st["h_valid"] = torch.empty(D, dtype=torch.uint8, pin_memory=True)
-        h2d += st["h_x"].numel() + st["h_o"].numel() * 8
-        d2h += N * 29 + (D + 1) * 8 + D
+    L.alp_parse_batch_host.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] + [ctypes.c_void_p] * 7 + \
+        [ctypes.c_int64, ctypes.c_void_p]
+    h_total = ctypes.c_int64(0)
+
     def e2e_step():
         for st in sets:
-            st["d_x"].copy_(st["h_x"], non_blocking=True)
-            st["d_o"].copy_(st["h_o"], non_blocking=True)
-            call(st, st["d_x"], st["d_o"])
-            outs = [p.value for p in st["ptrs"]]
-            for dst, src in zip(st["h_out"] + [st["h_noff"], st["h_valid"]], outs):
-                if dst.numel() and L.alp_memcpy(st["g"].h, ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(src),
-                                                dst.numel()) != 0:
-                    raise RuntimeError("alp_memcpy failed")
+            ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+            rc = L.alp_parse_batch_host(st["g"].h, ptr(st["h_x"]), ptr(st["h_o"]), st["n_docs"],
+                                        *[ptr(t) for t in st["h_out"]], ptr(st["h_noff"]), ptr(st["h_valid"]),
+                                        st["N"].value, ctypes.byref(h_total))
+            if rc != 0 or h_total.value != st["N"].value:
+                raise RuntimeError("alp_parse_batch_host failed rc=%d" % rc)
 
     e2e_step()
     ms_e2e, _ = _timed(e2e_step, max(1, min(args.steps, 3)), local, dist)
+    h2d = d2h = 0
+    for st in sets:
+        moved = _ctx_counts(st["g"])
+        h2d += moved["h2d"]
+        d2h += moved["d2h"]
+    # the host arrays of the last e2e call, byte for byte, against alp_parse_batch's on the device
+    for st in sets:
+        tree, noff, val = st["g"].parse_batch_int(st["x"], st["o"])
+        dev = [tree.parent, tree.tag, tree.kind, tree.start, tree.end, noff, val]
+        for h, d in zip(st["h_out"] + [st["h_noff"], st["h_valid"]], dev):
+            if not torch.equal(h.to(d.device), d.contiguous().view(torch.uint8)):
+                raise RuntimeError("alp_parse_batch_host output differs from alp_parse_batch")
+        del tree, noff, val, dev
 
     # the same batches captured once each as a CUDA graph (alp_parse_graph_*),
     # replayed; outputs compared with alp_parse_batch's on the device
@@ -686,7 +697,8 @@ def run_batch(args, rank: int, world: int, local: int):
     line = _line("input GB/s batched lex+parse (json.alp + sexp.alp documents, bit-exact)",
                  _gbs(world, n_bytes, ms), world, args, ms, cfg, alg, kern,
                  {"value": _gbs(world, n_bytes, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": h2d,
-                  "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e}, clocks, units=units)
+                  "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e, "api": "alp_parse_batch_host, pinned buffers",
+                  "bit_exact_vs_device": True}, clocks, units=units)
     line["path_roofline"]["scope"] = ("both alp_parse_batch calls: input bytes + 29 B per node + 17 B per "
                                       "document (offsets in, node offsets and validity out), over the step time")
     if graph:

@@ -65,9 +65,9 @@ int alp_set_stream(alp_ctx* ctx, void* stream);
  * [10] brackets, [11] brackets left for the bracket-matching search after
  * the pairs closed between adjacent positions are removed; [12] device
  * allocations (cudaMalloc calls) this context has made so far; [13], [14]
- * data bytes the last host-buffer call (alp_parse_host, alp_lex_host,
- * alp_lex_host_stream) moved to the device (input) and to the host (tree or
- * tokens).  No reference counterpart (measurement support). */
+ * data bytes the last host-buffer call (alp_parse_host, alp_parse_batch_host,
+ * alp_lex_host, alp_lex_host_stream) moved to the device (input) and to the
+ * host (tree or tokens).  No reference counterpart (measurement support). */
 int alp_ctx_info(const alp_ctx* ctx, int64_t* out, int n_out);
 
 /* Per-kernel timing (no reference counterpart; measurement support): when on,
@@ -328,6 +328,15 @@ int alp_lex_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int64
 int alp_parse_batch(alp_ctx* ctx, const uint8_t* d_in, const int64_t* d_off, int64_t n_docs,
                     int64_t** d_parent, uint32_t** d_tag, uint8_t** d_kind, int64_t** d_start,
                     int64_t** d_end, int64_t** d_node_off, uint8_t** d_valid, int64_t* n_node_total);
+/* alp_parse_batch from and into host memory: h_off[0..n_docs] (starting at 0, not
+ * decreasing) on the host, the trees' nodes into arrays of capacity cap (the
+ * node total is set, with ALP_ERR_CAPACITY, when cap is short), h_node_off[n_docs
+ * + 1] and h_valid[n_docs].  Parents and spans cross PCIe as 32-bit values widened
+ * on the host, as in alp_parse_host. */
+int alp_parse_batch_host(alp_ctx* ctx, const uint8_t* h_in, const int64_t* h_off, int64_t n_docs,
+                         int64_t* h_parent, uint32_t* h_tag, uint8_t* h_kind, int64_t* h_start,
+                         int64_t* h_end, int64_t* h_node_off, uint8_t* h_valid, int64_t cap,
+                         int64_t* n_node_total);
 
 /* The reference's test wire format, written from batch results in host memory
  * (host code only, no GPU work): the `.outputs` files that `alpacc test`

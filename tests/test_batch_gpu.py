@@ -109,6 +109,58 @@ def test_parse_batch(has_gpu, name):
     assert n_valid > 300
 
 
+@pytest.mark.parametrize("name", ["json", "sexp"])
+def test_parse_batch_host(has_gpu, name):
+    """alp_parse_batch_host (host offsets in, parents and spans back as 32-bit values
+    widened on the host): the same arrays as alp_parse_batch on the device, for a batch
+    with empty, rejected and broken documents and one large enough for several copy
+    chunks; every accepted document against the oracle; a short capacity reports the
+    node total; offsets that decrease are refused."""
+    import ctypes
+    from alpacc_b200 import api
+    g, o = _ctx(name, "both")
+    good, bad = _special(name)
+    docs = _docs(name, 300, 93)
+    for i in range(0, 30, 3):
+        d = bytearray(docs[i])
+        j = max((k for k, c in enumerate(d) if c in b")]}"), default=None)
+        if j is not None:
+            del d[j]
+            docs[i] = bytes(d)
+    big = synth.json_doc(12 << 20, 16, 95) if name == "json" else synth.sexp_doc(12 << 20, 20, 95)
+    docs = _layout(name, docs + good + bad + [big.tobytes()])
+    data, off = _pack(docs)
+    tree, node_off, valid = g.parse_batch_int(data, off)
+    want = [x.cpu().numpy() for x in (tree.parent, tree.tag, tree.kind, tree.start, tree.end)]
+    want_off, want_valid = node_off.cpu().numpy(), valid.cpu().numpy()
+    got = g.parse_batch_host(data, off)
+    assert len(got[0]) == len(want[0]) > (1 << 21)
+    for a, b in zip(got[:5], want):
+        np.testing.assert_array_equal(a, b.astype(a.dtype))
+    np.testing.assert_array_equal(got[5], want_off)
+    np.testing.assert_array_equal(got[6], want_valid)
+    for i in list(range(0, 60)) + [len(docs) - 3]:
+        w = o.lex_parse(docs[i])
+        assert bool(got[6][i]) == (w is not None)
+        if w is not None:
+            a, b = got[5][i], got[5][i + 1]
+            for x, y in zip(got[:5], w):
+                np.testing.assert_array_equal(x[a:b], y)
+    L = api.native()
+    total = ctypes.c_int64(0)
+    bufs = [np.empty(16, dt) for dt in (np.int64, np.uint32, np.uint8, np.int64, np.int64)]
+    no, nv = np.empty(len(docs) + 1, np.int64), np.empty(len(docs), np.uint8)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = L.alp_parse_batch_host(g.h, vp(data), vp(off), len(docs), *[vp(b) for b in bufs], vp(no), vp(nv), 16,
+                                ctypes.byref(total))
+    assert rc == 5 and total.value == len(want[0])
+    off2 = off.copy()
+    off2[3], off2[4] = off2[4], off2[3] - 1
+    rc = L.alp_parse_batch_host(g.h, vp(data), vp(off2), len(docs), *[vp(b) for b in bufs], vp(no), vp(nv), 16,
+                                ctypes.byref(total))
+    assert rc == 1
+
+
 def test_single_doc_batch_equals_parse(has_gpu):
     g, o = _ctx("json", "both")
     d = synth.json_doc(300000, 16, 12345)
