@@ -54,7 +54,7 @@ struct DevBuf {
 // ---------------------------------------------------------------------------
 constexpr size_t WIDEN_SLICE = (size_t)1 << 18;
 constexpr int RING_SLOTS = 16;
-constexpr int HOST_WORKERS = 6;
+constexpr int HOST_WORKERS = 8;
 constexpr long long RING_CHUNK = 1LL << 20;
 
 __attribute__((target("avx2"))) void widen_avx2(const int32_t* s, int64_t* d, size_t n) {

@@ -272,7 +272,7 @@ int alp_parse_into(alp_ctx* ctx, const uint8_t* d_in, int64_t n, int64_t* d_pare
  * and host threads sign-extend each landed 1 Mi-value chunk into the caller's
  * arrays while later chunks are still in flight; the call returns when every
  * output is written.  The threads: the CPUs the process may run on, less the
- * calling thread, at most six; or ALP_HOST_THREADS when that is set (read once
+ * calling thread, at most eight; or ALP_HOST_THREADS when that is set (read once
  * per context). */
 int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_parent, uint32_t* h_tag,
                    uint8_t* h_kind, int64_t* h_start, int64_t* h_end, int64_t cap, int64_t* n_node,
