@@ -531,6 +531,14 @@ def run_lex(args, rank: int, world: int, local: int):
     e2e_stream()
     if n2.value != whole[0] or not all(torch.equal(o[:M], w) for o, w in zip(outs, whole[1])):
         raise RuntimeError("alp_lex_host_stream tokens differ from alp_lex_host")
+    # both host calls widen 32-bit spans on the host: their tokens against alp_lex's
+    # 64-bit device arrays, element for element
+    step()
+    dev = [api._wrap(g.h, p.value, M, dt, f"cuda:{local}") for p, dt in zip(ptrs, (torch.int32, torch.int64,
+                                                                                     torch.int64))]
+    if not all(torch.equal(o[:M].to(d.device), d) for o, d in zip(outs, dev)):
+        raise RuntimeError("alp_lex_host_stream tokens differ from alp_lex's device arrays")
+    del dev
     ms_e2e, _ = _timed(e2e_stream, max(1, min(args.steps, 5)), local, dist)
     moved = _ctx_counts(g)  # the spans cross as 32-bit values
     if dist:
@@ -550,7 +558,7 @@ def run_lex(args, rank: int, world: int, local: int):
                   "d2h_bytes_per_step": moved["d2h"], "ms_per_step": ms_e2e,
                   "api": "alp_lex_host_stream, 32 MiB pieces, pinned host buffers",
                   "d2h_form": "i32 spans (sign-extended into the caller's i64 arrays on the host while later "
-                              "chunks are in flight), u32 ids",
+                              "chunks are in flight), u32 ids", "bit_exact_vs_device": True,
                   "whole_input": {"api": "alp_lex_host", "value": _gbs(world, size, ms_whole),
                                   "ms_per_step": ms_whole}}, clocks,
                  units={"n": size, "m": M}, parse_layout=False)
