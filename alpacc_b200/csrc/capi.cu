@@ -1945,6 +1945,96 @@ int alp_write_reference_format(int mode, int64_t n_docs, const uint8_t* valid, c
     return ALP_OK;
 }
 
+// The check of lexerTestsCompare / lexerParserTestsCompare / parserTestsCompare
+// (src/Alpacc/Test/Lexer.hs:181-231, LexerParser.hs:342-392, Parser.hs:140-167):
+// equal numbers of results, then the results equal input by input.
+int alp_compare_reference_format(int mode, const uint8_t* a, size_t a_len, const uint8_t* b, size_t b_len,
+                                 int64_t* first_diff, int* field) {
+    if (!first_diff || !field || (a_len && !a) || (b_len && !b)) return ALP_ERR_ARG;
+    *first_diff = -1;
+    *field = -1;
+    int nf;
+    switch (mode) {
+        case ALP_WIRE_LEXER: nf = 3; break;
+        case ALP_WIRE_LEXPARSE: nf = 5; break;
+        case ALP_WIRE_PARSER: nf = 1; break;
+        default: return ALP_ERR_ARG;
+    }
+    const size_t rec = mode == ALP_WIRE_LEXER ? 24 : (mode == ALP_WIRE_LEXPARSE ? 33 : 8);
+    // one file's inputs: (accepted, element count, first record); false when malformed
+    // (truncated, a boolean or kind byte out of range, bytes after the last input)
+    struct Item {
+        bool ok;
+        uint64_t n;
+        const uint8_t* r;
+    };
+    auto u64 = [](const uint8_t* q) {
+        uint64_t v = 0;
+        for (int k = 0; k < 8; ++k) v = v << 8 | q[k];
+        return v;
+    };
+    auto scan = [&](const uint8_t* f, size_t len, std::vector<Item>& items) -> bool {
+        if (len < 8) return false;
+        const uint64_t count = u64(f);
+        size_t p = 8;
+        if (count > len) return false;  // at least one byte per input
+        items.reserve((size_t)count);
+        for (uint64_t i = 0; i < count; ++i) {
+            if (p >= len || f[p] > 1) return false;
+            if (!f[p++]) {
+                items.push_back({false, 0, nullptr});
+                continue;
+            }
+            if (len - p < 8) return false;
+            const uint64_t n = u64(f + p);
+            p += 8;
+            if (n > (len - p) / rec) return false;
+            if (mode == ALP_WIRE_LEXPARSE)
+                for (uint64_t e = 0; e < n; ++e)
+                    if (f[p + e * rec] > 1) return false;
+            items.push_back({true, n, f + p});
+            p += (size_t)n * rec;
+        }
+        return p == len;
+    };
+    std::vector<Item> x, y;
+    if (!scan(a, a_len, x) || !scan(b, b_len, y)) return ALP_ERR_ARG;
+    // different numbers of results fail before any result is compared
+    const size_t m = std::min(x.size(), y.size());
+    if (x.size() != y.size()) {
+        *first_diff = (int64_t)m;
+        return ALP_OK;
+    }
+    for (size_t i = 0; i < m; ++i) {
+        if (x[i].ok != y[i].ok || x[i].n != y[i].n) {
+            *first_diff = (int64_t)i;
+            return ALP_OK;
+        }
+        if (!x[i].ok) continue;
+        // the first differing field of the first differing record, in record order
+        // (lexer: term, start, end; lexer+parser: kind, parent, id, start, end)
+        for (uint64_t e = 0; e < x[i].n; ++e) {
+            const uint8_t *u = x[i].r + e * rec, *v = y[i].r + e * rec;
+            if (memcmp(u, v, rec) == 0) continue;
+            *first_diff = (int64_t)i;
+            int k = 0, o = 0;
+            if (mode == ALP_WIRE_LEXPARSE) {
+                if (u[0] != v[0]) {
+                    *field = 0;
+                    return ALP_OK;
+                }
+                k = 1;
+                o = 1;
+            }
+            for (; k < nf; ++k, o += 8)
+                if (memcmp(u + o, v + o, 8) != 0) break;
+            *field = k;
+            return ALP_OK;
+        }
+    }
+    return ALP_OK;
+}
+
 int alp_memcpy(alp_ctx* ctx, void* dst, const void* src, size_t bytes) {
     if (!ctx || (bytes && (!dst || !src))) return ALP_ERR_ARG;
     CK(cudaSetDevice(ctx->device));

@@ -364,6 +364,21 @@ int alp_write_reference_format(int mode, int64_t n_docs, const uint8_t* valid, c
                                const int64_t* start, const int64_t* end, uint8_t* out, size_t cap,
                                size_t* len);
 
+/* The comparison `alpacc test compare` makes (src/Alpacc/Test/Lexer.hs:181-231,
+ * LexerParser.hs:342-392, Parser.hs:140-167), on two such files held in host
+ * memory (host code only): *first_diff = -1 when every input has the same
+ * result, else the first input whose result differs (accepted in one file and
+ * rejected in the other, a different element count, or a different element);
+ * files with different numbers of results differ at the first input only one
+ * of them has, whatever the shared ones hold.  *field names the first
+ * differing field of the first differing element, in record order (lexer:
+ * term, start, end; lexer+parser: kind, parent, id, start, end; parser: the
+ * production), else -1.  ALP_ERR_ARG for an unknown mode or a malformed file
+ * (truncated, a boolean or kind byte other than 0 or 1, bytes after the last
+ * input). */
+int alp_compare_reference_format(int mode, const uint8_t* a, size_t a_len, const uint8_t* b, size_t b_len,
+                                 int64_t* first_diff, int* field);
+
 /* The batched parse as a CUDA graph (no reference counterpart).  alp_parse_batch
  * waits on the host three times (input size, token total, node and bracket
  * totals) to size its outputs; for a fixed batch shape this set-up captures the

@@ -177,3 +177,70 @@ def test_c_abi_writer_errors():
     assert f(0, 1, _ptr(valid), _ptr(off), _ptr(ids), None, None, None, None, None, 0, ctypes.byref(n)) == 1
     bad = np.array([2, 1], np.int64)
     assert f(2, 1, _ptr(valid), _ptr(bad), _ptr(ids), None, None, None, None, None, 0, ctypes.byref(n)) == 1
+
+
+def _c_compare():
+    import ctypes
+    from alpacc_b200 import build
+    lib = ctypes.CDLL(build.build_cuda())
+    f = lib.alp_compare_reference_format
+    f.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t,
+                  ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int)]
+
+    def cmp(mode, a: bytes, b: bytes):
+        d, k = ctypes.c_int64(7), ctypes.c_int(7)
+        rc = f(mode, a, len(a), b, len(b), ctypes.byref(d), ctypes.byref(k))
+        return rc, d.value, k.value
+    return cmp
+
+
+def test_c_abi_comparator():
+    """alp_compare_reference_format (host code in the C library, no GPU) agrees with
+    this module's compare on equal files and on each kind of difference, names the
+    first differing input and field, and refuses malformed files."""
+    cmp = _c_compare()
+    rng = np.random.default_rng(5)
+
+    def tree(n):
+        kind = rng.integers(0, 2, n).astype(np.uint8)
+        start = rng.integers(0, 1000, n).astype(np.int64)
+        return (rng.integers(0, 50, n).astype(np.int64), rng.integers(0, 30, n).astype(np.uint32), kind,
+                np.where(kind == 1, start, 0), np.where(kind == 1, start + 3, 0))
+
+    res = [tree(5), None, tree(0), tree(9), tree(2)]
+    res[3][2][4] = 1  # a terminal: its start and end are written
+    a = wire.write_lexparse_outputs(res)
+    assert cmp(1, a, a) == (0, -1, -1) and wire.compare(a, a, "lexer-parser") is None
+    # each field of element 4 of input 3, in record order (kind, parent, id, start, end)
+    for k, f in ((0, 2), (1, 0), (2, 1), (3, 3), (4, 4)):
+        r2 = [None if t is None else tuple(x.copy() for x in t) for t in res]
+        if f == 2:  # a kind flip makes start/end 0 on the production side too
+            r2[3][2][4] ^= 1
+        else:
+            r2[3][f][4] += 1
+        b = wire.write_lexparse_outputs(r2)
+        got = cmp(1, a, b)
+        assert got[0] == 0 and got[1] == 3 and got[2] == k, (k, got)
+        assert wire.compare(a, b, "lexer-parser") is not None
+    # acceptance differs; element counts differ; result counts differ
+    assert cmp(1, a, wire.write_lexparse_outputs([res[0], tree(1)] + res[2:]))[:2] == (0, 1)
+    assert cmp(1, a, wire.write_lexparse_outputs(res[:3] + [tree(8), res[4]]))[:3] == (0, 3, -1)
+    assert cmp(1, a, wire.write_lexparse_outputs(res[:4]))[:3] == (0, 4, -1)
+    # lexer and parser-only files
+    toks = [(np.array([1, 2], np.uint64), np.array([0, 3], np.uint64), np.array([3, 5], np.uint64)), None]
+    la = wire.write_lexer_outputs(toks)
+    lb = wire.write_lexer_outputs([(toks[0][0], toks[0][1], np.array([3, 6], np.uint64)), None])
+    assert cmp(0, la, la)[1] == -1 and cmp(0, la, lb) == (0, 0, 2)
+    pa = wire.write_parser_outputs([np.array([4, 5, 6]), None, np.array([], np.int64)])
+    pb = wire.write_parser_outputs([np.array([4, 5, 6]), None, np.array([1])])
+    assert cmp(2, pa, pa)[1] == -1 and cmp(2, pa, pb) == (0, 2, -1)
+    assert cmp(2, pa, wire.write_parser_outputs([np.array([4, 7, 6]), None, np.array([], np.int64)])) == (0, 0, 0)
+    # malformed: truncated, trailing bytes, a boolean or kind byte out of range, unknown mode
+    assert cmp(1, a, a[:-1])[0] == 1 and cmp(1, a + b"\x00", a)[0] == 1
+    bad_bool = bytearray(a)
+    bad_bool[8] = 2
+    assert cmp(1, bytes(bad_bool), a)[0] == 1
+    bad_kind = bytearray(a)
+    bad_kind[8 + 1 + 8] = 3
+    assert cmp(1, bytes(bad_kind), a)[0] == 1
+    assert cmp(9, a, a)[0] == 1
