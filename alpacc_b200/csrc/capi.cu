@@ -69,7 +69,10 @@ __attribute__((target("avx2"))) void widen_avx2(const int32_t* s, int64_t* d, si
 }
 
 void widen(const int32_t* s, int64_t* d, size_t n) {
-    static const bool avx2 = __builtin_cpu_supports("avx2");
+    static const bool avx2 = [] {
+        __builtin_cpu_init();
+        return __builtin_cpu_supports("avx2") != 0;
+    }();
     if (avx2 && ((uintptr_t)d & 7) == 0) {
         widen_avx2(s, d, n);
         return;
@@ -92,8 +95,16 @@ int host_workers() {
 
 class HostPool {
   public:
+    // As many of `workers` threads as the system grants; with none, the calling
+    // thread widens every slice itself (help / wait).
     explicit HostPool(int workers) {
-        for (int i = 0; i < workers; ++i) th_.emplace_back([this] { run(); });
+        for (int i = 0; i < workers; ++i) {
+            try {
+                th_.emplace_back([this] { run(); });
+            } catch (...) {
+                break;
+            }
+        }
     }
     ~HostPool() {
         {
