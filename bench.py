@@ -10,7 +10,9 @@ are larger than L2, so no flush is needed between steps.
                  with CUDA events around the ``alp_parse`` calls).
 * ``e2e``     -- the same through ``alp_parse_host``: pinned host bytes in,
                  the whole tree back to pinned host memory, copies inside
-                 the timed region.
+                 the timed region (parents and spans cross as 32-bit values
+                 and are widened on the host; the bytes moved are the ones the
+                 call reports).
 * ``roofline``-- algorithmic bytes (input + 29 B per output node: i64 parent,
                  u32 tag, u8 kind, i64 start, i64 end) over the step time,
                  against the measured HBM copy bandwidth; plus a per-kernel
@@ -29,7 +31,8 @@ Other workloads (``--workload``), one JSON line each, same keys:
 * ``batch``  -- 100,000 JSON documents and 50,000 sexp documents with
                 log-normal sizes (median 4 KiB, sigma 1.5, capped at 4 MiB),
                 each set in one ``alp_parse_batch`` call per step; algorithmic
-                bytes input + 29 B per node + offsets and validity.
+                bytes input + 29 B per node + offsets and validity; e2e through
+                ``alp_parse_batch_host``.
 * ``spec``   -- learned boundary-state speculation for the json.alp and
                 sexp.alp lexers: the MLP trained on the GPU on exact boundary
                 states of documents from other seeds, then
