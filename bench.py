@@ -433,6 +433,51 @@ def _max_over_ranks(ms: float, dist, device) -> float:
     return float(t.item())
 
 
+def _e2e_two_contexts(L, g, h_in, size, N, outs, k, stream, dist, local, world):
+    """alp_parse_host on two contexts from two host threads, k calls each, back to back;
+    per-document time = elapsed / (2 k).  ctypes releases the GIL during each call."""
+    import ctypes
+    import threading
+    import torch
+    from alpacc_b200 import api, tables
+    g2 = api.Grammar(tables.load("json", "both"), device=local)
+    g2._stream()
+    outs2 = [torch.empty(o.shape, dtype=o.dtype, pin_memory=True) for o in outs]
+    errs = []
+
+    def calls(gx, ox, n_calls):
+        n_, v_ = ctypes.c_int64(0), ctypes.c_int(0)
+        for _ in range(n_calls):
+            rc = L.alp_parse_host(gx.h, ctypes.c_void_p(h_in.data_ptr()), size,
+                                  *[ctypes.c_void_p(o.data_ptr()) for o in ox], N, ctypes.byref(n_), ctypes.byref(v_))
+            if rc != 0 or not v_.value or n_.value != N:
+                errs.append(rc)
+
+    calls(g2, outs2, 1)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    th = [threading.Thread(target=calls, args=(gx, ox, k)) for gx, ox in ((g, outs), (g2, outs2))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if errs:
+        raise RuntimeError("alp_parse_host failed on a second context: %r" % errs[:3])
+    same = all(torch.equal(a, b) for a, b in zip(outs, outs2))
+    ms = _max_over_ranks(e0.elapsed_time(e1) / (2 * k), dist, local)
+    del outs2, g2
+    if not same:
+        raise RuntimeError("the two contexts' trees differ")
+    return {"value": _gbs(world, size, ms), "unit": "GB/s", "ms_per_doc": ms,
+            "contexts": 2, "calls": 2 * k, "trees_equal": True,
+            "note": "throughput of a document stream, not one call's latency (the line's e2e value)"}
+
+
 def _gbs(world: int, bytes_per_rank: int, ms: float) -> float:
     """Whole-job input GB/s: every rank processes bytes_per_rank (weak scaling)."""
     return world * bytes_per_rank / (ms * 1e-3) / 1e9
@@ -1036,6 +1081,7 @@ def main():
     ap.add_argument("--no-parity", action="store_true", help="skip the full-size comparison with the oracle")
     ap.add_argument("--no-graph", action="store_true", help="batch workload: skip the CUDA-graph replay")
     ap.add_argument("--no-spec", action="store_true", help="default workload: skip the learned-speculation object")
+    ap.add_argument("--no-two", action="store_true", help="default workload: skip the two-context serving figure")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes (no autotuner run): for "
                     "launch lists whose first launches should be the measured ones")
     ap.add_argument("--tuning", default=None, help="comma-separated tuning values (alp_tune_set) instead of the "
@@ -1139,6 +1185,10 @@ def main():
     # the bytes the call moved: parents and spans cross as 32-bit values
     moved = _ctx_counts(g)
     pcie = _pcie(local, moved["h2d"], moved["d2h"])
+    # a stream of such documents served by two contexts on two host threads, each making
+    # the same synchronous alp_parse_host calls (one call's input copy and device work
+    # overlap the other's tree copy out): documents per second as input GB/s
+    two = _e2e_two_contexts(L, g, h_in, size, N, outs, k_e2e, stream, dist, local, world) if not args.no_two else None
 
     # full-size parity: the tree the e2e call brought back against the oracle
     # (sequential restatement of the generated lex_int + parse_int)
@@ -1188,7 +1238,7 @@ def main():
         "roofline": roof,
         "path_roofline": path,
         "e2e": {"value": _gbs(world, size, ms_e2e), "unit": "GB/s", "h2d_bytes_per_step": moved["h2d"],
-                "d2h_bytes_per_step": moved["d2h"], "ms_per_step": ms_e2e, "pcie": pcie,
+                "d2h_bytes_per_step": moved["d2h"], "ms_per_step": ms_e2e, "pcie": pcie, "two_contexts": two,
                 "d2h_form": "i32 parents and spans (sign-extended into the caller's i64 arrays on the host "
                             "while later chunks are in flight), u32 tags, u8 kinds"},
         "gpu_launches": launches_per_step * args.steps,
