@@ -1187,8 +1187,11 @@ def main():
     pcie = _pcie(local, moved["h2d"], moved["d2h"])
     # a stream of such documents served by two contexts on two host threads, each making
     # the same synchronous alp_parse_host calls (one call's input copy and device work
-    # overlap the other's tree copy out): documents per second as input GB/s
-    two = _e2e_two_contexts(L, g, h_in, size, N, outs, k_e2e, stream, dist, local, world) if not args.no_two else None
+    # overlap the other's tree copy out): documents per second as input GB/s; one GPU only
+    # (a second set of pinned tree buffers and widening threads per rank)
+    two = None
+    if not args.no_two and world == 1:
+        two = _e2e_two_contexts(L, g, h_in, size, N, outs, k_e2e, stream, dist, local, world)
 
     # full-size parity: the tree the e2e call brought back against the oracle
     # (sequential restatement of the generated lex_int + parse_int)
