@@ -2186,7 +2186,8 @@ int alp_lex_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, uint32_t* h_term,
                  int64_t* h_end, int64_t cap, int64_t* n_tok, int* valid) {
     int rc = check_in(ctx, h_in, n, true);
     if (rc) return rc;
-    if (!n_tok || !valid) return fail(ctx, ALP_ERR_ARG, "null output");
+    if (!n_tok || !valid || cap < 0 || (cap > 0 && (!h_term || !h_start || !h_end)))
+        return fail(ctx, ALP_ERR_ARG, "null output");
     CK(cudaSetDevice(ctx->device));
     if ((rc = grow(ctx, ctx->tmp[0], (size_t)n + 16))) return rc;
     if (n) CK(cudaMemcpyAsync(ctx->tmp[0].p, h_in, (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
@@ -3075,7 +3076,8 @@ int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_pare
                    int64_t* h_start, int64_t* h_end, int64_t cap, int64_t* n_node, int* valid) {
     int rc = check_in(ctx, h_in, n, true);
     if (rc) return rc;
-    if (!n_node || !valid) return fail(ctx, ALP_ERR_ARG, "null output");
+    if (!n_node || !valid || cap < 0 || (cap > 0 && (!h_parent || !h_tag || !h_kind || !h_start || !h_end)))
+        return fail(ctx, ALP_ERR_ARG, "null output");
     CK(cudaSetDevice(ctx->device));
     if ((rc = grow(ctx, ctx->tmp[T_HIN], (size_t)n + 16))) return rc;
     if (n) CK(cudaMemcpyAsync(ctx->tmp[T_HIN].p, h_in, (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
@@ -3083,7 +3085,7 @@ int alp_parse_host(alp_ctx* ctx, const uint8_t* h_in, int64_t n, int64_t* h_pare
     // spans may be narrowed for the host during the searches (on cp_out); every return
     // below waits for that stream, so that no copy outlives the call
     alp_ctx::HostTree ht{h_tag, h_kind, h_start, h_end, (long long)cap, false, false};
-    ctx->host_tree = (cap > 0 && h_tag && h_kind && h_start && h_end) ? &ht : nullptr;
+    ctx->host_tree = cap > 0 ? &ht : nullptr;
     ctx->copies.clear();
     ctx->last_h2d = n;
     ctx->last_d2h = 0;

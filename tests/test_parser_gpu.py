@@ -206,6 +206,28 @@ def test_host_widening_chunks(has_gpu):
         np.testing.assert_array_equal(a, b)
 
 
+def test_host_null_outputs(has_gpu):
+    """A host output array missing while the capacity is positive: ALP_ERR_ARG before any
+    work; a capacity of 0 with no arrays: ALP_ERR_CAPACITY with the node count."""
+    import ctypes
+    from alpacc_b200 import api
+    g, o, _ = _ctx("json")
+    d = _gen("json", 5000, 24)
+    n_want = len(o.lex_parse(d.tobytes())[0])
+    bufs = [np.zeros(n_want, dt) for dt in (np.int64, np.uint32, np.uint8, np.int64, np.int64)]
+    n, valid = ctypes.c_int64(0), ctypes.c_int(0)
+    vp = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+    L = api.native()
+    for miss in range(5):
+        args = [vp(b) if i != miss else None for i, b in enumerate(bufs)]
+        assert L.alp_parse_host(g.h, vp(d), len(d), *args, n_want, ctypes.byref(n), ctypes.byref(valid)) == 1
+    assert L.alp_parse_host(g.h, vp(d), len(d), None, None, None, None, None, 0, ctypes.byref(n),
+                            ctypes.byref(valid)) == 5 and n.value == n_want
+    got = g.parse_host(d)  # the context is fine afterwards
+    for a, w in zip(got, o.lex_parse(d.tobytes())):
+        np.testing.assert_array_equal(a, w)
+
+
 def test_host_buffers_too_small(has_gpu):
     """A host capacity below the node count: ALP_ERR_CAPACITY with the count needed, and
     nothing written past the capacity (no copy was started early)."""
