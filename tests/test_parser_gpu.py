@@ -206,6 +206,23 @@ def test_host_widening_chunks(has_gpu):
         np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("name", ["json", "arithmetic", "sexp"])
+def test_host_buffers_short_inputs(has_gpu, name):
+    """alp_parse_host on every short input over a small alphabet (trees of a few nodes,
+    rejections, the empty input) against the oracle."""
+    g, o, _ = _ctx(name)
+    alpha = {"json": b'[]1 ', "arithmetic": b"1+()", "sexp": b"()a "}[name]
+    for L in range(0, 4):
+        for t in itertools.product(alpha, repeat=L):
+            d = bytes(t)
+            want = o.lex_parse(d)
+            got = g.parse_host(np.frombuffer(d, np.uint8))
+            assert (got is None) == (want is None), d
+            if want is not None:
+                for a, b in zip(got, want):
+                    np.testing.assert_array_equal(a, b)
+
+
 def test_host_null_outputs(has_gpu):
     """A host output array missing while the capacity is positive: ALP_ERR_ARG before any
     work; a capacity of 0 with no arrays: ALP_ERR_CAPACITY with the node count."""
