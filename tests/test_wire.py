@@ -244,3 +244,43 @@ def test_c_abi_comparator():
     bad_kind[8 + 1 + 8] = 3
     assert cmp(1, bytes(bad_kind), a)[0] == 1
     assert cmp(9, a, a)[0] == 1
+
+
+@pytest.mark.parametrize("mode,name", [(0, "lexer"), (1, "lexer-parser"), (2, "parser")])
+def test_c_abi_comparator_fuzz(mode, name):
+    """Single-byte changes to a file of each kind: the C comparator and this module's
+    compare agree on equal / different, and on what is malformed (ValueError here,
+    ALP_ERR_ARG there)."""
+    cmp = _c_compare()
+    rng = np.random.default_rng(11 + mode)
+    res = []
+    for i in range(6):
+        if i == 2:
+            res.append(None)
+            continue
+        n = int(rng.integers(0, 5))
+        if mode == 0:
+            s = rng.integers(0, 100, n).astype(np.uint64)
+            res.append((rng.integers(0, 9, n).astype(np.uint64), s, s + 2))
+        elif mode == 1:
+            kind = rng.integers(0, 2, n).astype(np.uint8)
+            s = rng.integers(0, 100, n).astype(np.int64)
+            res.append((rng.integers(0, 9, n).astype(np.int64), rng.integers(0, 9, n).astype(np.uint32), kind,
+                        np.where(kind == 1, s, 0), np.where(kind == 1, s + 2, 0)))
+        else:
+            res.append(rng.integers(0, 9, n).astype(np.uint64))
+    writer = {0: wire.write_lexer_outputs, 1: wire.write_lexparse_outputs, 2: wire.write_parser_outputs}[mode]
+    a = writer(res)
+    for _ in range(300):
+        b = bytearray(a)
+        j = int(rng.integers(0, len(b)))
+        b[j] = int(rng.integers(0, 256))
+        b = bytes(b)
+        rc, diff, _ = cmp(mode, a, b)
+        try:
+            py = wire.compare(a, b, name)
+        except ValueError:
+            assert rc == 1, (j, b[j])
+            continue
+        assert rc == 0, (j, b[j])
+        assert (diff == -1) == (py is None), (j, b[j], diff, py)
