@@ -29,7 +29,7 @@ NVCC_FLAGS = [
 
 def _sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
-                  [os.path.join(HERE, "..", "include", "alpacc_b200.h")])
+                  glob.glob(os.path.join(CSRC, "*.h")) + [os.path.join(HERE, "..", "include", "alpacc_b200.h")])
 
 
 def needs_build() -> bool:
